@@ -1,0 +1,312 @@
+"""Benchmark of the single-spin-flip SA sweep on one or more B200s.
+
+Workload (one "step"): the 2D +-J spin glass, L = 128 periodic square lattice
+(16384 spins, J in {-1,+1} with p = 1/2, h = 0, seed 2), 1024 replicas,
+num_sweeps = 2000 with the geometric beta schedule 0.1 -> 5 that SASampler
+builds (1000 betas x 2 sweeps), followed by the FP64 energy of every replica.
+Metric: spin-flip attempts/s = 1024 * 16384 * 2000 per step / step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl ours (default): the library through its C ABI.  ``value`` has the
+inputs resident in HBM; ``e2e`` is the same call with pinned host buffers, the
+initial spins copied in and the final spins + energies copied out every step.
+--impl reference: OpenJij's CPU path (the oracle's FP64 restatement with the
+reference's Xorshift stream, one read per host thread), on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_SIDE = 128
+REPLICAS = 1024
+NUM_SWEEPS = 2000
+BETA_MIN, BETA_MAX = 0.1, 5.0
+SEED_INSTANCE = 2
+# algorithmic state traffic of one attempt: 4 neighbour reads + 1 own read +
+# 1 write, at one bit per spin in the bit-packed layout
+ALGO_BYTES_PER_ATTEMPT = 6.0 / 8.0
+WORKLOAD = "2d_pm_j_lattice_L128_R1024_S2000"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_from_profiles():
+    """DRAM bytes per launch of the annealing kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "sa_bitpacked_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_launch_full_workload"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _instance():
+    from openjij_b200 import instances as I
+    m, _ = I.lattice_pm_j(L_SIDE, seed=SEED_INSTANCE)
+    betas, mcs = I.geometric_betas(BETA_MIN, BETA_MAX, NUM_SWEEPS)
+    return m, betas, mcs
+
+
+def cpu_reference(m, betas, mcs, reads, threads):
+    """OpenJij's CPU path (oracle restatement, FP64, Xorshift): ``reads`` reads,
+    one per host thread; returns attempts/s."""
+    from oracle import oracle as O
+    g = O.AugCSR(m)
+    rng = np.random.default_rng(0)
+    init = rng.choice(np.array([-1, 1], np.int8), size=(reads, g.n))
+    seeds = np.arange(1, reads + 1, dtype=np.uint64)
+    t0 = time.perf_counter()
+    O.ref_sa_many(g, init, betas, mcs, seeds, threads=threads)
+    dt = time.perf_counter() - t0
+    attempts = reads * g.n * float(np.sum(mcs))
+    return attempts / dt, dt
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    m, betas, mcs = _instance()
+    threads = os.cpu_count() or 1
+    reads = threads  # one read per host thread, the full 2000-sweep schedule
+    for _ in range(args.warmup):
+        cpu_reference(m, betas, mcs, min(reads, threads), threads)
+    vals, times = [], []
+    for _ in range(args.steps):
+        v, dt = cpu_reference(m, betas, mcs, reads, threads)
+        vals.append(v)
+        times.append(dt)
+    value = float(np.mean(vals))
+    sample = f"{reads} reads x {NUM_SWEEPS} sweeps of the L=128 lattice per step"
+    line = {
+        "impl": "reference", "metric": "spin-flip attempts/s", "value": value,
+        "unit": "attempts/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_reads_per_step": reads, "host_threads": threads},
+        "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from openjij_b200 import _native as N
+    from oracle import oracle as O  # CPU baseline only
+    m, betas, mcs = _instance()
+    g_or = O.AugCSR(m)
+    n = g_or.n
+    R = REPLICAS
+    stream = torch.cuda.current_stream()
+    ctx = N.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    graph = N.Graph(ctx, n, g_or.indptr, g_or.indices, g_or.data)
+    rng = np.random.default_rng(1000 + rank)
+    init_host = rng.choice(np.array([-1, 1], np.int8), size=(R, n))
+    init_dev = torch.from_numpy(init_host).cuda()
+    work = torch.empty_like(init_dev)
+    energies = torch.empty(R, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    attempts_per_step = float(R) * n * float(np.sum(mcs))
+    seed0 = 12345 + 1000003 * rank
+
+    def step(k, timed_events=None):
+        work.copy_(init_dev)
+        st = N.sa_run(graph, work, betas, mcs, seed=seed0 + k, energies=energies, device=True)
+        return st
+
+    for k in range(args.warmup):
+        flush.zero_()
+        step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kern_ms, launches = [], 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (state fits in L2)
+            starts[k].record(stream)
+            st = step(args.warmup + k)
+            ends[k].record(stream)
+            kern_ms.append(st["anneal_ms"])
+            launches += st["launches"] + 1  # + the device-to-device copy of the initial spins
+        torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = float(np.mean(step_ms))
+    kms = float(np.mean(kern_ms))
+    if dist:
+        t = torch.tensor([ms, kms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kms = float(t[0]), float(t[1])
+    value = attempts_per_step * ws / (ms / 1000.0)
+
+    # e2e: the same call with pinned host buffers (H2D spins in, D2H spins + energies out)
+    host_spins = torch.empty((R, n), dtype=torch.int8).pin_memory()
+    host_e = torch.empty(R, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for k in range(max(1, min(args.steps, 5))):
+        host_spins.numpy()[...] = init_host
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        N.sa_run(graph, host_spins.numpy(), betas, mcs, seed=seed0 + k, energies=host_e.numpy())
+        e2e_ms.append(1000.0 * (time.perf_counter() - t0))
+    e2 = float(np.mean(e2e_ms))
+    if dist:
+        t = torch.tensor([e2], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2 = float(t[0])
+    e2e_value = attempts_per_step * ws / (e2 / 1000.0)
+
+    peak, peak_kind = _peaks()
+    achieved = attempts_per_step * ALGO_BYTES_PER_ATTEMPT / (kms / 1000.0) / 1e9
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, dt = cpu_reference(m, betas, mcs, threads, threads)
+        cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
+               "sample": f"{threads} reads x {NUM_SWEEPS} sweeps of the same lattice, one read per "
+                         f"thread, {dt:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": "spin-flip attempts/s", "value": value, "unit": "attempts/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded +-J lattice)",
+            "config": {"workload": WORKLOAD, "L": L_SIDE, "spins": n, "replicas": R,
+                       "num_sweeps": NUM_SWEEPS, "beta": [BETA_MIN, BETA_MAX],
+                       "kernel": "bitpacked", "l2": "flushed between steps (256 MB write)",
+                       "attempts_per_step": attempts_per_step},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": _traffic_from_profiles(),
+                         "peak_kind": peak_kind, "kernel": "sa_msc_kernel<4>",
+                         "kernel_ms": kms,
+                         "algorithmic_bytes_per_attempt": ALGO_BYTES_PER_ATTEMPT},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(R * n),
+                    "d2h_bytes_per_step": int(R * n + 8 * R), "ms_per_step": e2},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    graph.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

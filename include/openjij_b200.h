@@ -1,0 +1,134 @@
+/*
+ * openjij_b200 — C ABI of the B200 single-spin-flip annealing library.
+ *
+ * This is the drop-in boundary for OpenJij's SASampler / SQASampler hot path.
+ * The reference has no C ABI: its path is the pybind11 module `cxxjij`
+ * (openjij/main.cpp:27-227, openjij/declare.hpp) over header-only templates.
+ * Each entry point below names the reference interface it replaces.  The
+ * library's own pybind11 host (openjij_b200/csrc/cxxjij_host.cpp) keeps the
+ * `cxxjij` Python surface and calls only these functions.
+ *
+ * Conventions
+ *  - Every function returns oj_status (0 = OJ_OK) and never throws.
+ *  - Spins are int8 in {-1, +1}.  SA layout [R][n], SQA layout [R][T][n].
+ *  - Pointers are host pointers unless OJ_DEVICE_POINTERS is set in `flags`,
+ *    in which case spins / energies are device pointers on the context's GPU.
+ *  - Work is issued on the context's stream; with host pointers the call
+ *    returns after the results are copied back.
+ *  - One context per host thread (a context is not thread safe).
+ */
+#ifndef OPENJIJ_B200_H
+#define OPENJIJ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t oj_status;
+enum {
+  OJ_OK = 0,
+  OJ_ERR_ARG = 1,         /* invalid argument (reference: std::invalid_argument / runtime_error) */
+  OJ_ERR_OOM = 2,         /* device or host allocation failed */
+  OJ_ERR_CUDA = 3,        /* CUDA runtime error */
+  OJ_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  OJ_ERR_BOUNDS = 5,      /* a device-side index check failed */
+  OJ_ERR_UNSUPPORTED = 6, /* requested kernel cannot run this graph / size */
+  OJ_ERR_NODEVICE = 7     /* no CUDA device / extension built without sm_100a */
+};
+
+/* flags */
+#define OJ_DEVICE_POINTERS 0x1u
+/* kernel selection (bits 4..7) */
+#define OJ_KERNEL_SHIFT 4
+#define OJ_KERNEL_MASK (0xFu << OJ_KERNEL_SHIFT)
+#define OJ_KERNEL_AUTO (0u << OJ_KERNEL_SHIFT)
+#define OJ_KERNEL_COLOUR (1u << OJ_KERNEL_SHIFT)     /* colour-class kernel, any sparse graph, FP32 */
+#define OJ_KERNEL_DENSE_PLAIN (2u << OJ_KERNEL_SHIFT) /* sequential dense, one warp per replica, FP32 */
+#define OJ_KERNEL_BITPACKED (3u << OJ_KERNEL_SHIFT)  /* 32 replicas per word, couplings +-c, h = 0 */
+#define OJ_KERNEL_DENSE_TC (4u << OJ_KERNEL_SHIFT)   /* sequential dense, delayed tensor-core field updates */
+
+typedef struct oj_ctx oj_ctx;
+typedef struct oj_graph oj_graph;
+
+typedef struct oj_graph_info {
+  int32_t n;              /* number of spins (dummy excluded) */
+  int64_t nnz;            /* off-diagonal couplings (both triangles) */
+  int32_t num_colours;    /* greedy colouring of the coupling graph */
+  int32_t max_degree;
+  int32_t min_degree;
+  int32_t bimodal;        /* all |J_ij| equal, all h_i = 0 */
+  int32_t integer_exact;  /* J_ij, h_i multiples of 1/2, |J| <= 256, |h| <= 2^21:
+                            FP32 fields and BF16 couplings are exact */
+  double coupling_abs;    /* |J| when bimodal */
+} oj_graph_info;
+
+typedef struct oj_run_stats {
+  int32_t kernel;        /* OJ_KERNEL_* >> OJ_KERNEL_SHIFT actually used */
+  int32_t launches;      /* kernels launched by the call */
+  int64_t sweeps;        /* sweeps after expanding one_mc_step */
+  double attempts;       /* spin-flip attempts = R * T * n * sweeps */
+  float anneal_ms;       /* device time of the annealing kernel(s) */
+  float total_ms;        /* device time of the whole call incl. copies */
+} oj_run_stats;
+
+const char* oj_version(void);
+const char* oj_status_string(oj_status s);
+
+/* Context: device, stream, reusable device workspace.  No reference
+ * counterpart (the reference keeps state inside each system object). */
+oj_status oj_ctx_create(int32_t device, oj_ctx** out);
+oj_status oj_ctx_destroy(oj_ctx* ctx);
+oj_status oj_ctx_set_stream(oj_ctx* ctx, void* cuda_stream);
+oj_status oj_ctx_synchronize(oj_ctx* ctx);
+const char* oj_ctx_last_error(const oj_ctx* ctx);
+
+/* Graph upload.  Replaces cxxjij.graph.Dense(num_spins).set_interaction_matrix
+ * (openjij/declare.hpp:75-129; include/openjij/graph/dense.hpp:117-140) and
+ * cxxjij.graph.CSRSparse(csr) (declare.hpp:195-217; csr_sparse.hpp:96-101).
+ * Input is the symmetric augmented (n+1)x(n+1) matrix exactly as
+ * get_interactions() returns it: J in [0,n)x[0,n), h in row/column n, 1 at
+ * (n,n).  Diagonal J_ii must be zero (dense.hpp:127-131). */
+oj_status oj_graph_create_dense(oj_ctx* ctx, int32_t n, const double* J_aug, oj_graph** out);
+oj_status oj_graph_create_csr(oj_ctx* ctx, int32_t n, const int64_t* indptr,
+                              const int32_t* indices, const double* data, oj_graph** out);
+oj_status oj_graph_destroy(oj_graph* g);
+oj_status oj_graph_query(const oj_graph* g, oj_graph_info* out);
+
+/* Simulated annealing over R replicas.  Replaces the per-read loop
+ * BaseSampler._cxxjij_sampling (openjij/sampler/sampler.py:116-140) around
+ * Algorithm<SingleSpinFlip>::run(ClassicalIsing, rng, schedule)
+ * (include/openjij/algorithm/algorithm.hpp:26-56,
+ *  include/openjij/updater/single_spin_flip.hpp:66-95; binding
+ *  openjij/declare.hpp:687-793).  The schedule is (betas[k], mcs[k]) for
+ * k < num_sched, as ClassicalSchedule (schedule_list.hpp:121-127).
+ * spins [R][n] in/out.  energies [R] (may be NULL): FP64 energy
+ * sum_{i<j} J_ij s_i s_j + sum_i h_i s_i (dense.hpp:176-192). */
+oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
+                    const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
+                    uint32_t flags, double* energies, oj_run_stats* stats);
+
+/* Discrete-time path-integral SQA over R replicas x T Trotter slices.
+ * Replaces Algorithm<SingleSpinFlip>::run(TransverseIsing, rng, schedule)
+ * (single_spin_flip.hpp:127-258; transverse_ising.hpp:54-224) with schedule
+ * (betas[k], s[k], mcs[k]) as TransverseFieldSchedule (schedule_list.hpp:62-76).
+ * T >= 2 (transverse_ising.hpp:78-81).  spins [R][T][n] in/out.
+ * energies [R][T] (may be NULL): FP64 classical energy of each slice.
+ * best_slice [R] (may be NULL): get_solution()'s slice, the first slice of
+ * minimum energy (include/openjij/result/get_solution.hpp:59-84). */
+oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32_t num_slices,
+                     int8_t* spins, double gamma, const double* betas, const double* s,
+                     const int32_t* mcs, int32_t num_sched, uint64_t seed, uint32_t flags,
+                     double* energies, int32_t* best_slice, oj_run_stats* stats);
+
+/* FP64 energies of R spin vectors [R][n].  Replaces Dense::energy /
+ * CSRSparse::energy (dense.hpp:176-192, csr_sparse.hpp:139-155). */
+oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, const int8_t* spins,
+                    uint32_t flags, double* energies);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPENJIJ_B200_H */

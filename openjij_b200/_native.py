@@ -1,0 +1,222 @@
+"""ctypes binding of libojb200.so (the C ABI declared in include/openjij_b200.h).
+
+This is the thin, allocation-free Python view of the C ABI used by the tests
+and the benchmark.  It fails loudly when the library is missing: there is no
+CPU fallback for the sweep.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libojb200.so")
+
+OJ_OK = 0
+OJ_ERR_ARG = 1
+OJ_ERR_OOM = 2
+OJ_ERR_CUDA = 3
+OJ_ERR_TIMEOUT = 4
+OJ_ERR_BOUNDS = 5
+OJ_ERR_UNSUPPORTED = 6
+OJ_ERR_NODEVICE = 7
+
+OJ_DEVICE_POINTERS = 0x1
+KERNEL_SHIFT = 4
+KERNELS = {"auto": 0, "colour": 1, "dense_plain": 2, "bitpacked": 3, "dense_tc": 4}
+KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
+
+# every symbol the header declares
+EXPORTS = [
+    "oj_version", "oj_status_string", "oj_ctx_create", "oj_ctx_destroy", "oj_ctx_set_stream",
+    "oj_ctx_synchronize", "oj_ctx_last_error", "oj_graph_create_dense", "oj_graph_create_csr",
+    "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
+]
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("n", C.c_int32), ("nnz", C.c_int64), ("num_colours", C.c_int32),
+                ("max_degree", C.c_int32), ("min_degree", C.c_int32), ("bimodal", C.c_int32),
+                ("integer_exact", C.c_int32), ("coupling_abs", C.c_double)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("launches", C.c_int32), ("sweeps", C.c_int64),
+                ("attempts", C.c_double), ("anneal_ms", C.c_float), ("total_ms", C.c_float)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["kernel"] = KERNEL_NAMES.get(d["kernel"], d["kernel"])
+        return d
+
+
+class OJError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load libojb200.so; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libojb200.so not found at {LIB_PATH}; run openjij_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, u32, u64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
+        L.oj_version.restype = C.c_char_p
+        L.oj_status_string.restype = C.c_char_p
+        L.oj_status_string.argtypes = [i32]
+        L.oj_ctx_create.argtypes = [i32, C.POINTER(vp)]
+        L.oj_ctx_destroy.argtypes = [vp]
+        L.oj_ctx_set_stream.argtypes = [vp, vp]
+        L.oj_ctx_synchronize.argtypes = [vp]
+        L.oj_ctx_last_error.argtypes = [vp]
+        L.oj_ctx_last_error.restype = C.c_char_p
+        L.oj_graph_create_dense.argtypes = [vp, i32, vp, C.POINTER(vp)]
+        L.oj_graph_create_csr.argtypes = [vp, i32, vp, vp, vp, C.POINTER(vp)]
+        L.oj_graph_destroy.argtypes = [vp]
+        L.oj_graph_query.argtypes = [vp, C.POINTER(GraphInfo)]
+        L.oj_sa_run.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, u32, vp, C.POINTER(RunStats)]
+        L.oj_sqa_run.argtypes = [vp, vp, i32, i32, vp, dbl, vp, vp, vp, i32, u64, u32, vp, vp,
+                                 C.POINTER(RunStats)]
+        L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
+        for name in EXPORTS:
+            if name not in ("oj_version", "oj_status_string", "oj_ctx_last_error"):
+                getattr(L, name).restype = i32
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):  # torch tensor on the device
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+class Context:
+    """Owns an oj_ctx (device, stream, workspace)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        st = lib().oj_ctx_create(device, C.byref(self._h))
+        if st != OJ_OK:
+            raise OJError(st, "oj_ctx_create: " + lib().oj_status_string(st).decode())
+        self.device = device
+
+    def check(self, st, what):
+        if st != OJ_OK:
+            msg = lib().oj_ctx_last_error(self._h).decode()
+            raise OJError(st, f"{what}: {lib().oj_status_string(st).decode()}: {msg}")
+
+    def set_stream(self, stream_handle: int):
+        self.check(lib().oj_ctx_set_stream(self._h, C.c_void_p(stream_handle)), "set_stream")
+
+    def synchronize(self):
+        self.check(lib().oj_ctx_synchronize(self._h), "synchronize")
+
+    def close(self):
+        if self._h:
+            lib().oj_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """Owns an oj_graph built from the symmetric augmented (n+1)x(n+1) matrix."""
+
+    def __init__(self, ctx: Context, n: int, indptr, indices, data):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        self._keep = (np.ascontiguousarray(indptr, np.int64), np.ascontiguousarray(indices, np.int32),
+                      np.ascontiguousarray(data, np.float64))
+        ip, ix, dv = self._keep
+        ctx.check(lib().oj_graph_create_csr(ctx._h, int(n), _ptr(ip), _ptr(ix), _ptr(dv),
+                                            C.byref(self._h)), "oj_graph_create_csr")
+        self._keep = None
+        self.n = int(n)
+
+    @staticmethod
+    def from_dense(ctx: Context, J_aug):
+        J = np.ascontiguousarray(J_aug, np.float64)
+        g = Graph.__new__(Graph)
+        g.ctx = ctx
+        g._h = C.c_void_p()
+        ctx.check(lib().oj_graph_create_dense(ctx._h, J.shape[0] - 1, _ptr(J), C.byref(g._h)),
+                  "oj_graph_create_dense")
+        g.n = J.shape[0] - 1
+        g._keep = None
+        return g
+
+    def info(self) -> dict:
+        inf = GraphInfo()
+        self.ctx.check(lib().oj_graph_query(self._h, C.byref(inf)), "oj_graph_query")
+        return {k: getattr(inf, k) for k, _ in inf._fields_}
+
+    def close(self):
+        if self._h:
+            lib().oj_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _flags(kernel, device):
+    f = KERNELS[kernel] << KERNEL_SHIFT
+    if device:
+        f |= OJ_DEVICE_POINTERS
+    return f
+
+
+def sa_run(g: Graph, spins, betas, mcs, seed, kernel="auto", energies=None, device=False):
+    """spins: int8 [R][n] numpy (in/out) or device tensor/pointer with device=True."""
+    R = spins.shape[0] if hasattr(spins, "shape") else None
+    b = np.ascontiguousarray(betas, np.float64)
+    m = np.ascontiguousarray(mcs, np.int32)
+    st = RunStats()
+    g.ctx.check(lib().oj_sa_run(g.ctx._h, g._h, int(R), _ptr(spins), _ptr(b), _ptr(m), len(b),
+                                int(seed) & 0xFFFFFFFFFFFFFFFF, _flags(kernel, device), _ptr(energies),
+                                C.byref(st)), "oj_sa_run")
+    return st.as_dict()
+
+
+def sqa_run(g: Graph, spins, gamma, betas, s, mcs, seed, energies=None, best=None, kernel="auto",
+            device=False):
+    """spins: int8 [R][T][n]."""
+    R, T = spins.shape[0], spins.shape[1]
+    b = np.ascontiguousarray(betas, np.float64)
+    sv = np.ascontiguousarray(s, np.float64)
+    m = np.ascontiguousarray(mcs, np.int32)
+    st = RunStats()
+    g.ctx.check(lib().oj_sqa_run(g.ctx._h, g._h, int(R), int(T), _ptr(spins), float(gamma), _ptr(b),
+                                 _ptr(sv), _ptr(m), len(b), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                 _flags(kernel, device), _ptr(energies), _ptr(best), C.byref(st)),
+                "oj_sqa_run")
+    return st.as_dict()
+
+
+def energy(g: Graph, spins, out=None, device=False):
+    R = spins.shape[0]
+    if out is None:
+        out = np.zeros(R, np.float64)
+    g.ctx.check(lib().oj_energy(g.ctx._h, g._h, int(R), _ptr(spins),
+                                OJ_DEVICE_POINTERS if device else 0, _ptr(out)), "oj_energy")
+    return out

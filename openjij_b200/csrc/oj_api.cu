@@ -1,0 +1,489 @@
+// C ABI entry points (include/openjij_b200.h): context, graph upload, the SA
+// and SQA runs with their planner, FP64 energies.  No exception crosses the
+// ABI; every CUDA error becomes a status with a message in the context.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "oj_internal.h"
+
+namespace oj {
+oj_status finish_graph(oj_ctx* ctx, oj_graph* g);
+cudaError_t ensure_dense(oj_graph* g);
+}  // namespace oj
+
+using namespace oj;
+
+namespace {
+
+constexpr const char* kVersion = "openjij_b200 0.1.0 (sm_100a)";
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+oj_status cuda_fail(oj_ctx* ctx, cudaError_t e, const char* where) {
+  if (ctx) ctx->last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? OJ_ERR_OOM : OJ_ERR_CUDA;
+}
+
+#define OJ_CK(call, where)                              \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+  } while (0)
+
+oj_status arg_fail(oj_ctx* ctx, const char* msg) {
+  if (ctx) ctx->last_error = msg;
+  return OJ_ERR_ARG;
+}
+
+// Expands (param_k, mcs_k) into one entry per sweep, as Algorithm::run does
+// (include/openjij/algorithm/algorithm.hpp:47-54).
+template <class T>
+oj_status expand(oj_ctx* ctx, const T* params, const int32_t* mcs, int32_t num_sched, std::vector<T>& out) {
+  out.clear();
+  for (int32_t k = 0; k < num_sched; ++k) {
+    if (mcs[k] < 0) return arg_fail(ctx, "one_mc_step must be non-negative");
+    for (int32_t m = 0; m < mcs[k]; ++m) out.push_back(params[k]);
+  }
+  return OJ_OK;
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Thresholds of the bit-packed kernel: thr[k][m] = floor(exp(-beta_k*2c*m)*2^32),
+// m = 1..D (dE = 2c*m); always[k] bit m when the probability is 1.
+void msc_thresholds(const std::vector<float>& betas, double c, int D, std::vector<uint32_t>& thr,
+                    std::vector<uint32_t>& always) {
+  const size_t S = betas.size();
+  thr.assign(S * (D + 1), 0u);
+  always.assign(S, 0u);
+  for (size_t k = 0; k < S; ++k)
+    for (int m = 1; m <= D; ++m) {
+      const double p = std::exp(-(double)betas[k] * 2.0 * c * (double)m);
+      const double t = std::floor(std::ldexp(p, 32));
+      uint32_t v;
+      if (p >= 1.0) {
+        always[k] |= 1u << m;
+        v = 0xFFFFFFFFu;
+      } else {
+        v = t >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)t;
+      }
+      thr[k * (D + 1) + m] = v;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* oj_version(void) { return kVersion; }
+
+const char* oj_status_string(oj_status s) {
+  switch (s) {
+    case OJ_OK: return "ok";
+    case OJ_ERR_ARG: return "invalid argument";
+    case OJ_ERR_OOM: return "out of memory";
+    case OJ_ERR_CUDA: return "CUDA error";
+    case OJ_ERR_TIMEOUT: return "device wait timed out";
+    case OJ_ERR_BOUNDS: return "device bounds check failed";
+    case OJ_ERR_UNSUPPORTED: return "unsupported by the selected kernel";
+    case OJ_ERR_NODEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+oj_status oj_ctx_create(int32_t device, oj_ctx** out) {
+  if (!out) return OJ_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return OJ_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= count) return OJ_ERR_ARG;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return OJ_ERR_CUDA;
+  if (prop.major < 10) return OJ_ERR_NODEVICE;  // the kernels are built for sm_100a only
+  oj_ctx* ctx = new (std::nothrow) oj_ctx();
+  if (!ctx) return OJ_ERR_OOM;
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  DeviceGuard dg(device);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return OJ_ERR_CUDA;
+  }
+  ctx->own_stream = true;
+  for (auto& e : ctx->ev) cudaEventCreate(&e);
+  *out = ctx;
+  return OJ_OK;
+}
+
+oj_status oj_ctx_destroy(oj_ctx* ctx) {
+  if (!ctx) return OJ_OK;
+  {
+    DeviceGuard dg(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->spins.release();
+    ctx->words.release();
+    ctx->params.release();
+    ctx->energies.release();
+    ctx->best.release();
+    ctx->aux.release();
+    for (auto& e : ctx->ev)
+      if (e) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+  return OJ_OK;
+}
+
+oj_status oj_ctx_set_stream(oj_ctx* ctx, void* stream) {
+  if (!ctx) return OJ_ERR_ARG;
+  DeviceGuard dg(ctx->device);
+  if (ctx->own_stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  ctx->own_stream = false;
+  return OJ_OK;
+}
+
+oj_status oj_ctx_synchronize(oj_ctx* ctx) {
+  if (!ctx) return OJ_ERR_ARG;
+  DeviceGuard dg(ctx->device);
+  OJ_CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+  return OJ_OK;
+}
+
+const char* oj_ctx_last_error(const oj_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+oj_status oj_graph_create_csr(oj_ctx* ctx, int32_t n, const int64_t* indptr, const int32_t* indices,
+                              const double* data, oj_graph** out) {
+  if (!ctx || !out || n < 0 || !indptr) return arg_fail(ctx, "null argument or negative size");
+  *out = nullptr;
+  if (indptr[0] != 0 || indptr[n + 1] < indptr[0]) return arg_fail(ctx, "invalid indptr");
+  const int64_t nnz = indptr[n + 1];
+  if (nnz > 0 && (!indices || !data)) return arg_fail(ctx, "null indices/data");
+  DeviceGuard dg(ctx->device);
+  oj_graph* g = new (std::nothrow) oj_graph();
+  if (!g) return OJ_ERR_OOM;
+  g->device = ctx->device;
+  g->n = n;
+  try {
+    g->aug_indptr.assign(indptr, indptr + n + 2);
+    g->aug_indices.assign(indices, indices + nnz);
+    g->aug_data.assign(data, data + nnz);
+  } catch (...) {
+    delete g;
+    return OJ_ERR_OOM;
+  }
+  for (int i = 0; i <= n; ++i)
+    if (indptr[i + 1] < indptr[i]) {
+      delete g;
+      return arg_fail(ctx, "indptr must be non-decreasing");
+    }
+  oj_status s;
+  try {
+    s = finish_graph(ctx, g);
+  } catch (...) {
+    s = OJ_ERR_OOM;
+  }
+  if (s != OJ_OK) {
+    delete g;
+    return s;
+  }
+  *out = g;
+  return OJ_OK;
+}
+
+oj_status oj_graph_create_dense(oj_ctx* ctx, int32_t n, const double* J, oj_graph** out) {
+  if (!ctx || !out || n < 0 || !J) return arg_fail(ctx, "null argument or negative size");
+  const int64_t n1 = (int64_t)n + 1;
+  std::vector<int64_t> ip;
+  std::vector<int32_t> ix;
+  std::vector<double> dv;
+  try {
+    ip.reserve(n1 + 1);
+    ip.push_back(0);
+    for (int64_t i = 0; i < n1; ++i) {
+      for (int64_t j = 0; j < n1; ++j) {
+        const double v = J[i * n1 + j];
+        if (v != 0.0 || i == j) {
+          ix.push_back((int32_t)j);
+          dv.push_back(v);
+        }
+      }
+      ip.push_back((int64_t)ix.size());
+    }
+  } catch (...) {
+    return OJ_ERR_OOM;
+  }
+  return oj_graph_create_csr(ctx, n, ip.data(), ix.data(), dv.data(), out);
+}
+
+oj_status oj_graph_destroy(oj_graph* g) {
+  delete g;
+  return OJ_OK;
+}
+
+oj_status oj_graph_query(const oj_graph* g, oj_graph_info* out) {
+  if (!g || !out) return OJ_ERR_ARG;
+  *out = g->info;
+  return OJ_OK;
+}
+
+oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, const double* betas,
+                    const int32_t* mcs, int32_t num_sched, uint64_t seed, uint32_t flags, double* energies,
+                    oj_run_stats* stats) {
+  if (!ctx || !gc || R < 0 || num_sched < 0) return arg_fail(ctx, "null argument or negative size");
+  if (num_sched > 0 && (!betas || !mcs)) return arg_fail(ctx, "null schedule");
+  oj_graph* g = const_cast<oj_graph*>(gc);
+  if (g->device != ctx->device) return arg_fail(ctx, "graph belongs to another device");
+  const int n = g->n;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (R == 0 || n == 0) return OJ_OK;
+  if (!spins) return arg_fail(ctx, "null spins");
+  for (int32_t k = 0; k < num_sched; ++k)
+    if (!(betas[k] >= 0.0) || std::isinf(betas[k])) return arg_fail(ctx, "beta must be finite and >= 0");
+  DeviceGuard dg(ctx->device);
+  std::vector<double> bexp;
+  if (oj_status s = expand(ctx, betas, mcs, num_sched, bexp)) return s;
+  const int64_t S = (int64_t)bexp.size();
+  std::vector<float> bf(bexp.begin(), bexp.end());
+  const bool devp = (flags & OJ_DEVICE_POINTERS) != 0;
+  uint32_t kernel = flags & OJ_KERNEL_MASK;
+  const oj_graph_info& inf = g->info;
+  if (kernel == OJ_KERNEL_AUTO) {
+    if (inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1)
+      kernel = OJ_KERNEL_BITPACKED;
+    else if (inf.num_colours > 64 && (int64_t)n * n * 4 <= ((int64_t)8 << 30))
+      kernel = OJ_KERNEL_DENSE_PLAIN;
+    else
+      kernel = OJ_KERNEL_COLOUR;
+  }
+  if (kernel == OJ_KERNEL_BITPACKED &&
+      !(inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1)) {
+    ctx->last_error = "bit-packed kernel needs a regular graph with couplings +-c (degree <= 8) and h = 0";
+    return OJ_ERR_UNSUPPORTED;
+  }
+  if (kernel == OJ_KERNEL_DENSE_TC) {
+    ctx->last_error = "tensor-core dense kernel not available in this build";
+    return OJ_ERR_UNSUPPORTED;
+  }
+  cudaStream_t st = ctx->stream;
+  const size_t spin_bytes = (size_t)R * n;
+  int8_t* d_spins = spins;
+  if (!devp) {
+    OJ_CK(ctx->spins.ensure(spin_bytes), "alloc spins");
+    d_spins = ctx->spins.as<int8_t>();
+  } else if (!is_device_ptr(spins)) {
+    return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
+  }
+  int launches = 0;
+  OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
+  if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
+  if (kernel == OJ_KERNEL_BITPACKED) {
+    const int D = inf.max_degree;
+    const int G = (R + 31) / 32;
+    std::string why;
+    const int P = msc_choose_cluster(g, G, ctx->sm_count);
+    cudaError_t pe = msc_prepare(g, P, &why);
+    if (pe != cudaSuccess) {
+      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
+      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+    }
+    std::vector<uint32_t> thr, alw;
+    msc_thresholds(bf, inf.coupling_abs, D, thr, alw);
+    const size_t pbytes = (thr.size() + alw.size()) * 4;
+    OJ_CK(ctx->params.ensure(std::max<size_t>(pbytes, 16)), "alloc params");
+    uint32_t* d_thr = ctx->params.as<uint32_t>();
+    uint32_t* d_alw = d_thr + thr.size();
+    if (S > 0) {
+      OJ_CK(cudaMemcpyAsync(d_thr, thr.data(), thr.size() * 4, cudaMemcpyHostToDevice, st), "H2D thr");
+      OJ_CK(cudaMemcpyAsync(d_alw, alw.data(), alw.size() * 4, cudaMemcpyHostToDevice, st), "H2D always");
+    }
+    OJ_CK(ctx->words.ensure((size_t)G * n * 4), "alloc words");
+    uint32_t* d_words = ctx->words.as<uint32_t>();
+    OJ_CK(launch_pack(d_spins, R, n, d_words, st), "pack");
+    ++launches;
+    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+    if (S > 0) OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, seed, st, &launches), "sa bit-packed kernel");
+    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+    OJ_CK(launch_unpack(d_words, R, n, d_spins, st), "unpack");
+    ++launches;
+  } else {
+    OJ_CK(ctx->params.ensure(std::max<size_t>(bf.size() * 4, 16)), "alloc params");
+    float* d_beta = ctx->params.as<float>();
+    if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+    if (kernel == OJ_KERNEL_DENSE_PLAIN) OJ_CK(ensure_dense(g), "dense J upload");
+    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+    if (S > 0) {
+      if (kernel == OJ_KERNEL_DENSE_PLAIN)
+        OJ_CK(launch_sa_dense_plain(g, R, d_spins, d_beta, S, seed, st, &launches), "sa dense kernel");
+      else
+        OJ_CK(launch_sa_colour(g, R, d_spins, d_beta, S, seed, st, &launches), "sa colour kernel");
+    }
+    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  }
+  if (energies) {
+    double* d_e = energies;
+    if (!devp) {
+      OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
+      d_e = ctx->energies.as<double>();
+    }
+    OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+    ++launches;
+    if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+  }
+  if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
+  OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
+  if (!devp || stats) OJ_CK(cudaStreamSynchronize(st), "run");
+  if (stats) {
+    stats->kernel = (int32_t)(kernel >> OJ_KERNEL_SHIFT);
+    stats->launches = launches;
+    stats->sweeps = S;
+    stats->attempts = (double)R * n * (double)S;
+    cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+  }
+  return OJ_OK;
+}
+
+oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8_t* spins, double gamma,
+                     const double* betas, const double* s, const int32_t* mcs, int32_t num_sched,
+                     uint64_t seed, uint32_t flags, double* energies, int32_t* best_slice,
+                     oj_run_stats* stats) {
+  if (!ctx || !gc || R < 0 || num_sched < 0) return arg_fail(ctx, "null argument or negative size");
+  if (T < 2) return arg_fail(ctx, "trotter slices must be equal or larger than 2.");
+  if (num_sched > 0 && (!betas || !s || !mcs)) return arg_fail(ctx, "null schedule");
+  oj_graph* g = const_cast<oj_graph*>(gc);
+  if (g->device != ctx->device) return arg_fail(ctx, "graph belongs to another device");
+  const int n = g->n;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (R == 0 || n == 0) return OJ_OK;
+  if (!spins) return arg_fail(ctx, "null spins");
+  uint32_t kernel = flags & OJ_KERNEL_MASK;
+  if (kernel != OJ_KERNEL_AUTO && kernel != OJ_KERNEL_COLOUR) {
+    ctx->last_error = "SQA runs on the colour-class kernel";
+    return OJ_ERR_UNSUPPORTED;
+  }
+  kernel = OJ_KERNEL_COLOUR;
+  DeviceGuard dg(ctx->device);
+  // per-schedule-entry coefficients (single_spin_flip.hpp:147-148, 215-217)
+  std::vector<float2> coef_sched(num_sched);
+  for (int32_t k = 0; k < num_sched; ++k) {
+    const double beta = betas[k], sk = s[k];
+    const double a = sk * (beta / (double)(size_t)T);
+    const double B = (1 / 2.) * std::log(std::tanh(beta * gamma * (1.0 - sk) / (double)(size_t)T));
+    coef_sched[k] = make_float2((float)a, (float)B);
+  }
+  std::vector<float2> coef;
+  if (oj_status st_ = expand(ctx, coef_sched.data(), mcs, num_sched, coef)) return st_;
+  const int64_t S = (int64_t)coef.size();
+  const bool devp = (flags & OJ_DEVICE_POINTERS) != 0;
+  cudaStream_t st = ctx->stream;
+  const size_t spin_bytes = (size_t)R * T * n;
+  int8_t* d_spins = spins;
+  if (!devp) {
+    OJ_CK(ctx->spins.ensure(spin_bytes), "alloc spins");
+    d_spins = ctx->spins.as<int8_t>();
+  } else if (!is_device_ptr(spins)) {
+    return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
+  }
+  int launches = 0;
+  OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
+  if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
+  OJ_CK(ctx->params.ensure(std::max<size_t>(coef.size() * sizeof(float2), 16)), "alloc params");
+  float2* d_coef = ctx->params.as<float2>();
+  if (S > 0) OJ_CK(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(float2), cudaMemcpyHostToDevice, st), "H2D coef");
+  OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+  if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, seed, st, &launches), "sqa kernel");
+  OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  if (energies || best_slice) {
+    double* d_e = (devp && energies) ? energies : nullptr;
+    if (!d_e) {
+      OJ_CK(ctx->energies.ensure((size_t)R * T * 8), "alloc energies");
+      d_e = ctx->energies.as<double>();
+    }
+    OJ_CK(launch_energy(g, R * T, d_spins, d_e, st), "energy kernel");
+    ++launches;
+    if (energies && !devp)
+      OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * T * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+    if (best_slice) {
+      int32_t* d_b = devp ? best_slice : nullptr;
+      if (!d_b) {
+        OJ_CK(ctx->best.ensure((size_t)R * 4), "alloc best");
+        d_b = ctx->best.as<int32_t>();
+      }
+      OJ_CK(launch_best_slice(d_e, R, T, d_b, st), "best slice");
+      ++launches;
+      if (!devp) OJ_CK(cudaMemcpyAsync(best_slice, d_b, (size_t)R * 4, cudaMemcpyDeviceToHost, st), "D2H best");
+    }
+  }
+  if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
+  OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
+  if (!devp || stats) OJ_CK(cudaStreamSynchronize(st), "run");
+  if (stats) {
+    stats->kernel = (int32_t)(kernel >> OJ_KERNEL_SHIFT);
+    stats->launches = launches;
+    stats->sweeps = S;
+    stats->attempts = (double)R * T * n * (double)S;
+    cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+  }
+  return OJ_OK;
+}
+
+oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t R, const int8_t* spins, uint32_t flags,
+                    double* energies) {
+  if (!ctx || !g || R < 0 || (R > 0 && (!spins || !energies))) return arg_fail(ctx, "null argument");
+  if (R == 0) return OJ_OK;
+  if (g->n == 0) {
+    for (int32_t r = 0; r < R; ++r) energies[r] = 0.0;
+    return OJ_OK;
+  }
+  DeviceGuard dg(ctx->device);
+  const bool devp = (flags & OJ_DEVICE_POINTERS) != 0;
+  cudaStream_t st = ctx->stream;
+  const int8_t* d_spins = spins;
+  double* d_e = energies;
+  if (!devp) {
+    OJ_CK(ctx->aux.ensure((size_t)R * g->n), "alloc spins");
+    OJ_CK(cudaMemcpyAsync(ctx->aux.ptr, spins, (size_t)R * g->n, cudaMemcpyHostToDevice, st), "H2D spins");
+    d_spins = ctx->aux.as<int8_t>();
+    OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
+    d_e = ctx->energies.as<double>();
+  }
+  OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+  if (!devp) {
+    OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+    OJ_CK(cudaStreamSynchronize(st), "energy");
+  }
+  return OJ_OK;
+}
+
+}  // extern "C"

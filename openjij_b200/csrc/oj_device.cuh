@@ -1,0 +1,83 @@
+// Device-side building blocks shared by every sweep kernel: the Philox4x32-10
+// counter-based generator and the -ln(u) acceptance variate.
+//
+// Random stream definitions (key = (seed & 0xffffffff, seed >> 32)):
+//   SA, colour-class and sequential dense kernels:
+//     u(r, k, i)    = Philox((i, k, r >> 2, TAG_SA))[r & 3]
+//   SQA colour-class kernel:
+//     u(r, t, k, i) = Philox((i, k, r, ((t>>3)<<9) | ((t&1)<<8) | TAG_SQA))[(t>>1) & 3]
+//   bit-packed SA kernel (32 replicas per word, group g):
+//     W_l(g, k, i)  = Philox((i, k, g, ((l>>2)<<8) | TAG_SA_MSC))[l & 3],  l = 0..31
+// with r the replica, t the Trotter slice, k the sweep (one_mc_step repeats
+// included) and i the site.  Results are therefore independent of how the
+// replicas are spread over CTAs, clusters or GPUs.
+#pragma once
+#include <cstdint>
+
+namespace ojd {
+
+constexpr uint32_t TAG_SA = 0x5Au;
+constexpr uint32_t TAG_SQA = 0xA5u;
+constexpr uint32_t TAG_SA_MSC = 0x3Cu;
+
+struct u4 {
+  uint32_t x, y, z, w;
+};
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): per round
+// (c0,c1,c2,c3) <- (hi(M1*c2)^c1^k0, lo(M1*c2), hi(M0*c0)^c3^k1, lo(M0*c0)),
+// key bumped by the Weyl constants between rounds.
+__device__ __forceinline__ u4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                     uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t lo0 = 0xD2511F53u * c0;
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2);
+    c0 = hi1 ^ c1 ^ k0;
+    c1 = lo1;
+    c2 = hi0 ^ c3 ^ k1;
+    c3 = lo0;
+  }
+  return u4{c0, c1, c2, c3};
+}
+
+__device__ __forceinline__ uint32_t pick(const u4& v, int j) {
+  return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+
+// -ln(u), u = (2*(x>>9)+1) * 2^-24 in (0,1).  u = m*2^e with m reduced to
+// [sqrt(1/2), sqrt(2)]; ln m = 2 atanh(z), z = (m-1)/(m+1), series through
+// z^9 (truncation error < 1e-9).  Each step is a single IEEE round-to-nearest
+// operation (explicit _rn intrinsics, no contraction), so host code doing the
+// same operations reproduces the bits.
+__device__ __forceinline__ float neglog(uint32_t x) {
+  const uint32_t k = x >> 9;
+  const float u = __fmul_rn(__uint2float_rn(2u * k + 1u), 0x1p-24f);
+  const uint32_t b = __float_as_uint(u);
+  int e = (int)(b >> 23) - 127;
+  float m = __uint_as_float((b & 0x007FFFFFu) | 0x3F800000u);
+  if (m > 0x1.6a09e6p+0f) {
+    m = __fmul_rn(m, 0.5f);
+    e += 1;
+  }
+  const float num = __fsub_rn(m, 1.0f);
+  const float den = __fadd_rn(m, 1.0f);
+  const float z = __fdiv_rn(num, den);
+  const float z2 = __fmul_rn(z, z);
+  float p = __fmaf_rn(z2, 0x1.c71c72p-4f, 0x1.24924ap-3f);
+  p = __fmaf_rn(p, z2, 0x1.99999ap-3f);
+  p = __fmaf_rn(p, z2, 0x1.555556p-2f);
+  const float tz = __fmul_rn(z2, p);
+  const float z2x = __fadd_rn(z, z);
+  const float lnm = __fmaf_rn(z2x, tz, z2x);
+  const float lnu = __fmaf_rn(__int2float_rn(e), 0x1.62e430p-1f, lnm);
+  return -lnu;
+}
+
+}  // namespace ojd

@@ -1,0 +1,123 @@
+// Internal host-side structures of libojb200: the context, the uploaded graph
+// with its host analysis (colouring, bimodality, partition plans) and the
+// kernel launchers.  Not part of the public C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/openjij_b200.h"
+
+namespace oj {
+
+// Grow-only device buffer owned by a context or graph.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+// Partition of the sites of a regular +-c graph over the CTAs of one thread
+// block cluster, used by the bit-packed SA kernel.  Each CTA (part p) keeps the
+// words of its own sites and a halo copy of remote neighbours in shared memory.
+// Local slots: [0, nloc) own sites sorted by (colour, site); [nloc, nloc+nhalo)
+// halo sites sorted by (colour, site).
+struct MscPlan {
+  int P = 0;       // CTAs per cluster
+  int D = 0;       // degree (regular graph)
+  int ncol = 0;
+  int slots = 0;   // max over parts of nloc + nhalo
+  int nlocmax = 0;
+  int hmax = 0;
+  DevBuf tables;   // one allocation; the pointers below index into it
+  // part-major arrays
+  int32_t* gidx = nullptr;   // [P][slots] global site of each slot (-1 = pad)
+  int32_t* coff = nullptr;   // [P][ncol+1] colour offsets of own sites
+  int32_t* hoff = nullptr;   // [P][ncol+1] colour offsets into the refresh list
+  uint32_t* hsrc = nullptr;  // [P][hmax] (owner part << 16) | owner slot
+  uint16_t* hdst = nullptr;  // [P][hmax] local halo slot
+  uint16_t* nbr = nullptr;   // [P][nlocmax][D] local slots of the neighbours
+  uint16_t* jm = nullptr;    // [P][nlocmax] bit l set when J(site, nbr l) > 0
+};
+
+}  // namespace oj
+
+struct oj_graph {
+  int device = 0;
+  int n = 0;
+  // symmetric augmented CSR exactly as received (FP64), for energies
+  std::vector<int64_t> aug_indptr;
+  std::vector<int32_t> aug_indices;
+  std::vector<double> aug_data;
+  // neighbour lists without diagonal, dummy column and zeros (CSR column order)
+  std::vector<int32_t> rp, ci;
+  std::vector<double> val64;
+  std::vector<float> val;
+  std::vector<double> h64;
+  std::vector<float> h;
+  std::vector<int32_t> colour, order, coff;  // greedy colouring; sites sorted by colour
+  oj_graph_info info{};
+  bool regular = false;
+  // device copies
+  oj::DevBuf d_rp, d_ci, d_val, d_h, d_val64, d_h64, d_order, d_coff;
+  oj::DevBuf d_dense;  // FP32 dense J (n x n), created on first use
+  std::unique_ptr<oj::MscPlan> msc;
+  ~oj_graph();
+};
+
+struct oj_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  oj::DevBuf spins, words, params, energies, best, aux;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace oj {
+
+// ---- launchers (each returns cudaGetLastError() after the launch) ---------
+
+cudaError_t launch_sa_colour(const oj_graph* g, int R, int8_t* spins, const float* betas,
+                             int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches);
+cudaError_t launch_sqa_colour(const oj_graph* g, int R, int T, int8_t* spins, const float2* coef,
+                              int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches);
+cudaError_t launch_sa_dense_plain(const oj_graph* g, int R, int8_t* spins, const float* betas,
+                                  int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches);
+cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
+                          const uint32_t* always, int64_t nsweeps, uint64_t seed, cudaStream_t st,
+                          int* launches);
+cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
+cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
+cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,
+                          cudaStream_t st);
+cudaError_t launch_best_slice(const double* energies, int R, int T, int32_t* best, cudaStream_t st);
+
+// Kernel limits used by the planner.
+int sa_colour_max_smem_sites();
+int msc_max_degree();
+cudaError_t msc_prepare(oj_graph* g, int P, std::string* why);
+int msc_choose_cluster(const oj_graph* g, int G, int sm_count);
+
+}  // namespace oj

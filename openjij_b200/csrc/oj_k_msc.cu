@@ -1,0 +1,357 @@
+// Bit-packed ("multi-spin coded") SA sweep for regular graphs with couplings
+// +-c and no fields — the 2D +-J lattice and random regular +-J graphs.
+//
+// Word (g, i) holds site i of replicas 32g..32g+31, bit j set iff that
+// replica's spin is -1.  For bond (i, j) the bit word
+//     unsat = b_i ^ b_j ^ (J_ij > 0 ? ~0 : 0)
+// marks the replicas where the bond is unsatisfied (J s_i s_j > 0); with u the
+// per-replica count of unsatisfied bonds, flipping s_i changes the energy by
+// dE = 2c(d - 2u) (the reference's dE_i = -2 s_i sum_j J_ij s_j,
+// include/openjij/system/classical_ising.hpp:87-90).  Replicas with dE <= 0
+// flip (single_spin_flip.hpp:80); the others flip when the 32-bit uniform U
+// is below thr[k][d-2u] = floor(exp(-beta_k*dE)*2^32).  U is compared one
+// bit level at a time for all 32 replicas at once, most significant level
+// first, drawing a fresh Philox word per level; the loop stops as soon as
+// every replica is decided, so a site word costs ~log2(32)+2 words on average.
+//
+// Sites follow the classes of a greedy colouring (checkerboard on a bipartite
+// lattice).  One thread block cluster owns one replica group: its P CTAs split
+// the sites into contiguous ranges, keep their own words plus a halo copy of
+// the remote neighbours in shared memory, and after each colour class copy
+// the just-updated halo words out of the owners' shared memory (DSMEM).  One
+// cluster barrier per colour class; nothing touches global memory between
+// the initial load and the final store.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
+#include "oj_device.cuh"
+#include "oj_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace oj {
+namespace {
+
+constexpr int kMscThreads = 256;
+constexpr int kMscMaxDegree = 8;
+constexpr int kMscSmemWords = 52 * 1024;  // 208 KB of words per CTA
+
+struct MscArgs {
+  const int32_t* gidx;
+  const int32_t* coff;
+  const int32_t* hoff;
+  const uint32_t* hsrc;
+  const uint16_t* hdst;
+  const uint16_t* nbr;
+  const uint16_t* jm;
+  int slots, nlocmax, hmax, ncol;
+  int n;
+  uint32_t* words;
+  const uint32_t* thr;     // [nsweeps][D+1]
+  const uint32_t* always;  // [nsweeps]
+  int64_t nsweeps;
+  uint32_t k0, k1;
+};
+
+template <int D>
+__device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restrict__ Wsh,
+                                             const uint16_t* __restrict__ nb, uint32_t jmk,
+                                             const uint32_t* __restrict__ thr_k, uint32_t alw,
+                                             uint32_t site, uint32_t sweep, uint32_t grp, uint32_t k0,
+                                             uint32_t k1) {
+  constexpr int NB = D <= 1 ? 1 : (D <= 3 ? 2 : (D <= 7 ? 3 : 4));
+  constexpr int UMAX = (D + 1) / 2;  // classes u = 0..UMAX-1 have dE > 0
+  uint32_t cnt[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) cnt[b] = 0u;
+#pragma unroll
+  for (int l = 0; l < D; ++l) {
+    uint32_t x = w ^ Wsh[nb[l]] ^ (0u - ((jmk >> l) & 1u));
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const uint32_t t = cnt[b] & x;
+      cnt[b] ^= x;
+      x = t;
+    }
+  }
+  uint32_t cls[UMAX];
+  uint32_t tv[UMAX];
+  uint32_t uphill = 0u, pending = 0u, flip = 0u;
+#pragma unroll
+  for (int u = 0; u < UMAX; ++u) {
+    uint32_t m = 0xFFFFFFFFu;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) m &= ((u >> b) & 1) ? cnt[b] : ~cnt[b];
+    uphill |= m;
+    const int dm = D - 2 * u;
+    tv[u] = thr_k[dm];
+    if ((alw >> dm) & 1u) {
+      flip |= m;
+      m = 0u;
+    } else if (tv[u] == 0u) {
+      m = 0u;
+    }
+    cls[u] = m;
+    pending |= m;
+  }
+  flip |= ~uphill;
+  uint32_t lt = 0u;
+#pragma unroll 1
+  for (int q = 0; q < 8 && pending; ++q) {
+    const ojd::u4 r = ojd::philox(site, sweep, grp, ((uint32_t)q << 8) | ojd::TAG_SA_MSC, k0, k1);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int bitpos = 31 - (4 * q + l);
+      uint32_t pm = 0u;
+#pragma unroll
+      for (int u = 0; u < UMAX; ++u) pm |= cls[u] & (0u - ((tv[u] >> bitpos) & 1u));
+      const uint32_t wl = ojd::pick(r, l);
+      lt |= pending & pm & ~wl;
+      pending &= ~(pm ^ wl);
+    }
+  }
+  return w ^ (flip | lt);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kMscThreads) sa_msc_kernel(MscArgs a) {
+  extern __shared__ uint32_t Wsh[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int p = (int)cl.block_rank();
+  const int g = blockIdx.y;
+  const int32_t* gid = a.gidx + (size_t)p * a.slots;
+  const int32_t* co = a.coff + (size_t)p * (a.ncol + 1);
+  const int32_t* ho = a.hoff + (size_t)p * (a.ncol + 1);
+  const uint32_t* hs = a.hsrc + (size_t)p * a.hmax;
+  const uint16_t* hd = a.hdst + (size_t)p * a.hmax;
+  const uint16_t* nbr = a.nbr + (size_t)p * a.nlocmax * D;
+  const uint16_t* jm = a.jm + (size_t)p * a.nlocmax;
+  const int nloc = co[a.ncol];
+  const int nhalo = ho[a.ncol];
+  uint32_t* gw = a.words + (size_t)g * a.n;
+  for (int s = threadIdx.x; s < nloc + nhalo; s += blockDim.x) Wsh[s] = gw[gid[s]];
+  __syncthreads();
+  for (int64_t k = 0; k < a.nsweeps; ++k) {
+    const uint32_t* thr_k = a.thr + (size_t)k * (D + 1);
+    const uint32_t alw = a.always[k];
+    for (int c = 0; c < a.ncol; ++c) {
+      const int lo = co[c], hi = co[c + 1];
+      for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+        const uint32_t w = Wsh[s];
+        Wsh[s] = msc_site<D>(w, Wsh, nbr + (size_t)s * D, jm[s], thr_k, alw, (uint32_t)gid[s],
+                             (uint32_t)k, (uint32_t)g, a.k0, a.k1);
+      }
+      cl.sync();
+      const int hlo = ho[c], hhi = ho[c + 1];
+      for (int e = hlo + threadIdx.x; e < hhi; e += blockDim.x) {
+        const uint32_t src = hs[e];
+        const uint32_t* remote = cl.map_shared_rank(Wsh, (int)(src >> 16));
+        Wsh[hd[e]] = remote[src & 0xFFFFu];
+      }
+      __syncthreads();
+    }
+  }
+  for (int s = threadIdx.x; s < nloc; s += blockDim.x) gw[gid[s]] = Wsh[s];
+  cl.sync();  // keep this CTA's shared memory alive until every peer is done reading it
+}
+
+template <int D>
+cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st) {
+  auto kern = sa_msc_kernel<D>;
+  const size_t smem = (size_t)pl.slots * sizeof(uint32_t);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(pl.P, G, 1);
+  cfg.blockDim = dim3(kMscThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = pl.P;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+}  // namespace
+
+int msc_max_degree() { return kMscMaxDegree; }
+
+int msc_choose_cluster(const oj_graph* g, int G, int sm_count) {
+  if (const char* env = std::getenv("OJ_MSC_CLUSTER")) {
+    const int v = std::atoi(env);
+    if (v == 1 || v == 2 || v == 4 || v == 8) return v;
+  }
+  int P = 1;
+  // smallest power of two that fills the SMs, within the portable cluster limit
+  while (P < 8 && G * P < sm_count) P <<= 1;
+  // shared memory: words of own sites + halo must fit
+  while (P < 8 && (g->n / P) * 5 / 4 > kMscSmemWords) P <<= 1;
+  return P;
+}
+
+// Host-side partition of the sites over the P CTAs of a cluster.
+cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
+  if (g->msc && g->msc->P == P) return cudaSuccess;
+  const int n = g->n;
+  const int D = g->info.max_degree;
+  const int ncol = g->info.num_colours;
+  std::vector<int> bound(P + 1);
+  for (int p = 0; p <= P; ++p) bound[p] = (int)(((int64_t)p * n) / P);
+  std::vector<int> part_of(n), slot_of(n);
+  struct Part {
+    std::vector<int> own, halo;  // global site ids in slot order
+    std::vector<int> coff, hoff;
+  };
+  std::vector<Part> parts(P);
+  auto by_colour = [&](int a, int b) {
+    return g->colour[a] != g->colour[b] ? g->colour[a] < g->colour[b] : a < b;
+  };
+  for (int p = 0; p < P; ++p) {
+    Part& pt = parts[p];
+    for (int i = bound[p]; i < bound[p + 1]; ++i) {
+      pt.own.push_back(i);
+      part_of[i] = p;
+    }
+    std::sort(pt.own.begin(), pt.own.end(), by_colour);
+    for (size_t s = 0; s < pt.own.size(); ++s) slot_of[pt.own[s]] = (int)s;
+  }
+  int slots = 0, nlocmax = 0, hmax = 0;
+  for (int p = 0; p < P; ++p) {
+    Part& pt = parts[p];
+    std::vector<char> mark(n, 0);
+    for (int i : pt.own)
+      for (int q = g->rp[i]; q < g->rp[i + 1]; ++q) {
+        const int j = g->ci[q];
+        if (part_of[j] != p && !mark[j]) {
+          mark[j] = 1;
+          pt.halo.push_back(j);
+        }
+      }
+    std::sort(pt.halo.begin(), pt.halo.end(), by_colour);
+    pt.coff.assign(ncol + 1, 0);
+    pt.hoff.assign(ncol + 1, 0);
+    for (int i : pt.own) pt.coff[g->colour[i] + 1]++;
+    for (int j : pt.halo) pt.hoff[g->colour[j] + 1]++;
+    for (int c = 0; c < ncol; ++c) {
+      pt.coff[c + 1] += pt.coff[c];
+      pt.hoff[c + 1] += pt.hoff[c];
+    }
+    slots = std::max(slots, (int)(pt.own.size() + pt.halo.size()));
+    nlocmax = std::max(nlocmax, (int)pt.own.size());
+    hmax = std::max(hmax, (int)pt.halo.size());
+  }
+  if (slots > 65535 || slots > kMscSmemWords) {
+    if (why) *why = "bit-packed kernel: partition does not fit shared memory; use a larger cluster";
+    return cudaErrorInvalidValue;
+  }
+  hmax = std::max(hmax, 1);
+  // host images of the tables
+  std::vector<int32_t> gidx((size_t)P * slots, 0), coff((size_t)P * (ncol + 1)), hoff((size_t)P * (ncol + 1));
+  std::vector<uint32_t> hsrc((size_t)P * hmax, 0);
+  std::vector<uint16_t> hdst((size_t)P * hmax, 0), nbr((size_t)P * nlocmax * D, 0), jm((size_t)P * nlocmax, 0);
+  for (int p = 0; p < P; ++p) {
+    Part& pt = parts[p];
+    const int nloc = (int)pt.own.size();
+    std::vector<int> local_slot_of_halo(n, -1);
+    for (size_t h = 0; h < pt.halo.size(); ++h) local_slot_of_halo[pt.halo[h]] = nloc + (int)h;
+    for (int s = 0; s < nloc; ++s) gidx[(size_t)p * slots + s] = pt.own[s];
+    for (size_t h = 0; h < pt.halo.size(); ++h) {
+      const int j = pt.halo[h];
+      gidx[(size_t)p * slots + nloc + h] = j;
+      hsrc[(size_t)p * hmax + h] = ((uint32_t)part_of[j] << 16) | (uint32_t)slot_of[j];
+      hdst[(size_t)p * hmax + h] = (uint16_t)(nloc + h);
+    }
+    for (int c = 0; c <= ncol; ++c) {
+      coff[(size_t)p * (ncol + 1) + c] = pt.coff[c];
+      hoff[(size_t)p * (ncol + 1) + c] = pt.hoff[c];
+    }
+    for (int s = 0; s < nloc; ++s) {
+      const int i = pt.own[s];
+      uint16_t bits = 0;
+      int l = 0;
+      for (int q = g->rp[i]; q < g->rp[i + 1]; ++q, ++l) {
+        const int j = g->ci[q];
+        const int ls = part_of[j] == p ? slot_of[j] : local_slot_of_halo[j];
+        nbr[((size_t)p * nlocmax + s) * D + l] = (uint16_t)ls;
+        if (g->val64[q] > 0) bits |= (uint16_t)(1u << l);
+      }
+      jm[(size_t)p * nlocmax + s] = bits;
+    }
+  }
+  auto plan = std::make_unique<MscPlan>();
+  plan->P = P;
+  plan->D = D;
+  plan->ncol = ncol;
+  plan->slots = slots;
+  plan->nlocmax = nlocmax;
+  plan->hmax = hmax;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b_gidx = al(gidx.size() * 4), b_coff = al(coff.size() * 4), b_hoff = al(hoff.size() * 4),
+               b_hsrc = al(hsrc.size() * 4), b_hdst = al(hdst.size() * 2), b_nbr = al(nbr.size() * 2),
+               b_jm = al(jm.size() * 2);
+  cudaError_t e = plan->tables.ensure(b_gidx + b_coff + b_hoff + b_hsrc + b_hdst + b_nbr + b_jm);
+  if (e != cudaSuccess) return e;
+  char* base = plan->tables.as<char>();
+  size_t off = 0;
+  auto put = [&](auto*& dst, const auto& vec, size_t bytes) -> cudaError_t {
+    dst = reinterpret_cast<std::remove_reference_t<decltype(dst)>>(base + off);
+    off += bytes;
+    return cudaMemcpy(dst, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice);
+  };
+  if ((e = put(plan->gidx, gidx, b_gidx)) != cudaSuccess) return e;
+  if ((e = put(plan->coff, coff, b_coff)) != cudaSuccess) return e;
+  if ((e = put(plan->hoff, hoff, b_hoff)) != cudaSuccess) return e;
+  if ((e = put(plan->hsrc, hsrc, b_hsrc)) != cudaSuccess) return e;
+  if ((e = put(plan->hdst, hdst, b_hdst)) != cudaSuccess) return e;
+  if ((e = put(plan->nbr, nbr, b_nbr)) != cudaSuccess) return e;
+  if ((e = put(plan->jm, jm, b_jm)) != cudaSuccess) return e;
+  g->msc = std::move(plan);
+  return cudaSuccess;
+}
+
+cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
+                          const uint32_t* always, int64_t nsweeps, uint64_t seed, cudaStream_t st,
+                          int* launches) {
+  const MscPlan& pl = *g->msc;
+  MscArgs a;
+  a.gidx = pl.gidx;
+  a.coff = pl.coff;
+  a.hoff = pl.hoff;
+  a.hsrc = pl.hsrc;
+  a.hdst = pl.hdst;
+  a.nbr = pl.nbr;
+  a.jm = pl.jm;
+  a.slots = pl.slots;
+  a.nlocmax = pl.nlocmax;
+  a.hmax = pl.hmax;
+  a.ncol = pl.ncol;
+  a.n = g->n;
+  a.words = words;
+  a.thr = thr;
+  a.always = always;
+  a.nsweeps = nsweeps;
+  a.k0 = (uint32_t)seed;
+  a.k1 = (uint32_t)(seed >> 32);
+  if (launches) ++*launches;
+  switch (pl.D) {
+    case 1: return launch_d<1>(pl, a, G, st);
+    case 2: return launch_d<2>(pl, a, G, st);
+    case 3: return launch_d<3>(pl, a, G, st);
+    case 4: return launch_d<4>(pl, a, G, st);
+    case 5: return launch_d<5>(pl, a, G, st);
+    case 6: return launch_d<6>(pl, a, G, st);
+    case 7: return launch_d<7>(pl, a, G, st);
+    case 8: return launch_d<8>(pl, a, G, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace oj

@@ -1,0 +1,304 @@
+"""ORACLE — test infrastructure only (ctypes front end of liboj_oracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline / reference
+arm may import this module; the openjij_b200 package never does.  It exposes
+
+* the FP64 restatement of OpenJij's CPU single-spin-flip path with the
+  reference's Xorshift stream (``ref_*``), pinned by the reference's own
+  known-answer tests (tests/test_cxx.py, tests/cxxtest/sampler/quadraitc.hpp);
+* replays of the B200 kernels' update order and Philox stream (``replay_*``).
+
+Graphs are passed as the symmetric augmented (n+1)x(n+1) matrix in CSR form,
+exactly what ``Dense.get_interactions()`` / ``CSRSparse.get_interactions()``
+return in the reference (include/openjij/graph/dense.hpp:280-282).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import scipy.sparse as sp
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboj_oracle.so")
+_lib = None
+
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile liboj_oracle.so with the committed Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
+        L.orc_neglog.argtypes = [C.c_uint32]
+        L.orc_neglog.restype = C.c_float
+        L.orc_greedy_colour.argtypes = [C.c_int, _i64p, _i32p, _i32p]
+        L.orc_gen_spin.argtypes = [C.c_uint64, C.c_int, C.c_int, _i8p]
+        L.orc_classical_schedule.argtypes = [C.c_double, C.c_double, C.c_int64, _f64p]
+        L.orc_transverse_schedule.argtypes = [C.c_int64, _f64p]
+        L.orc_energy.argtypes = [C.c_int, _i64p, _i32p, _f64p, _i8p]
+        L.orc_energy.restype = C.c_double
+        L.orc_ref_sa.argtypes = [C.c_int, _i64p, _i32p, _f64p, _i8p, _f64p, _i64p, C.c_int64,
+                                 C.c_uint64, C.c_int]
+        L.orc_ref_sa_many.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f64p, _i64p,
+                                      C.c_int64, _u64p, C.c_int]
+        L.orc_ref_sqa.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, C.c_double, _f64p,
+                                  _f64p, _i64p, C.c_int64, C.c_uint64, C.c_int, _i8p]
+        L.orc_ref_sqa_many.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p,
+                                       C.c_double, _f64p, _f64p, _i64p, C.c_int64, _u64p, C.c_int]
+        L.orc_replay_sa.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f32p, C.c_int64,
+                                    C.c_uint64, C.c_int, C.c_int]
+        L.orc_replay_sqa.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _f32p,
+                                     _f32p, C.c_int64, C.c_uint64, C.c_int]
+        L.orc_replay_sa_msc.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _u32p, _u32p,
+                                        C.c_int, _u32p, C.c_int64, C.c_uint64, C.c_int]
+        L.orc_msc_thresholds.argtypes = [_f32p, C.c_int64, C.c_double, C.c_int, _u32p, _u32p]
+        L.orc_sqa_coefficients.argtypes = [_f64p, _f64p, C.c_int64, C.c_double, C.c_int, _f32p, _f32p]
+        L.orc_gen_spin_seq.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _i8p]
+        _lib = L
+    return _lib
+
+
+def _threads(threads):
+    return int(threads if threads else (os.cpu_count() or 1))
+
+
+# ---------------------------------------------------------------------------
+# instance helpers
+# ---------------------------------------------------------------------------
+
+class AugCSR:
+    """Symmetric augmented (n+1)x(n+1) matrix (h in row/col n, 1 in the corner)."""
+
+    def __init__(self, mat):
+        m = sp.csr_matrix(mat, dtype=np.float64)
+        m.sort_indices()
+        self.n = m.shape[0] - 1
+        self.indptr = np.ascontiguousarray(m.indptr, dtype=np.int64)
+        self.indices = np.ascontiguousarray(m.indices, dtype=np.int32)
+        self.data = np.ascontiguousarray(m.data, dtype=np.float64)
+        self.mat = m
+
+    @staticmethod
+    def from_ising(h, J, n=None):
+        """h: dict or array; J: dict {(i,j): v} (any i != j order, summed)."""
+        if n is None:
+            keys = list(h.keys()) if isinstance(h, dict) else list(range(len(h)))
+            for (i, j) in J:
+                keys += [i, j]
+            n = (max(keys) + 1) if keys else 0
+        A = np.zeros((n + 1, n + 1))
+        hv = h.items() if isinstance(h, dict) else enumerate(h)
+        for i, v in hv:
+            A[i, n] += v
+        for (i, j), v in J.items():
+            a, b = min(i, j), max(i, j)
+            A[a, b] += v
+        A[n, n] = 1.0
+        S = np.triu(A) + np.triu(A, 1).T
+        return AugCSR(S)
+
+    @staticmethod
+    def from_upper(upper):
+        """Upper-triangular augmented matrix (reference layout) -> symmetric."""
+        U = np.triu(np.asarray(upper, dtype=np.float64))
+        return AugCSR(U + np.triu(U, 1).T)
+
+    def args(self):
+        return (self.n, self.indptr, self.indices, self.data)
+
+
+# ---------------------------------------------------------------------------
+# building blocks
+# ---------------------------------------------------------------------------
+
+def philox4x32_10(ctr, key):
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox4x32_10(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
+    return out
+
+
+def neglog(x: int) -> float:
+    return float(lib().orc_neglog(int(x) & 0xFFFFFFFF))
+
+
+def greedy_colour(g: AugCSR):
+    nb = neighbour_csr(g)
+    out = np.zeros(g.n, np.int32)
+    lib().orc_greedy_colour(g.n, nb[0], nb[1], out)
+    return out
+
+
+def neighbour_csr(g: AugCSR):
+    """Neighbour lists without diagonal / dummy column and without zeros."""
+    rp = [0]
+    ci = []
+    for i in range(g.n):
+        for p in range(g.indptr[i], g.indptr[i + 1]):
+            j = g.indices[p]
+            if j != i and j != g.n and g.data[p] != 0.0:
+                ci.append(j)
+        rp.append(len(ci))
+    return np.asarray(rp, np.int64), np.asarray(ci, np.int32)
+
+
+def gen_spin(seed: int, n: int, engine: str = "xorshift"):
+    out = np.zeros(n, np.int8)
+    lib().orc_gen_spin(int(seed), n, 0 if engine == "xorshift" else 1, out)
+    return out
+
+
+def gen_spin_seq(seed: int, n: int, count: int, engine: str = "xorshift"):
+    out = np.zeros((count, n), np.int8)
+    lib().orc_gen_spin_seq(int(seed), n, count, 0 if engine == "xorshift" else 1, out)
+    return out
+
+
+def classical_schedule(beta_min, beta_max, num_call):
+    out = np.zeros(num_call, np.float64)
+    lib().orc_classical_schedule(float(beta_min), float(beta_max), int(num_call), out)
+    return out
+
+
+def transverse_schedule(num_call):
+    out = np.zeros(num_call, np.float64)
+    lib().orc_transverse_schedule(int(num_call), out)
+    return out
+
+
+def energy(g: AugCSR, spins):
+    s = np.ascontiguousarray(spins, np.int8)
+    return float(lib().orc_energy(*g.args(), s))
+
+
+def energies(g: AugCSR, spins2d):
+    return np.array([energy(g, s) for s in np.asarray(spins2d)])
+
+
+# ---------------------------------------------------------------------------
+# reference restatement
+# ---------------------------------------------------------------------------
+
+def ref_sa(g: AugCSR, init, betas, mcs, seed, engine="xorshift"):
+    s = np.array(init, np.int8, copy=True)
+    b = np.ascontiguousarray(betas, np.float64)
+    m = np.ascontiguousarray(mcs, np.int64)
+    lib().orc_ref_sa(*g.args(), s, b, m, len(b), int(seed), 0 if engine == "xorshift" else 1)
+    return s
+
+
+def ref_sa_many(g: AugCSR, init2d, betas, mcs, seeds, threads=None):
+    s = np.array(init2d, np.int8, copy=True, order="C")
+    b = np.ascontiguousarray(betas, np.float64)
+    m = np.ascontiguousarray(mcs, np.int64)
+    sd = np.ascontiguousarray(seeds, np.uint64)
+    lib().orc_ref_sa_many(*g.args(), s.shape[0], s, b, m, len(b), sd, _threads(threads))
+    return s
+
+
+def ref_sqa(g: AugCSR, trotter_init, gamma, betas, ss, mcs, seed, engine="xorshift"):
+    """trotter_init: [T][n].  Returns (trotter spins [T][n], get_solution spins)."""
+    S = np.array(trotter_init, np.int8, copy=True, order="C")
+    T = S.shape[0]
+    best = np.zeros(g.n, np.int8)
+    lib().orc_ref_sqa(*g.args(), T, S, float(gamma), np.ascontiguousarray(betas, np.float64),
+                      np.ascontiguousarray(ss, np.float64), np.ascontiguousarray(mcs, np.int64),
+                      len(betas), int(seed), 0 if engine == "xorshift" else 1, best)
+    return S, best
+
+
+def ref_sqa_many(g: AugCSR, init3d, gamma, betas, ss, mcs, seeds, threads=None):
+    S = np.array(init3d, np.int8, copy=True, order="C")
+    R, T, _ = S.shape
+    lib().orc_ref_sqa_many(*g.args(), R, T, S, float(gamma),
+                           np.ascontiguousarray(betas, np.float64),
+                           np.ascontiguousarray(ss, np.float64),
+                           np.ascontiguousarray(mcs, np.int64), len(betas),
+                           np.ascontiguousarray(seeds, np.uint64), _threads(threads))
+    return S
+
+
+# ---------------------------------------------------------------------------
+# replays of the B200 kernels
+# ---------------------------------------------------------------------------
+
+def replay_sa(g: AugCSR, init2d, betas_per_sweep, seed, mode="colour", threads=None):
+    s = np.array(init2d, np.int8, copy=True, order="C")
+    b = np.ascontiguousarray(betas_per_sweep, np.float32)
+    lib().orc_replay_sa(*g.args(), s.shape[0], s, b, len(b), int(seed),
+                        0 if mode == "colour" else 1, _threads(threads))
+    return s
+
+
+def sqa_coefficients(betas, ss, gamma, T):
+    b = np.ascontiguousarray(betas, np.float64)
+    s = np.ascontiguousarray(ss, np.float64)
+    a = np.zeros(len(b), np.float32)
+    bb = np.zeros(len(b), np.float32)
+    lib().orc_sqa_coefficients(b, s, len(b), float(gamma), int(T), a, bb)
+    return a, bb
+
+
+def replay_sqa(g: AugCSR, init3d, coef_a, coef_b, seed, threads=None):
+    S = np.array(init3d, np.int8, copy=True, order="C")
+    R, T, _ = S.shape
+    a = np.ascontiguousarray(coef_a, np.float32)
+    bb = np.ascontiguousarray(coef_b, np.float32)
+    lib().orc_replay_sqa(*g.args(), R, T, S, a, bb, len(a), int(seed), _threads(threads))
+    return S
+
+
+def pack_words(spins2d):
+    """int8 [R][n] (R multiple of 32) -> u32 [R/32][n], bit j = (s == -1)."""
+    s = np.asarray(spins2d)
+    R, n = s.shape
+    G = R // 32
+    bits = (s.reshape(G, 32, n) < 0).astype(np.uint64)
+    w = np.zeros((G, n), np.uint64)
+    for j in range(32):
+        w |= bits[:, j, :] << np.uint64(j)
+    return w.astype(np.uint32)
+
+
+def unpack_words(words):
+    w = np.asarray(words, np.uint32)
+    G, n = w.shape
+    out = np.empty((G, 32, n), np.int8)
+    for j in range(32):
+        out[:, j, :] = np.where((w >> np.uint32(j)) & np.uint32(1), -1, 1)
+    return out.reshape(G * 32, n)
+
+
+def msc_thresholds(betas_per_sweep, c, dmax):
+    b = np.ascontiguousarray(betas_per_sweep, np.float32)
+    thr = np.zeros((len(b), dmax + 1), np.uint32)
+    alw = np.zeros(len(b), np.uint32)
+    lib().orc_msc_thresholds(b, len(b), float(c), int(dmax), thr, alw)
+    return thr, alw
+
+
+def replay_sa_msc(g: AugCSR, init2d, thr, always, seed, threads=None):
+    """thr: [sweeps][dmax+1] u32; always: [sweeps] u32 bitmask."""
+    w = np.ascontiguousarray(pack_words(init2d), np.uint32)
+    thr = np.ascontiguousarray(thr, np.uint32)
+    alw = np.ascontiguousarray(always, np.uint32)
+    lib().orc_replay_sa_msc(*g.args(), w.shape[0], w, thr, thr.shape[1] - 1, alw, thr.shape[0],
+                            int(seed), _threads(threads))
+    return unpack_words(w)

@@ -1,0 +1,149 @@
+"""Spin-for-spin parity of every sweep kernel with the oracle's replay, through
+the C ABI (libojb200.so).  Integer and real couplings alike: the kernels and
+the replay perform the same FP32 operations in the same order."""
+import numpy as np
+import pytest
+
+from openjij_b200 import _native as N
+from openjij_b200 import instances as I
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(ctx, m):
+    g = O.AugCSR(m)
+    return g, N.Graph(ctx, g.n, g.indptr, g.indices, g.data)
+
+
+def _init(R, n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.choice(np.array([-1, 1], np.int8), size=(R, n))
+
+
+def _per_sweep(betas, mcs):
+    return np.repeat(np.asarray(betas, np.float64), mcs).astype(np.float32)
+
+
+@pytest.mark.parametrize("R", [1, 5, 8])
+def test_sa_colour_lattice_bit_exact(ctx, R):
+    m, _ = I.lattice_pm_j(8, seed=11)
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.1, 5.0, 40)
+    s0 = _init(R, g.n, 1)
+    s = s0.copy()
+    st = N.sa_run(dg, s, betas, mcs, seed=1234, kernel="colour")
+    assert st["kernel"] == "colour"
+    ref = O.replay_sa(g, s0, _per_sweep(betas, mcs), 1234, mode="colour")
+    np.testing.assert_array_equal(s, ref)
+
+
+def test_sa_colour_real_sparse_bit_exact(ctx):
+    rng = np.random.default_rng(3)
+    n = 60
+    J = np.triu(rng.uniform(-1, 1, (n, n)) * (rng.random((n, n)) < 0.1), 1)
+    h = rng.uniform(-1, 1, n)
+    A = I.dense_augmented(J + J.T, h)
+    g, dg = _graph(ctx, A)
+    betas, mcs = I.geometric_betas(0.1, 10.0, 30)
+    s0 = _init(7, n, 2)
+    s = s0.copy()
+    N.sa_run(dg, s, betas, mcs, seed=99, kernel="colour")
+    ref = O.replay_sa(g, s0, _per_sweep(betas, mcs), 99, mode="colour")
+    np.testing.assert_array_equal(s, ref)
+
+
+@pytest.mark.parametrize("n,R", [(40, 6), (100, 3), (33, 9)])
+def test_sa_dense_plain_bit_exact(ctx, n, R):
+    m, _ = I.dense_ising_uniform(n, seed=n)
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.1, 10.0, 25)
+    s0 = _init(R, n, 5)
+    s = s0.copy()
+    st = N.sa_run(dg, s, betas, mcs, seed=77, kernel="dense_plain")
+    assert st["kernel"] == "dense_plain"
+    ref = O.replay_sa(g, s0, _per_sweep(betas, mcs), 77, mode="dense")
+    np.testing.assert_array_equal(s, ref)
+
+
+@pytest.mark.parametrize("maker,R", [(lambda: I.lattice_pm_j(16, seed=2), 64),
+                                     (lambda: I.lattice_pm_j(12, seed=3), 40),
+                                     (lambda: I.random_regular_pm_j(96, 3, seed=4), 32)])
+def test_sa_bitpacked_bit_exact(ctx, maker, R):
+    m, _ = maker()
+    g, dg = _graph(ctx, m)
+    info = dg.info()
+    assert info["bimodal"] == 1
+    betas, mcs = I.geometric_betas(0.1, 5.0, 30)
+    bs = _per_sweep(betas, mcs)
+    s0 = _init(R, g.n, 9)
+    s = s0.copy()
+    st = N.sa_run(dg, s, betas, mcs, seed=2024, kernel="bitpacked")
+    assert st["kernel"] == "bitpacked"
+    thr, alw = O.msc_thresholds(bs, info["coupling_abs"], info["max_degree"])
+    Rp = ((R + 31) // 32) * 32
+    s0p = np.ones((Rp, g.n), np.int8)
+    s0p[:R] = s0
+    ref = O.replay_sa_msc(g, s0p, thr, alw, 2024)[:R]
+    np.testing.assert_array_equal(s, ref)
+
+
+@pytest.mark.parametrize("T", [8, 5, 2, 33])
+def test_sqa_colour_bit_exact(ctx, T):
+    m, _ = I.random_regular_pm_j(48, 3, seed=7)
+    g, dg = _graph(ctx, m)
+    R = 3
+    nsched = 20
+    ss = np.linspace(0.0, 1.0, nsched)
+    betas = np.full(nsched, 10.0)
+    mcs = np.ones(nsched, np.int32)
+    s0 = np.ascontiguousarray(np.broadcast_to(_init(R, g.n, 4)[:, None, :], (R, T, g.n)))
+    s = s0.copy()
+    best = np.zeros(R, np.int32)
+    en = np.zeros((R, T))
+    N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=5, energies=en, best=best)
+    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
+    ref = O.replay_sqa(g, s0, a, b, 5)
+    np.testing.assert_array_equal(s, ref)
+    for r in range(R):
+        e = O.energies(g, ref[r])
+        np.testing.assert_allclose(en[r], e, rtol=0, atol=1e-9)
+        assert best[r] == int(np.argmin(e))
+
+
+def test_energy_matches_oracle(ctx):
+    m, _ = I.dense_ising_uniform(50, seed=8)
+    g, dg = _graph(ctx, m)
+    s = _init(11, 50, 3)
+    e = N.energy(dg, s)
+    ref = O.energies(g, s)
+    np.testing.assert_allclose(e, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_zero_sweeps_and_empty(ctx):
+    m, _ = I.lattice_pm_j(4, seed=1)
+    g, dg = _graph(ctx, m)
+    s0 = _init(3, g.n, 1)
+    s = s0.copy()
+    N.sa_run(dg, s, np.zeros(0), np.zeros(0, np.int32), seed=1)
+    np.testing.assert_array_equal(s, s0)
+    s = np.zeros((0, g.n), np.int8)
+    N.sa_run(dg, s, [1.0], [1], seed=1)
+
+
+def test_bitpacked_rejects_non_bimodal(ctx):
+    m, _ = I.dense_ising_uniform(10, seed=1)
+    g, dg = _graph(ctx, m)
+    s = _init(2, 10, 1)
+    with pytest.raises(N.OJError) as ei:
+        N.sa_run(dg, s, [1.0], [1], seed=1, kernel="bitpacked")
+    assert ei.value.status == N.OJ_ERR_UNSUPPORTED
+
+
+def test_sqa_rejects_one_slice(ctx):
+    m, _ = I.lattice_pm_j(4, seed=1)
+    g, dg = _graph(ctx, m)
+    s = np.ones((1, 1, g.n), np.int8)
+    with pytest.raises(N.OJError) as ei:
+        N.sqa_run(dg, s, 1.0, [1.0], [0.5], [1], seed=1)
+    assert ei.value.status == N.OJ_ERR_ARG

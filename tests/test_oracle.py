@@ -1,0 +1,102 @@
+"""The oracle against the reference's own known answers (CPU only)."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+# tests/test_cxx.py:32-69 (= tests/cxxtest/testcase.hpp:33-77): J[i,i] is h_i
+CASE8 = {(0, 0): -0.1, (0, 1): -0.9, (0, 2): 0.2, (0, 3): 0.1, (0, 4): 1.3, (0, 5): 0.8, (0, 6): 0.9,
+         (0, 7): 0.4, (1, 1): -0.7, (1, 2): -1.6, (1, 3): 1.5, (1, 4): 1.5, (1, 5): 1.2, (1, 6): -1.5,
+         (1, 7): -1.7, (2, 2): -0.6, (2, 3): 1.2, (2, 4): -1.3, (2, 5): -0.5, (2, 6): -1.9, (2, 7): 1.2,
+         (3, 3): 0.8, (3, 4): -0.5, (3, 5): -0.4, (3, 6): -1.8, (3, 7): -2.0, (4, 4): 0.6, (4, 5): -2.0,
+         (4, 6): -1.9, (4, 7): 0.5, (5, 5): -1.8, (5, 6): -1.2, (5, 7): 1.8, (6, 6): 0.3, (6, 7): 1.4,
+         (7, 7): 1.8}
+GROUND8 = [-1, -1, 1, 1, 1, 1, 1, -1]
+
+
+def case8():
+    h = {i: v for (i, j), v in CASE8.items() if i == j}
+    J = {(i, j): v for (i, j), v in CASE8.items() if i != j}
+    return O.AugCSR.from_ising(h, J, 8)
+
+
+def test_philox_known_answers():
+    # Random123 known-answer vectors for philox4x32-10
+    assert list(O.philox4x32_10([0, 0, 0, 0], [0, 0])) == [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]
+    assert list(O.philox4x32_10([0xffffffff] * 4, [0xffffffff] * 2)) == \
+        [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]
+    assert list(O.philox4x32_10([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344],
+                                [0xa4093822, 0x299f31d0])) == [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]
+
+
+def test_neglog_accuracy():
+    rng = np.random.default_rng(0)
+    xs = list(rng.integers(0, 2**32, size=20000, dtype=np.uint64)) + [0, 1, 511, 512, 2**31, 2**32 - 1]
+    for x in xs:
+        u = (2 * (int(x) >> 9) + 1) * 2.0**-24
+        want = -math.log(u)
+        got = O.neglog(int(x))
+        assert got > 0
+        assert abs(got - want) <= 4e-7 * max(1.0, want), (x, got, want)
+
+
+def test_schedules_match_reference_formula():
+    b = O.classical_schedule(0.1, 100.0, 100)
+    assert b[0] == 0.1 and abs(b[-1] - 100.0) < 1e-9
+    s = O.transverse_schedule(100)
+    assert s[0] == 0.0 and abs(s[-1] - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("engine,spin_seed,mc_seed", [("xorshift", 1234, 5678), ("mt", 1, 1)])
+def test_reference_sa_finds_known_ground_state(engine, spin_seed, mc_seed):
+    # tests/test_cxx.py:224-275 (Xorshift) and tests/cxxtest/sampler/quadraitc.hpp:21-73 (mt19937(1))
+    g = case8()
+    init = O.gen_spin(spin_seed, 8, engine)
+    betas = O.classical_schedule(0.1, 100.0, 100)
+    out = O.ref_sa(g, init, betas, np.full(100, 100), mc_seed, engine)
+    assert list(out) == GROUND8
+
+
+def test_reference_sqa_finds_known_ground_state():
+    # tests/test_cxx.py:419-469: make_transverse_ising(gen_spin(1234), dense, 1.0, 10)
+    g = case8()
+    init = O.gen_spin(1234, 8)
+    ss = O.transverse_schedule(100)
+    _, best = O.ref_sqa(g, np.tile(init, (10, 1)), 1.0, np.full(100, 10.0), ss, np.full(100, 100), 5678)
+    assert list(best) == GROUND8
+
+
+def test_reference_sqa_mt_trotter_init():
+    # tests/cxxtest/sampler/quadraitc.hpp:75-102: 10 slices drawn from one mt19937(1), MC mt19937(1)
+    g = case8()
+    init = O.gen_spin_seq(1, 8, 10, "mt")
+    ss = O.transverse_schedule(100)
+    _, best = O.ref_sqa(g, init, 1.0, np.full(100, 10.0), ss, np.full(100, 100), 1, "mt")
+    assert list(best) == GROUND8
+
+
+def test_energy_layout_and_value():
+    g = case8()
+    # the ground state energy of the 8-spin instance
+    e = O.energy(g, np.array(GROUND8, np.int8))
+    assert abs(e - (-21.5)) < 1e-9
+
+
+def test_five_spin_sampler_case():
+    # tests/test_sampler.py:11-20: h={0:-1,1:-1,2:1,3:1}, J={(0,1):-1,(3,4):-1}, ground [1,1,-1,-1,-1], e=-6
+    g = O.AugCSR.from_ising({0: -1, 1: -1, 2: 1, 3: 1}, {(0, 1): -1, (3, 4): -1}, 5)
+    assert O.energy(g, np.array([1, 1, -1, -1, -1], np.int8)) == -6.0
+    betas, mcs = O.classical_schedule(0.1, 50.0, 100), np.full(100, 10)
+    out = O.ref_sa(g, O.gen_spin(1, 5), betas, mcs, 1)
+    assert O.energy(g, out) == -6.0
+
+
+def test_greedy_colouring_checkerboard():
+    from openjij_b200 import instances as I
+    m, _ = I.lattice_pm_j(8)
+    g = O.AugCSR(m)
+    col = O.greedy_colour(g)
+    ij = np.arange(64).reshape(8, 8)
+    assert np.array_equal(col.reshape(8, 8), (ij // 8 + ij % 8) % 2)
