@@ -125,10 +125,10 @@ def _dist():
     return ws, rank, local
 
 
-def _instance():
+def _instance(sweeps=None):
     from openjij_b200 import instances as I
     m, _ = I.lattice_pm_j(L_SIDE, seed=SEED_INSTANCE)
-    betas, mcs = I.geometric_betas(BETA_MIN, BETA_MAX, NUM_SWEEPS)
+    betas, mcs = I.geometric_betas(BETA_MIN, BETA_MAX, sweeps or NUM_SWEEPS)
     return m, betas, mcs
 
 
@@ -188,10 +188,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from openjij_b200 import _native as N
     from oracle import oracle as O  # CPU baseline only
-    m, betas, mcs = _instance()
+    m, betas, mcs = _instance(args.sweeps)
     g_or = O.AugCSR(m)
     n = g_or.n
-    R = REPLICAS
+    R = args.replicas or REPLICAS
     stream = torch.cuda.current_stream()
     ctx = N.Context(local)
     ctx.set_stream(stream.cuda_stream)
@@ -298,10 +298,13 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--sweeps", type=int, default=None,
+                    help="smaller case for profiling (default: the full 2000-sweep workload)")
+    ap.add_argument("--replicas", type=int, default=None, help="smaller case for profiling")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -40,8 +40,9 @@ struct DevBuf {
 // Partition of the sites of a regular +-c graph over the CTAs of one thread
 // block cluster, used by the bit-packed SA kernel.  Each CTA (part p) keeps the
 // words of its own sites and a halo copy of remote neighbours in shared memory.
-// Local slots: [0, nloc) own sites sorted by (colour, site); [nloc, nloc+nhalo)
-// halo sites sorted by (colour, site).
+// Local slots: [0, nloc) own sites sorted by (colour, boundary, site) where a
+// boundary site has a neighbour in another part; [nloc, nloc+nhalo) halo sites
+// sorted by (colour, site).
 struct MscPlan {
   int P = 0;       // CTAs per cluster
   int D = 0;       // degree (regular graph)
@@ -53,6 +54,7 @@ struct MscPlan {
   // part-major arrays
   int32_t* gidx = nullptr;   // [P][slots] global site of each slot (-1 = pad)
   int32_t* coff = nullptr;   // [P][ncol+1] colour offsets of own sites
+  int32_t* cb = nullptr;     // [P][ncol] first boundary slot of each colour (interior first)
   int32_t* hoff = nullptr;   // [P][ncol+1] colour offsets into the refresh list
   uint32_t* hsrc = nullptr;  // [P][hmax] (owner part << 16) | owner slot
   uint16_t* hdst = nullptr;  // [P][hmax] local halo slot

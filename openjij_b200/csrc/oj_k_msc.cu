@@ -12,20 +12,25 @@
 // is below thr[k][d-2u] = floor(exp(-beta_k*dE)*2^32).  U is compared one
 // bit level at a time for all 32 replicas at once, most significant level
 // first, drawing a fresh Philox word per level; the loop stops as soon as
-// every replica is decided, so a site word costs ~log2(32)+2 words on average.
+// every replica is decided.
 //
 // Sites follow the classes of a greedy colouring (checkerboard on a bipartite
 // lattice).  One thread block cluster owns one replica group: its P CTAs split
-// the sites into contiguous ranges, keep their own words plus a halo copy of
-// the remote neighbours in shared memory, and after each colour class copy
-// the just-updated halo words out of the owners' shared memory (DSMEM).  One
-// cluster barrier per colour class; nothing touches global memory between
-// the initial load and the final store.
+// the sites into contiguous ranges and keep, in shared memory, their own words,
+// a halo copy of the remote neighbours and the neighbour tables.  Per colour
+// class a CTA first updates its interior sites (no remote neighbour), then
+// waits on the cluster barrier (split arrive / wait, so the barrier latency
+// hides behind the interior work), copies the halo words of the previous class
+// out of the owners' shared memory (DSMEM), updates its boundary sites and
+// arrives.  Nothing touches global memory between the initial load and the
+// final store.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "oj_device.cuh"
@@ -36,13 +41,16 @@ namespace cg = cooperative_groups;
 namespace oj {
 namespace {
 
-constexpr int kMscThreads = 256;
+constexpr int kMscMaxThreads = 1024;
+constexpr int kMscDefaultThreads = 512;
 constexpr int kMscMaxDegree = 8;
-constexpr int kMscSmemWords = 52 * 1024;  // 208 KB of words per CTA
+constexpr int kMscMaxCluster = 16;
+constexpr size_t kMscSmemBytes = 200 * 1024;
 
 struct MscArgs {
   const int32_t* gidx;
   const int32_t* coff;
+  const int32_t* cb;
   const int32_t* hoff;
   const uint32_t* hsrc;
   const uint16_t* hdst;
@@ -57,14 +65,57 @@ struct MscArgs {
   uint32_t k0, k1;
 };
 
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// Per-sweep acceptance data of the uphill classes u = 0..UMAX-1 (dE = 2c(D-2u)).
+template <int D>
+struct MscSweep {
+  static constexpr int UMAX = (D + 1) / 2;
+  uint32_t tv[UMAX];  // thresholds
+  uint32_t alw;       // bit u: class u always accepts
+  uint32_t live;      // bit u: class u has a non-zero threshold and is not always-accept
+};
+
+template <int D>
+__device__ __forceinline__ MscSweep<D> msc_sweep(const uint32_t* __restrict__ thr_k, uint32_t always_k) {
+  MscSweep<D> sw;
+  sw.alw = 0u;
+  sw.live = 0u;
+#pragma unroll
+  for (int u = 0; u < MscSweep<D>::UMAX; ++u) {
+    const int dm = D - 2 * u;
+    sw.tv[u] = thr_k[dm];
+    if ((always_k >> dm) & 1u)
+      sw.alw |= 1u << u;
+    else if (sw.tv[u] != 0u)
+      sw.live |= 1u << u;
+  }
+  return sw;
+}
+
+// One bit level of the comparison U < thr for all 32 replicas.
+template <int D>
+__device__ __forceinline__ void msc_level(const MscSweep<D>& sw, const uint32_t (&cls)[MscSweep<D>::UMAX],
+                                          int bitpos, uint32_t wl, uint32_t& pending, uint32_t& lt) {
+  uint32_t pm = 0u;
+#pragma unroll
+  for (int u = 0; u < MscSweep<D>::UMAX; ++u) pm |= cls[u] & (0u - ((sw.tv[u] >> bitpos) & 1u));
+  lt |= pending & pm & ~wl;
+  pending &= ~(pm ^ wl);
+}
+
 template <int D>
 __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restrict__ Wsh,
                                              const uint16_t* __restrict__ nb, uint32_t jmk,
-                                             const uint32_t* __restrict__ thr_k, uint32_t alw,
-                                             uint32_t site, uint32_t sweep, uint32_t grp, uint32_t k0,
-                                             uint32_t k1) {
+                                             const MscSweep<D>& sw, uint32_t site, uint32_t sweep,
+                                             uint32_t grp, uint32_t k0, uint32_t k1) {
   constexpr int NB = D <= 1 ? 1 : (D <= 3 ? 2 : (D <= 7 ? 3 : 4));
-  constexpr int UMAX = (D + 1) / 2;  // classes u = 0..UMAX-1 have dE > 0
+  constexpr int UMAX = MscSweep<D>::UMAX;
   uint32_t cnt[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) cnt[b] = 0u;
@@ -79,7 +130,6 @@ __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restr
     }
   }
   uint32_t cls[UMAX];
-  uint32_t tv[UMAX];
   uint32_t uphill = 0u, pending = 0u, flip = 0u;
 #pragma unroll
   for (int u = 0; u < UMAX; ++u) {
@@ -87,14 +137,8 @@ __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restr
 #pragma unroll
     for (int b = 0; b < NB; ++b) m &= ((u >> b) & 1) ? cnt[b] : ~cnt[b];
     uphill |= m;
-    const int dm = D - 2 * u;
-    tv[u] = thr_k[dm];
-    if ((alw >> dm) & 1u) {
-      flip |= m;
-      m = 0u;
-    } else if (tv[u] == 0u) {
-      m = 0u;
-    }
+    if ((sw.alw >> u) & 1u) flip |= m;
+    m = ((sw.live >> u) & 1u) ? m : 0u;
     cls[u] = m;
     pending |= m;
   }
@@ -103,71 +147,113 @@ __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restr
 #pragma unroll 1
   for (int q = 0; q < 8 && pending; ++q) {
     const ojd::u4 r = ojd::philox(site, sweep, grp, ((uint32_t)q << 8) | ojd::TAG_SA_MSC, k0, k1);
-#pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const int bitpos = 31 - (4 * q + l);
-      uint32_t pm = 0u;
-#pragma unroll
-      for (int u = 0; u < UMAX; ++u) pm |= cls[u] & (0u - ((tv[u] >> bitpos) & 1u));
-      const uint32_t wl = ojd::pick(r, l);
-      lt |= pending & pm & ~wl;
-      pending &= ~(pm ^ wl);
-    }
+    msc_level<D>(sw, cls, 31 - 4 * q, r.x, pending, lt);
+    msc_level<D>(sw, cls, 30 - 4 * q, r.y, pending, lt);
+    msc_level<D>(sw, cls, 29 - 4 * q, r.z, pending, lt);
+    msc_level<D>(sw, cls, 28 - 4 * q, r.w, pending, lt);
   }
   return w ^ (flip | lt);
 }
 
+// Updates own slots [lo, hi), two independent sites per thread and iteration.
 template <int D>
-__global__ void __launch_bounds__(kMscThreads) sa_msc_kernel(MscArgs a) {
-  extern __shared__ uint32_t Wsh[];
+__device__ __forceinline__ void msc_range(int lo, int hi, uint32_t* __restrict__ Wsh,
+                                          const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
+                                          const uint16_t* __restrict__ nbr, const MscSweep<D>& sw,
+                                          uint32_t k, uint32_t g, uint32_t k0, uint32_t k1) {
+  const int T = blockDim.x;
+  for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
+    const int s2 = s + T;
+    const uint32_t a = msc_site<D>(Wsh[s], Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, k0, k1);
+    if (s2 < hi) {
+      const uint32_t b =
+          msc_site<D>(Wsh[s2], Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, k0, k1);
+      Wsh[s2] = b;
+    }
+    Wsh[s] = a;
+  }
+}
+
+// Shared memory: words[slots] | gid[nlocmax] | jm[nlocmax] | nbr[nlocmax][D]
+template <int D>
+__global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
+  extern __shared__ __align__(16) uint32_t Wsh[];
   cg::cluster_group cl = cg::this_cluster();
   const int p = (int)cl.block_rank();
   const int g = blockIdx.y;
-  const int32_t* gid = a.gidx + (size_t)p * a.slots;
+  const int32_t* gid_g = a.gidx + (size_t)p * a.slots;
   const int32_t* co = a.coff + (size_t)p * (a.ncol + 1);
+  const int32_t* cb = a.cb + (size_t)p * a.ncol;
   const int32_t* ho = a.hoff + (size_t)p * (a.ncol + 1);
   const uint32_t* hs = a.hsrc + (size_t)p * a.hmax;
   const uint16_t* hd = a.hdst + (size_t)p * a.hmax;
-  const uint16_t* nbr = a.nbr + (size_t)p * a.nlocmax * D;
-  const uint16_t* jm = a.jm + (size_t)p * a.nlocmax;
+  const uint16_t* nbr_g = a.nbr + (size_t)p * a.nlocmax * D;
+  const uint16_t* jm_g = a.jm + (size_t)p * a.nlocmax;
+  int32_t* gid = reinterpret_cast<int32_t*>(Wsh + a.slots);
+  uint16_t* jm = reinterpret_cast<uint16_t*>(gid + a.nlocmax);
+  uint16_t* nbr = jm + a.nlocmax;
   const int nloc = co[a.ncol];
   const int nhalo = ho[a.ncol];
   uint32_t* gw = a.words + (size_t)g * a.n;
-  for (int s = threadIdx.x; s < nloc + nhalo; s += blockDim.x) Wsh[s] = gw[gid[s]];
+  for (int s = threadIdx.x; s < nloc + nhalo; s += blockDim.x) Wsh[s] = gw[gid_g[s]];
+  for (int s = threadIdx.x; s < nloc; s += blockDim.x) {
+    gid[s] = gid_g[s];
+    jm[s] = jm_g[s];
+  }
+  for (int s = threadIdx.x; s < nloc * D; s += blockDim.x) nbr[s] = nbr_g[s];
   __syncthreads();
+  cluster_arrive();
+  int prev = -1;  // colour class updated by the previous phase
   for (int64_t k = 0; k < a.nsweeps; ++k) {
-    const uint32_t* thr_k = a.thr + (size_t)k * (D + 1);
-    const uint32_t alw = a.always[k];
+    const MscSweep<D> sw = msc_sweep<D>(a.thr + (size_t)k * (D + 1), a.always[k]);
     for (int c = 0; c < a.ncol; ++c) {
-      const int lo = co[c], hi = co[c + 1];
-      for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
-        const uint32_t w = Wsh[s];
-        Wsh[s] = msc_site<D>(w, Wsh, nbr + (size_t)s * D, jm[s], thr_k, alw, (uint32_t)gid[s],
-                             (uint32_t)k, (uint32_t)g, a.k0, a.k1);
-      }
-      cl.sync();
-      const int hlo = ho[c], hhi = ho[c + 1];
-      for (int e = hlo + threadIdx.x; e < hhi; e += blockDim.x) {
-        const uint32_t src = hs[e];
-        const uint32_t* remote = cl.map_shared_rank(Wsh, (int)(src >> 16));
-        Wsh[hd[e]] = remote[src & 0xFFFFu];
+      msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, (uint32_t)k, (uint32_t)g, a.k0, a.k1);
+      cluster_wait();
+      if (prev >= 0) {
+        const int hlo = ho[prev], hhi = ho[prev + 1];
+        for (int e = hlo + threadIdx.x; e < hhi; e += blockDim.x) {
+          const uint32_t src = hs[e];
+          const uint32_t* remote = cl.map_shared_rank(Wsh, (int)(src >> 16));
+          Wsh[hd[e]] = remote[src & 0xFFFFu];
+        }
       }
       __syncthreads();
+      msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, (uint32_t)k, (uint32_t)g, a.k0, a.k1);
+      cluster_arrive();
+      __syncthreads();
+      prev = c;
     }
   }
+  cluster_wait();
   for (int s = threadIdx.x; s < nloc; s += blockDim.x) gw[gid[s]] = Wsh[s];
-  cl.sync();  // keep this CTA's shared memory alive until every peer is done reading it
+}
+
+size_t msc_smem_bytes(const MscPlan& pl) {
+  return (size_t)pl.slots * 4 + (size_t)pl.nlocmax * (4 + 2 + 2 * pl.D) + 16;
+}
+
+int msc_threads() {
+  int threads = kMscDefaultThreads;
+  if (const char* env = std::getenv("OJ_MSC_THREADS")) {
+    const int v = std::atoi(env);
+    if (v >= 32 && v <= kMscMaxThreads && v % 32 == 0) threads = v;
+  }
+  return threads;
 }
 
 template <int D>
 cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st) {
   auto kern = sa_msc_kernel<D>;
-  const size_t smem = (size_t)pl.slots * sizeof(uint32_t);
+  const size_t smem = msc_smem_bytes(pl);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if (pl.P > 8) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(pl.P, G, 1);
-  cfg.blockDim = dim3(kMscThreads, 1, 1);
+  cfg.blockDim = dim3(msc_threads(), 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -184,16 +270,23 @@ cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st
 
 int msc_max_degree() { return kMscMaxDegree; }
 
+// Cluster size: the number of CTAs per replica group.  One CTA per SM, as
+// many CTAs as fit on the SMs (measured on the L=128 lattice: one 512-thread
+// CTA per SM beats two smaller ones and uneven multi-CTA packings), within the
+// shared-memory budget and the 16-CTA non-portable cluster limit.
 int msc_choose_cluster(const oj_graph* g, int G, int sm_count) {
   if (const char* env = std::getenv("OJ_MSC_CLUSTER")) {
     const int v = std::atoi(env);
-    if (v == 1 || v == 2 || v == 4 || v == 8) return v;
+    if (v >= 1 && v <= kMscMaxCluster) return v;
   }
-  int P = 1;
-  // smallest power of two that fills the SMs, within the portable cluster limit
-  while (P < 8 && G * P < sm_count) P <<= 1;
-  // shared memory: words of own sites + halo must fit
-  while (P < 8 && (g->n / P) * 5 / 4 > kMscSmemWords) P <<= 1;
+  const int D = g->info.max_degree;
+  auto fits = [&](int P) {
+    const size_t per = (size_t)((g->n + P - 1) / P);
+    return per * (4 + 6 + 2 * (size_t)D) + per / 2 * 4 <= kMscSmemBytes;
+  };
+  int P = std::max(1, std::min(kMscMaxCluster, sm_count / std::max(G, 1)));
+  while (P > 1 && g->n / P < 256) --P;
+  while (P < kMscMaxCluster && !fits(P)) ++P;
   return P;
 }
 
@@ -206,21 +299,25 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
   std::vector<int> bound(P + 1);
   for (int p = 0; p <= P; ++p) bound[p] = (int)(((int64_t)p * n) / P);
   std::vector<int> part_of(n), slot_of(n);
+  std::vector<char> is_bnd(n, 0);
+  for (int p = 0; p < P; ++p)
+    for (int i = bound[p]; i < bound[p + 1]; ++i) part_of[i] = p;
+  for (int i = 0; i < n; ++i)
+    for (int q = g->rp[i]; q < g->rp[i + 1]; ++q)
+      if (part_of[g->ci[q]] != part_of[i]) is_bnd[i] = 1;
   struct Part {
     std::vector<int> own, halo;  // global site ids in slot order
-    std::vector<int> coff, hoff;
+    std::vector<int> coff, cb, hoff;
   };
   std::vector<Part> parts(P);
-  auto by_colour = [&](int a, int b) {
-    return g->colour[a] != g->colour[b] ? g->colour[a] < g->colour[b] : a < b;
-  };
   for (int p = 0; p < P; ++p) {
     Part& pt = parts[p];
-    for (int i = bound[p]; i < bound[p + 1]; ++i) {
-      pt.own.push_back(i);
-      part_of[i] = p;
-    }
-    std::sort(pt.own.begin(), pt.own.end(), by_colour);
+    for (int i = bound[p]; i < bound[p + 1]; ++i) pt.own.push_back(i);
+    std::sort(pt.own.begin(), pt.own.end(), [&](int a, int b) {
+      if (g->colour[a] != g->colour[b]) return g->colour[a] < g->colour[b];
+      if (is_bnd[a] != is_bnd[b]) return is_bnd[a] < is_bnd[b];
+      return a < b;
+    });
     for (size_t s = 0; s < pt.own.size(); ++s) slot_of[pt.own[s]] = (int)s;
   }
   int slots = 0, nlocmax = 0, hmax = 0;
@@ -235,8 +332,11 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
           pt.halo.push_back(j);
         }
       }
-    std::sort(pt.halo.begin(), pt.halo.end(), by_colour);
+    std::sort(pt.halo.begin(), pt.halo.end(), [&](int a, int b) {
+      return g->colour[a] != g->colour[b] ? g->colour[a] < g->colour[b] : a < b;
+    });
     pt.coff.assign(ncol + 1, 0);
+    pt.cb.assign(ncol, 0);
     pt.hoff.assign(ncol + 1, 0);
     for (int i : pt.own) pt.coff[g->colour[i] + 1]++;
     for (int j : pt.halo) pt.hoff[g->colour[j] + 1]++;
@@ -244,17 +344,22 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
       pt.coff[c + 1] += pt.coff[c];
       pt.hoff[c + 1] += pt.hoff[c];
     }
+    for (int c = 0; c < ncol; ++c) {
+      int s = pt.coff[c];
+      while (s < pt.coff[c + 1] && !is_bnd[pt.own[s]]) ++s;
+      pt.cb[c] = s;
+    }
     slots = std::max(slots, (int)(pt.own.size() + pt.halo.size()));
     nlocmax = std::max(nlocmax, (int)pt.own.size());
     hmax = std::max(hmax, (int)pt.halo.size());
   }
-  if (slots > 65535 || slots > kMscSmemWords) {
+  if (slots > 65535 || (size_t)slots * 4 + (size_t)nlocmax * (6 + 2 * D) + 16 > kMscSmemBytes) {
     if (why) *why = "bit-packed kernel: partition does not fit shared memory; use a larger cluster";
     return cudaErrorInvalidValue;
   }
   hmax = std::max(hmax, 1);
-  // host images of the tables
-  std::vector<int32_t> gidx((size_t)P * slots, 0), coff((size_t)P * (ncol + 1)), hoff((size_t)P * (ncol + 1));
+  std::vector<int32_t> gidx((size_t)P * slots, 0), coff((size_t)P * (ncol + 1)), cbv((size_t)P * ncol),
+      hoff((size_t)P * (ncol + 1));
   std::vector<uint32_t> hsrc((size_t)P * hmax, 0);
   std::vector<uint16_t> hdst((size_t)P * hmax, 0), nbr((size_t)P * nlocmax * D, 0), jm((size_t)P * nlocmax, 0);
   for (int p = 0; p < P; ++p) {
@@ -273,6 +378,7 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
       coff[(size_t)p * (ncol + 1) + c] = pt.coff[c];
       hoff[(size_t)p * (ncol + 1) + c] = pt.hoff[c];
     }
+    for (int c = 0; c < ncol; ++c) cbv[(size_t)p * ncol + c] = pt.cb[c];
     for (int s = 0; s < nloc; ++s) {
       const int i = pt.own[s];
       uint16_t bits = 0;
@@ -294,10 +400,10 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
   plan->nlocmax = nlocmax;
   plan->hmax = hmax;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t b_gidx = al(gidx.size() * 4), b_coff = al(coff.size() * 4), b_hoff = al(hoff.size() * 4),
-               b_hsrc = al(hsrc.size() * 4), b_hdst = al(hdst.size() * 2), b_nbr = al(nbr.size() * 2),
-               b_jm = al(jm.size() * 2);
-  cudaError_t e = plan->tables.ensure(b_gidx + b_coff + b_hoff + b_hsrc + b_hdst + b_nbr + b_jm);
+  const size_t b_gidx = al(gidx.size() * 4), b_coff = al(coff.size() * 4), b_cb = al(cbv.size() * 4),
+               b_hoff = al(hoff.size() * 4), b_hsrc = al(hsrc.size() * 4), b_hdst = al(hdst.size() * 2),
+               b_nbr = al(nbr.size() * 2), b_jm = al(jm.size() * 2);
+  cudaError_t e = plan->tables.ensure(b_gidx + b_coff + b_cb + b_hoff + b_hsrc + b_hdst + b_nbr + b_jm);
   if (e != cudaSuccess) return e;
   char* base = plan->tables.as<char>();
   size_t off = 0;
@@ -308,6 +414,7 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
   };
   if ((e = put(plan->gidx, gidx, b_gidx)) != cudaSuccess) return e;
   if ((e = put(plan->coff, coff, b_coff)) != cudaSuccess) return e;
+  if ((e = put(plan->cb, cbv, b_cb)) != cudaSuccess) return e;
   if ((e = put(plan->hoff, hoff, b_hoff)) != cudaSuccess) return e;
   if ((e = put(plan->hsrc, hsrc, b_hsrc)) != cudaSuccess) return e;
   if ((e = put(plan->hdst, hdst, b_hdst)) != cudaSuccess) return e;
@@ -324,6 +431,7 @@ cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint3
   MscArgs a;
   a.gidx = pl.gidx;
   a.coff = pl.coff;
+  a.cb = pl.cb;
   a.hoff = pl.hoff;
   a.hsrc = pl.hsrc;
   a.hdst = pl.hdst;
