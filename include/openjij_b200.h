@@ -105,10 +105,15 @@ oj_status oj_graph_query(const oj_graph* g, oj_graph_info* out);
  *  openjij/declare.hpp:687-793).  The schedule is (betas[k], mcs[k]) for
  * k < num_sched, as ClassicalSchedule (schedule_list.hpp:121-127).
  * spins [R][n] in/out.  energies [R] (may be NULL): FP64 energy
- * sum_{i<j} J_ij s_i s_j + sum_i h_i s_i (dense.hpp:176-192). */
+ * sum_{i<j} J_ij s_i s_j + sum_i h_i s_i (dense.hpp:176-192).
+ * Random numbers are a pure function of (seed, global sweep, global replica,
+ * site): first_sweep is the global index of this call's first sweep and
+ * replica_offset (a multiple of 32) the global index of replica 0, so a run
+ * split over several calls or several GPUs reproduces the unsplit run. */
 oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
                     const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
-                    uint32_t flags, double* energies, oj_run_stats* stats);
+                    int64_t first_sweep, int64_t replica_offset, uint32_t flags, double* energies,
+                    oj_run_stats* stats);
 
 /* Discrete-time path-integral SQA over R replicas x T Trotter slices.
  * Replaces Algorithm<SingleSpinFlip>::run(TransverseIsing, rng, schedule)
@@ -120,8 +125,9 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t
  * minimum energy (include/openjij/result/get_solution.hpp:59-84). */
 oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32_t num_slices,
                      int8_t* spins, double gamma, const double* betas, const double* s,
-                     const int32_t* mcs, int32_t num_sched, uint64_t seed, uint32_t flags,
-                     double* energies, int32_t* best_slice, oj_run_stats* stats);
+                     const int32_t* mcs, int32_t num_sched, uint64_t seed, int64_t first_sweep,
+                     int64_t replica_offset, uint32_t flags, double* energies,
+                     int32_t* best_slice, oj_run_stats* stats);
 
 /* FP64 energies of R spin vectors [R][n].  Replaces Dense::energy /
  * CSRSparse::energy (dense.hpp:176-192, csr_sparse.hpp:139-155). */

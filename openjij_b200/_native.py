@@ -82,8 +82,9 @@ def lib():
         L.oj_graph_create_csr.argtypes = [vp, i32, vp, vp, vp, C.POINTER(vp)]
         L.oj_graph_destroy.argtypes = [vp]
         L.oj_graph_query.argtypes = [vp, C.POINTER(GraphInfo)]
-        L.oj_sa_run.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, u32, vp, C.POINTER(RunStats)]
-        L.oj_sqa_run.argtypes = [vp, vp, i32, i32, vp, dbl, vp, vp, vp, i32, u64, u32, vp, vp,
+        L.oj_sa_run.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64, u32, vp,
+                                C.POINTER(RunStats)]
+        L.oj_sqa_run.argtypes = [vp, vp, i32, i32, vp, dbl, vp, vp, vp, i32, u64, i64, i64, u32, vp, vp,
                                  C.POINTER(RunStats)]
         L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
         for name in EXPORTS:
@@ -186,20 +187,21 @@ def _flags(kernel, device):
     return f
 
 
-def sa_run(g: Graph, spins, betas, mcs, seed, kernel="auto", energies=None, device=False):
+def sa_run(g: Graph, spins, betas, mcs, seed, kernel="auto", energies=None, device=False,
+           first_sweep=0, replica_offset=0):
     """spins: int8 [R][n] numpy (in/out) or device tensor/pointer with device=True."""
     R = spins.shape[0] if hasattr(spins, "shape") else None
     b = np.ascontiguousarray(betas, np.float64)
     m = np.ascontiguousarray(mcs, np.int32)
     st = RunStats()
     g.ctx.check(lib().oj_sa_run(g.ctx._h, g._h, int(R), _ptr(spins), _ptr(b), _ptr(m), len(b),
-                                int(seed) & 0xFFFFFFFFFFFFFFFF, _flags(kernel, device), _ptr(energies),
-                                C.byref(st)), "oj_sa_run")
+                                int(seed) & 0xFFFFFFFFFFFFFFFF, int(first_sweep), int(replica_offset),
+                                _flags(kernel, device), _ptr(energies), C.byref(st)), "oj_sa_run")
     return st.as_dict()
 
 
 def sqa_run(g: Graph, spins, gamma, betas, s, mcs, seed, energies=None, best=None, kernel="auto",
-            device=False):
+            device=False, first_sweep=0, replica_offset=0):
     """spins: int8 [R][T][n]."""
     R, T = spins.shape[0], spins.shape[1]
     b = np.ascontiguousarray(betas, np.float64)
@@ -208,7 +210,8 @@ def sqa_run(g: Graph, spins, gamma, betas, s, mcs, seed, energies=None, best=Non
     st = RunStats()
     g.ctx.check(lib().oj_sqa_run(g.ctx._h, g._h, int(R), int(T), _ptr(spins), float(gamma), _ptr(b),
                                  _ptr(sv), _ptr(m), len(b), int(seed) & 0xFFFFFFFFFFFFFFFF,
-                                 _flags(kernel, device), _ptr(energies), _ptr(best), C.byref(st)),
+                                 int(first_sweep), int(replica_offset), _flags(kernel, device),
+                                 _ptr(energies), _ptr(best), C.byref(st)),
                 "oj_sqa_run")
     return st.as_dict()
 

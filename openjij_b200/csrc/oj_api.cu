@@ -63,6 +63,17 @@ oj_status expand(oj_ctx* ctx, const T* params, const int32_t* mcs, int32_t num_s
   return OJ_OK;
 }
 
+oj_status rng_base(oj_ctx* ctx, uint64_t seed, int64_t first_sweep, int64_t replica_offset, RngBase* rb) {
+  if (first_sweep < 0 || first_sweep > 0xFFFFFFFFll) return arg_fail(ctx, "first_sweep out of range");
+  if (replica_offset < 0 || replica_offset > 0xFFFFFFFFll || (replica_offset & 31) != 0)
+    return arg_fail(ctx, "replica_offset must be a non-negative multiple of 32");
+  rb->k0 = (uint32_t)seed;
+  rb->k1 = (uint32_t)(seed >> 32);
+  rb->sweep0 = (uint32_t)first_sweep;
+  rb->rep0 = (uint32_t)replica_offset;
+  return OJ_OK;
+}
+
 bool is_device_ptr(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -257,8 +268,8 @@ oj_status oj_graph_query(const oj_graph* g, oj_graph_info* out) {
 }
 
 oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, const double* betas,
-                    const int32_t* mcs, int32_t num_sched, uint64_t seed, uint32_t flags, double* energies,
-                    oj_run_stats* stats) {
+                    const int32_t* mcs, int32_t num_sched, uint64_t seed, int64_t first_sweep,
+                    int64_t replica_offset, uint32_t flags, double* energies, oj_run_stats* stats) {
   if (!ctx || !gc || R < 0 || num_sched < 0) return arg_fail(ctx, "null argument or negative size");
   if (num_sched > 0 && (!betas || !mcs)) return arg_fail(ctx, "null schedule");
   oj_graph* g = const_cast<oj_graph*>(gc);
@@ -269,6 +280,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   if (!spins) return arg_fail(ctx, "null spins");
   for (int32_t k = 0; k < num_sched; ++k)
     if (!(betas[k] >= 0.0) || std::isinf(betas[k])) return arg_fail(ctx, "beta must be finite and >= 0");
+  RngBase rb;
+  if (oj_status s = rng_base(ctx, seed, first_sweep, replica_offset, &rb)) return s;
   DeviceGuard dg(ctx->device);
   std::vector<double> bexp;
   if (oj_status s = expand(ctx, betas, mcs, num_sched, bexp)) return s;
@@ -331,7 +344,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(launch_pack(d_spins, R, n, d_words, st), "pack");
     ++launches;
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-    if (S > 0) OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, seed, st, &launches), "sa bit-packed kernel");
+    if (S > 0) OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, rb, st, &launches), "sa bit-packed kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_unpack(d_words, R, n, d_spins, st), "unpack");
     ++launches;
@@ -343,9 +356,9 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0) {
       if (kernel == OJ_KERNEL_DENSE_PLAIN)
-        OJ_CK(launch_sa_dense_plain(g, R, d_spins, d_beta, S, seed, st, &launches), "sa dense kernel");
+        OJ_CK(launch_sa_dense_plain(g, R, d_spins, d_beta, S, rb, st, &launches), "sa dense kernel");
       else
-        OJ_CK(launch_sa_colour(g, R, d_spins, d_beta, S, seed, st, &launches), "sa colour kernel");
+        OJ_CK(launch_sa_colour(g, R, d_spins, d_beta, S, rb, st, &launches), "sa colour kernel");
     }
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   }
@@ -375,8 +388,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
 
 oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8_t* spins, double gamma,
                      const double* betas, const double* s, const int32_t* mcs, int32_t num_sched,
-                     uint64_t seed, uint32_t flags, double* energies, int32_t* best_slice,
-                     oj_run_stats* stats) {
+                     uint64_t seed, int64_t first_sweep, int64_t replica_offset, uint32_t flags,
+                     double* energies, int32_t* best_slice, oj_run_stats* stats) {
   if (!ctx || !gc || R < 0 || num_sched < 0) return arg_fail(ctx, "null argument or negative size");
   if (T < 2) return arg_fail(ctx, "trotter slices must be equal or larger than 2.");
   if (num_sched > 0 && (!betas || !s || !mcs)) return arg_fail(ctx, "null schedule");
@@ -392,6 +405,8 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     return OJ_ERR_UNSUPPORTED;
   }
   kernel = OJ_KERNEL_COLOUR;
+  RngBase rb;
+  if (oj_status st_ = rng_base(ctx, seed, first_sweep, replica_offset, &rb)) return st_;
   DeviceGuard dg(ctx->device);
   // per-schedule-entry coefficients (single_spin_flip.hpp:147-148, 215-217)
   std::vector<float2> coef_sched(num_sched);
@@ -421,7 +436,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   float2* d_coef = ctx->params.as<float2>();
   if (S > 0) OJ_CK(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(float2), cudaMemcpyHostToDevice, st), "H2D coef");
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-  if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, seed, st, &launches), "sqa kernel");
+  if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, rb, st, &launches), "sqa kernel");
   OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   if (energies || best_slice) {
     double* d_e = (devp && energies) ? energies : nullptr;

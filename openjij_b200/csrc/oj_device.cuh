@@ -46,6 +46,38 @@ __device__ __forceinline__ u4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint
   return u4{c0, c1, c2, c3};
 }
 
+// Philox key schedule (the ten round keys), precomputed on the host and
+// passed as a kernel parameter so that every round reads its key from the
+// constant bank instead of adding the Weyl increment.
+struct Keys {
+  uint32_t k0[10];
+  uint32_t k1[10];
+};
+
+inline Keys make_keys(uint32_t k0, uint32_t k1) {
+  Keys K;
+  for (int r = 0; r < 10; ++r) {
+    K.k0[r] = k0;
+    K.k1[r] = k1;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return K;
+}
+
+__device__ __forceinline__ u4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const Keys& K) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    c0 = (uint32_t)(p1 >> 32) ^ c1 ^ K.k0[r];
+    c1 = (uint32_t)p1;
+    c2 = (uint32_t)(p0 >> 32) ^ c3 ^ K.k1[r];
+    c3 = (uint32_t)p0;
+  }
+  return u4{c0, c1, c2, c3};
+}
+
 __device__ __forceinline__ uint32_t pick(const u4& v, int j) {
   return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
 }

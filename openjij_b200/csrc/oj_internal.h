@@ -99,16 +99,25 @@ struct oj_ctx {
 
 namespace oj {
 
+// Counter base of a run: Philox key and the global indices of the first sweep
+// and the first replica, so that a run split over calls (first_sweep) or over
+// GPUs (replica_offset) draws exactly the numbers of the unsplit run.
+struct RngBase {
+  uint32_t k0, k1;
+  uint32_t sweep0;
+  uint32_t rep0;
+};
+
 // ---- launchers (each returns cudaGetLastError() after the launch) ---------
 
 cudaError_t launch_sa_colour(const oj_graph* g, int R, int8_t* spins, const float* betas,
-                             int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches);
+                             int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
 cudaError_t launch_sqa_colour(const oj_graph* g, int R, int T, int8_t* spins, const float2* coef,
-                              int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches);
+                              int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
 cudaError_t launch_sa_dense_plain(const oj_graph* g, int R, int8_t* spins, const float* betas,
-                                  int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches);
+                                  int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
 cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
-                          const uint32_t* always, int64_t nsweeps, uint64_t seed, cudaStream_t st,
+                          const uint32_t* always, int64_t nsweeps, RngBase rb, cudaStream_t st,
                           int* launches);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);

@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(kColourThreads)
                      const float* __restrict__ val, const float* __restrict__ h,
                      const int32_t* __restrict__ order, const int32_t* __restrict__ coff, int ncol,
                      int n, int R, int8_t* __restrict__ spins, const float* __restrict__ betas,
-                     int64_t nsweeps, uint32_t key0, uint32_t key1) {
+                     int64_t nsweeps, RngBase rb) {
   extern __shared__ int8_t sh[];
   const int q = blockIdx.x;
   const int r0 = 4 * q;
@@ -65,7 +65,8 @@ __global__ void __launch_bounds__(kColourThreads)
           if (nr > 2) f2 = __fadd_rn(f2, S[2 * n + j] > 0 ? v : -v);
           if (nr > 3) f3 = __fadd_rn(f3, S[3 * n + j] > 0 ? v : -v);
         }
-        const ojd::u4 rnd = ojd::philox((uint32_t)i, (uint32_t)k, (uint32_t)q, ojd::TAG_SA, key0, key1);
+        const ojd::u4 rnd = ojd::philox((uint32_t)i, rb.sweep0 + (uint32_t)k, (rb.rep0 >> 2) + (uint32_t)q,
+                                        ojd::TAG_SA, rb.k0, rb.k1);
         const float fs[4] = {f0, f1, f2, f3};
 #pragma unroll
         for (int rl = 0; rl < 4; ++rl) {
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(kSqaThreads)
                       const float* __restrict__ val, const float* __restrict__ h,
                       const int32_t* __restrict__ order, const int32_t* __restrict__ coff, int ncol,
                       int n, int T, int8_t* __restrict__ spins, const float2* __restrict__ coef,
-                      int64_t nsweeps, uint32_t key0, uint32_t key1) {
+                      int64_t nsweeps, RngBase rb) {
   extern __shared__ int8_t sh[];
   const int r = blockIdx.x;
   const size_t tn = (size_t)T * n;
@@ -120,9 +121,9 @@ __global__ void __launch_bounds__(kSqaThreads)
           const int i = order[lo + (it - a * cnt)];
           const int tq = 8 * a + par;
           if (tq + 6 < tmin || tq >= tmax) continue;
-          const ojd::u4 rnd = ojd::philox((uint32_t)i, (uint32_t)k, (uint32_t)r,
+          const ojd::u4 rnd = ojd::philox((uint32_t)i, rb.sweep0 + (uint32_t)k, rb.rep0 + (uint32_t)r,
                                           ((uint32_t)a << 9) | ((uint32_t)par << 8) | ojd::TAG_SQA,
-                                          key0, key1);
+                                          rb.k0, rb.k1);
           const float hi_f = h[i];
           const int p0 = rp[i], p1 = rp[i + 1];
 #pragma unroll
@@ -227,11 +228,10 @@ __global__ void unpack_kernel(const uint32_t* __restrict__ words, int R, int n, 
 int sa_colour_max_smem_sites() { return kSmemBudget / 4; }
 
 cudaError_t launch_sa_colour(const oj_graph* g, int R, int8_t* spins, const float* betas,
-                             int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches) {
+                             int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches) {
   const int quads = (R + 3) / 4;
   const size_t smem = (size_t)4 * g->n;
   const bool use_smem = smem <= (size_t)kSmemBudget;
-  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   if (use_smem) {
     auto kern = sa_colour_kernel<true>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -239,22 +239,21 @@ cudaError_t launch_sa_colour(const oj_graph* g, int R, int8_t* spins, const floa
     kern<<<quads, kColourThreads, smem, st>>>(g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(),
                                              g->d_val.as<float>(), g->d_h.as<float>(),
                                              g->d_order.as<int32_t>(), g->d_coff.as<int32_t>(),
-                                             g->info.num_colours, g->n, R, spins, betas, nsweeps, k0, k1);
+                                             g->info.num_colours, g->n, R, spins, betas, nsweeps, rb);
   } else {
     sa_colour_kernel<false><<<quads, kColourThreads, 0, st>>>(
         g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(), g->d_val.as<float>(), g->d_h.as<float>(),
         g->d_order.as<int32_t>(), g->d_coff.as<int32_t>(), g->info.num_colours, g->n, R, spins,
-        betas, nsweeps, k0, k1);
+        betas, nsweeps, rb);
   }
   if (launches) ++*launches;
   return cudaGetLastError();
 }
 
 cudaError_t launch_sqa_colour(const oj_graph* g, int R, int T, int8_t* spins, const float2* coef,
-                              int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches) {
+                              int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches) {
   const size_t smem = (size_t)T * g->n;
   const bool use_smem = smem <= (size_t)kSmemBudget;
-  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   if (use_smem) {
     auto kern = sqa_colour_kernel<true>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -262,12 +261,12 @@ cudaError_t launch_sqa_colour(const oj_graph* g, int R, int T, int8_t* spins, co
     kern<<<R, kSqaThreads, smem, st>>>(g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(),
                                         g->d_val.as<float>(), g->d_h.as<float>(),
                                         g->d_order.as<int32_t>(), g->d_coff.as<int32_t>(),
-                                        g->info.num_colours, g->n, T, spins, coef, nsweeps, k0, k1);
+                                        g->info.num_colours, g->n, T, spins, coef, nsweeps, rb);
   } else {
     sqa_colour_kernel<false><<<R, kSqaThreads, 0, st>>>(
         g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(), g->d_val.as<float>(), g->d_h.as<float>(),
         g->d_order.as<int32_t>(), g->d_coff.as<int32_t>(), g->info.num_colours, g->n, T, spins,
-        coef, nsweeps, k0, k1);
+        coef, nsweeps, rb);
   }
   if (launches) ++*launches;
   return cudaGetLastError();

@@ -15,7 +15,7 @@ namespace {
 __global__ void __launch_bounds__(128)
     sa_dense_plain_kernel(const float* __restrict__ J, const float* __restrict__ h, int n, int R,
                           int8_t* __restrict__ spins, const float* __restrict__ betas,
-                          int64_t nsweeps, uint32_t key0, uint32_t key1, int warps_per_cta) {
+                          int64_t nsweeps, RngBase rb, int warps_per_cta) {
   extern __shared__ float shf[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = blockIdx.x * warps_per_cta + warp;
@@ -35,14 +35,16 @@ __global__ void __launch_bounds__(128)
     f[j] = acc;
   }
   __syncwarp();
-  const uint32_t c2 = (uint32_t)(r >> 2);
-  const int lane_r = r & 3;
+  const uint32_t rg = rb.rep0 + (uint32_t)r;  // global replica index
+  const uint32_t c2 = rg >> 2;
+  const int lane_r = (int)(rg & 3u);
   for (int64_t k = 0; k < nsweeps; ++k) {
     const float beta = betas[k];
     for (int i0 = 0; i0 < n; i0 += 32) {
       float L = 0.0f;
       if (i0 + lane < n)
-        L = ojd::neglog(ojd::pick(ojd::philox((uint32_t)(i0 + lane), (uint32_t)k, c2, ojd::TAG_SA, key0, key1), lane_r));
+        L = ojd::neglog(ojd::pick(
+            ojd::philox((uint32_t)(i0 + lane), rb.sweep0 + (uint32_t)k, c2, ojd::TAG_SA, rb.k0, rb.k1), lane_r));
       const int cnt = min(32, n - i0);
       for (int ii = 0; ii < cnt; ++ii) {
         const int i = i0 + ii;
@@ -68,7 +70,7 @@ __global__ void __launch_bounds__(128)
 }  // namespace
 
 cudaError_t launch_sa_dense_plain(const oj_graph* g, int R, int8_t* spins, const float* betas,
-                                  int64_t nsweeps, uint64_t seed, cudaStream_t st, int* launches) {
+                                  int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches) {
   const int n = g->n;
   const size_t per_warp = (size_t)n * 5;
   int wpc = 4;
@@ -80,7 +82,7 @@ cudaError_t launch_sa_dense_plain(const oj_graph* g, int R, int8_t* spins, const
   if (e != cudaSuccess) return e;
   const int blocks = (R + wpc - 1) / wpc;
   kern<<<blocks, 32 * wpc, smem, st>>>(g->d_dense.as<float>(), g->d_h.as<float>(), n, R, spins, betas,
-                                       nsweeps, (uint32_t)seed, (uint32_t)(seed >> 32), wpc);
+                                       nsweeps, rb, wpc);
   if (launches) ++*launches;
   return cudaGetLastError();
 }

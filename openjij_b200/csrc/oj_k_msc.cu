@@ -62,7 +62,9 @@ struct MscArgs {
   const uint32_t* thr;     // [nsweeps][D+1]
   const uint32_t* always;  // [nsweeps]
   int64_t nsweeps;
-  uint32_t k0, k1;
+  ojd::Keys keys;
+  uint32_t sweep0;  // global index of the first sweep
+  uint32_t group0;  // global index of the first replica group
 };
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -113,7 +115,7 @@ template <int D>
 __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restrict__ Wsh,
                                              const uint16_t* __restrict__ nb, uint32_t jmk,
                                              const MscSweep<D>& sw, uint32_t site, uint32_t sweep,
-                                             uint32_t grp, uint32_t k0, uint32_t k1) {
+                                             uint32_t grp, const ojd::Keys& K) {
   constexpr int NB = D <= 1 ? 1 : (D <= 3 ? 2 : (D <= 7 ? 3 : 4));
   constexpr int UMAX = MscSweep<D>::UMAX;
   uint32_t cnt[NB];
@@ -144,9 +146,10 @@ __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restr
   }
   flip |= ~uphill;
   uint32_t lt = 0u;
-#pragma unroll 1
-  for (int q = 0; q < 8 && pending; ++q) {
-    const ojd::u4 r = ojd::philox(site, sweep, grp, ((uint32_t)q << 8) | ojd::TAG_SA_MSC, k0, k1);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    if (!pending) break;
+    const ojd::u4 r = ojd::philox(site, sweep, grp, ((uint32_t)q << 8) | ojd::TAG_SA_MSC, K);
     msc_level<D>(sw, cls, 31 - 4 * q, r.x, pending, lt);
     msc_level<D>(sw, cls, 30 - 4 * q, r.y, pending, lt);
     msc_level<D>(sw, cls, 29 - 4 * q, r.z, pending, lt);
@@ -160,14 +163,14 @@ template <int D>
 __device__ __forceinline__ void msc_range(int lo, int hi, uint32_t* __restrict__ Wsh,
                                           const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
                                           const uint16_t* __restrict__ nbr, const MscSweep<D>& sw,
-                                          uint32_t k, uint32_t g, uint32_t k0, uint32_t k1) {
+                                          uint32_t k, uint32_t g, const ojd::Keys& K) {
   const int T = blockDim.x;
   for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
     const int s2 = s + T;
-    const uint32_t a = msc_site<D>(Wsh[s], Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, k0, k1);
+    const uint32_t a = msc_site<D>(Wsh[s], Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, K);
     if (s2 < hi) {
       const uint32_t b =
-          msc_site<D>(Wsh[s2], Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, k0, k1);
+          msc_site<D>(Wsh[s2], Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, K);
       Wsh[s2] = b;
     }
     Wsh[s] = a;
@@ -206,8 +209,9 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
   int prev = -1;  // colour class updated by the previous phase
   for (int64_t k = 0; k < a.nsweeps; ++k) {
     const MscSweep<D> sw = msc_sweep<D>(a.thr + (size_t)k * (D + 1), a.always[k]);
+    const uint32_t kk = a.sweep0 + (uint32_t)k, gg = a.group0 + (uint32_t)g;
     for (int c = 0; c < a.ncol; ++c) {
-      msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, (uint32_t)k, (uint32_t)g, a.k0, a.k1);
+      msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_wait();
       if (prev >= 0) {
         const int hlo = ho[prev], hhi = ho[prev + 1];
@@ -218,7 +222,7 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
         }
       }
       __syncthreads();
-      msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, (uint32_t)k, (uint32_t)g, a.k0, a.k1);
+      msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_arrive();
       __syncthreads();
       prev = c;
@@ -425,7 +429,7 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
 }
 
 cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
-                          const uint32_t* always, int64_t nsweeps, uint64_t seed, cudaStream_t st,
+                          const uint32_t* always, int64_t nsweeps, RngBase rb, cudaStream_t st,
                           int* launches) {
   const MscPlan& pl = *g->msc;
   MscArgs a;
@@ -446,8 +450,9 @@ cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint3
   a.thr = thr;
   a.always = always;
   a.nsweeps = nsweeps;
-  a.k0 = (uint32_t)seed;
-  a.k1 = (uint32_t)(seed >> 32);
+  a.keys = ojd::make_keys(rb.k0, rb.k1);
+  a.sweep0 = rb.sweep0;
+  a.group0 = rb.rep0 >> 5;
   if (launches) ++*launches;
   switch (pl.D) {
     case 1: return launch_d<1>(pl, a, G, st);

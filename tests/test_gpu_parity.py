@@ -147,3 +147,63 @@ def test_sqa_rejects_one_slice(ctx):
     with pytest.raises(N.OJError) as ei:
         N.sqa_run(dg, s, 1.0, [1.0], [0.5], [1], seed=1)
     assert ei.value.status == N.OJ_ERR_ARG
+
+
+@pytest.mark.parametrize("kernel,maker", [
+    ("bitpacked", lambda: I.lattice_pm_j(16, seed=5)),
+    ("colour", lambda: I.lattice_pm_j(8, seed=6)),
+    ("dense_plain", lambda: I.dense_ising_uniform(30, seed=7)),
+])
+def test_split_run_equals_single_run(ctx, kernel, maker):
+    """A schedule run in two calls (first_sweep = sweeps of the first call)
+    reproduces the one-call run bit for bit."""
+    m, _ = maker()
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.1, 5.0, 24)
+    s0 = _init(64, g.n, 3)
+    whole = s0.copy()
+    N.sa_run(dg, whole, betas, mcs, seed=11, kernel=kernel)
+    part = s0.copy()
+    N.sa_run(dg, part, betas[:10], mcs[:10], seed=11, kernel=kernel)
+    N.sa_run(dg, part, betas[10:], mcs[10:], seed=11, kernel=kernel, first_sweep=int(np.sum(mcs[:10])))
+    np.testing.assert_array_equal(part, whole)
+
+
+@pytest.mark.parametrize("kernel", ["bitpacked", "colour", "dense_plain"])
+def test_replica_shards_equal_whole(ctx, kernel):
+    """Replicas [32, 96) run alone with replica_offset=32 equal the same
+    replicas of a 96-replica run: results do not depend on the sharding."""
+    m, _ = I.lattice_pm_j(8, seed=8) if kernel != "dense_plain" else I.dense_ising_uniform(20, seed=8)
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.1, 5.0, 12)
+    s0 = _init(96, g.n, 4)
+    whole = s0.copy()
+    N.sa_run(dg, whole, betas, mcs, seed=21, kernel=kernel)
+    shard = s0[32:].copy()
+    N.sa_run(dg, shard, betas, mcs, seed=21, kernel=kernel, replica_offset=32)
+    np.testing.assert_array_equal(shard, whole[32:])
+
+
+def test_sqa_split_and_shard(ctx):
+    m, _ = I.random_regular_pm_j(40, 3, seed=9)
+    g, dg = _graph(ctx, m)
+    T, nsched = 6, 12
+    ss = np.linspace(0.0, 1.0, nsched)
+    betas = np.full(nsched, 8.0)
+    mcs = np.ones(nsched, np.int32)
+    s0 = np.ascontiguousarray(np.broadcast_to(_init(64, g.n, 5)[:, None, :], (64, T, g.n)))
+    whole = s0.copy()
+    N.sqa_run(dg, whole, 1.0, betas, ss, mcs, seed=3)
+    part = s0[32:].copy()
+    N.sqa_run(dg, part, 1.0, betas[:5], ss[:5], mcs[:5], seed=3, replica_offset=32)
+    N.sqa_run(dg, part, 1.0, betas[5:], ss[5:], mcs[5:], seed=3, replica_offset=32, first_sweep=5)
+    np.testing.assert_array_equal(part, whole[32:])
+
+
+def test_replica_offset_must_be_multiple_of_32(ctx):
+    m, _ = I.lattice_pm_j(4, seed=1)
+    g, dg = _graph(ctx, m)
+    s = _init(4, g.n, 1)
+    with pytest.raises(N.OJError) as ei:
+        N.sa_run(dg, s, [1.0], [1], seed=1, replica_offset=5)
+    assert ei.value.status == N.OJ_ERR_ARG
