@@ -1,0 +1,893 @@
+// pybind11 host module `cxxjij` of openjij_b200: OpenJij's cxxjij Python
+// surface (graph / system / algorithm / utility / result) for the
+// single-spin-flip path, with every sweep executed on the GPU through the C
+// ABI of include/openjij_b200.h.
+//
+// Reference bindings mirrored here (names, arguments, errors):
+//   openjij/declare.hpp:43-129   Graph, Dense          openjij/main.cpp:43-47
+//   openjij/declare.hpp:195-217  CSRSparse
+//   openjij/declare.hpp:409-438  ClassicalIsing        openjij/main.cpp:68-73
+//   openjij/declare.hpp:585-641  TransverseIsing       openjij/main.cpp:80-85
+//   openjij/declare.hpp:687-793  Algorithm_SingleSpinFlip_run (4 overloads)
+//   openjij/declare.hpp:795-879  updater parameters, schedules, make_*_schedule_list
+//   openjij/declare.hpp:881-888  get_solution
+// Extensions: a system may hold R replicas (2-D initial spins, or 3-D Trotter
+// spins); the whole batch anneals in one GPU call.
+#include <pybind11/functional.h>
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "openjij_b200.h"
+
+namespace py = pybind11;
+using namespace pybind11::literals;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device context
+// ---------------------------------------------------------------------------
+
+std::mutex g_ctx_mu;
+oj_ctx* g_ctx = nullptr;
+int g_device = -1;
+
+int default_device() {
+  const char* env = std::getenv("OPENJIJ_B200_DEVICE");
+  return env ? std::atoi(env) : 0;
+}
+
+oj_ctx* ctx() {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (!g_ctx) {
+    const int dev = g_device >= 0 ? g_device : default_device();
+    oj_ctx* c = nullptr;
+    const oj_status s = oj_ctx_create(dev, &c);
+    if (s != OJ_OK)
+      throw std::runtime_error(std::string("openjij_b200: cannot open CUDA device ") + std::to_string(dev) +
+                               ": " + oj_status_string(s));
+    g_ctx = c;
+    g_device = dev;
+  }
+  return g_ctx;
+}
+
+void check(oj_status s, const char* what) {
+  if (s == OJ_OK) return;
+  std::string msg = std::string(what) + ": " + oj_status_string(s);
+  if (g_ctx) {
+    const char* d = oj_ctx_last_error(g_ctx);
+    if (d && *d) msg += std::string(": ") + d;
+  }
+  if (s == OJ_ERR_ARG) throw std::invalid_argument(msg);
+  throw std::runtime_error(msg);
+}
+
+struct RunInfo {
+  std::string kernel;
+  int launches = 0;
+  long long sweeps = 0;
+  double attempts = 0;
+  double anneal_ms = 0, total_ms = 0;
+};
+RunInfo g_last_run;
+
+void record(const oj_run_stats& st) {
+  static const char* names[] = {"auto", "colour", "dense_plain", "bitpacked", "dense_tc"};
+  g_last_run.kernel = (st.kernel >= 0 && st.kernel < 5) ? names[st.kernel] : "?";
+  g_last_run.launches += st.launches;
+  g_last_run.sweeps += st.sweeps;
+  g_last_run.attempts += st.attempts;
+  g_last_run.anneal_ms += st.anneal_ms;
+  g_last_run.total_ms += st.total_ms;
+}
+
+// ---------------------------------------------------------------------------
+// reference random engine for gen_spin (include/openjij/utility/random.hpp:39-87)
+// ---------------------------------------------------------------------------
+
+class Xorshift {
+ public:
+  using result_type = uint_fast32_t;
+  static constexpr unsigned min() { return 0u; }
+  static constexpr unsigned max() { return UINT_MAX; }
+  explicit Xorshift(unsigned s) : w(s) {}
+  unsigned operator()() {
+    unsigned t = x ^ (x << 11);
+    x = y;
+    y = z;
+    z = w;
+    return w = (w ^ (w >> 19)) ^ (t ^ (t >> 8));
+  }
+
+ private:
+  unsigned x = 123456789u, y = 362436069u, z = 521288629u, w;
+};
+
+// ---------------------------------------------------------------------------
+// graphs
+// ---------------------------------------------------------------------------
+
+struct Graph {
+  explicit Graph(size_t n) : n_(n) {}
+  virtual ~Graph() = default;
+  template <class Eng>
+  std::vector<int> gen_spin(Eng& eng) const {  // include/openjij/graph/graph.hpp:54-65
+    std::vector<int> s(n_);
+    std::uniform_int_distribution<> uid(0, 1);
+    for (auto& e : s) e = 2 * uid(eng) - 1;
+    return s;
+  }
+  template <class Eng>
+  std::vector<int> gen_binary(Eng& eng) const {
+    std::vector<int> s(n_);
+    std::uniform_int_distribution<> uid(0, 1);
+    for (auto& e : s) e = uid(eng);
+    return s;
+  }
+  size_t size() const { return n_; }
+  size_t n_;
+};
+
+// Symmetric augmented matrix in CSR form plus the device copy built from it.
+struct AugCSR {
+  size_t n = 0;
+  std::vector<int64_t> indptr;
+  std::vector<int32_t> indices;
+  std::vector<double> data;
+};
+
+struct DeviceGraph {
+  oj_graph* h = nullptr;
+  ~DeviceGraph() {
+    if (h) oj_graph_destroy(h);
+  }
+};
+
+// Energy E(s) = sum_{i<j} J_ij s_i s_j + sum_i h_i s_i (dense.hpp:176-192).
+double aug_energy(const AugCSR& a, const std::vector<int>& s) {
+  if (s.size() != a.n) throw std::out_of_range("Out of range in energy in graph.");
+  double e = 0.0;
+  for (size_t i = 0; i < a.n; ++i) {
+    double acc = 0.0;
+    for (int64_t p = a.indptr[i]; p < a.indptr[i + 1]; ++p) {
+      const size_t j = (size_t)a.indices[p];
+      if (j < i) continue;
+      if (j == a.n)
+        acc += a.data[p];
+      else if (j > i)
+        acc += a.data[p] * s[j];
+    }
+    e += s[i] * acc;
+  }
+  return e;
+}
+
+struct Dense : Graph {
+  explicit Dense(size_t n) : Graph(n), J_((n + 1) * (n + 1), 0.0) { at(n, n) = 1.0; }
+  double& at(size_t i, size_t j) { return J_[i * (n_ + 1) + j]; }
+  double at(size_t i, size_t j) const { return J_[i * (n_ + 1) + j]; }
+  // J(i, j): coupling for i != j, h_i for i == j (dense.hpp:213-260)
+  double get(size_t i, size_t j) const {
+    if (i >= n_ || j >= n_) throw std::out_of_range("index out of range");
+    return i != j ? at(std::min(i, j), std::max(i, j)) : at(i, n_);
+  }
+  void set(size_t i, size_t j, double v) {
+    if (i >= n_ || j >= n_) throw std::out_of_range("index out of range");
+    if (i != j) {
+      at(i, j) = v;
+      at(j, i) = v;
+    } else {
+      at(i, n_) = v;
+      at(n_, i) = v;
+    }
+    dev_.reset();
+  }
+  void set_interaction_matrix(py::array_t<double, py::array::c_style | py::array::forcecast> m) {
+    if (m.ndim() != 2 || m.shape(0) != m.shape(1)) throw std::runtime_error("interaction.rows() != interaction.cols()");
+    if ((size_t)m.shape(0) != n_ + 1) throw std::runtime_error("invalid matrix size.");
+    auto v = m.unchecked<2>();
+    for (size_t i = 0; i < n_; ++i)
+      if (v(i, i) != 0) throw std::runtime_error("The diagonal elements of interaction matrix must be zero.");
+    if (v(n_, n_) != 1) throw std::runtime_error("The right bottom element of interaction matrix must be unity.");
+    for (size_t i = 0; i <= n_; ++i)  // selfadjointView<Upper>: the upper triangle defines the matrix
+      for (size_t j = i; j <= n_; ++j) {
+        at(i, j) = v(i, j);
+        at(j, i) = v(i, j);
+      }
+    dev_.reset();
+  }
+  py::array_t<double> get_interactions() const {
+    py::array_t<double> out({n_ + 1, n_ + 1});
+    std::copy(J_.begin(), J_.end(), out.mutable_data());
+    return out;
+  }
+  AugCSR aug() const {
+    AugCSR a;
+    a.n = n_;
+    a.indptr.push_back(0);
+    for (size_t i = 0; i <= n_; ++i) {
+      for (size_t j = 0; j <= n_; ++j) {
+        const double v = at(i, j);
+        if (v != 0.0 || i == j) {
+          a.indices.push_back((int32_t)j);
+          a.data.push_back(v);
+        }
+      }
+      a.indptr.push_back((int64_t)a.indices.size());
+    }
+    return a;
+  }
+  double energy(const std::vector<int>& s) const { return aug_energy(aug(), s); }
+  oj_graph* device() const {
+    if (!dev_) {
+      auto d = std::make_shared<DeviceGraph>();
+      check(oj_graph_create_dense(ctx(), (int32_t)n_, J_.data(), &d->h), "oj_graph_create_dense");
+      dev_ = d;
+    }
+    return dev_->h;
+  }
+  std::vector<double> J_;
+  mutable std::shared_ptr<DeviceGraph> dev_;
+};
+
+struct CSRSparse : Graph {
+  // The reference stores selfadjointView<Upper>() of the given matrix
+  // (csr_sparse.hpp:96-101): only the upper triangle (with h in column n) is read.
+  explicit CSRSparse(const py::object& mat) : Graph(0) {
+    py::object csr = mat.attr("tocsr")();
+    py::tuple shape = csr.attr("shape");
+    const size_t rows = shape[0].cast<size_t>(), cols = shape[1].cast<size_t>();
+    if (rows != cols) throw std::runtime_error("interaction.rows() != interaction.cols()");
+    if (rows == 0) throw std::runtime_error("invalid matrix size.");
+    n_ = rows - 1;
+    auto ip = py::array_t<int64_t, py::array::forcecast>(csr.attr("indptr"));
+    auto ix = py::array_t<int64_t, py::array::forcecast>(csr.attr("indices"));
+    auto dv = py::array_t<double, py::array::forcecast>(csr.attr("data"));
+    std::vector<std::vector<std::pair<int32_t, double>>> rowsv(rows);
+    auto ipu = ip.unchecked<1>();
+    auto ixu = ix.unchecked<1>();
+    auto dvu = dv.unchecked<1>();
+    for (size_t i = 0; i < rows; ++i)
+      for (int64_t p = ipu(i); p < ipu(i + 1); ++p) {
+        const size_t j = (size_t)ixu(p);
+        const double v = dvu(p);
+        if (j < i || v == 0.0) continue;
+        rowsv[i].emplace_back((int32_t)j, v);
+        if (j != i) rowsv[j].emplace_back((int32_t)i, v);
+      }
+    a_.n = n_;
+    a_.indptr.push_back(0);
+    for (size_t i = 0; i < rows; ++i) {
+      auto& r = rowsv[i];
+      std::sort(r.begin(), r.end());
+      for (size_t q = 0; q < r.size(); ++q) {
+        if (q + 1 < r.size() && r[q + 1].first == r[q].first) {
+          r[q + 1].second += r[q].second;
+          continue;
+        }
+        a_.indices.push_back(r[q].first);
+        a_.data.push_back(r[q].second);
+      }
+      a_.indptr.push_back((int64_t)a_.indices.size());
+    }
+  }
+  py::object get_interactions() const {
+    py::module_ sp = py::module_::import("scipy.sparse");
+    py::array_t<double> d(a_.data.size());
+    py::array_t<int32_t> ix(a_.indices.size());
+    py::array_t<int64_t> ip(a_.indptr.size());
+    std::copy(a_.data.begin(), a_.data.end(), d.mutable_data());
+    std::copy(a_.indices.begin(), a_.indices.end(), ix.mutable_data());
+    std::copy(a_.indptr.begin(), a_.indptr.end(), ip.mutable_data());
+    return sp.attr("csr_matrix")(py::make_tuple(d, ix, ip), "shape"_a = py::make_tuple(n_ + 1, n_ + 1));
+  }
+  double energy(const std::vector<int>& s) const { return aug_energy(a_, s); }
+  oj_graph* device() const {
+    if (!dev_) {
+      auto d = std::make_shared<DeviceGraph>();
+      check(oj_graph_create_csr(ctx(), (int32_t)n_, a_.indptr.data(), a_.indices.data(), a_.data.data(), &d->h),
+            "oj_graph_create_csr");
+      dev_ = d;
+    }
+    return dev_->h;
+  }
+  AugCSR a_;
+  mutable std::shared_ptr<DeviceGraph> dev_;
+};
+
+// ---------------------------------------------------------------------------
+// schedules (include/openjij/utility/schedule_list.hpp)
+// ---------------------------------------------------------------------------
+
+struct ClassicalParam {
+  double beta = 0;
+};
+struct TransverseParam {
+  double beta = 0, s = 0;
+};
+struct ClassicalSchedule {
+  ClassicalParam updater_parameter;
+  size_t one_mc_step = 0;
+};
+struct TransverseSchedule {
+  TransverseParam updater_parameter;
+  size_t one_mc_step = 0;
+};
+
+// schedule_list.hpp:165-181
+std::vector<ClassicalSchedule> make_classical_schedule_list(double beta_min, double beta_max, size_t one_mc_step,
+                                                            size_t num_call_updater) {
+  double r_beta = std::pow(beta_max / beta_min, 1.0 / static_cast<double>(num_call_updater - 1));
+  double beta = beta_min;
+  std::vector<ClassicalSchedule> out(num_call_updater);
+  for (auto& s : out) {
+    s.one_mc_step = one_mc_step;
+    s.updater_parameter.beta = beta;
+    beta *= r_beta;
+  }
+  return out;
+}
+
+// schedule_list.hpp:193-207
+std::vector<TransverseSchedule> make_transverse_field_schedule_list(double beta, size_t one_mc_step,
+                                                                    size_t num_call_updater) {
+  double ds = 1.0 / static_cast<double>(num_call_updater - 1);
+  double s = 0;
+  std::vector<TransverseSchedule> out(num_call_updater);
+  for (auto& e : out) {
+    e.one_mc_step = one_mc_step;
+    e.updater_parameter.beta = beta;
+    e.updater_parameter.s = s;
+    s += ds;
+  }
+  return out;
+}
+
+std::vector<ClassicalSchedule> classical_from_list(const py::list& lst) {
+  std::vector<ClassicalSchedule> out;
+  for (auto item : lst) {
+    if (py::isinstance<ClassicalSchedule>(item)) {
+      out.push_back(item.cast<ClassicalSchedule>());
+      continue;
+    }
+    auto t = item.cast<py::sequence>();
+    if (t.size() != 2) throw std::invalid_argument("schedule is list of (beta, one_mc_step)");
+    ClassicalSchedule s;
+    s.updater_parameter.beta = t[0].cast<double>();
+    s.one_mc_step = t[1].cast<size_t>();
+    out.push_back(s);
+  }
+  return out;
+}
+
+std::vector<TransverseSchedule> transverse_from_list(const py::list& lst) {
+  std::vector<TransverseSchedule> out;
+  for (auto item : lst) {
+    if (py::isinstance<TransverseSchedule>(item)) {
+      out.push_back(item.cast<TransverseSchedule>());
+      continue;
+    }
+    auto t = item.cast<py::sequence>();
+    if (t.size() != 2) throw std::invalid_argument("schedule is list of ((beta, s), one_mc_step)");
+    auto bs = t[0].cast<py::sequence>();
+    TransverseSchedule s;
+    s.updater_parameter.beta = bs[0].cast<double>();
+    s.updater_parameter.s = bs[1].cast<double>();
+    s.one_mc_step = t[1].cast<size_t>();
+    out.push_back(s);
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// systems
+// ---------------------------------------------------------------------------
+
+template <class G>
+std::shared_ptr<G> snapshot(const G& g) {
+  return std::make_shared<G>(g);
+}
+
+// Parses 1-D (one replica) or 2-D ([R][n]) +-1 spins.
+std::vector<int8_t> parse_spins(const py::handle& obj, size_t n, int* R_out) {
+  auto arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
+  if (!arr) throw std::invalid_argument("spins must be array-like");
+  int R = 1;
+  size_t len = 0;
+  if (arr.ndim() == 1) {
+    len = (size_t)arr.shape(0);
+  } else if (arr.ndim() == 2) {
+    R = (int)arr.shape(0);
+    len = (size_t)arr.shape(1);
+  } else {
+    throw std::invalid_argument("spins must be 1-D or 2-D");
+  }
+  if (len != n && len != n + 1) throw std::invalid_argument("the size of the initial spins does not match the graph");
+  std::vector<int8_t> out((size_t)R * n);
+  const double* p = arr.data();
+  for (int r = 0; r < R; ++r)
+    for (size_t i = 0; i < n; ++i) {
+      const double v = p[(size_t)r * len + i];
+      if (v != 1.0 && v != -1.0) throw std::invalid_argument("spins must be -1 or +1");
+      out[(size_t)r * n + i] = (int8_t)v;
+    }
+  *R_out = R;
+  return out;
+}
+
+template <class G>
+struct ClassicalIsing {
+  ClassicalIsing(const py::object& init, const G& g) : graph(snapshot(g)), num_spins(g.size()) { reset(init); }
+  void reset(const py::object& init) { spins = parse_spins(init, num_spins, &R); }
+  py::array_t<double> get_spin() const {
+    std::vector<ssize_t> shape = R == 1 ? std::vector<ssize_t>{(ssize_t)num_spins + 1}
+                                        : std::vector<ssize_t>{R, (ssize_t)num_spins + 1};
+    py::array_t<double> out(shape);
+    double* o = out.mutable_data();
+    for (int r = 0; r < R; ++r) {
+      for (size_t i = 0; i < num_spins; ++i) o[(size_t)r * (num_spins + 1) + i] = spins[(size_t)r * num_spins + i];
+      o[(size_t)r * (num_spins + 1) + num_spins] = 1.0;
+    }
+    return out;
+  }
+  void set_spin(const py::object& v) { reset(v); }
+  py::array_t<double> energies() const {
+    py::array_t<double> out(R);
+    if (num_spins == 0) {
+      std::fill(out.mutable_data(), out.mutable_data() + R, 0.0);
+      return out;
+    }
+    oj_graph* dg = graph->device();
+    const int8_t* sp = spins.data();
+    double* e = out.mutable_data();
+    check(oj_energy(ctx(), dg, R, sp, 0, e), "oj_energy");
+    return out;
+  }
+  std::shared_ptr<G> graph;
+  size_t num_spins;
+  int R = 1;
+  std::vector<int8_t> spins;
+};
+
+template <class G>
+struct TransverseIsing {
+  TransverseIsing(const py::object& trotter, const G& g, double gamma_) : graph(snapshot(g)), num_classical_spins(g.size()), gamma(gamma_) {
+    reset_trotter(trotter);
+  }
+  TransverseIsing(const py::object& classical, const G& g, double gamma_, size_t T_)
+      : graph(snapshot(g)), num_classical_spins(g.size()), gamma(gamma_) {
+    if (!(T_ >= 2)) throw std::invalid_argument("trotter slices must be equal or larger than 2.");
+    T = (int)T_;
+    reset_classical(classical);
+  }
+  // [T][n] (one replica) or [R][T][n]
+  void reset_trotter(const py::object& obj) {
+    auto arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
+    if (!arr) throw std::invalid_argument("trotter spins must be array-like");
+    const size_t n = num_classical_spins;
+    int Rn = 1, Tn = 0;
+    size_t len = 0;
+    if (arr.ndim() == 2) {
+      Tn = (int)arr.shape(0);
+      len = (size_t)arr.shape(1);
+    } else if (arr.ndim() == 3) {
+      Rn = (int)arr.shape(0);
+      Tn = (int)arr.shape(1);
+      len = (size_t)arr.shape(2);
+    } else {
+      throw std::invalid_argument("trotter spins must be [T][n] or [R][T][n]");
+    }
+    if (!(Tn >= 2)) throw std::invalid_argument("trotter slices must be equal or larger than 2.");
+    if (len != n && len != n + 1) throw std::invalid_argument("the size of the trotter spins does not match the graph");
+    R = Rn;
+    T = Tn;
+    spins.assign((size_t)R * T * n, 1);
+    const double* p = arr.data();
+    for (size_t idx = 0; idx < (size_t)R * T; ++idx)
+      for (size_t i = 0; i < n; ++i) {
+        const double v = p[idx * len + i];
+        if (v != 1.0 && v != -1.0) throw std::invalid_argument("spins must be -1 or +1");
+        spins[idx * n + i] = (int8_t)v;
+      }
+  }
+  void reset_classical(const py::object& obj) {
+    const size_t n = num_classical_spins;
+    int Rn = 1;
+    std::vector<int8_t> cl = parse_spins(obj, n, &Rn);
+    R = Rn;
+    spins.assign((size_t)R * T * n, 1);
+    for (int r = 0; r < R; ++r)
+      for (int t = 0; t < T; ++t)
+        std::copy(cl.begin() + (size_t)r * n, cl.begin() + (size_t)(r + 1) * n, spins.begin() + ((size_t)r * T + t) * n);
+  }
+  // 1-D: classical spins copied into every slice; 2-D: [T][n]; 3-D: [R][T][n]
+  void reset(const py::object& obj) {
+    auto arr = py::array::ensure(obj);
+    if (!arr || arr.ndim() == 1)
+      reset_classical(obj);
+    else
+      reset_trotter(obj);
+  }
+  // (n+1) x T (one replica, reference layout) or R x (n+1) x T
+  py::array_t<double> get_trotter() const {
+    const size_t n = num_classical_spins;
+    std::vector<ssize_t> shape = R == 1 ? std::vector<ssize_t>{(ssize_t)n + 1, T}
+                                        : std::vector<ssize_t>{R, (ssize_t)n + 1, T};
+    py::array_t<double> out(shape);
+    double* o = out.mutable_data();
+    for (int r = 0; r < R; ++r)
+      for (size_t i = 0; i <= n; ++i)
+        for (int t = 0; t < T; ++t)
+          o[((size_t)r * (n + 1) + i) * T + t] = i < n ? spins[((size_t)r * T + t) * n + i] : 1.0;
+    return out;
+  }
+  void set_trotter(const py::object& v) {
+    // accepts the reference layout (n+1) x T / R x (n+1) x T
+    auto arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(v);
+    if (!arr || (arr.ndim() != 2 && arr.ndim() != 3)) throw std::invalid_argument("trotter_spins must be 2-D or 3-D");
+    py::object t = arr.ndim() == 2 ? arr.attr("T") : arr.attr("transpose")(0, 2, 1);
+    reset_trotter(t);
+  }
+  py::array_t<double> energies() const {
+    const size_t n = num_classical_spins;
+    py::array_t<double> out(std::vector<ssize_t>{R, T});
+    if (n == 0) {
+      std::fill(out.mutable_data(), out.mutable_data() + (size_t)R * T, 0.0);
+      return out;
+    }
+    check(oj_energy(ctx(), graph->device(), R * T, spins.data(), 0, out.mutable_data()), "oj_energy");
+    return out;
+  }
+  std::shared_ptr<G> graph;
+  size_t num_classical_spins;
+  double gamma;
+  int R = 1, T = 0;
+  std::vector<int8_t> spins;  // [R][T][n]
+};
+
+uint64_t random_seed() {
+  std::random_device rd;
+  return ((uint64_t)rd() << 32) ^ (uint64_t)rd();
+}
+
+uint32_t kernel_flag(const std::string& k) {
+  if (k == "auto" || k.empty()) return OJ_KERNEL_AUTO;
+  if (k == "colour" || k == "color") return OJ_KERNEL_COLOUR;
+  if (k == "dense_plain") return OJ_KERNEL_DENSE_PLAIN;
+  if (k == "bitpacked") return OJ_KERNEL_BITPACKED;
+  if (k == "dense_tc") return OJ_KERNEL_DENSE_TC;
+  throw std::invalid_argument("unknown kernel " + k);
+}
+
+std::string g_kernel = "auto";
+
+// Algorithm<SingleSpinFlip>::run (algorithm.hpp:26-56) for R classical replicas.
+template <class G>
+void run_classical(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<ClassicalSchedule>& sched,
+                   const std::function<void(const ClassicalIsing<G>&, double)>& cb) {
+  g_last_run = RunInfo();
+  if (sys.num_spins == 0 || sched.empty()) {
+    if (cb)
+      for (auto& s : sched)
+        for (size_t m = 0; m < s.one_mc_step; ++m) cb(sys, s.updater_parameter.beta);
+    return;
+  }
+  oj_graph* dg = sys.graph->device();
+  const uint32_t flags = kernel_flag(g_kernel);
+  if (!cb) {
+    std::vector<double> betas;
+    std::vector<int32_t> mcs;
+    for (auto& s : sched) {
+      if (s.updater_parameter.beta < 0) throw std::invalid_argument("beta must be >= 0");
+      betas.push_back(s.updater_parameter.beta);
+      mcs.push_back((int32_t)s.one_mc_step);
+    }
+    oj_run_stats st;
+    oj_status rc;
+    {
+      py::gil_scoped_release release;
+      rc = oj_sa_run(ctx(), dg, sys.R, sys.spins.data(), betas.data(), mcs.data(), (int32_t)betas.size(), seed, 0, 0,
+                     flags, nullptr, &st);
+    }
+    check(rc, "Algorithm_SingleSpinFlip_run");
+    record(st);
+    return;
+  }
+  // with a callback: one GPU call per updater call, the global sweep index
+  // carried in first_sweep so the random stream equals the one-call run
+  int64_t sweep = 0;
+  for (auto& s : sched) {
+    for (size_t m = 0; m < s.one_mc_step; ++m) {
+      const double b = s.updater_parameter.beta;
+      const int32_t one = 1;
+      oj_run_stats st;
+      oj_status rc;
+      {
+        py::gil_scoped_release release;
+        rc = oj_sa_run(ctx(), dg, sys.R, sys.spins.data(), &b, &one, 1, seed, sweep, 0, flags, nullptr, &st);
+      }
+      check(rc, "Algorithm_SingleSpinFlip_run");
+      record(st);
+      ++sweep;
+      cb(sys, b);
+    }
+  }
+}
+
+template <class G>
+void run_transverse(TransverseIsing<G>& sys, uint64_t seed, const std::vector<TransverseSchedule>& sched,
+                    const std::function<void(const TransverseIsing<G>&, std::pair<double, double>)>& cb) {
+  g_last_run = RunInfo();
+  if (sys.num_classical_spins == 0 || sched.empty()) {
+    if (cb)
+      for (auto& s : sched)
+        for (size_t m = 0; m < s.one_mc_step; ++m) cb(sys, {s.updater_parameter.beta, s.updater_parameter.s});
+    return;
+  }
+  oj_graph* dg = sys.graph->device();
+  if (!cb) {
+    std::vector<double> betas, ss;
+    std::vector<int32_t> mcs;
+    for (auto& s : sched) {
+      betas.push_back(s.updater_parameter.beta);
+      ss.push_back(s.updater_parameter.s);
+      mcs.push_back((int32_t)s.one_mc_step);
+    }
+    oj_run_stats st;
+    oj_status rc;
+    {
+      py::gil_scoped_release release;
+      rc = oj_sqa_run(ctx(), dg, sys.R, sys.T, sys.spins.data(), sys.gamma, betas.data(), ss.data(), mcs.data(),
+                      (int32_t)betas.size(), seed, 0, 0, 0, nullptr, nullptr, &st);
+    }
+    check(rc, "Algorithm_SingleSpinFlip_run");
+    record(st);
+    return;
+  }
+  int64_t sweep = 0;
+  for (auto& s : sched) {
+    for (size_t m = 0; m < s.one_mc_step; ++m) {
+      const double b = s.updater_parameter.beta, sv = s.updater_parameter.s;
+      const int32_t one = 1;
+      oj_run_stats st;
+      oj_status rc;
+      {
+        py::gil_scoped_release release;
+        rc = oj_sqa_run(ctx(), dg, sys.R, sys.T, sys.spins.data(), sys.gamma, &b, &sv, &one, 1, seed, sweep, 0, 0,
+                        nullptr, nullptr, &st);
+      }
+      check(rc, "Algorithm_SingleSpinFlip_run");
+      record(st);
+      ++sweep;
+      cb(sys, {b, sv});
+    }
+  }
+}
+
+// get_solution (get_solution.hpp:39-49): spins times the dummy spin (always +1)
+template <class G>
+py::object solution(const ClassicalIsing<G>& sys) {
+  const size_t n = sys.num_spins;
+  if (sys.R == 1) return py::cast(std::vector<int>(sys.spins.begin(), sys.spins.end()));
+  py::list out;
+  for (int r = 0; r < sys.R; ++r)
+    out.append(std::vector<int>(sys.spins.begin() + (size_t)r * n, sys.spins.begin() + (size_t)(r + 1) * n));
+  return out;
+}
+
+// get_solution (get_solution.hpp:59-84): the first slice of minimum energy
+template <class G>
+py::object solution(const TransverseIsing<G>& sys) {
+  const size_t n = sys.num_classical_spins;
+  std::vector<double> e((size_t)sys.R * sys.T, 0.0);
+  if (n > 0) check(oj_energy(ctx(), sys.graph->device(), sys.R * sys.T, sys.spins.data(), 0, e.data()), "oj_energy");
+  py::list out;
+  for (int r = 0; r < sys.R; ++r) {
+    int best = 0;
+    double m = DBL_MAX;
+    for (int t = 0; t < sys.T; ++t)
+      if (e[(size_t)r * sys.T + t] < m) {
+        m = e[(size_t)r * sys.T + t];
+        best = t;
+      }
+    const auto b = sys.spins.begin() + ((size_t)r * sys.T + best) * n;
+    std::vector<int> v(b, b + n);
+    if (sys.R == 1) return py::cast(v);
+    out.append(v);
+  }
+  return out;
+}
+
+template <class G>
+void bind_graph_systems(py::module_& msys, py::module_& malg, py::module_& mres, const std::string& suffix) {
+  using CI = ClassicalIsing<G>;
+  using TI = TransverseIsing<G>;
+  py::class_<CI>(msys, ("ClassicalIsing" + suffix).c_str(), py::module_local())
+      .def(py::init<const py::object&, const G&>(), "init_spin"_a, "init_interaction"_a)
+      .def("reset_spins", &CI::reset, "init_spin"_a)
+      .def_property("spin", &CI::get_spin, &CI::set_spin)
+      .def_property_readonly("interaction", [](const CI& s) { return s.graph->get_interactions(); })
+      .def_readonly("num_spins", &CI::num_spins)
+      .def_readonly("num_replicas", &CI::R)
+      .def("energies", &CI::energies);
+  msys.def(
+      "make_classical_ising", [](const py::object& init, const G& g) { return CI(init, g); }, "init_spin"_a,
+      "init_interaction"_a);
+
+  py::class_<TI>(msys, ("TransverseIsing" + suffix).c_str(), py::module_local())
+      .def(py::init<const py::object&, const G&, double>(), "init_spin"_a, "init_interaction"_a, "gamma"_a)
+      .def(py::init<const py::object&, const G&, double, size_t>(), "init_classical_spins"_a, "init_interaction"_a,
+           "gamma"_a, "num_trotter_slices"_a)
+      .def("reset_spins", &TI::reset, "init_trotter_spins"_a)
+      .def_property("trotter_spins", &TI::get_trotter, &TI::set_trotter)
+      .def_property_readonly("interaction", [](const TI& s) { return s.graph->get_interactions(); })
+      .def_readonly("num_classical_spins", &TI::num_classical_spins)
+      .def_readonly("num_replicas", &TI::R)
+      .def_readonly("num_trotter_slices", &TI::T)
+      .def_readwrite("gamma", &TI::gamma)
+      .def("energies", &TI::energies);
+  msys.def(
+      "make_transverse_ising", [](const py::object& tr, const G& g, double gamma) { return TI(tr, g, gamma); },
+      "init_trotter_spins"_a, "init_interaction"_a, "gamma"_a);
+  msys.def(
+      "make_transverse_ising",
+      [](const py::object& cl, const G& g, double gamma, size_t T) { return TI(cl, g, gamma, T); },
+      "classical_spins"_a, "init_interaction"_a, "gamma"_a, "num_trotter_slices"_a);
+
+  using CCb = std::function<void(const CI&, double)>;
+  using TCb = std::function<void(const TI&, std::pair<double, double>)>;
+  const char* name = "Algorithm_SingleSpinFlip_run";
+  // classical: with seed / without seed; ScheduleList or list of tuples
+  malg.def(
+      name, [](CI& s, uint64_t seed, const py::list& sched, const CCb& cb) { run_classical(s, seed, classical_from_list(sched), cb); },
+      "system"_a, "seed"_a, "schedule_list"_a, "callback"_a = nullptr);
+  malg.def(
+      name, [](CI& s, const py::list& sched, const CCb& cb) { run_classical(s, random_seed(), classical_from_list(sched), cb); },
+      "system"_a, "schedule_list"_a, "callback"_a = nullptr);
+  malg.def(
+      name, [](TI& s, uint64_t seed, const py::list& sched, const TCb& cb) { run_transverse(s, seed, transverse_from_list(sched), cb); },
+      "system"_a, "seed"_a, "schedule_list"_a, "callback"_a = nullptr);
+  malg.def(
+      name, [](TI& s, const py::list& sched, const TCb& cb) { run_transverse(s, random_seed(), transverse_from_list(sched), cb); },
+      "system"_a, "schedule_list"_a, "callback"_a = nullptr);
+  mres.def("get_solution", [](const CI& s) { return solution(s); }, "system"_a);
+  mres.def("get_solution", [](const TI& s) { return solution(s); }, "system"_a);
+}
+
+}  // namespace
+
+PYBIND11_MODULE(_cxxjij, m) {
+  m.doc() = "openjij_b200 cxxjij: OpenJij's cxxjij API with the sweeps on the GPU";
+  py::module_ mg = m.def_submodule("graph", "graph submodule");
+  py::module_ ms = m.def_submodule("system", "system submodule");
+  py::module_ ma = m.def_submodule("algorithm", "algorithm submodule");
+  py::module_ mu = m.def_submodule("utility", "utility submodule");
+  py::module_ mr = m.def_submodule("result", "result submodule");
+
+  // ---- graph
+  py::class_<Graph, std::shared_ptr<Graph>>(mg, "Graph", py::module_local())
+      .def(py::init<size_t>(), "num_spins"_a)
+      .def("gen_spin", [](const Graph& g, size_t seed) { Xorshift e((unsigned)seed); return g.gen_spin(e); }, "seed"_a)
+      .def("gen_spin", [](const Graph& g) { Xorshift e(std::random_device{}()); return g.gen_spin(e); })
+      .def("gen_binary", [](const Graph& g, size_t seed) { Xorshift e((unsigned)seed); return g.gen_binary(e); }, "seed"_a)
+      .def("gen_binary", [](const Graph& g) { Xorshift e(std::random_device{}()); return g.gen_binary(e); })
+      .def("size", &Graph::size);
+
+  py::class_<Dense, Graph, std::shared_ptr<Dense>>(mg, "Dense", py::module_local())
+      .def(py::init<size_t>(), "num_spins"_a)
+      .def(py::init<const Dense&>(), "other"_a)
+      .def("set_interaction_matrix", &Dense::set_interaction_matrix, "interaction"_a)
+      .def("get_interactions", &Dense::get_interactions)
+      .def("calc_energy", [](const Dense& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
+      .def("energy", [](const Dense& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
+      .def("__setitem__", [](Dense& g, std::pair<size_t, size_t> k, double v) { g.set(k.first, k.second, v); }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Dense& g, std::pair<size_t, size_t> k) { return g.get(k.first, k.second); }, "key"_a)
+      .def("__setitem__", [](Dense& g, size_t k, double v) { g.set(k, k, v); }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Dense& g, size_t k) { return g.get(k, k); }, "key"_a);
+
+  py::class_<CSRSparse, Graph, std::shared_ptr<CSRSparse>>(mg, "CSRSparse", py::module_local())
+      .def(py::init<const py::object&>(), "interaction"_a)
+      .def(py::init<const CSRSparse&>(), "other"_a)
+      .def("get_interactions", &CSRSparse::get_interactions)
+      .def("calc_energy", [](const CSRSparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
+      .def("energy", [](const CSRSparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a);
+
+  // ---- utility
+  py::class_<ClassicalParam>(mu, "ClassicalUpdaterParameter", py::module_local())
+      .def(py::init<>())
+      .def(py::init([](double b) { return ClassicalParam{b}; }), "beta"_a)
+      .def_readwrite("beta", &ClassicalParam::beta)
+      .def("__repr__", [](const ClassicalParam& p) { return "(beta: " + std::to_string(p.beta) + ")"; });
+  py::class_<TransverseParam>(mu, "TransverseFieldUpdaterParameter", py::module_local())
+      .def(py::init<>())
+      .def(py::init([](double b, double s) { return TransverseParam{b, s}; }), "beta"_a, "s"_a)
+      .def(py::init([](std::pair<double, double> t) { return TransverseParam{t.first, t.second}; }), "obj"_a)
+      .def_readwrite("beta", &TransverseParam::beta)
+      .def_readwrite("s", &TransverseParam::s)
+      .def("__repr__", [](const TransverseParam& p) {
+        return "(beta: " + std::to_string(p.beta) + ", s: " + std::to_string(p.s) + ")";
+      });
+  py::class_<ClassicalSchedule>(mu, "ClassicalSchedule", py::module_local())
+      .def(py::init<>())
+      .def(py::init([](std::pair<ClassicalParam, size_t> o) { return ClassicalSchedule{o.first, o.second}; }), "obj"_a)
+      .def_readwrite("one_mc_step", &ClassicalSchedule::one_mc_step)
+      .def_readwrite("updater_parameter", &ClassicalSchedule::updater_parameter)
+      .def("__repr__", [](const ClassicalSchedule& s) {
+        return "((beta: " + std::to_string(s.updater_parameter.beta) + ") mcs: " + std::to_string(s.one_mc_step) + ")";
+      });
+  py::class_<TransverseSchedule>(mu, "TransverseFieldSchedule", py::module_local())
+      .def(py::init<>())
+      .def(py::init([](std::pair<TransverseParam, size_t> o) { return TransverseSchedule{o.first, o.second}; }), "obj"_a)
+      .def_readwrite("one_mc_step", &TransverseSchedule::one_mc_step)
+      .def_readwrite("updater_parameter", &TransverseSchedule::updater_parameter)
+      .def("__repr__", [](const TransverseSchedule& s) {
+        return "((beta: " + std::to_string(s.updater_parameter.beta) + ", s: " + std::to_string(s.updater_parameter.s) +
+               ") mcs: " + std::to_string(s.one_mc_step) + ")";
+      });
+  mu.def("make_classical_schedule_list", &make_classical_schedule_list, "beta_min"_a, "beta_max"_a, "one_mc_step"_a,
+         "num_call_updater"_a);
+  mu.def("make_transverse_field_schedule_list", &make_transverse_field_schedule_list, "beta"_a, "one_mc_step"_a,
+         "num_call_updater"_a);
+  mu.def(
+      "make_schedule_list",
+      [](const std::vector<std::pair<double, size_t>>& tl) {
+        std::vector<ClassicalSchedule> out;
+        for (auto& e : tl) out.push_back(ClassicalSchedule{ClassicalParam{e.first}, e.second});
+        return out;
+      },
+      "tuplelist"_a);
+  mu.def(
+      "make_schedule_list",
+      [](const std::vector<std::pair<std::pair<double, double>, size_t>>& tl) {
+        std::vector<TransverseSchedule> out;
+        for (auto& e : tl) out.push_back(TransverseSchedule{TransverseParam{e.first.first, e.first.second}, e.second});
+        return out;
+      },
+      "tuplelist"_a);
+
+  // ---- systems, algorithm, result
+  bind_graph_systems<Dense>(ms, ma, mr, "_Dense");
+  bind_graph_systems<CSRSparse>(ms, ma, mr, "_CSRSparse");
+
+  // ---- runtime controls (no reference counterpart)
+  m.def(
+      "set_device",
+      [](int dev) {
+        std::lock_guard<std::mutex> lk(g_ctx_mu);
+        if (g_ctx) {
+          oj_ctx_destroy(g_ctx);
+          g_ctx = nullptr;
+        }
+        g_device = dev;
+      },
+      "device"_a);
+  m.def("set_kernel", [](const std::string& k) {
+    kernel_flag(k);
+    g_kernel = k;
+  }, "kernel"_a);
+  m.def("last_run_info", []() {
+    py::dict d;
+    d["kernel"] = g_last_run.kernel;
+    d["launches"] = g_last_run.launches;
+    d["sweeps"] = g_last_run.sweeps;
+    d["attempts"] = g_last_run.attempts;
+    d["anneal_ms"] = g_last_run.anneal_ms;
+    d["total_ms"] = g_last_run.total_ms;
+    return d;
+  });
+  m.def("version", []() { return std::string(oj_version()); });
+}

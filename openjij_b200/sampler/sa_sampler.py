@@ -1,0 +1,191 @@
+"""Simulated annealing sampler (reference: openjij/sampler/sa_sampler.py:42-329).
+
+Same parameters, defaults and schedule construction as the reference's
+``SASampler``; the reads anneal together on the GPU.  Differences, by design:
+
+* reads are replicas with their own counter-based random streams, so with a
+  ``seed`` the reads start from the same initial state (as in the reference,
+  sa_sampler.py:253-258) but no longer repeat each other;
+* ``updater`` accepts "single spin flip" only (Swendsen-Wang is not part of
+  this library).
+"""
+from __future__ import annotations
+
+from typing import Optional, Union
+
+import numpy as np
+
+import openjij_b200.cxxjij as cxxjij
+from openjij_b200.model.model import BinaryQuadraticModel
+from openjij_b200.sampler.sampler import BaseSampler, _as_bqm, spins_from_initial_state
+
+
+class SASampler(BaseSampler):
+    """Sampler with simulated annealing (single spin flip Metropolis)."""
+
+    @property
+    def parameters(self):
+        return {"beta_min": ["parameters"], "beta_max": ["parameters"]}
+
+    def __init__(self):
+        self._default_params = {
+            "beta_min": None,
+            "beta_max": None,
+            "num_sweeps": 1000,
+            "schedule": None,
+            "num_reads": 1,
+        }
+        self._params = self._default_params.copy()
+        self._make_system = {"singlespinflip": cxxjij.system.make_classical_ising}
+        self._algorithm = {"singlespinflip": cxxjij.algorithm.Algorithm_SingleSpinFlip_run}
+        self.schedule_info = {}
+
+    def _convert_validation_schedule(self, schedule):
+        """(sa_sampler.py:109-135) list of (beta, one_mc_step) -> ClassicalSchedule list."""
+        if not isinstance(schedule, (list, np.ndarray)):
+            raise ValueError("schedule should be list or numpy.array")
+        if isinstance(schedule[0], cxxjij.utility.ClassicalSchedule):
+            return list(schedule)
+        if len(schedule[0]) != 2:
+            raise ValueError("schedule is list of tuple or list (beta : float, step_length : int)")
+        beta = np.array(schedule).T[0]
+        if not np.all(0 <= beta):
+            raise ValueError("schedule beta range is '0 <= beta'.")
+        out = []
+        for b, step in schedule:
+            s = cxxjij.utility.ClassicalSchedule()
+            s.one_mc_step = int(step)
+            s.updater_parameter.beta = float(b)
+            out.append(s)
+        return out
+
+    def sample(
+        self,
+        bqm: Union[BinaryQuadraticModel, object],
+        beta_min: Optional[float] = None,
+        beta_max: Optional[float] = None,
+        num_sweeps: Optional[int] = None,
+        num_reads: Optional[int] = None,
+        schedule: Optional[list] = None,
+        initial_state: Optional[Union[list, dict]] = None,
+        updater: Optional[str] = None,
+        sparse: Optional[bool] = None,
+        reinitialize_state: Optional[bool] = None,
+        seed: Optional[int] = None,
+    ):
+        if updater is None:
+            updater = "single spin flip"
+        if sparse is None:
+            sparse = True
+        if reinitialize_state is None:
+            reinitialize_state = True
+        name = updater.lower().replace("_", "").replace(" ", "")
+        if name not in self._make_system:
+            raise ValueError('updater is one of "single spin flip"')
+        model = _as_bqm(bqm, bool(sparse))
+        ising_graph, offset = model.get_cxxjij_ising_graph()
+        self._set_params(beta_min=beta_min, beta_max=beta_max, num_sweeps=num_sweeps,
+                         num_reads=num_reads, schedule=schedule)
+        if self._params["schedule"] is None:
+            self._params["schedule"], beta_range = geometric_ising_beta_schedule(
+                cxxgraph=ising_graph, beta_max=self._params["beta_max"],
+                beta_min=self._params["beta_min"], num_sweeps=self._params["num_sweeps"], seed=seed)
+            self.schedule_info = {"beta_max": beta_range[0], "beta_min": beta_range[1],
+                                  "num_sweeps": self._params["num_sweeps"]}
+        else:
+            self._params["schedule"] = self._convert_validation_schedule(self._params["schedule"])
+            self.schedule_info = {"schedule": "custom schedule"}
+
+        n = ising_graph.size()
+        if initial_state is None:
+            def init_generator(R):
+                if seed is not None:  # every read starts from gen_spin(seed) (sa_sampler.py:253-258)
+                    return np.tile(np.asarray(ising_graph.gen_spin(int(seed)), np.int8), (R, 1))
+                rng = np.random.default_rng()
+                return rng.choice(np.array([-1, 1], np.int8), size=(R, n))
+        else:
+            s0 = spins_from_initial_state(initial_state, model, n)
+
+            def init_generator(R):
+                return np.tile(s0, (R, 1))
+
+        algorithm = self._algorithm[name]
+        system = self._make_system[name](init_generator(1), ising_graph) if n > 0 else None
+        response = self._cxxjij_sampling(model, init_generator, algorithm, system, reinitialize_state,
+                                         seed, offset)
+        response.info["schedule"] = self.schedule_info
+        return response
+
+
+def geometric_ising_beta_schedule(cxxgraph, beta_max=None, beta_min=None, num_sweeps=1000, seed=None):
+    """Geometric beta schedule (reference: sa_sampler.py:853-976).
+
+    With both ends given the schedule is make_classical_schedule_list(beta_min,
+    beta_max, m, num_sweeps // m), m = max(1, num_sweeps // 1000).  A missing
+    end is estimated from the energy changes of random spin configurations,
+    by the reference's procedure (median / minimum positive dE, bisection for
+    beta_min, the 1/1000 final acceptance target for beta_max).
+    """
+    if seed is not None:
+        np.random.seed(seed)
+    THRESHOLD = 1e-8
+    dE_max, dE_min, rate_dE = 1.0, 1.0, 0.5
+    J = cxxgraph.get_interactions()
+    dense = isinstance(J, np.ndarray)
+    if beta_min is None or beta_max is None:
+        if J.shape[0] <= 1:
+            dE_max = dE_min = 1.0
+        else:
+            spins = np.random.choice([-1, 1], size=(J.shape[0], 2))
+            spins[-1, :] = 1
+            quad = J[:-1, :-1] @ spins[:-1, :] * (-2 * spins[:-1, :])
+            hcol = J[:-1, -1][:, np.newaxis] if dense else J[:-1, -1].toarray()
+            lin = hcol * spins[:-1]
+            quad_abs = np.abs(quad)
+            if np.any(quad_abs > THRESHOLD):
+                rate_dE = np.max(np.abs(lin[quad_abs > THRESHOLD]) /
+                                 (quad_abs[quad_abs > THRESHOLD].mean() + THRESHOLD))
+            positive = quad[quad > THRESHOLD]
+            if len(positive) == 0:
+                dE_min, dE_max = 1.0, 1.1
+            else:
+                dE_max = np.median(positive, axis=0).mean()
+                dE_min = np.min(positive, axis=0).mean()
+    n = J.shape[0]
+    prob_init = 9 / 10 - 8 / 10 * np.tanh(rate_dE / 50) + THRESHOLD
+    prob_final = 1 / 1000
+    if beta_min is None:
+        lo, hi = -np.log(prob_init) / dE_max, -np.log(prob_init) / dE_min
+        for _ in range(5):
+            b = (lo + hi) / 2
+            f = 2 * b * prob_init - np.exp(-b * dE_min) + np.exp(-b * dE_max)
+            if abs(f) < 1e-8:
+                break
+            if f > 0:
+                hi = b
+            else:
+                lo = b
+        beta_min = lo
+        floor = beta_min * 0.8
+        beta_min = floor + (beta_min * 1.5 - floor) * np.tanh(num_sweeps / n)
+    if beta_max is None:
+        absJ = np.abs(J) if dense else abs(J).toarray()
+        int_min = max(np.min(absJ[absJ > THRESHOLD]), dE_min / 10.0)
+        b_int = -np.log(prob_final) / int_min
+        b_dE = -np.log(prob_final) / dE_min
+        if rate_dE < 2:
+            lo, hi = min(b_dE, b_int), max(b_dE, b_int)
+            beta_max = lo + (hi - lo) * np.tanh(num_sweeps / (2 * n))
+        else:
+            last = min(100, num_sweeps // 10 + 1)
+            beta_max = -np.log(prob_final) / max(dE_min, int_min) / last
+        if beta_max < beta_min:
+            beta_max = beta_min * 10.0
+    if rate_dE > 1:
+        beta_min *= rate_dE
+        beta_max *= rate_dE
+    per_beta = max(1, num_sweeps // 1000)
+    schedule = cxxjij.utility.make_classical_schedule_list(
+        beta_min=float(beta_min), beta_max=float(beta_max), one_mc_step=per_beta,
+        num_call_updater=num_sweeps // per_beta)
+    return schedule, [beta_max, beta_min]
