@@ -50,6 +50,15 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def _traffic_from_profiles():
     """DRAM bytes per launch of the annealing kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "sa_bitpacked_traffic.json")
@@ -125,11 +134,40 @@ def _dist():
     return ws, rank, local
 
 
-def _instance(sweeps=None):
+def _workload(config, sweeps=None, replicas=None):
+    """The seeded workloads of the five benchmark configurations.  Config 2 is
+    the default bench line; the others are measured with --config."""
     from openjij_b200 import instances as I
-    m, _ = I.lattice_pm_j(L_SIDE, seed=SEED_INSTANCE)
-    betas, mcs = I.geometric_betas(BETA_MIN, BETA_MAX, sweeps or NUM_SWEEPS)
-    return m, betas, mcs
+    w = {"config": config, "kind": "sa", "T": 1}
+    if config == 1:
+        m, _ = I.dense_ising_uniform(100, seed=1)
+        S, R, bmin, bmax = 1000, 100, 0.1, 10.0
+        w.update(name="dense_ising_N100_R100_S1000", kernel="auto", bound="tensor")
+    elif config == 2:
+        m, _ = I.lattice_pm_j(L_SIDE, seed=SEED_INSTANCE)
+        S, R, bmin, bmax = NUM_SWEEPS, REPLICAS, BETA_MIN, BETA_MAX
+        w.update(name=WORKLOAD, kernel="auto", bound="hbm")
+    elif config == 3:
+        m, _ = I.dense_qubo_int(2048, seed=3)
+        S, R, bmin, bmax = 1000, 4096, 0.05, 5.0
+        w.update(name="dense_qubo_int_N2048_R4096_S1000", kernel="auto", bound="tensor")
+    elif config == 4:
+        m, _ = I.random_regular_pm_j(4096, 3, seed=4)
+        S, R = 1000, 256
+        w.update(name="sqa_3regular_N4096_T32_R256_S1000", kind="sqa", T=32, kernel="auto", bound="hbm",
+                 gamma=1.0, beta=10.0)
+    else:
+        raise SystemExit(f"unknown config {config}")
+    S = sweeps or S
+    R = replicas or R
+    w.update(matrix=m, replicas=R, sweeps=S)
+    if w["kind"] == "sa":
+        w["betas"], w["mcs"] = I.geometric_betas(bmin, bmax, S)
+    else:
+        w["betas"] = np.full(S, w["beta"])
+        w["s"] = np.linspace(0.0, 1.0, S)  # Gamma(1-s): 1 -> 0
+        w["mcs"] = np.ones(S, np.int32)
+    return w
 
 
 def cpu_reference(m, betas, mcs, reads, threads):
@@ -147,34 +185,65 @@ def cpu_reference(m, betas, mcs, reads, threads):
     return attempts / dt, dt
 
 
+def cpu_reference_sqa(w, threads):
+    """OpenJij's CPU SQA path (oracle restatement): one read per thread on a
+    bounded number of sweeps (at most 100) of the workload's schedule."""
+    from oracle import oracle as O
+    g = O.AugCSR(w["matrix"])
+    k = min(len(w["betas"]), 100)
+    rng = np.random.default_rng(0)
+    init = rng.choice(np.array([-1, 1], np.int8), size=(threads, w["T"], g.n))
+    seeds = np.arange(1, threads + 1, dtype=np.uint64)
+    t0 = time.perf_counter()
+    O.ref_sqa_many(g, init, w["gamma"], w["betas"][:k], w["s"][:k], w["mcs"][:k], seeds, threads=threads)
+    dt = time.perf_counter() - t0
+    return threads * w["T"] * g.n * float(np.sum(w["mcs"][:k])) / dt, dt
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    m, betas, mcs = _instance()
+    w = _workload(args.config, args.sweeps, args.replicas)
     threads = os.cpu_count() or 1
-    reads = threads  # one read per host thread, the full 2000-sweep schedule
+    reads = threads  # one read per host thread
+
+    def one():
+        if w["kind"] == "sa":
+            return cpu_reference(w["matrix"], w["betas"], w["mcs"], reads, threads)
+        return cpu_reference_sqa(w, threads)
+
     for _ in range(args.warmup):
-        cpu_reference(m, betas, mcs, min(reads, threads), threads)
+        one()
     vals, times = [], []
     for _ in range(args.steps):
-        v, dt = cpu_reference(m, betas, mcs, reads, threads)
+        v, dt = one()
         vals.append(v)
         times.append(dt)
     value = float(np.mean(vals))
-    sample = f"{reads} reads x {NUM_SWEEPS} sweeps of the L=128 lattice per step"
+    sweeps = int(np.sum(w["mcs"])) if w["kind"] == "sa" else min(int(np.sum(w["mcs"])), 100)
+    sample = f"{reads} reads x {sweeps} sweeps of {w['name']} per step, one read per host thread"
     line = {
         "impl": "reference", "metric": "spin-flip attempts/s", "value": value,
         "unit": "attempts/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_reads_per_step": reads, "host_threads": threads},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded instance)",
+        "config": {"workload": w["name"], "sample_reads_per_step": reads, "host_threads": threads},
         "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _algo_per_attempt(w, n):
+    """Algorithmic bytes (hbm-bound kernels) or flops (dense kernels) per attempt."""
+    if w["config"] == 2:
+        return ALGO_BYTES_PER_ATTEMPT, "GB/s"
+    if w["kind"] == "sqa":
+        return 7.0 / 8.0 if w.get("bitpacked") else 7.0, "GB/s"  # 3 spatial + 2 Trotter + read + write
+    return 2.0 * n, "TFLOP/s"  # one field-row update of 2n flop per attempt
 
 
 def run_ours(args):
@@ -188,31 +257,42 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from openjij_b200 import _native as N
     from oracle import oracle as O  # CPU baseline only
-    m, betas, mcs = _instance(args.sweeps)
-    g_or = O.AugCSR(m)
+    w = _workload(args.config, args.sweeps, args.replicas)
+    kernel = args.kernel or w["kernel"]
+    g_or = O.AugCSR(w["matrix"])
     n = g_or.n
-    R = args.replicas or REPLICAS
+    R, T = w["replicas"], w["T"]
+    betas, mcs = w["betas"], w["mcs"]
     stream = torch.cuda.current_stream()
     ctx = N.Context(local)
     ctx.set_stream(stream.cuda_stream)
     graph = N.Graph(ctx, n, g_or.indptr, g_or.indices, g_or.data)
     rng = np.random.default_rng(1000 + rank)
-    init_host = rng.choice(np.array([-1, 1], np.int8), size=(R, n))
+    shape = (R, n) if w["kind"] == "sa" else (R, T, n)
+    init_host = rng.choice(np.array([-1, 1], np.int8), size=shape)
     init_dev = torch.from_numpy(init_host).cuda()
     work = torch.empty_like(init_dev)
-    energies = torch.empty(R, dtype=torch.float64, device="cuda")
+    energies = torch.empty(R * T, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    attempts_per_step = float(R) * n * float(np.sum(mcs))
+    attempts_per_step = float(R) * T * n * float(np.sum(mcs))
     seed0 = 12345 + 1000003 * rank
+    rep0 = 0  # every rank runs its own full workload (weak scaling)
 
-    def step(k, timed_events=None):
+    def run(spins, seed, device, en):
+        if w["kind"] == "sa":
+            return N.sa_run(graph, spins, betas, mcs, seed=seed, energies=en, device=device, kernel=kernel,
+                            replica_offset=rep0)
+        return N.sqa_run(graph, spins, w["gamma"], betas, w["s"], mcs, seed=seed, energies=en,
+                         device=device, kernel=kernel, replica_offset=rep0)
+
+    def step(k):
         work.copy_(init_dev)
-        st = N.sa_run(graph, work, betas, mcs, seed=seed0 + k, energies=energies, device=True)
-        return st
+        return run(work, seed0 + k, True, energies)
 
     for k in range(args.warmup):
         flush.zero_()
-        step(k)
+        st = step(k)
+    used_kernel = st["kernel"] if args.warmup else kernel
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -222,14 +302,15 @@ def run_ours(args):
     kern_ms, launches = [], 0
     with ClockSampler(local) as clk:
         for k in range(args.steps):
-            flush.zero_()  # L2 flush between timed steps (state fits in L2)
+            flush.zero_()  # L2 flush between timed steps (the state fits in L2)
             starts[k].record(stream)
             st = step(args.warmup + k)
             ends[k].record(stream)
             kern_ms.append(st["anneal_ms"])
+            used_kernel = st["kernel"]
             launches += st["launches"] + 1  # + the device-to-device copy of the initial spins
         torch.cuda.synchronize()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     ms = float(np.mean(step_ms))
     kms = float(np.mean(kern_ms))
     if dist:
@@ -238,16 +319,16 @@ def run_ours(args):
         ms, kms = float(t[0]), float(t[1])
     value = attempts_per_step * ws / (ms / 1000.0)
 
-    # e2e: the same call with pinned host buffers (H2D spins in, D2H spins + energies out)
-    host_spins = torch.empty((R, n), dtype=torch.int8).pin_memory()
-    host_e = torch.empty(R, dtype=torch.float64).pin_memory()
+    # e2e: the same C-ABI call with pinned host buffers (spins in; spins + energies out)
+    host_spins = torch.empty(shape, dtype=torch.int8).pin_memory()
+    host_e = torch.empty(R * T, dtype=torch.float64).pin_memory()
     e2e_ms = []
     for k in range(max(1, min(args.steps, 5))):
         host_spins.numpy()[...] = init_host
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        N.sa_run(graph, host_spins.numpy(), betas, mcs, seed=seed0 + k, energies=host_e.numpy())
+        run(host_spins.numpy(), seed0 + k, False, host_e.numpy())
         e2e_ms.append(1000.0 * (time.perf_counter() - t0))
     e2 = float(np.mean(e2e_ms))
     if dist:
@@ -256,33 +337,45 @@ def run_ours(args):
         e2 = float(t[0])
     e2e_value = attempts_per_step * ws / (e2 / 1000.0)
 
-    peak, peak_kind = _peaks()
-    achieved = attempts_per_step * ALGO_BYTES_PER_ATTEMPT / (kms / 1000.0) / 1e9
+    hbm_peak, peak_kind = _peaks()
+    per, unit = _algo_per_attempt(w, n)
+    if unit == "GB/s":
+        achieved = attempts_per_step * per / (kms / 1000.0) / 1e9
+        peak = hbm_peak
+    else:
+        achieved = attempts_per_step * per / (kms / 1000.0) / 1e12
+        peak, peak_kind = _tensor_peak()
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu and w["kind"] == "sa":
         threads = os.cpu_count() or 1
-        v, dt = cpu_reference(m, betas, mcs, threads, threads)
+        v, dt = cpu_reference(w["matrix"], betas, mcs, threads, threads)
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
-               "sample": f"{threads} reads x {NUM_SWEEPS} sweeps of the same lattice, one read per "
-                         f"thread, {dt:.1f} s"}
+               "sample": f"{threads} reads x {int(np.sum(mcs))} sweeps of the same instance, one read "
+                         f"per host thread, {dt:.1f} s"}
+    elif rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, dt = cpu_reference_sqa(w, threads)
+        cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
+               "sample": f"{threads} reads x {T} slices x {min(int(np.sum(mcs)), 100)} sweeps, one read per "
+                         f"host thread, {dt:.1f} s"}
     if rank == 0:
         line = {
             "metric": "spin-flip attempts/s", "value": value, "unit": "attempts/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic (seeded +-J lattice)",
-            "config": {"workload": WORKLOAD, "L": L_SIDE, "spins": n, "replicas": R,
-                       "num_sweeps": NUM_SWEEPS, "beta": [BETA_MIN, BETA_MAX],
-                       "kernel": "bitpacked", "l2": "flushed between steps (256 MB write)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32" if used_kernel == "bitpacked" else "f32",
+            "data": "synthetic (seeded instance)",
+            "config": {"workload": w["name"], "spins": n, "replicas": R, "trotter": T,
+                       "num_sweeps": int(np.sum(mcs)), "kernel": used_kernel,
+                       "l2": "flushed between steps (256 MB write)",
                        "attempts_per_step": attempts_per_step},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": _traffic_from_profiles(),
-                         "peak_kind": peak_kind, "kernel": "sa_msc_kernel<4>",
-                         "kernel_ms": kms,
-                         "algorithmic_bytes_per_attempt": ALGO_BYTES_PER_ATTEMPT},
+            "roofline": {"bound": w["bound"], "achieved": achieved, "peak": peak, "unit": unit,
+                         "frac": achieved / peak,
+                         "traffic": _traffic_from_profiles() if args.config == 2 else None,
+                         "peak_kind": peak_kind, "kernel_ms": kms,
+                         "algorithmic_per_attempt": per},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(R * n),
-                    "d2h_bytes_per_step": int(R * n + 8 * R), "ms_per_step": e2},
+            "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(R * T * n),
+                    "d2h_bytes_per_step": int(R * T * n + 8 * R * T), "ms_per_step": e2},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
@@ -305,6 +398,10 @@ def main():
     ap.add_argument("--sweeps", type=int, default=None,
                     help="smaller case for profiling (default: the full 2000-sweep workload)")
     ap.add_argument("--replicas", type=int, default=None, help="smaller case for profiling")
+    ap.add_argument("--config", type=int, default=2,
+                    help="benchmark configuration 1-4 (default 2: the L=128 +-J lattice)")
+    ap.add_argument("--kernel", default=None,
+                    help="force a kernel: colour, dense_plain, bitpacked, dense_tc (default: planner)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
