@@ -129,6 +129,25 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32
                      int64_t replica_offset, uint32_t flags, double* energies,
                      int32_t* best_slice, oj_run_stats* stats);
 
+/* Allocation-free variant of oj_sa_run's bit-packed path, for callers that
+ * cannot call cudaMalloc while they run (device memory already reserved by
+ * another framework's allocator, or code that cannot accept cudaMalloc's
+ * implicit device synchronisation).  No counterpart in the reference.
+ * Runs the same kernel and random stream as oj_sa_run with OJ_KERNEL_BITPACKED,
+ * so results are identical for the same arguments.  All per-call scratch lives
+ * in one fixed 16 MiB device array inside the library (held by every GPU that
+ * loads it until exit): words (ceil(R/32) * n * 4 B) plus thresholds
+ * (sweeps * (degree+1) * 4 B) plus sweeps * 4 B must fit, else OJ_ERR_ARG.
+ * spins: DEVICE pointer [R][n], in/out.  The graph must be regular with
+ * couplings +-c, h = 0, and must have run oj_sa_run once (which builds its
+ * site partition), else OJ_ERR_UNSUPPORTED.  The call is asynchronous on the
+ * context's stream.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture; calls overlapping on one GPU
+ * share the array and race. */
+oj_status oj_sa_run_bitpacked_noalloc(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
+                                      const double* betas, const int32_t* mcs, int32_t num_sched,
+                                      uint64_t seed, int64_t first_sweep, int64_t replica_offset);
+
 /* FP64 energies of R spin vectors [R][n].  Replaces Dense::energy /
  * CSRSparse::energy (dense.hpp:176-192, csr_sparse.hpp:139-155). */
 oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, const int8_t* spins,

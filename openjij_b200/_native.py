@@ -33,6 +33,7 @@ EXPORTS = [
     "oj_version", "oj_status_string", "oj_ctx_create", "oj_ctx_destroy", "oj_ctx_set_stream",
     "oj_ctx_synchronize", "oj_ctx_last_error", "oj_graph_create_dense", "oj_graph_create_csr",
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
+    "oj_sa_run_bitpacked_noalloc",
 ]
 
 
@@ -87,6 +88,7 @@ def lib():
         L.oj_sqa_run.argtypes = [vp, vp, i32, i32, vp, dbl, vp, vp, vp, i32, u64, i64, i64, u32, vp, vp,
                                  C.POINTER(RunStats)]
         L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
+        L.oj_sa_run_bitpacked_noalloc.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64]
         for name in EXPORTS:
             if name not in ("oj_version", "oj_status_string", "oj_ctx_last_error"):
                 getattr(L, name).restype = i32
@@ -214,6 +216,16 @@ def sqa_run(g: Graph, spins, gamma, betas, s, mcs, seed, energies=None, best=Non
                                  _ptr(energies), _ptr(best), C.byref(st)),
                 "oj_sqa_run")
     return st.as_dict()
+
+
+def sa_run_bitpacked_noalloc(g: Graph, spins_dev, betas, mcs, seed, first_sweep=0, replica_offset=0):
+    """The allocation-free bit-packed run; spins_dev is a device tensor [R][n]."""
+    b = np.ascontiguousarray(betas, np.float64)
+    m = np.ascontiguousarray(mcs, np.int32)
+    g.ctx.check(lib().oj_sa_run_bitpacked_noalloc(g.ctx._h, g._h, int(spins_dev.shape[0]), _ptr(spins_dev),
+                                                  _ptr(b), _ptr(m), len(b), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                                  int(first_sweep), int(replica_offset)),
+                "oj_sa_run_bitpacked_noalloc")
 
 
 def energy(g: Graph, spins, out=None, device=False):
