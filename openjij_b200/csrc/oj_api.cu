@@ -304,8 +304,12 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     return OJ_ERR_UNSUPPORTED;
   }
   if (kernel == OJ_KERNEL_DENSE_TC) {
-    ctx->last_error = "tensor-core dense kernel not available in this build";
-    return OJ_ERR_UNSUPPORTED;
+    std::string why;
+    cudaError_t pe = dense_tc_prepare(g, &why);
+    if (pe != cudaSuccess) {
+      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
+      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+    }
   }
   cudaStream_t st = ctx->stream;
   const size_t spin_bytes = (size_t)R * n;
@@ -355,7 +359,10 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     if (kernel == OJ_KERNEL_DENSE_PLAIN) OJ_CK(ensure_dense(g), "dense J upload");
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0) {
-      if (kernel == OJ_KERNEL_DENSE_PLAIN)
+      if (kernel == OJ_KERNEL_DENSE_TC) {
+        OJ_CK(cudaMemsetAsync(g->tc->status.ptr, 0, sizeof(int), st), "status reset");
+        OJ_CK(launch_sa_dense_tc(g, R, d_spins, d_beta, S, rb, 16, st, &launches), "sa dense tensor-core kernel");
+      } else if (kernel == OJ_KERNEL_DENSE_PLAIN)
         OJ_CK(launch_sa_dense_plain(g, R, d_spins, d_beta, S, rb, st, &launches), "sa dense kernel");
       else
         OJ_CK(launch_sa_colour(g, R, d_spins, d_beta, S, rb, st, &launches), "sa colour kernel");
@@ -374,7 +381,15 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   }
   if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
   OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
-  if (!devp || stats) OJ_CK(cudaStreamSynchronize(st), "run");
+  if (!devp || stats || kernel == OJ_KERNEL_DENSE_TC) OJ_CK(cudaStreamSynchronize(st), "run");
+  if (kernel == OJ_KERNEL_DENSE_TC && S > 0) {
+    int flag = 0;
+    OJ_CK(cudaMemcpy(&flag, g->tc->status.ptr, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+    if (flag) {
+      ctx->last_error = "tensor-core dense kernel: a bounded device wait timed out";
+      return OJ_ERR_TIMEOUT;
+    }
+  }
   if (stats) {
     stats->kernel = (int32_t)(kernel >> OJ_KERNEL_SHIFT);
     stats->launches = launches;

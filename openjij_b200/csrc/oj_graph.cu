@@ -30,6 +30,13 @@ oj_graph::~oj_graph() {
   d_coff.release();
   d_dense.release();
   if (msc) msc->tables.release();
+  if (tc) {
+    tc->bt_hi.release();
+    tc->bt_lo.release();
+    tc->jblk.release();
+    tc->h.release();
+    tc->status.release();
+  }
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
 }
 

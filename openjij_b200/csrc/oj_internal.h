@@ -62,6 +62,15 @@ struct MscPlan {
   uint16_t* jm = nullptr;    // [P][nlocmax] bit l set when J(site, nbr l) > 0
 };
 
+// Tiled couplings of the tensor-core dense kernel: J in BF16 (and the BF16
+// remainder J - bf16(J) for non-exact couplings) as the MMA B tiles of every
+// (32-spin block, CTA column range), FP32 32x32 in-block tiles and padded h.
+struct TcPlan {
+  int P = 0, ncta = 0, bpc = 0, nblk = 0;
+  bool exact = true;
+  DevBuf bt_hi, bt_lo, jblk, h, status;
+};
+
 }  // namespace oj
 
 struct oj_graph {
@@ -84,6 +93,7 @@ struct oj_graph {
   oj::DevBuf d_rp, d_ci, d_val, d_h, d_val64, d_h64, d_order, d_coff;
   oj::DevBuf d_dense;  // FP32 dense J (n x n), created on first use
   std::unique_ptr<oj::MscPlan> msc;
+  std::unique_ptr<oj::TcPlan> tc;
   ~oj_graph();
 };
 
@@ -119,6 +129,9 @@ cudaError_t launch_sa_dense_plain(const oj_graph* g, int R, int8_t* spins, const
 cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
                           const uint32_t* always, int64_t nsweeps, RngBase rb, cudaStream_t st,
                           int* launches);
+cudaError_t launch_sa_dense_tc(const oj_graph* g, int R, int8_t* spins, const float* betas, int64_t nsweeps,
+                               RngBase rb, int recompute, cudaStream_t st, int* launches);
+cudaError_t dense_tc_prepare(oj_graph* g, std::string* why);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,

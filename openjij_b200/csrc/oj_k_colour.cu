@@ -156,29 +156,60 @@ __global__ void __launch_bounds__(kSqaThreads)
   }
 }
 
-// FP64 energy of one spin vector per CTA:
-// E = sum_i s_i (h_i + 1/2 sum_j J_ij s_j)  (= dense.hpp:176-192).
+// FP64 energies of 32 spin vectors per CTA:
+// E = sum_{i<j} J_ij s_i s_j + sum_i h_i s_i  (= dense.hpp:176-192).
+// The 32 vectors' spins at a site are packed into one word (bit r set iff
+// s = -1), so every coupling is read once for 32 vectors and s_i s_j is the
+// xor of two words.  Partial sums are combined in a fixed order, so the result
+// does not depend on timing.
 constexpr int kEnergyThreads = 256;
 __global__ void __launch_bounds__(kEnergyThreads)
     energy_kernel(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                  const double* __restrict__ val, const double* __restrict__ h, int n,
+                  const double* __restrict__ val, const double* __restrict__ h, int n, int count,
                   const int8_t* __restrict__ spins, double* __restrict__ out) {
-  const int8_t* s = spins + (size_t)blockIdx.x * n;
-  double acc = 0.0;
+  extern __shared__ uint32_t wsh[];  // [n] words, then [8][32] partial sums
+  const int v0 = blockIdx.x * 32;
+  const int nv = min(32, count - v0);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double f = 0.0;
-    for (int p = rp[i]; p < rp[i + 1]; ++p) f += val[p] * (double)s[ci[p]];
-    acc += (double)s[i] * (h[i] + 0.5 * f);
+    uint32_t w = 0;
+    for (int r = 0; r < nv; ++r)
+      if (spins[(size_t)(v0 + r) * n + i] < 0) w |= 1u << r;
+    wsh[i] = w;
   }
-  __shared__ double red[kEnergyThreads / 32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  double acc[32];
+#pragma unroll
+  for (int r = 0; r < 32; ++r) acc[r] = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t wi = wsh[i];
+    const double hi = h[i];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) acc[r] += ((wi >> r) & 1u) ? -hi : hi;
+    const int p1 = rp[i + 1];
+    for (int p = rp[i]; p < p1; ++p) {
+      const int j = ci[p];
+      if (j <= i) continue;
+      const uint32_t x = wi ^ wsh[j];
+      const double v = val[p];
+#pragma unroll
+      for (int r = 0; r < 32; ++r) acc[r] += ((x >> r) & 1u) ? -v : v;
+    }
+  }
+  // warp reduction, then warps in order
+  double* part = reinterpret_cast<double*>(wsh + ((n + 1) & ~1));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int r = 0; r < 32; ++r) {
+    double x = acc[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) part[warp * 32 + r] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < nv) {
     double t = 0.0;
-    for (int w = 0; w < kEnergyThreads / 32; ++w) t += red[w];
-    out[blockIdx.x] = t;
+    for (int w = 0; w < kEnergyThreads / 32; ++w) t += part[w * 32 + threadIdx.x];
+    out[v0 + threadIdx.x] = t;
   }
 }
 
@@ -274,9 +305,15 @@ cudaError_t launch_sqa_colour(const oj_graph* g, int R, int T, int8_t* spins, co
 
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
-  energy_kernel<<<count, kEnergyThreads, 0, st>>>(g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(),
-                                                  g->d_val64.as<double>(), g->d_h64.as<double>(),
-                                                  g->n, spins, out);
+  const size_t smem = (size_t)((g->n + 1) & ~1) * 4 + (kEnergyThreads / 32) * 32 * 8;
+  auto kern = energy_kernel;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<(count + 31) / 32, kEnergyThreads, smem, st>>>(g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(),
+                                                        g->d_val64.as<double>(), g->d_h64.as<double>(), g->n,
+                                                        count, spins, out);
   return cudaGetLastError();
 }
 

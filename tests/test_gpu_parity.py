@@ -207,3 +207,47 @@ def test_replica_offset_must_be_multiple_of_32(ctx):
     with pytest.raises(N.OJError) as ei:
         N.sa_run(dg, s, [1.0], [1], seed=1, replica_offset=5)
     assert ei.value.status == N.OJ_ERR_ARG
+
+
+@pytest.mark.parametrize("n,R", [(200, 128), (700, 130), (1100, 64)])
+def test_sa_dense_tc_bit_exact_integer(ctx, n, R):
+    """Tensor-core delayed updates: for half-integer couplings every product and
+    sum is exact, so the trajectory equals the sequential replay spin for spin."""
+    m, _ = I.dense_qubo_int(n, seed=n)
+    g, dg = _graph(ctx, m)
+    assert dg.info()["integer_exact"] == 1
+    betas, mcs = I.geometric_betas(0.05, 5.0, 12)
+    s0 = _init(R, n, 3)
+    s = s0.copy()
+    st = N.sa_run(dg, s, betas, mcs, seed=4242, kernel="dense_tc")
+    assert st["kernel"] == "dense_tc"
+    ref = O.replay_sa(g, s0, _per_sweep(betas, mcs), 4242, mode="dense")
+    np.testing.assert_array_equal(s, ref)
+
+
+def test_sa_dense_tc_equals_plain_integer(ctx):
+    m, _ = I.dense_qubo_int(512, seed=9)
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.05, 5.0, 30)
+    s0 = _init(160, 512, 8)
+    a, b = s0.copy(), s0.copy()
+    N.sa_run(dg, a, betas, mcs, seed=77, kernel="dense_tc")
+    N.sa_run(dg, b, betas, mcs, seed=77, kernel="dense_plain")
+    np.testing.assert_array_equal(a, b)
+
+
+def test_sa_dense_tc_real_couplings_statistics(ctx):
+    """Real couplings: the BF16 hi/lo split is not exact, so trajectories may
+    part from the FP32 plain kernel after a near-tie; the final-energy
+    distributions must agree (two-sample comparison of the means)."""
+    m, _ = I.dense_qubo_normal(300, seed=11)
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.1, 10.0, 60)
+    s0 = _init(256, 300, 2)
+    a, b = s0.copy(), s0.copy()
+    ea, eb = np.zeros(256), np.zeros(256)
+    N.sa_run(dg, a, betas, mcs, seed=5, kernel="dense_tc", energies=ea)
+    N.sa_run(dg, b, betas, mcs, seed=6, kernel="dense_plain", energies=eb)
+    se = np.sqrt(ea.var() / len(ea) + eb.var() / len(eb))
+    assert abs(ea.mean() - eb.mean()) < 4 * se + 1e-9
+    np.testing.assert_allclose(ea, O.energies(g, a), rtol=1e-12, atol=1e-9)
