@@ -139,16 +139,16 @@ __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.w
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void sweepers_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 // -ln(u) of replica r for the 32 sites of block kb in sweep k, written to
 // L[j][t] (t = r - tile base).  One Philox call serves four replicas of a site
 // (the stream u(r,k,i) = Philox(i, k, r>>2)[r&3]); a rotation inside each
 // group of four lanes hands every lane its own four values per call.
-__device__ __forceinline__ void produce_L(float* L, int t, uint32_t r, int kb, uint32_t k, const ojd::Keys& K) {
+__device__ __forceinline__ void produce_L(float* L, int t, uint32_t r, int kb, uint32_t k, const ojd::Keys& K,
+                                          int q0, int q1, int qstep) {
   const int lane = threadIdx.x & 31, m = lane & 3, qb = lane & ~3;
 #pragma unroll 1
-  for (int q = 0; q < 8; ++q) {
+  for (int q = q0; q < q1; q += qstep) {
     const uint32_t site = (uint32_t)(kb * kBlk + 4 * q + m);
     const ojd::u4 v = ojd::philox(site, k, r >> 2, ojd::TAG_SA, K);
 #pragma unroll
@@ -173,12 +173,12 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
   const uint32_t btile = (uint32_t)Ncta * kBlk * 2;  // bytes of one B tile
   // ---- shared memory carve-up
   unsigned char* A = sm;                                     // 2 x 8 KB MMA A operand (dS / S tiles)
-  unsigned char* Ds = A + 2 * 8192;                          // 2 x 8 KB dS staged by the block's owner
-  unsigned char* Bh = Ds + 2 * 8192;                         // 2 x btile (hi)
+  unsigned char* Bh = A + 2 * 8192;                          // 2 x btile (hi)
   unsigned char* Bl = Bh + 2 * btile;                        // 2 x btile (lo), if any
-  float* Jb = reinterpret_cast<float*>(Bl + (has_lo ? 2 * btile : 0));  // 32 x 32 FP32
-  float* Lb = Jb + kBlk * kBlk;                              // 2 x 32 x 128 FP32
-  uint32_t* bits = reinterpret_cast<uint32_t*>(Lb + 2 * kBlk * kTile);  // [nblk][128]
+  float* Jb = reinterpret_cast<float*>(Bl + (has_lo ? 2 * btile : 0));  // 2 x 32 x 32 FP32
+  float* Lb = Jb + 2 * kBlk * kBlk;                          // 2 x 32 x 128 FP32
+  float* Hb = Lb + 2 * kBlk * kTile;                         // 2 x 32 FP32
+  uint32_t* bits = reinterpret_cast<uint32_t*>(Hb + 2 * kBlk);  // [nblk][128]
   uint64_t* bar = reinterpret_cast<uint64_t*>(bits + (size_t)nblk * kTile);  // mma, bfull[2]
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 4);
   uint64_t* bar_mma = bar;
@@ -289,10 +289,33 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
   };
 
   recompute();
-  // L for the first block this CTA owns (sweep 0)
-  const int first_own = cta * bpc;
-  if (tid >= kTile) produce_L(Lb, tid - kTile, a.rep0 + r_base + (tid - kTile), first_own, a.sweep0, a.keys);
-  int own_count = 0;  // owned blocks swept so far (selects the L slot)
+  // Blocks are owned round-robin: block kb belongs to CTA kb % P.  The g-th
+  // block owned by this CTA (counting across sweeps) is block (g % bpc)*P + cta
+  // of sweep g / bpc; its -ln(u) values and in-block couplings are prepared by
+  // the producer warps into slot g & 1 while other CTAs own the sweep.
+  const int64_t own_total = a.nsweeps * bpc;
+  // part `part` of `parts` of the inputs of owned block g, by all 256 threads:
+  // thread = (replica tid % 128, half tid / 128); the block's 8 groups of four
+  // sites are split over the parts and the two halves.
+  auto produce = [&](int64_t g, int part, int parts) {
+    const int okb = (int)(g % bpc) * a.P + cta;
+    const uint32_t ok_sweep = a.sweep0 + (uint32_t)(g / bpc);
+    const int slot = (int)(g & 1);
+    if (part == 0) {
+      float* Jd = Jb + slot * kBlk * kBlk;
+      for (int e = tid; e < kBlk * kBlk; e += kThreads) Jd[e] = a.jblk[(size_t)okb * kBlk * kBlk + e];
+      if (tid < kBlk) Hb[slot * kBlk + tid] = a.h[okb * kBlk + tid];
+    }
+    const int q0 = (8 * part) / parts, q1 = (8 * (part + 1)) / parts;
+    const int t = tid & (kTile - 1), half = tid >> 7;
+    produce_L(Lb + slot * kBlk * kTile, t, a.rep0 + r_base + t, okb, ok_sweep, a.keys, q0 + half, q1, 2);
+  };
+  int64_t own_count = 0;    // owned blocks swept so far
+  int64_t produced = 0;     // owned blocks whose inputs are ready
+  int part = 0;             // parts of the next owned block done
+  const int parts = a.P > 1 ? a.P - 1 : 1;
+  if (own_total > 0) produce(0, 0, 1);
+  produced = 1;
   if (tid == 0) load_b(0, 0);
   __syncthreads();
   cluster_arrive();
@@ -301,7 +324,6 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
   int64_t gblk = 0;  // global block counter (buffer parity)
   for (int64_t k = 0; k < a.nsweeps; ++k) {
     const float beta = a.betas[k];
-    const uint32_t kk = a.sweep0 + (uint32_t)k;
     if (a.recompute > 0 && k > 0 && (k % a.recompute) == 0) {
       // drain: the next-block load issued at the end of the last sweep
       if (tid == 0) wait_full((int)(gblk & 1));
@@ -313,7 +335,7 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
     }
     for (int kb = 0; kb < nblk; ++kb, ++gblk) {
       const int buf = (int)(gblk & 1);
-      const int owner = kb / bpc;
+      const int owner = kb % a.P;
       // prefetch the next block's B tile into the other buffer (free: its last
       // MMAs completed before the previous block's cluster barrier)
       if (tid == 0) {
@@ -322,30 +344,48 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
         if (more) load_b(nkb, buf ^ 1);
       }
       if (owner == cta) {
-        const int lslot = own_count & 1;
+        const int slot = (int)(own_count & 1);
         if (tid < kTile) {
-          // in-block couplings and this block's fields
-          for (int e = tid; e < kBlk * kBlk; e += kTile) Jb[e] = a.jblk[(size_t)kb * kBlk * kBlk + e];
-          sweepers_sync();
+          const float* Jd = Jb + slot * kBlk * kBlk;
           float f[32];
-          tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)((kb - owner * bpc) * kBlk), f);
+          tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)((kb / a.P) * kBlk), f);
 #pragma unroll
-          for (int j = 0; j < 32; ++j) f[j] = __fadd_rn(f[j], a.h[kb * kBlk + j]);
-          uint32_t w = bits[kb * kTile + tid];
+          for (int j = 0; j < 32; ++j) f[j] = __fadd_rn(f[j], Hb[slot * kBlk + j]);
+          const uint32_t w = bits[kb * kTile + tid];
           uint32_t flips = 0;
-          const float* L = Lb + lslot * kBlk * kTile;
+          const float* L = Lb + slot * kBlk * kTile;
+          // Four sub-blocks of 8 sites: inside a sub-block every decision
+          // updates the fields still ahead in it at once (short dependent
+          // chain); the sub-block's flips then reach the later fields as one
+          // rank-8 update.  Every field accumulates c_j * J_jm in increasing
+          // j, one rounding each (c_j * J_jm is exact), as in the sequential
+          // kernel.
+          float c[32], Lr[32];
+          const int nvalid = a.n - kb * kBlk;  // sites of this block below n
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const bool neg = (w >> j) & 1u;
-            const float dE = neg ? 2.0f * f[j] : -2.0f * f[j];
-            const bool acc = (kb * kBlk + j < a.n) && (dE <= 0.0f || __fmul_rn(beta, dE) < L[j * kTile + tid]);
-            const float c = acc ? (neg ? 2.0f : -2.0f) : 0.0f;
+          for (int j = 0; j < 32; ++j) Lr[j] = j < nvalid ? L[j * kTile + tid] : -1.0f;
 #pragma unroll
-            for (int m = j + 1; m < 32; ++m) f[m] = __fadd_rn(f[m], __fmul_rn(c, Jb[j * kBlk + m]));
-            flips |= acc ? (1u << j) : 0u;
+          for (int sb = 0; sb < 4; ++sb) {
+#pragma unroll
+            for (int j = 8 * sb; j < 8 * sb + 8; ++j) {
+              const bool neg = (w >> j) & 1u;
+              const float s2 = neg ? 2.0f : -2.0f;  // -2 s: dE = -2 s f, and the flip's dS
+              const float dE = s2 * f[j];
+              // padded sites (L = -1) never flip
+              const bool acc = Lr[j] >= 0.0f && (dE <= 0.0f || __fmul_rn(beta, dE) < Lr[j]);
+              c[j] = acc ? s2 : 0.0f;
+              flips |= acc ? (1u << j) : 0u;
+#pragma unroll
+              for (int m = j + 1; m < 8 * sb + 8; ++m) f[m] = __fmaf_rn(c[j], Jd[j * kBlk + m], f[m]);
+            }
+#pragma unroll
+            for (int m = 8 * sb + 8; m < 32; ++m) {
+#pragma unroll
+              for (int j = 8 * sb; j < 8 * sb + 8; ++j) f[m] = __fmaf_rn(c[j], Jd[j * kBlk + m], f[m]);
+            }
           }
           const uint32_t nw = w ^ flips;
-          // dS row (BF16: +-2 where flipped: new s - old s) into every CTA's A buffer
+          // dS row (BF16: +-2 where flipped = new s - old s) into every CTA's A buffer
           uint32_t pk[16];
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
@@ -355,45 +395,35 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
             pk[e] = d0 | (d1 << 16);
           }
           const int roff = (tid >> 3) * 512 + (tid & 7) * 16;
-          unsigned char* Dr = Ds + buf * 8192 + roff;
+          for (int p = 0; p < a.P; ++p) {
+            unsigned char* Ab = cl.map_shared_rank(A, p) + buf * 8192 + roff;
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
-            *reinterpret_cast<uint4*>(Dr + q * 128) = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
-          bits[kb * kTile + tid] = nw;
-        } else {
-          // draw -ln(u) for the next block this CTA owns
-          int nkb = kb + 1;
-          uint32_t nk = kk;
-          if (nkb >= (owner + 1) * bpc || nkb >= nblk) {
-            nkb = first_own;
-            nk = kk + 1;
+            for (int q = 0; q < 4; ++q)
+              *reinterpret_cast<uint4*>(Ab + q * 128) = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+            *cl.map_shared_rank(bits + kb * kTile + tid, p) = nw;
           }
-          if (k + 1 < a.nsweeps || nk == kk)
-            produce_L(Lb + (lslot ^ 1) * kBlk * kTile, tid - kTile, a.rep0 + r_base + (tid - kTile), nkb, nk,
-                      a.keys);
+          asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
         }
         ++own_count;
+      } else if (produced <= own_count && produced < own_total) {
+        produce(produced, part, parts);
+        if (++part == parts) {
+          part = 0;
+          ++produced;
+        }
+      }
+      if (a.P == 1 && produced <= own_count && produced < own_total) {
+        // single-CTA cluster: no foreign blocks to hide behind
+        __syncthreads();
+        produce(produced, 0, 1);
+        ++produced;
       }
       tc_fence_before();
       cluster_arrive();
       cluster_wait();
       tc_fence_after();
-      // every CTA pulls the owner's dS rows (and new spin words) into its own
-      // MMA operand buffer
-      if (tid < kTile) {
-        const int roff = (tid >> 3) * 512 + (tid & 7) * 16;
-        const unsigned char* src = cl.map_shared_rank(Ds, owner) + buf * 8192 + roff;
-        unsigned char* dst = A + buf * 8192 + roff;
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          *reinterpret_cast<uint4*>(dst + q * 128) = *reinterpret_cast<const uint4*>(src + q * 128);
-        if (owner != cta) bits[kb * kTile + tid] = *cl.map_shared_rank(bits + kb * kTile + tid, owner);
-        proxy_fence();
-      }
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
       if (tid == 0) {
+        proxy_fence();
         wait_full(buf);
         issue_mma(buf, buf, 1u);
         wait_mma();
@@ -405,7 +435,7 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
   }
   // ---- write back the spins of the owned blocks
   for (int idx = tid; idx < bpc * kTile; idx += kThreads) {
-    const int kb = cta * bpc + idx / kTile, t = idx % kTile;
+    const int kb = (idx / kTile) * a.P + cta, t = idx % kTile;
     const int r = r_base + t;
     if (kb >= nblk || r >= a.R) continue;
     const uint32_t w = bits[kb * kTile + t];
@@ -427,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
 
 size_t dense_tc_smem(const TcPlan& pl) {
   const size_t btile = (size_t)pl.ncta * kBlk * 2;
-  return 4 * 8192 + 2 * btile * (pl.exact ? 1 : 2) + kBlk * kBlk * 4 + 2 * kBlk * kTile * 4 +
+  return 2 * 8192 + 2 * btile * (pl.exact ? 1 : 2) + 2 * kBlk * kBlk * 4 + 2 * kBlk * kTile * 4 + 2 * kBlk * 4 +
          (size_t)pl.nblk * kTile * 4 + 4 * 8 + 16;
 }
 
@@ -459,7 +489,7 @@ cudaError_t dense_tc_prepare(oj_graph* g, std::string* why) {
       const size_t base = ((size_t)kb * P + c) * tile_elems;
       for (int row = 0; row < ncta; ++row)
         for (int k = 0; k < kBlk; ++k) {
-          const int i = kb * kBlk + k, j = c * ncta + row;
+          const int i = kb * kBlk + k, j = ((row / kBlk) * P + c) * kBlk + row % kBlk;
           const float v = (float)J[(size_t)i * npad + j];
           const __nv_bfloat16 bh = __float2bfloat16_rn(v);
           const size_t e = base + canon_off(row, k) / 2;
