@@ -237,12 +237,16 @@ def run_reference(args):
     return 0
 
 
-def _algo_per_attempt(w, n):
-    """Algorithmic bytes (hbm-bound kernels) or flops (dense kernels) per attempt."""
+def _algo_per_attempt(w, n, kernel, degree):
+    """Algorithmic bytes (state-bound kernels) or flops (dense kernels) per attempt."""
     if w["config"] == 2:
         return ALGO_BYTES_PER_ATTEMPT, "GB/s"
     if w["kind"] == "sqa":
-        return 7.0 / 8.0 if w.get("bitpacked") else 7.0, "GB/s"  # 3 spatial + 2 Trotter + read + write
+        if kernel == "bitpacked":
+            # per site and slice group: own word read + write and d neighbour words
+            # (4 B each), shared by the T/2 slices of the group
+            return (2 + degree) * 4.0 / (w["T"] / 2.0), "GB/s"
+        return 2.0 + degree + 2.0, "GB/s"  # int8: d spatial + 2 Trotter neighbours + read + write
     return 2.0 * n, "TFLOP/s"  # one field-row update of 2n flop per attempt
 
 
@@ -338,7 +342,7 @@ def run_ours(args):
     e2e_value = attempts_per_step * ws / (e2 / 1000.0)
 
     hbm_peak, peak_kind = _peaks()
-    per, unit = _algo_per_attempt(w, n)
+    per, unit = _algo_per_attempt(w, n, used_kernel, graph.info()["max_degree"])
     if unit == "GB/s":
         achieved = attempts_per_step * per / (kms / 1000.0) / 1e9
         peak = hbm_peak

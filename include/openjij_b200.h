@@ -122,7 +122,10 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t
  * T >= 2 (transverse_ising.hpp:78-81).  spins [R][T][n] in/out.
  * energies [R][T] (may be NULL): FP64 classical energy of each slice.
  * best_slice [R] (may be NULL): get_solution()'s slice, the first slice of
- * minimum energy (include/openjij/result/get_solution.hpp:59-84). */
+ * minimum energy (include/openjij/result/get_solution.hpp:59-84).
+ * Kernels: OJ_KERNEL_COLOUR (any graph) or OJ_KERNEL_BITPACKED (regular
+ * graph, couplings +-c, h = 0, degree <= 8, T <= 32: the T slices of a site
+ * in one 32-bit word); OJ_KERNEL_AUTO takes the bit-packed one when it applies. */
 oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32_t num_slices,
                      int8_t* spins, double gamma, const double* betas, const double* s,
                      const int32_t* mcs, int32_t num_sched, uint64_t seed, int64_t first_sweep,

@@ -105,6 +105,44 @@ void msc_thresholds(const std::vector<float>& betas, double c, int D, std::vecto
     }
 }
 
+// Thresholds of the bit-packed SQA kernel, class m = u*3 + k (u unsatisfied
+// spatial bonds of D, k aligned Trotter neighbours):
+//   dE = a*float(2c(D-2u)) + B*float(4-4k) in FP32 (each product and the sum rounded once);
+//   dE <= 0 -> always (mode[2s] bit m); NaN or exp(-dE) == 0 -> never;
+//   else thr[s][m] = min(2^32-1, floor(exp(-dE)*2^32)) and mode[2s+1] bit m.
+void sqa_msc_thresholds(const std::vector<float2>& coef, double c, int D, std::vector<uint32_t>& thr,
+                        std::vector<uint32_t>& mode) {
+  const int NC = (D + 1) * 3;
+  const size_t S = coef.size();
+  thr.assign(S * NC, 0u);
+  mode.assign(S * 2, 0u);
+  for (size_t k = 0; k < S; ++k) {
+    uint32_t always = 0, live = 0;
+    for (int u = 0; u <= D; ++u)
+      for (int kk = 0; kk < 3; ++kk) {
+        const int m = u * 3 + kk;
+        const float dEsp = (float)(2.0 * c * (double)(D - 2 * u));
+        const float dEtrot = (float)(4 - 4 * kk);
+        const float p1 = coef[k].x * dEsp;
+        const float p2 = coef[k].y * dEtrot;
+        const float dE = p1 + p2;
+        uint32_t v = 0;
+        if (std::isnan(dE)) {
+          v = 0;
+        } else if (dE <= 0.0f) {
+          always |= 1u << m;
+        } else {
+          const double t = std::floor(std::ldexp(std::exp(-(double)dE), 32));
+          v = t >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)t;
+          if (v) live |= 1u << m;
+        }
+        thr[k * NC + m] = v;
+      }
+    mode[2 * k] = always;
+    mode[2 * k + 1] = live;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -415,11 +453,17 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   if (R == 0 || n == 0) return OJ_OK;
   if (!spins) return arg_fail(ctx, "null spins");
   uint32_t kernel = flags & OJ_KERNEL_MASK;
-  if (kernel != OJ_KERNEL_AUTO && kernel != OJ_KERNEL_COLOUR) {
-    ctx->last_error = "SQA runs on the colour-class kernel";
+  const bool msc_ok = g->info.bimodal && g->regular && T <= 32 && sqa_msc_fits(g);
+  if (kernel == OJ_KERNEL_AUTO) kernel = msc_ok ? OJ_KERNEL_BITPACKED : OJ_KERNEL_COLOUR;
+  if (kernel != OJ_KERNEL_COLOUR && kernel != OJ_KERNEL_BITPACKED) {
+    ctx->last_error = "SQA runs on the colour-class or the bit-packed kernel";
     return OJ_ERR_UNSUPPORTED;
   }
-  kernel = OJ_KERNEL_COLOUR;
+  if (kernel == OJ_KERNEL_BITPACKED && !msc_ok) {
+    ctx->last_error =
+        "bit-packed SQA needs a regular graph with couplings +-c (degree <= 8), h = 0, T <= 32 and n <= 65535";
+    return OJ_ERR_UNSUPPORTED;
+  }
   RngBase rb;
   if (oj_status st_ = rng_base(ctx, seed, first_sweep, replica_offset, &rb)) return st_;
   DeviceGuard dg(ctx->device);
@@ -447,12 +491,36 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   int launches = 0;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
-  OJ_CK(ctx->params.ensure(std::max<size_t>(coef.size() * sizeof(float2), 16)), "alloc params");
-  float2* d_coef = ctx->params.as<float2>();
-  if (S > 0) OJ_CK(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(float2), cudaMemcpyHostToDevice, st), "H2D coef");
-  OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-  if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, rb, st, &launches), "sqa kernel");
-  OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  if (kernel == OJ_KERNEL_BITPACKED) {
+    OJ_CK(sqa_msc_prepare(g), "bit-packed SQA tables");
+    std::vector<uint32_t> thr, mode;
+    sqa_msc_thresholds(coef, g->info.coupling_abs, g->info.max_degree, thr, mode);
+    OJ_CK(ctx->params.ensure(std::max<size_t>((thr.size() + mode.size()) * 4, 16)), "alloc params");
+    uint32_t* d_thr = ctx->params.as<uint32_t>();
+    uint32_t* d_mode = d_thr + thr.size();
+    if (S > 0) {
+      OJ_CK(cudaMemcpyAsync(d_thr, thr.data(), thr.size() * 4, cudaMemcpyHostToDevice, st), "H2D thr");
+      OJ_CK(cudaMemcpyAsync(d_mode, mode.data(), mode.size() * 4, cudaMemcpyHostToDevice, st), "H2D mode");
+    }
+    OJ_CK(ctx->words.ensure((size_t)R * n * 4), "alloc words");
+    uint32_t* d_words = ctx->words.as<uint32_t>();
+    OJ_CK(launch_sqa_pack(d_spins, R, T, n, d_words, st), "pack");
+    ++launches;
+    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+    if (S > 0) OJ_CK(launch_sqa_msc(g, R, T, d_words, d_thr, d_mode, S, rb, st, &launches), "sqa bit-packed kernel");
+    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+    OJ_CK(launch_sqa_unpack(d_words, R, T, n, d_spins, st), "unpack");
+    ++launches;
+  } else {
+    OJ_CK(ctx->params.ensure(std::max<size_t>(coef.size() * sizeof(float2), 16)), "alloc params");
+    float2* d_coef = ctx->params.as<float2>();
+    if (S > 0)
+      OJ_CK(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(float2), cudaMemcpyHostToDevice, st),
+            "H2D coef");
+    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+    if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, rb, st, &launches), "sqa kernel");
+    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  }
   if (energies || best_slice) {
     double* d_e = (devp && energies) ? energies : nullptr;
     if (!d_e) {

@@ -8,6 +8,8 @@
 //     u(r, t, k, i) = Philox((i, k, r, ((t>>3)<<9) | ((t&1)<<8) | TAG_SQA))[(t>>1) & 3]
 //   bit-packed SA kernel (32 replicas per word, group g):
 //     W_l(g, k, i)  = Philox((i, k, g, ((l>>2)<<8) | TAG_SA_MSC))[l & 3],  l = 0..31
+//   bit-packed SQA kernel (T slices per word, slice group q = 0, 1, 2):
+//     W_l(r, q, k, i) = Philox((i, k, r, ((l>>2)<<16) | (q<<8) | TAG_SQA_MSC))[l & 3]
 // with r the replica, t the Trotter slice, k the sweep (one_mc_step repeats
 // included) and i the site.  Results are therefore independent of how the
 // replicas are spread over CTAs, clusters or GPUs.
@@ -19,6 +21,7 @@ namespace ojd {
 constexpr uint32_t TAG_SA = 0x5Au;
 constexpr uint32_t TAG_SQA = 0xA5u;
 constexpr uint32_t TAG_SA_MSC = 0x3Cu;
+constexpr uint32_t TAG_SQA_MSC = 0xC3u;
 
 struct u4 {
   uint32_t x, y, z, w;

@@ -29,6 +29,8 @@ oj_graph::~oj_graph() {
   d_order.release();
   d_coff.release();
   d_dense.release();
+  sqa_nbr.release();
+  sqa_jm.release();
   if (msc) msc->tables.release();
   if (tc) {
     tc->bt_hi.release();

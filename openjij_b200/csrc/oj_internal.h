@@ -94,6 +94,7 @@ struct oj_graph {
   oj::DevBuf d_dense;  // FP32 dense J (n x n), created on first use
   std::unique_ptr<oj::MscPlan> msc;
   std::unique_ptr<oj::TcPlan> tc;
+  oj::DevBuf sqa_nbr, sqa_jm;  // bit-packed SQA tables: [n][D] neighbours (u16), [n] J>0 masks
   ~oj_graph();
 };
 
@@ -132,6 +133,12 @@ cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint3
 cudaError_t launch_sa_dense_tc(const oj_graph* g, int R, int8_t* spins, const float* betas, int64_t nsweeps,
                                RngBase rb, int recompute, cudaStream_t st, int* launches);
 cudaError_t dense_tc_prepare(oj_graph* g, std::string* why);
+cudaError_t launch_sqa_msc(const oj_graph* g, int R, int T, uint32_t* words, const uint32_t* thr,
+                           const uint32_t* mode, int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
+cudaError_t sqa_msc_prepare(oj_graph* g);
+bool sqa_msc_fits(const oj_graph* g);
+cudaError_t launch_sqa_pack(const int8_t* spins, int R, int T, int n, uint32_t* words, cudaStream_t st);
+cudaError_t launch_sqa_unpack(const uint32_t* words, int R, int T, int n, int8_t* spins, cudaStream_t st);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,

@@ -700,4 +700,112 @@ void orc_sqa_coefficients(const double* betas, const double* ss, int64_t count, 
   }
 }
 
+// Bit-packed SQA replay (regular graph, couplings +-c, h = 0, T <= 32).
+// Word (r, i) bit t = 1 iff slice t of replica r has s_i = -1.  Order: per
+// sweep k, slice groups {even t < T - T%2}, {odd t}, {T-1 if T odd} (grp 0, 1,
+// 2), per colour class, per site i of the class, every slice t of the group:
+//   u = unsatisfied bonds of (i, t); kk = Trotter neighbours t+-1 (mod T) with
+//   the same spin; class m = 3u + kk;
+//   always[k] bit m -> flip; live[k] bit m -> flip iff U < thr[k][m], where U's
+//   bit (31 - l) is bit t of W_l = Philox(ctr = (i, k, r, (l/4) << 16 | grp << 8
+//   | TAG_SQA_MSC))[l % 4]; otherwise no flip.
+// The slices of one group are decided from the word before the group's update
+// (they are never Trotter neighbours of each other, except t = 0 and T-1 with
+// T odd, which sit in different groups).
+// thr: [nsweeps][(dmax+1)*3], mode: [nsweeps][2] = (always, live).
+void orc_replay_sqa_msc(int n, const int64_t* indptr, const int32_t* indices, const double* data, int R,
+                        int T, uint32_t* words /*[R][n]*/, const uint32_t* thr, const uint32_t* mode, int dmax,
+                        int64_t nsweeps, uint64_t seed, int threads) {
+  Aug g{n, indptr, indices, data};
+  Nbr b = make_nbr(g);
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  int ncol = 0;
+  for (int c : col) ncol = std::max(ncol, c + 1);
+  std::vector<std::vector<int>> by_col(ncol);
+  for (int i = 0; i < n; ++i) by_col[col[i]].push_back(i);
+  const int upper = (T % 2 != 0) ? T - 1 : T;
+  std::vector<std::vector<int>> groups(3);
+  for (int t = 0; t < upper; t += 2) groups[0].push_back(t);
+  for (int t = 1; t < T; t += 2) groups[1].push_back(t);
+  if (T % 2 != 0) groups[2].push_back(T - 1);
+  const int NC = (dmax + 1) * 3;
+  parallel_for(R, threads, [&](int r) {
+    uint32_t* w = words + (size_t)r * n;
+    for (int64_t k = 0; k < nsweeps; ++k) {
+      const uint32_t* th = thr + (size_t)k * NC;
+      const uint32_t always = mode[2 * k], live = mode[2 * k + 1];
+      for (int grp = 0; grp < 3; ++grp) {
+        if (groups[grp].empty()) continue;
+        for (int c = 0; c < ncol; ++c)
+          for (int i : by_col[c]) {
+            const uint32_t wi = w[i];
+            uint32_t Wl[32];
+            for (int q = 0; q < 8; ++q) {
+              P4 r4 = philox((uint32_t)i, (uint32_t)k, (uint32_t)r,
+                             ((uint32_t)q << 16) | ((uint32_t)grp << 8) | TAG_SQA_MSC, k0, k1);
+              for (int l = 0; l < 4; ++l) Wl[4 * q + l] = r4.v[l];
+            }
+            uint32_t flip = 0;
+            for (int t : groups[grp]) {
+              const int bi = (wi >> t) & 1;
+              int u = 0;
+              for (int64_t p = b.rp[i]; p < b.rp[i + 1]; ++p) {
+                const int bj = (w[b.ci[p]] >> t) & 1;
+                // J s_i s_j > 0: unsatisfied; s_i s_j = +1 iff the bits agree
+                const bool same = bi == bj;
+                if ((b.val[p] > 0) == same) ++u;
+              }
+              const int tp = (t + 1) % T, tm = (t - 1 + T) % T;
+              const int kk = (((wi >> tp) & 1) == (uint32_t)bi) + (((wi >> tm) & 1) == (uint32_t)bi);
+              const int m = 3 * u + kk;
+              if ((always >> m) & 1u) {
+                flip |= 1u << t;
+              } else if ((live >> m) & 1u) {
+                uint32_t U = 0;
+                for (int l = 0; l < 32; ++l) U |= ((Wl[l] >> t) & 1u) << (31 - l);
+                if (U < th[m]) flip |= 1u << t;
+              }
+            }
+            w[i] = wi ^ flip;
+          }
+      }
+    }
+  });
+}
+
+// Thresholds of the bit-packed SQA kernel from the per-sweep FP32 coefficients
+// (a, B): for class m = 3u + kk, dE = a*float(2c(dmax-2u)) + B*float(4-4kk)
+// (FP32, products and sum each rounded once); dE <= 0 -> always; NaN -> never;
+// else thr = min(2^32-1, floor(exp(-dE)*2^32)), live when thr > 0.
+void orc_sqa_msc_thresholds(const float* coef_a, const float* coef_b, int64_t nsweeps, double c, int dmax,
+                            uint32_t* thr, uint32_t* mode) {
+  const int NC = (dmax + 1) * 3;
+  for (int64_t k = 0; k < nsweeps; ++k) {
+    uint32_t always = 0, live = 0;
+    for (int u = 0; u <= dmax; ++u)
+      for (int kk = 0; kk < 3; ++kk) {
+        const int m = 3 * u + kk;
+        const float dEsp = (float)(2.0 * c * (double)(dmax - 2 * u));
+        const float dEtrot = (float)(4 - 4 * kk);
+        const float p1 = coef_a[k] * dEsp;
+        const float p2 = coef_b[k] * dEtrot;
+        const float dE = p1 + p2;
+        uint32_t v = 0;
+        if (dE != dE) {
+          v = 0;
+        } else if (dE <= 0.0f) {
+          always |= 1u << m;
+        } else {
+          const double t = std::floor(std::ldexp(std::exp(-(double)dE), 32));
+          v = t >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)t;
+          if (v) live |= 1u << m;
+        }
+        thr[(size_t)k * NC + m] = v;
+      }
+    mode[2 * k] = always;
+    mode[2 * k + 1] = live;
+  }
+}
+
 }  // extern "C"

@@ -71,6 +71,9 @@ def lib():
                                         C.c_int, _u32p, C.c_int64, C.c_uint64, C.c_int]
         L.orc_msc_thresholds.argtypes = [_f32p, C.c_int64, C.c_double, C.c_int, _u32p, _u32p]
         L.orc_sqa_coefficients.argtypes = [_f64p, _f64p, C.c_int64, C.c_double, C.c_int, _f32p, _f32p]
+        L.orc_replay_sqa_msc.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _u32p, _u32p,
+                                         _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
+        L.orc_sqa_msc_thresholds.argtypes = [_f32p, _f32p, C.c_int64, C.c_double, C.c_int, _u32p, _u32p]
         L.orc_gen_spin_seq.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _i8p]
         _lib = L
     return _lib
@@ -302,3 +305,42 @@ def replay_sa_msc(g: AugCSR, init2d, thr, always, seed, threads=None):
     lib().orc_replay_sa_msc(*g.args(), w.shape[0], w, thr, thr.shape[1] - 1, alw, thr.shape[0],
                             int(seed), _threads(threads))
     return unpack_words(w)
+
+
+def pack_slices(spins3d):
+    """int8 [R][T][n] (T <= 32) -> u32 [R][n], bit t = (s_t == -1)."""
+    s = np.asarray(spins3d)
+    R, T, n = s.shape
+    w = np.zeros((R, n), np.uint64)
+    for t in range(T):
+        w |= (s[:, t, :] < 0).astype(np.uint64) << np.uint64(t)
+    return w.astype(np.uint32)
+
+
+def unpack_slices(words, T):
+    w = np.asarray(words, np.uint32)
+    R, n = w.shape
+    out = np.empty((R, T, n), np.int8)
+    for t in range(T):
+        out[:, t, :] = np.where((w >> np.uint32(t)) & np.uint32(1), -1, 1)
+    return out
+
+
+def sqa_msc_thresholds(coef_a, coef_b, c, dmax):
+    a = np.ascontiguousarray(coef_a, np.float32)
+    b = np.ascontiguousarray(coef_b, np.float32)
+    thr = np.zeros((len(a), (dmax + 1) * 3), np.uint32)
+    mode = np.zeros((len(a), 2), np.uint32)
+    lib().orc_sqa_msc_thresholds(a, b, len(a), float(c), int(dmax), thr, mode)
+    return thr, mode
+
+
+def replay_sqa_msc(g: AugCSR, init3d, thr, mode, seed, threads=None):
+    """Bit-packed SQA replay; thr [sweeps][(dmax+1)*3], mode [sweeps][2]."""
+    R, T, _ = np.shape(init3d)
+    w = np.ascontiguousarray(pack_slices(init3d), np.uint32)
+    thr = np.ascontiguousarray(thr, np.uint32)
+    mode = np.ascontiguousarray(mode, np.uint32)
+    dmax = thr.shape[1] // 3 - 1
+    lib().orc_replay_sqa_msc(*g.args(), R, T, w, thr, mode, dmax, thr.shape[0], int(seed), _threads(threads))
+    return unpack_slices(w, T)

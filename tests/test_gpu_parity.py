@@ -101,7 +101,8 @@ def test_sqa_colour_bit_exact(ctx, T):
     s = s0.copy()
     best = np.zeros(R, np.int32)
     en = np.zeros((R, T))
-    N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=5, energies=en, best=best)
+    st = N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=5, energies=en, best=best, kernel="colour")
+    assert st["kernel"] == "colour"
     a, b = O.sqa_coefficients(betas, ss, 1.0, T)
     ref = O.replay_sqa(g, s0, a, b, 5)
     np.testing.assert_array_equal(s, ref)
@@ -184,7 +185,63 @@ def test_replica_shards_equal_whole(ctx, kernel):
     np.testing.assert_array_equal(shard, whole[32:])
 
 
-def test_sqa_split_and_shard(ctx):
+def _scaled(m, c):
+    m = m.tocsr(copy=True) * c
+    m[m.shape[0] - 1, m.shape[0] - 1] = 1.0
+    return m
+
+
+@pytest.mark.parametrize("T", [2, 5, 31, 32])
+@pytest.mark.parametrize("which", ["regular3", "lattice", "regular5_real"])
+def test_sqa_bitpacked_bit_exact(ctx, T, which):
+    """Bit-packed SQA (the T slices of a site in one word) against its replay,
+    schedule ending at s = 1 (B = -inf: NaN and +-inf energy differences)."""
+    if which == "regular3":
+        m, c, D = I.random_regular_pm_j(48, 3, seed=7)[0], 1.0, 3
+    elif which == "lattice":
+        m, c, D = I.lattice_pm_j(8, seed=3)[0], 1.0, 4
+    else:
+        m, c, D = _scaled(I.random_regular_pm_j(60, 5, seed=2)[0], 0.37), 0.37, 5
+    g, dg = _graph(ctx, m)
+    R, nsched = 3, 16
+    ss = np.linspace(0.0, 1.0, nsched)
+    betas = np.full(nsched, 6.0)
+    mcs = np.where(np.arange(nsched) % 3 == 0, 2, 1).astype(np.int32)
+    s0 = np.ascontiguousarray(np.broadcast_to(_init(R, g.n, 4)[:, None, :], (R, T, g.n)))
+    s0 = s0.copy()
+    s0[:, T // 2, :] = _init(R, g.n, 8)
+    s = s0.copy()
+    best = np.zeros(R, np.int32)
+    en = np.zeros((R, T))
+    st = N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=9, energies=en, best=best, kernel="bitpacked")
+    assert st["kernel"] == "bitpacked"
+    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
+    thr, mode = O.sqa_msc_thresholds(np.repeat(a, mcs), np.repeat(b, mcs), c, D)
+    ref = O.replay_sqa_msc(g, s0, thr, mode, 9)
+    np.testing.assert_array_equal(s, ref)
+    for r in range(R):
+        e = O.energies(g, ref[r])
+        np.testing.assert_allclose(en[r], e, rtol=0, atol=1e-9)
+        # real couplings: equal-energy slices may differ in the last bits, so the
+        # first minimum is taken over the kernel's own energies
+        assert best[r] == int(np.argmin(en[r]))
+        assert e[best[r]] == pytest.approx(e.min(), abs=1e-9)
+
+
+def test_sqa_auto_picks_bitpacked_on_regular_pm_j(ctx):
+    m, _ = I.random_regular_pm_j(40, 3, seed=1)
+    g, dg = _graph(ctx, m)
+    s = np.ones((2, 8, g.n), np.int8)
+    assert N.sqa_run(dg, s, 1.0, [5.0], [0.5], [1], seed=1)["kernel"] == "bitpacked"
+    s = np.ones((2, 33, g.n), np.int8)
+    assert N.sqa_run(dg, s, 1.0, [5.0], [0.5], [1], seed=1)["kernel"] == "colour"
+    with pytest.raises(N.OJError) as ei:
+        N.sqa_run(dg, s, 1.0, [5.0], [0.5], [1], seed=1, kernel="bitpacked")
+    assert ei.value.status == N.OJ_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("kernel", ["bitpacked", "colour"])
+def test_sqa_split_and_shard(ctx, kernel):
     m, _ = I.random_regular_pm_j(40, 3, seed=9)
     g, dg = _graph(ctx, m)
     T, nsched = 6, 12
@@ -193,10 +250,11 @@ def test_sqa_split_and_shard(ctx):
     mcs = np.ones(nsched, np.int32)
     s0 = np.ascontiguousarray(np.broadcast_to(_init(64, g.n, 5)[:, None, :], (64, T, g.n)))
     whole = s0.copy()
-    N.sqa_run(dg, whole, 1.0, betas, ss, mcs, seed=3)
+    N.sqa_run(dg, whole, 1.0, betas, ss, mcs, seed=3, kernel=kernel)
     part = s0[32:].copy()
-    N.sqa_run(dg, part, 1.0, betas[:5], ss[:5], mcs[:5], seed=3, replica_offset=32)
-    N.sqa_run(dg, part, 1.0, betas[5:], ss[5:], mcs[5:], seed=3, replica_offset=32, first_sweep=5)
+    N.sqa_run(dg, part, 1.0, betas[:5], ss[:5], mcs[:5], seed=3, replica_offset=32, kernel=kernel)
+    N.sqa_run(dg, part, 1.0, betas[5:], ss[5:], mcs[5:], seed=3, replica_offset=32, first_sweep=5,
+              kernel=kernel)
     np.testing.assert_array_equal(part, whole[32:])
 
 

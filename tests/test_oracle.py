@@ -100,3 +100,76 @@ def test_greedy_colouring_checkerboard():
     col = O.greedy_colour(g)
     ij = np.arange(64).reshape(8, 8)
     assert np.array_equal(col.reshape(8, 8), (ij // 8 + ij % 8) % 2)
+
+
+def _py_replay_sqa_msc(g, init3d, thr, mode, seed):
+    """Slice-by-slice Python restatement of the bit-packed SQA replay (tiny sizes)."""
+    R, T, n = init3d.shape
+    S = init3d.astype(np.int64).copy()
+    nb = [[(int(g.indices[p]), g.data[p]) for p in range(g.indptr[i], g.indptr[i + 1])
+           if g.indices[p] != i and g.indices[p] != n and g.data[p] != 0] for i in range(n)]
+    col = O.greedy_colour(g)
+    classes = [[i for i in range(n) if col[i] == c] for c in range(max(col) + 1)]
+    upper = T - 1 if T % 2 else T
+    groups = [list(range(0, upper, 2)), list(range(1, T, 2)), [T - 1] if T % 2 else []]
+    k0, k1 = seed & 0xFFFFFFFF, seed >> 32
+    for r in range(R):
+        for k in range(thr.shape[0]):
+            always, live = int(mode[k, 0]), int(mode[k, 1])
+            for q, grp in enumerate(groups):
+                if not grp:
+                    continue
+                for cl in classes:
+                    for i in cl:
+                        before = S[r, :, i].copy()
+                        W = []
+                        for qq in range(8):
+                            W += list(O.philox4x32_10([i, k, r, (qq << 16) | (q << 8) | 0xC3], [k0, k1]))
+                        for t in grp:
+                            si = before[t]
+                            u = sum(1 for j, v in nb[i] if v * si * S[r, t, j] > 0)
+                            kk = int(before[(t + 1) % T] == si) + int(before[(t - 1) % T] == si)
+                            m = 3 * u + kk
+                            if (always >> m) & 1:
+                                S[r, t, i] = -si
+                            elif (live >> m) & 1:
+                                U = sum(((int(W[l]) >> t) & 1) << (31 - l) for l in range(32))
+                                if U < int(thr[k, m]):
+                                    S[r, t, i] = -si
+    return S.astype(np.int8)
+
+
+@pytest.mark.parametrize("T", [2, 3, 6])
+def test_bitpacked_sqa_replay_matches_python_restatement(T):
+    rng = np.random.default_rng(T)
+    n = 8  # ring of 8 with +-1 couplings: 2-regular
+    J = {(i, (i + 1) % n): float(rng.choice([-1.0, 1.0])) for i in range(n)}
+    g = O.AugCSR.from_ising(np.zeros(n), J, n)
+    ss = np.linspace(0.0, 1.0, 5)
+    betas = np.full(5, 3.0)
+    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
+    thr, mode = O.sqa_msc_thresholds(a, b, 1.0, 2)
+    init = rng.choice(np.array([-1, 1], np.int8), size=(2, T, n))
+    got = O.replay_sqa_msc(g, init, thr, mode, seed=0x1234_0000_0007)
+    want = _py_replay_sqa_msc(g, init, thr, mode, seed=0x1234_0000_0007)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_bitpacked_sqa_thresholds_classes():
+    # a = 0.25, B = -0.5: dE = 0.25*2(2-2u) - 0.5*(4-4k) for D = 2
+    thr, mode = O.sqa_msc_thresholds(np.array([0.25], np.float32), np.array([-0.5], np.float32), 1.0, 2)
+    for u in range(3):
+        for k in range(3):
+            m = 3 * u + k
+            dE = 0.25 * 2 * (2 - 2 * u) - 0.5 * (4 - 4 * k)
+            if dE <= 0:
+                assert (mode[0, 0] >> m) & 1 and thr[0, m] == 0
+            else:
+                assert (mode[0, 1] >> m) & 1
+                assert thr[0, m] == math.floor(math.exp(-dE) * 2 ** 32)
+    # s = 1 -> B = -inf: k = 1 is NaN (never), k = 0 always, k = 2 never
+    thr, mode = O.sqa_msc_thresholds(np.array([0.1], np.float32), np.array([-np.inf], np.float32), 1.0, 2)
+    for u in range(3):
+        assert (mode[0, 0] >> (3 * u)) & 1
+        assert not (mode[0, 0] >> (3 * u + 1)) & 1 and not (mode[0, 1] >> (3 * u + 1)) & 1
+        assert not (mode[0, 0] >> (3 * u + 2)) & 1 and not (mode[0, 1] >> (3 * u + 2)) & 1
