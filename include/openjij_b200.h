@@ -124,8 +124,10 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t
  * best_slice [R] (may be NULL): get_solution()'s slice, the first slice of
  * minimum energy (include/openjij/result/get_solution.hpp:59-84).
  * Kernels: OJ_KERNEL_COLOUR (any graph) or OJ_KERNEL_BITPACKED (regular
- * graph, couplings +-c, h = 0, degree <= 8, T <= 32: the T slices of a site
- * in one 32-bit word); OJ_KERNEL_AUTO takes the bit-packed one when it applies. */
+ * graph, couplings +-c, h = 0, degree <= 8): for even T <= 64 the even and
+ * the odd slices of 32/(T/2) replicas (rounded down to a power of two) in two
+ * 32-bit words per site; otherwise, for T <= 32, the T slices of one replica
+ * in one word.  OJ_KERNEL_AUTO takes the bit-packed kernel when it applies. */
 oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32_t num_slices,
                      int8_t* spins, double gamma, const double* betas, const double* s,
                      const int32_t* mcs, int32_t num_sched, uint64_t seed, int64_t first_sweep,

@@ -453,15 +453,17 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   if (R == 0 || n == 0) return OJ_OK;
   if (!spins) return arg_fail(ctx, "null spins");
   uint32_t kernel = flags & OJ_KERNEL_MASK;
+  const bool split_ok = sqa_split_applies(g, T);
   const bool msc_ok = g->info.bimodal && g->regular && T <= 32 && sqa_msc_fits(g);
-  if (kernel == OJ_KERNEL_AUTO) kernel = msc_ok ? OJ_KERNEL_BITPACKED : OJ_KERNEL_COLOUR;
+  if (kernel == OJ_KERNEL_AUTO) kernel = (split_ok || msc_ok) ? OJ_KERNEL_BITPACKED : OJ_KERNEL_COLOUR;
   if (kernel != OJ_KERNEL_COLOUR && kernel != OJ_KERNEL_BITPACKED) {
     ctx->last_error = "SQA runs on the colour-class or the bit-packed kernel";
     return OJ_ERR_UNSUPPORTED;
   }
-  if (kernel == OJ_KERNEL_BITPACKED && !msc_ok) {
+  if (kernel == OJ_KERNEL_BITPACKED && !split_ok && !msc_ok) {
     ctx->last_error =
-        "bit-packed SQA needs a regular graph with couplings +-c (degree <= 8), h = 0, T <= 32 and n <= 65535";
+        "bit-packed SQA needs a regular graph with couplings +-c (degree <= 8), h = 0 and an even T <= 64 "
+        "(or T <= 32 and n <= 65535)";
     return OJ_ERR_UNSUPPORTED;
   }
   RngBase rb;
@@ -491,7 +493,35 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   int launches = 0;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
-  if (kernel == OJ_KERNEL_BITPACKED) {
+  if (kernel == OJ_KERNEL_BITPACKED && split_ok) {
+    const int P = sqa_split_replicas_per_group(T);
+    const int G = (R + P - 1) / P;
+    std::string why;
+    const cudaError_t pe = sqa_split_prepare(g, G, ctx->sm_count, &why);
+    if (pe != cudaSuccess) {
+      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
+      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+    }
+    std::vector<uint32_t> thr, mode;
+    sqa_msc_thresholds(coef, g->info.coupling_abs, g->info.max_degree, thr, mode);
+    OJ_CK(ctx->params.ensure(std::max<size_t>((thr.size() + mode.size()) * 4, 16)), "alloc params");
+    uint32_t* d_thr = ctx->params.as<uint32_t>();
+    uint32_t* d_mode = d_thr + thr.size();
+    if (S > 0) {
+      OJ_CK(cudaMemcpyAsync(d_thr, thr.data(), thr.size() * 4, cudaMemcpyHostToDevice, st), "H2D thr");
+      OJ_CK(cudaMemcpyAsync(d_mode, mode.data(), mode.size() * 4, cudaMemcpyHostToDevice, st), "H2D mode");
+    }
+    OJ_CK(ctx->words.ensure((size_t)G * 2 * n * 4), "alloc words");
+    uint32_t* d_words = ctx->words.as<uint32_t>();
+    OJ_CK(launch_sqa_split_pack(d_spins, R, T, n, G, d_words, st), "pack");
+    ++launches;
+    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+    if (S > 0)
+      OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rb, st, &launches), "sqa slice-split kernel");
+    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+    OJ_CK(launch_sqa_split_unpack(d_words, R, T, n, G, d_spins, st), "unpack");
+    ++launches;
+  } else if (kernel == OJ_KERNEL_BITPACKED) {
     OJ_CK(sqa_msc_prepare(g), "bit-packed SQA tables");
     std::vector<uint32_t> thr, mode;
     sqa_msc_thresholds(coef, g->info.coupling_abs, g->info.max_degree, thr, mode);

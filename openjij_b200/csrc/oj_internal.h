@@ -139,6 +139,15 @@ cudaError_t sqa_msc_prepare(oj_graph* g);
 bool sqa_msc_fits(const oj_graph* g);
 cudaError_t launch_sqa_pack(const int8_t* spins, int R, int T, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_sqa_unpack(const uint32_t* words, int R, int T, int n, int8_t* spins, cudaStream_t st);
+int sqa_split_replicas_per_group(int T);
+bool sqa_split_applies(const oj_graph* g, int T);
+cudaError_t sqa_split_prepare(oj_graph* g, int G, int sm_count, std::string* why);
+cudaError_t launch_sqa_split(const oj_graph* g, int G, int T, uint32_t* words, const uint32_t* thr,
+                             const uint32_t* mode, int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
+cudaError_t launch_sqa_split_pack(const int8_t* spins, int R, int T, int n, int G, uint32_t* words,
+                                  cudaStream_t st);
+cudaError_t launch_sqa_split_unpack(const uint32_t* words, int R, int T, int n, int G, int8_t* spins,
+                                    cudaStream_t st);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,

@@ -201,7 +201,8 @@ P4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint3
 constexpr uint32_t TAG_SA = 0x5Au;       // c3 of the generic / dense SA stream
 constexpr uint32_t TAG_SQA = 0xA5u;      // low byte of c3 of the SQA stream
 constexpr uint32_t TAG_SA_MSC = 0x3Cu;   // low byte of c3 of the bit-packed SA stream
-constexpr uint32_t TAG_SQA_MSC = 0xC3u;  // low byte of c3 of the bit-packed SQA stream
+constexpr uint32_t TAG_SQA_MSC = 0xC3u;    // low byte of c3 of the bit-packed SQA stream
+constexpr uint32_t TAG_SQA_SPLIT = 0x69u;  // low byte of c3 of the slice-split SQA stream
 
 inline float f_of(uint32_t b) {
   float f;
@@ -806,6 +807,77 @@ void orc_sqa_msc_thresholds(const float* coef_a, const float* coef_b, int64_t ns
     mode[2 * k] = always;
     mode[2 * k + 1] = live;
   }
+}
+
+// Slice-split bit-packed SQA replay (regular graph, couplings +-c, h = 0, even
+// T <= 64), on spins [R][T][n].  H = T/2, P = largest power of two with
+// P*H <= 32; replica r belongs to group g = r / P and its slice t to bit
+// b = (r % P)*H + t/2 of half q = t % 2.  Order: per sweep k, half q = 0 (even
+// slices) then q = 1 (odd slices), per colour class, per site i of the class,
+// every slice t of the half:
+//   u = unsatisfied bonds of (i, t); kk = Trotter neighbours t+-1 (mod T) with
+//   the same spin; class m = 3u + kk;
+//   always[k] bit m -> flip; live[k] bit m -> flip iff U < thr[k][m], where U's
+//   bit (31 - l) is bit b of W_l = Philox(ctr = (i, k, g, (l/4) << 16 | q << 8 |
+//   TAG_SQA_SPLIT))[l % 4]; otherwise no flip.
+// The slices of one half are not Trotter neighbours of each other, so updating
+// them one after another equals deciding them together.
+void orc_replay_sqa_split(int n, const int64_t* indptr, const int32_t* indices, const double* data, int R,
+                          int T, int8_t* tspins /*[R][T][n]*/, const uint32_t* thr, const uint32_t* mode,
+                          int dmax, int64_t nsweeps, uint64_t seed, int threads) {
+  Aug g{n, indptr, indices, data};
+  Nbr b = make_nbr(g);
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  int ncol = 0;
+  for (int c : col) ncol = std::max(ncol, c + 1);
+  std::vector<std::vector<int>> by_col(ncol);
+  for (int i = 0; i < n; ++i) by_col[col[i]].push_back(i);
+  const int H = T / 2;
+  int P = 1;
+  while (2 * P * H <= 32) P *= 2;
+  const int NC = (dmax + 1) * 3;
+  const int G = (R + P - 1) / P;
+  parallel_for(G, threads, [&](int gi) {
+    for (int64_t k = 0; k < nsweeps; ++k) {
+      const uint32_t* th = thr + (size_t)k * NC;
+      const uint32_t always = mode[2 * k], live = mode[2 * k + 1];
+      for (int q = 0; q < 2; ++q)
+        for (int c = 0; c < ncol; ++c)
+          for (int i : by_col[c]) {
+            uint32_t Wl[32];
+            for (int qq = 0; qq < 8; ++qq) {
+              P4 r4 = philox((uint32_t)i, (uint32_t)k, (uint32_t)gi,
+                             ((uint32_t)qq << 16) | ((uint32_t)q << 8) | TAG_SQA_SPLIT, k0, k1);
+              for (int l = 0; l < 4; ++l) Wl[4 * qq + l] = r4.v[l];
+            }
+            for (int p = 0; p < P; ++p) {
+              const int r = gi * P + p;
+              if (r >= R) break;
+              int8_t* S = tspins + (size_t)r * T * n;
+              for (int t = q; t < T; t += 2) {
+                const int bit = p * H + t / 2;
+                const int si = S[(size_t)t * n + i];
+                int u = 0;
+                for (int64_t e = b.rp[i]; e < b.rp[i + 1]; ++e)
+                  if (b.val[e] * si * S[(size_t)t * n + b.ci[e]] > 0) ++u;
+                const int tp = (t + 1) % T, tm = (t - 1 + T) % T;
+                const int kk = (S[(size_t)tp * n + i] == si) + (S[(size_t)tm * n + i] == si);
+                const int m = 3 * u + kk;
+                bool flip = false;
+                if ((always >> m) & 1u) {
+                  flip = true;
+                } else if ((live >> m) & 1u) {
+                  uint32_t U = 0;
+                  for (int l = 0; l < 32; ++l) U |= ((Wl[l] >> bit) & 1u) << (31 - l);
+                  flip = U < th[m];
+                }
+                if (flip) S[(size_t)t * n + i] = (int8_t)-si;
+              }
+            }
+          }
+    }
+  });
 }
 
 }  // extern "C"

@@ -74,6 +74,8 @@ def lib():
         L.orc_replay_sqa_msc.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _u32p, _u32p,
                                          _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
         L.orc_sqa_msc_thresholds.argtypes = [_f32p, _f32p, C.c_int64, C.c_double, C.c_int, _u32p, _u32p]
+        L.orc_replay_sqa_split.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _u32p,
+                                           _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
         L.orc_gen_spin_seq.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _i8p]
         _lib = L
     return _lib
@@ -344,3 +346,14 @@ def replay_sqa_msc(g: AugCSR, init3d, thr, mode, seed, threads=None):
     dmax = thr.shape[1] // 3 - 1
     lib().orc_replay_sqa_msc(*g.args(), R, T, w, thr, mode, dmax, thr.shape[0], int(seed), _threads(threads))
     return unpack_slices(w, T)
+
+
+def replay_sqa_split(g: AugCSR, init3d, thr, mode, seed, threads=None):
+    """Slice-split bit-packed SQA replay on [R][T][n] spins (even T <= 64)."""
+    S = np.array(init3d, np.int8, copy=True, order="C")
+    R, T, _ = S.shape
+    thr = np.ascontiguousarray(thr, np.uint32)
+    mode = np.ascontiguousarray(mode, np.uint32)
+    dmax = thr.shape[1] // 3 - 1
+    lib().orc_replay_sqa_split(*g.args(), R, T, S, thr, mode, dmax, thr.shape[0], int(seed), _threads(threads))
+    return S

@@ -191,11 +191,22 @@ def _scaled(m, c):
     return m
 
 
-@pytest.mark.parametrize("T", [2, 5, 31, 32])
+def _sqa_bitpacked_replay(g, s0, betas, ss, mcs, c, D, seed):
+    """Even T: slice-split layout; odd T: one replica per word."""
+    T = s0.shape[1]
+    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
+    thr, mode = O.sqa_msc_thresholds(np.repeat(a, mcs), np.repeat(b, mcs), c, D)
+    if T % 2 == 0:
+        return O.replay_sqa_split(g, s0, thr, mode, seed)
+    return O.replay_sqa_msc(g, s0, thr, mode, seed)
+
+
+@pytest.mark.parametrize("T,R", [(2, 3), (2, 40), (5, 3), (10, 9), (31, 3), (32, 3), (64, 2)])
 @pytest.mark.parametrize("which", ["regular3", "lattice", "regular5_real"])
-def test_sqa_bitpacked_bit_exact(ctx, T, which):
-    """Bit-packed SQA (the T slices of a site in one word) against its replay,
-    schedule ending at s = 1 (B = -inf: NaN and +-inf energy differences)."""
+def test_sqa_bitpacked_bit_exact(ctx, T, R, which):
+    """Bit-packed SQA against its replay (even T: even / odd slices of several
+    replicas in two words; odd T: the slices of one replica in one word), with
+    a schedule ending at s = 1 (B = -inf: NaN and +-inf energy differences)."""
     if which == "regular3":
         m, c, D = I.random_regular_pm_j(48, 3, seed=7)[0], 1.0, 3
     elif which == "lattice":
@@ -203,7 +214,7 @@ def test_sqa_bitpacked_bit_exact(ctx, T, which):
     else:
         m, c, D = _scaled(I.random_regular_pm_j(60, 5, seed=2)[0], 0.37), 0.37, 5
     g, dg = _graph(ctx, m)
-    R, nsched = 3, 16
+    nsched = 16
     ss = np.linspace(0.0, 1.0, nsched)
     betas = np.full(nsched, 6.0)
     mcs = np.where(np.arange(nsched) % 3 == 0, 2, 1).astype(np.int32)
@@ -215,9 +226,7 @@ def test_sqa_bitpacked_bit_exact(ctx, T, which):
     en = np.zeros((R, T))
     st = N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=9, energies=en, best=best, kernel="bitpacked")
     assert st["kernel"] == "bitpacked"
-    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
-    thr, mode = O.sqa_msc_thresholds(np.repeat(a, mcs), np.repeat(b, mcs), c, D)
-    ref = O.replay_sqa_msc(g, s0, thr, mode, 9)
+    ref = _sqa_bitpacked_replay(g, s0, betas, ss, mcs, c, D, 9)
     np.testing.assert_array_equal(s, ref)
     for r in range(R):
         e = O.energies(g, ref[r])
@@ -226,6 +235,29 @@ def test_sqa_bitpacked_bit_exact(ctx, T, which):
         # first minimum is taken over the kernel's own energies
         assert best[r] == int(np.argmin(en[r]))
         assert e[best[r]] == pytest.approx(e.min(), abs=1e-9)
+
+
+@pytest.mark.parametrize("cluster", [None, "3", "16"])
+@pytest.mark.parametrize("which,T,R", [("lattice", 16, 4), ("regular3", 8, 20), ("regular3", 32, 6)])
+def test_sqa_slice_split_clusters(ctx, monkeypatch, cluster, which, T, R):
+    """Sites split over the CTAs of a cluster (halo refresh through distributed
+    shared memory) give the replay's spins."""
+    if cluster:
+        monkeypatch.setenv("OJ_SQA_CLUSTER", cluster)
+    if which == "lattice":
+        m, D = I.lattice_pm_j(32, seed=12)[0], 4
+    else:
+        m, D = I.random_regular_pm_j(1200, 3, seed=13)[0], 3
+    g, dg = _graph(ctx, m)
+    nsched = 10
+    ss = np.linspace(0.0, 0.9, nsched)
+    betas = np.full(nsched, 4.0)
+    mcs = np.ones(nsched, np.int32)
+    s0 = np.random.default_rng(3).choice(np.array([-1, 1], np.int8), size=(R, T, g.n))
+    s = s0.copy()
+    st = N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=21, kernel="bitpacked")
+    assert st["kernel"] == "bitpacked"
+    np.testing.assert_array_equal(s, _sqa_bitpacked_replay(g, s0, betas, ss, mcs, 1.0, D, 21))
 
 
 def test_sqa_auto_picks_bitpacked_on_regular_pm_j(ctx):
@@ -244,7 +276,7 @@ def test_sqa_auto_picks_bitpacked_on_regular_pm_j(ctx):
 def test_sqa_split_and_shard(ctx, kernel):
     m, _ = I.random_regular_pm_j(40, 3, seed=9)
     g, dg = _graph(ctx, m)
-    T, nsched = 6, 12
+    T, nsched = (6 if kernel == "bitpacked" else 5), 12
     ss = np.linspace(0.0, 1.0, nsched)
     betas = np.full(nsched, 8.0)
     mcs = np.ones(nsched, np.int32)

@@ -173,3 +173,57 @@ def test_bitpacked_sqa_thresholds_classes():
         assert (mode[0, 0] >> (3 * u)) & 1
         assert not (mode[0, 0] >> (3 * u + 1)) & 1 and not (mode[0, 1] >> (3 * u + 1)) & 1
         assert not (mode[0, 0] >> (3 * u + 2)) & 1 and not (mode[0, 1] >> (3 * u + 2)) & 1
+
+
+def _py_replay_sqa_split(g, init3d, thr, mode, seed):
+    """Python restatement of the slice-split bit-packed SQA replay (tiny sizes)."""
+    R, T, n = init3d.shape
+    H = T // 2
+    P = 1
+    while 2 * P * H <= 32:
+        P *= 2
+    S = init3d.astype(np.int64).copy()
+    nb = [[(int(g.indices[p]), g.data[p]) for p in range(g.indptr[i], g.indptr[i + 1])
+           if g.indices[p] != i and g.indices[p] != n and g.data[p] != 0] for i in range(n)]
+    col = O.greedy_colour(g)
+    classes = [[i for i in range(n) if col[i] == c] for c in range(max(col) + 1)]
+    k0, k1 = seed & 0xFFFFFFFF, seed >> 32
+    for r in range(R):
+        gi, p = divmod(r, P)
+        for k in range(thr.shape[0]):
+            always, live = int(mode[k, 0]), int(mode[k, 1])
+            for q in (0, 1):
+                for cl in classes:
+                    for i in cl:
+                        W = []
+                        for qq in range(8):
+                            W += list(O.philox4x32_10([i, k, gi, (qq << 16) | (q << 8) | 0x69], [k0, k1]))
+                        for t in range(q, T, 2):
+                            bit = p * H + t // 2
+                            si = S[r, t, i]
+                            u = sum(1 for j, v in nb[i] if v * si * S[r, t, j] > 0)
+                            kk = int(S[r, (t + 1) % T, i] == si) + int(S[r, (t - 1) % T, i] == si)
+                            m = 3 * u + kk
+                            if (always >> m) & 1:
+                                S[r, t, i] = -si
+                            elif (live >> m) & 1:
+                                U = sum(((int(W[l]) >> bit) & 1) << (31 - l) for l in range(32))
+                                if U < int(thr[k, m]):
+                                    S[r, t, i] = -si
+    return S.astype(np.int8)
+
+
+@pytest.mark.parametrize("T,R", [(2, 3), (6, 9), (32, 3)])
+def test_slice_split_sqa_replay_matches_python_restatement(T, R):
+    rng = np.random.default_rng(10 + T)
+    n = 6
+    J = {(i, (i + 1) % n): float(rng.choice([-1.0, 1.0])) for i in range(n)}
+    g = O.AugCSR.from_ising(np.zeros(n), J, n)
+    ss = np.linspace(0.0, 1.0, 3)
+    betas = np.full(3, 3.0)
+    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
+    thr, mode = O.sqa_msc_thresholds(a, b, 1.0, 2)
+    init = rng.choice(np.array([-1, 1], np.int8), size=(R, T, n))
+    got = O.replay_sqa_split(g, init, thr, mode, seed=0x9_0000_0003)
+    want = _py_replay_sqa_split(g, init, thr, mode, seed=0x9_0000_0003)
+    np.testing.assert_array_equal(got, want)
