@@ -156,6 +156,15 @@ def _workload(config, sweeps=None, replicas=None):
         S, R = 1000, 256
         w.update(name="sqa_3regular_N4096_T32_R256_S1000", kind="sqa", T=32, kernel="auto", bound="hbm",
                  gamma=1.0, beta=10.0)
+    elif config == 5:
+        mats = [m.toarray() for m, _ in I.uneven_qubo_batch(512, 64, 1024, seed=5)]
+        S = sweeps or 500
+        reads = replicas or 32
+        betas, mcs = I.geometric_betas(0.1, 10.0, S)
+        w.update(name="batched_uneven_qubo_512x_N64-1024_R32_S500", kind="batch", kernel="batched",
+                 bound="tensor", mats=mats, reads=np.full(len(mats), reads, np.int32), betas=betas, mcs=mcs,
+                 replicas=reads, sweeps=S)
+        return w
     else:
         raise SystemExit(f"unknown config {config}")
     S = sweeps or S
@@ -200,6 +209,28 @@ def cpu_reference_sqa(w, threads):
     return threads * w["T"] * g.n * float(np.sum(w["mcs"][:k])) / dt, dt
 
 
+def cpu_reference_batch(w, threads, budget_s=8.0):
+    """OpenJij's CPU path on the batch: instances in order, one read per host
+    thread each, until about ``budget_s`` seconds of work; returns attempts/s,
+    seconds and the number of instances run."""
+    from oracle import oracle as O
+    attempts, spent, count = 0.0, 0.0, 0
+    sweeps = float(np.sum(w["mcs"]))
+    for A in w["mats"]:
+        g = O.AugCSR(A)
+        rng = np.random.default_rng(count)
+        init = rng.choice(np.array([-1, 1], np.int8), size=(threads, g.n))
+        seeds = np.arange(1, threads + 1, dtype=np.uint64)
+        t0 = time.perf_counter()
+        O.ref_sa_many(g, init, w["betas"], w["mcs"], seeds, threads=threads)
+        spent += time.perf_counter() - t0
+        attempts += threads * g.n * sweeps
+        count += 1
+        if spent > budget_s:
+            break
+    return attempts / spent, spent, count
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -207,10 +238,14 @@ def run_reference(args):
     w = _workload(args.config, args.sweeps, args.replicas)
     threads = os.cpu_count() or 1
     reads = threads  # one read per host thread
+    batch_count = [0]
 
     def one():
         if w["kind"] == "sa":
             return cpu_reference(w["matrix"], w["betas"], w["mcs"], reads, threads)
+        if w["kind"] == "batch":
+            v, dt, batch_count[0] = cpu_reference_batch(w, threads, budget_s=4.0)
+            return v, dt
         return cpu_reference_sqa(w, threads)
 
     for _ in range(args.warmup):
@@ -221,8 +256,11 @@ def run_reference(args):
         vals.append(v)
         times.append(dt)
     value = float(np.mean(vals))
-    sweeps = int(np.sum(w["mcs"])) if w["kind"] == "sa" else min(int(np.sum(w["mcs"])), 100)
+    sweeps = min(int(np.sum(w["mcs"])), 100) if w["kind"] == "sqa" else int(np.sum(w["mcs"]))
     sample = f"{reads} reads x {sweeps} sweeps of {w['name']} per step, one read per host thread"
+    if w["kind"] == "batch":
+        sample = (f"the first {batch_count[0]} instances of {w['name']}, {reads} reads x {sweeps} sweeps each "
+                  f"per step, one read per host thread")
     line = {
         "impl": "reference", "metric": "spin-flip attempts/s", "value": value,
         "unit": "attempts/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -248,6 +286,120 @@ def _algo_per_attempt(w, n, kernel, degree):
             return (2 + degree) * 4.0 / (w["T"] / 2.0), "GB/s"
         return 2.0 + degree + 2.0, "GB/s"  # int8: d spatial + 2 Trotter neighbours + read + write
     return 2.0 * n, "TFLOP/s"  # one field-row update of 2n flop per attempt
+
+
+def run_ours_batch(args, w):
+    """Config 5: every instance of the batch in one oj_sa_run_batched call."""
+    import torch
+    from openjij_b200 import _native as N
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    ctx = N.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    mats, reads = w["mats"], w["reads"]
+    batch = N.Batch(ctx, mats)
+    sizes = np.array([m.shape[0] - 1 for m in mats], np.int64)
+    total = int(np.sum(reads * sizes))
+    nrep = int(np.sum(reads))
+    rng = np.random.default_rng(1000 + rank)
+    init_host = rng.choice(np.array([-1, 1], np.int8), size=total)
+    init_dev = torch.from_numpy(init_host).cuda()
+    work = torch.empty_like(init_dev)
+    energies = torch.empty(nrep, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    betas, mcs = w["betas"], w["mcs"]
+    S = int(np.sum(mcs))
+    attempts_per_step = float(total) * S
+    seed0 = 4242 + 1000003 * rank
+    inst0 = 0  # every rank runs the whole batch (weak scaling)
+
+    def step(k, spins, en, device):
+        return N.sa_run_batched(batch, reads, spins, betas, mcs, seed=seed0 + k, energies=en, device=device,
+                                instance_offset=inst0)
+
+    for k in range(args.warmup):
+        flush.zero_()
+        work.copy_(init_dev)
+        step(k, work, energies, True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kern_ms, launches = [], 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            work.copy_(init_dev)
+            st = step(args.warmup + k, work, energies, True)
+            ends[k].record(stream)
+            kern_ms.append(st["anneal_ms"])
+            launches += st["launches"] + 1
+        torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in zip(starts, ends)]))
+    kms = float(np.mean(kern_ms))
+    if dist:
+        t = torch.tensor([ms, kms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kms = float(t[0]), float(t[1])
+    value = attempts_per_step * ws / (ms / 1000.0)
+    host_spins = torch.empty(total, dtype=torch.int8).pin_memory()
+    host_e = torch.empty(nrep, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for k in range(max(1, min(args.steps, 5))):
+        host_spins.numpy()[...] = init_host
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step(k, host_spins.numpy(), host_e.numpy(), False)
+        e2e_ms.append(1000.0 * (time.perf_counter() - t0))
+    e2 = float(np.mean(e2e_ms))
+    if dist:
+        t = torch.tensor([e2], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2 = float(t[0])
+    peak, peak_kind = _tensor_peak()
+    flops = float(np.sum(reads * 2.0 * sizes * sizes)) * S  # algorithmic 2n flop per attempt
+    achieved = flops / (kms / 1000.0) / 1e12
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, dt, cnt = cpu_reference_batch(w, threads)
+        cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
+               "sample": f"the first {cnt} instances, {threads} reads x {S} sweeps each, one read per host "
+                         f"thread, {dt:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": "spin-flip attempts/s", "value": value, "unit": "attempts/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded instances)",
+            "config": {"workload": w["name"], "instances": len(mats), "spins_total": int(np.sum(sizes)),
+                       "replicas_per_instance": int(w["replicas"]), "num_sweeps": S, "kernel": "batched",
+                       "l2": "flushed between steps (256 MB write)", "attempts_per_step": attempts_per_step},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "kernel_ms": kms,
+                         "algorithmic_per_attempt": "2n flop"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": attempts_per_step * ws / (e2 / 1000.0), "unit": "attempts/s",
+                    "h2d_bytes_per_step": total, "d2h_bytes_per_step": total + 8 * nrep, "ms_per_step": e2},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
 
 
 def run_ours(args):
@@ -403,12 +555,14 @@ def main():
                     help="smaller case for profiling (default: the full 2000-sweep workload)")
     ap.add_argument("--replicas", type=int, default=None, help="smaller case for profiling")
     ap.add_argument("--config", type=int, default=2,
-                    help="benchmark configuration 1-4 (default 2: the L=128 +-J lattice)")
+                    help="benchmark configuration 1-5 (default 2: the L=128 +-J lattice)")
     ap.add_argument("--kernel", default=None,
                     help="force a kernel: colour, dense_plain, bitpacked, dense_tc (default: planner)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == 5:
+        return run_ours_batch(args, _workload(5, args.sweeps, args.replicas))
     return run_ours(args)
 
 

@@ -52,6 +52,7 @@ enum {
 
 typedef struct oj_ctx oj_ctx;
 typedef struct oj_graph oj_graph;
+typedef struct oj_batch oj_batch;
 
 typedef struct oj_graph_info {
   int32_t n;              /* number of spins (dummy excluded) */
@@ -157,6 +158,32 @@ oj_status oj_sa_run_bitpacked_noalloc(oj_ctx* ctx, const oj_graph* g, int32_t nu
  * CSRSparse::energy (dense.hpp:176-192, csr_sparse.hpp:139-155). */
 oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, const int8_t* spins,
                     uint32_t flags, double* energies);
+
+/* A batch of dense instances of uneven size for oj_sa_run_batched.  Instance
+ * k has n[k] spins (0 <= n[k] <= 1024) and its augmented (n[k]+1)^2 matrix,
+ * row-major exactly as graph.Dense.get_interactions() returns it (J with zero
+ * diagonal, h in row/column n[k], 1 in the corner; dense.hpp:117-140), at
+ * J_aug + offset[k].  Invalid matrices -> OJ_ERR_ARG.  The reference has no
+ * batch object: each instance is its own graph::Dense. */
+oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset,
+                                const double* J_aug, oj_batch** out);
+oj_status oj_batch_destroy(oj_batch* b);
+
+/* Simulated annealing of every instance of a batch in one persistent kernel
+ * launch.  Replaces a loop of SASampler.sample calls over instances
+ * (openjij/sampler/sa_sampler.py:137-329), each a per-read loop of
+ * Algorithm<SingleSpinFlip>::run (algorithm.hpp:26-56,
+ * single_spin_flip.hpp:66-95) on a graph::Dense.  reads[k] replicas of
+ * instance k; spins concatenated instance by instance, [reads[k]][n[k]] each,
+ * in/out; energies [sum reads] FP64 (may be NULL).  One schedule (betas[j],
+ * mcs[j]) for all instances.  first_sweep as in oj_sa_run; instance_offset is
+ * the global index of instance 0 (random numbers are a pure function of seed,
+ * global instance, replica, sweep and site, so a batch split over calls or
+ * GPUs reproduces the whole).  flags: OJ_DEVICE_POINTERS only. */
+oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads, int8_t* spins,
+                            const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
+                            int64_t first_sweep, int64_t instance_offset, uint32_t flags, double* energies,
+                            oj_run_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -33,7 +33,7 @@ EXPORTS = [
     "oj_version", "oj_status_string", "oj_ctx_create", "oj_ctx_destroy", "oj_ctx_set_stream",
     "oj_ctx_synchronize", "oj_ctx_last_error", "oj_graph_create_dense", "oj_graph_create_csr",
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
-    "oj_sa_run_bitpacked_noalloc",
+    "oj_sa_run_bitpacked_noalloc", "oj_batch_create_dense", "oj_batch_destroy", "oj_sa_run_batched",
 ]
 
 
@@ -89,6 +89,10 @@ def lib():
                                  C.POINTER(RunStats)]
         L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
         L.oj_sa_run_bitpacked_noalloc.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64]
+        L.oj_batch_create_dense.argtypes = [vp, i32, vp, vp, vp, C.POINTER(vp)]
+        L.oj_batch_destroy.argtypes = [vp]
+        L.oj_sa_run_batched.argtypes = [vp, vp, vp, vp, vp, vp, i32, u64, i64, i64, u32, vp,
+                                        C.POINTER(RunStats)]
         for name in EXPORTS:
             if name not in ("oj_version", "oj_status_string", "oj_ctx_last_error"):
                 getattr(L, name).restype = i32
@@ -235,3 +239,46 @@ def energy(g: Graph, spins, out=None, device=False):
     g.ctx.check(lib().oj_energy(g.ctx._h, g._h, int(R), _ptr(spins),
                                 OJ_DEVICE_POINTERS if device else 0, _ptr(out)), "oj_energy")
     return out
+
+
+class Batch:
+    """Owns an oj_batch: dense instances of uneven size, given as their
+    augmented (n+1)x(n+1) matrices (numpy arrays)."""
+
+    def __init__(self, ctx: Context, mats):
+        self.ctx = ctx
+        self.n = np.array([m.shape[0] - 1 for m in mats], np.int32)
+        sizes = np.array([(k + 1) * (k + 1) for k in self.n], np.int64)
+        self.offset = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        flat = np.concatenate([np.ascontiguousarray(m, np.float64).ravel() for m in mats]) if len(mats) \
+            else np.zeros(1)
+        self._h = C.c_void_p()
+        ctx.check(lib().oj_batch_create_dense(ctx._h, len(mats), _ptr(self.n), _ptr(self.offset), _ptr(flat),
+                                              C.byref(self._h)), "oj_batch_create_dense")
+
+    def close(self):
+        if self._h:
+            lib().oj_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sa_run_batched(b: Batch, reads, spins, betas, mcs, seed, energies=None, device=False, first_sweep=0,
+                   instance_offset=0):
+    """spins: int8, the instances' [reads[k]][n[k]] blocks concatenated."""
+    r = np.ascontiguousarray(reads, np.int32)
+    bb = np.ascontiguousarray(betas, np.float64)
+    m = np.ascontiguousarray(mcs, np.int32)
+    st = RunStats()
+    b.ctx.check(lib().oj_sa_run_batched(b.ctx._h, b._h, _ptr(r), _ptr(spins), _ptr(bb), _ptr(m), len(bb),
+                                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(first_sweep), int(instance_offset),
+                                        _flags("auto", device), _ptr(energies), C.byref(st)),
+                "oj_sa_run_batched")
+    d = st.as_dict()
+    d["kernel"] = "batched"
+    return d

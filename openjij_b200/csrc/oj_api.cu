@@ -3,8 +3,10 @@
 // ABI; every CUDA error becomes a status with a message in the context.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -201,6 +203,7 @@ oj_status oj_ctx_destroy(oj_ctx* ctx) {
     ctx->energies.release();
     ctx->best.release();
     ctx->aux.release();
+    ctx->batch.release();
     for (auto& e : ctx->ev)
       if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -610,6 +613,191 @@ oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t R, const int8_t* spi
   if (!devp) {
     OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
     OJ_CK(cudaStreamSynchronize(st), "energy");
+  }
+  return OJ_OK;
+}
+
+oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset,
+                                const double* J_aug, oj_batch** out) {
+  if (!ctx || !out || count < 0 || (count > 0 && (!n || !offset || !J_aug)))
+    return arg_fail(ctx, "null argument or negative size");
+  *out = nullptr;
+  const int nmax = batch_max_sites();
+  std::vector<int64_t> joff(count), hoff(count), j64off(count);
+  int64_t tot32 = 0, toth = 0, tot64 = 0;
+  int max_n = 0;
+  for (int32_t k = 0; k < count; ++k) {
+    if (n[k] < 0 || n[k] > nmax) return arg_fail(ctx, "batched instances need 0 <= n <= 1024");
+    if (offset[k] < 0) return arg_fail(ctx, "negative instance offset");
+    const int64_t npad = ((int64_t)n[k] + 127) / 128 * 128;
+    joff[k] = tot32;
+    hoff[k] = toth;
+    j64off[k] = tot64;
+    tot32 += (int64_t)n[k] * npad;
+    toth += npad;
+    tot64 += ((int64_t)n[k] + 1) * ((int64_t)n[k] + 1);
+    max_n = std::max(max_n, (int)n[k]);
+  }
+  std::vector<float> J32, h32;
+  std::vector<double> J64;
+  try {
+    J32.assign((size_t)std::max<int64_t>(tot32, 4), 0.0f);
+    h32.assign((size_t)std::max<int64_t>(toth, 4), 0.0f);
+    J64.assign((size_t)std::max<int64_t>(tot64, 1), 0.0);
+  } catch (...) {
+    return OJ_ERR_OOM;
+  }
+  for (int32_t k = 0; k < count; ++k) {
+    const int64_t nk = n[k], n1 = nk + 1, npad = (nk + 127) / 128 * 128;
+    const double* A = J_aug + offset[k];
+    // graph::Dense::set_interaction_matrix checks (dense.hpp:117-140)
+    if (A[nk * n1 + nk] != 1.0) return arg_fail(ctx, "the corner of an augmented matrix must be 1");
+    for (int64_t i = 0; i < n1; ++i) {
+      if (i < nk && A[i * n1 + i] != 0.0) return arg_fail(ctx, "the diagonal of J must be zero (h goes in column n)");
+      for (int64_t j = i + 1; j < n1; ++j)
+        if (A[i * n1 + j] != A[j * n1 + i]) return arg_fail(ctx, "an augmented matrix is not symmetric");
+    }
+    for (int64_t i = 0; i < nk; ++i) {
+      for (int64_t j = 0; j < nk; ++j) J32[(size_t)(joff[k] + i * npad + j)] = (float)A[i * n1 + j];
+      h32[(size_t)(hoff[k] + i)] = (float)A[i * n1 + nk];
+    }
+    std::memcpy(J64.data() + j64off[k], A, (size_t)(n1 * n1) * sizeof(double));
+  }
+  std::unique_ptr<oj_batch> b(new oj_batch());
+  b->device = ctx->device;
+  b->count = count;
+  b->max_n = max_n;
+  b->n.assign(n, n + count);
+  DeviceGuard dg(ctx->device);
+  auto up = [&](DevBuf& d, const void* src, size_t bytes) -> cudaError_t {
+    cudaError_t e = d.ensure(std::max<size_t>(bytes, 16));
+    if (e != cudaSuccess) return e;
+    return bytes ? cudaMemcpy(d.ptr, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  OJ_CK(up(b->d_J, J32.data(), J32.size() * 4), "upload J");
+  OJ_CK(up(b->d_h, h32.data(), h32.size() * 4), "upload h");
+  OJ_CK(up(b->d_J64, J64.data(), J64.size() * 8), "upload J64");
+  OJ_CK(up(b->d_joff, joff.data(), joff.size() * 8), "upload offsets");
+  OJ_CK(up(b->d_hoff, hoff.data(), hoff.size() * 8), "upload offsets");
+  OJ_CK(up(b->d_j64off, j64off.data(), j64off.size() * 8), "upload offsets");
+  OJ_CK(up(b->d_n, n, (size_t)count * 4), "upload sizes");
+  *out = b.release();
+  return OJ_OK;
+}
+
+oj_status oj_batch_destroy(oj_batch* b) {
+  delete b;
+  return OJ_OK;
+}
+
+oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads, int8_t* spins,
+                            const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
+                            int64_t first_sweep, int64_t instance_offset, uint32_t flags, double* energies,
+                            oj_run_stats* stats) {
+  if (!ctx || !b || num_sched < 0 || (b->count > 0 && !reads)) return arg_fail(ctx, "null argument or negative size");
+  if (num_sched > 0 && (!betas || !mcs)) return arg_fail(ctx, "null schedule");
+  if (b->device != ctx->device) return arg_fail(ctx, "batch belongs to another device");
+  if (instance_offset < 0 || instance_offset + b->count > (1 << 24))
+    return arg_fail(ctx, "instance_offset + count must be below 2^24");
+  if ((flags & OJ_KERNEL_MASK) != OJ_KERNEL_AUTO) {
+    ctx->last_error = "batched SA has a single kernel; pass OJ_KERNEL_AUTO";
+    return OJ_ERR_UNSUPPORTED;
+  }
+  for (int32_t k = 0; k < num_sched; ++k)
+    if (!(betas[k] >= 0.0) || std::isinf(betas[k])) return arg_fail(ctx, "beta must be finite and >= 0");
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  const int count = b->count;
+  std::vector<int64_t> soff(count), eoff(count);
+  int64_t sbytes = 0, nrep = 0;
+  int max_reads = 0;
+  double attempts_per_sweep = 0.0;
+  std::vector<int32_t> items;
+  const int W = batch_warps();
+  for (int k = 0; k < count; ++k) {
+    if (reads[k] < 0) return arg_fail(ctx, "negative read count");
+    soff[k] = sbytes;
+    eoff[k] = nrep;
+    sbytes += (int64_t)reads[k] * b->n[k];
+    nrep += reads[k];
+    max_reads = std::max(max_reads, (int)reads[k]);
+    attempts_per_sweep += (double)reads[k] * b->n[k];
+  }
+  if (nrep == 0) return OJ_OK;
+  if (!spins && sbytes > 0) return arg_fail(ctx, "null spins");
+  // work items (instance, group of W replicas), longest instance first
+  std::vector<int> order(count);
+  for (int k = 0; k < count; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->n[x] > b->n[y]; });
+  for (int k : order) {
+    if (b->n[k] == 0) continue;
+    for (int gq = 0; gq * W < reads[k]; ++gq) {
+      items.push_back(k);
+      items.push_back(gq);
+    }
+  }
+  const int nitems = (int)(items.size() / 2);
+  RngBase rb;
+  if (oj_status st_ = rng_base(ctx, seed, first_sweep, 0, &rb)) return st_;
+  DeviceGuard dg(ctx->device);
+  std::vector<double> bexp;
+  if (oj_status st_ = expand(ctx, betas, mcs, num_sched, bexp)) return st_;
+  const int64_t S = (int64_t)bexp.size();
+  std::vector<float> bf(bexp.begin(), bexp.end());
+  const bool devp = (flags & OJ_DEVICE_POINTERS) != 0;
+  cudaStream_t st = ctx->stream;
+  int8_t* d_spins = spins;
+  if (!devp) {
+    OJ_CK(ctx->spins.ensure(std::max<int64_t>(sbytes, 16)), "alloc spins");
+    d_spins = ctx->spins.as<int8_t>();
+  } else if (sbytes > 0 && !is_device_ptr(spins)) {
+    return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
+  }
+  // one staging buffer: reads | soff | eoff | items | counter | betas
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t b_reads = al((size_t)count * 4), b_soff = al((size_t)count * 8), b_eoff = al((size_t)count * 8),
+               b_items = al(items.size() * 4 + 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4);
+  OJ_CK(ctx->batch.ensure(b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta), "alloc batch tables");
+  char* base = ctx->batch.as<char>();
+  int32_t* d_reads = reinterpret_cast<int32_t*>(base);
+  int64_t* d_soff = reinterpret_cast<int64_t*>(base + b_reads);
+  int64_t* d_eoff = reinterpret_cast<int64_t*>(base + b_reads + b_soff);
+  int32_t* d_items = reinterpret_cast<int32_t*>(base + b_reads + b_soff + b_eoff);
+  int* d_counter = reinterpret_cast<int*>(base + b_reads + b_soff + b_eoff + b_items);
+  float* d_beta = reinterpret_cast<float*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt);
+  int launches = 0;
+  OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
+  if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(d_spins, spins, sbytes, cudaMemcpyHostToDevice, st), "H2D spins");
+  OJ_CK(cudaMemcpyAsync(d_reads, reads, (size_t)count * 4, cudaMemcpyHostToDevice, st), "H2D reads");
+  OJ_CK(cudaMemcpyAsync(d_soff, soff.data(), (size_t)count * 8, cudaMemcpyHostToDevice, st), "H2D offsets");
+  OJ_CK(cudaMemcpyAsync(d_eoff, eoff.data(), (size_t)count * 8, cudaMemcpyHostToDevice, st), "H2D offsets");
+  if (nitems) OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
+  if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+  OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+  if (S > 0 && nitems > 0)
+    OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
+                          (uint32_t)instance_offset, ctx->sm_count, st, &launches),
+          "sa batched kernel");
+  OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  if (energies) {
+    double* d_e = devp ? energies : nullptr;
+    if (!d_e) {
+      OJ_CK(ctx->energies.ensure((size_t)nrep * 8), "alloc energies");
+      d_e = ctx->energies.as<double>();
+    }
+    OJ_CK(launch_batch_energy(b, d_reads, d_soff, d_eoff, max_reads, d_spins, d_e, st), "batch energy kernel");
+    ++launches;
+    if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)nrep * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+  }
+  if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(spins, d_spins, sbytes, cudaMemcpyDeviceToHost, st), "D2H spins");
+  OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
+  OJ_CK(cudaStreamSynchronize(st), "run");
+  if (stats) {
+    stats->kernel = 0;
+    stats->launches = launches;
+    stats->sweeps = S;
+    stats->attempts = attempts_per_sweep * (double)S;
+    cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
   }
   return OJ_OK;
 }

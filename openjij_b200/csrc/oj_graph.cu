@@ -16,6 +16,20 @@
 
 #include "oj_internal.h"
 
+oj_batch::~oj_batch() {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  d_J.release();
+  d_h.release();
+  d_J64.release();
+  d_joff.release();
+  d_hoff.release();
+  d_j64off.release();
+  d_n.release();
+  if (cur >= 0 && cur != device) cudaSetDevice(cur);
+}
+
 oj_graph::~oj_graph() {
   int cur = -1;
   cudaGetDevice(&cur);

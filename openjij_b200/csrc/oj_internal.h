@@ -98,13 +98,25 @@ struct oj_graph {
   ~oj_graph();
 };
 
+// A batch of dense instances for the batched SA kernel: FP32 J with rows
+// padded to a multiple of 128 columns and FP32 h (the dynamics), and the FP64
+// augmented matrices as received (the energies).
+struct oj_batch {
+  int device = 0;
+  int count = 0;
+  int max_n = 0;
+  std::vector<int32_t> n;
+  oj::DevBuf d_J, d_h, d_J64, d_joff, d_hoff, d_j64off, d_n;
+  ~oj_batch();
+};
+
 struct oj_ctx {
   int device = 0;
   int sm_count = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string last_error;
-  oj::DevBuf spins, words, params, energies, best, aux;
+  oj::DevBuf spins, words, params, energies, best, aux, batch;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -148,6 +160,15 @@ cudaError_t launch_sqa_split_pack(const int8_t* spins, int R, int T, int n, int 
                                   cudaStream_t st);
 cudaError_t launch_sqa_split_unpack(const uint32_t* words, int R, int T, int n, int G, int8_t* spins,
                                     cudaStream_t st);
+int batch_max_sites();
+int batch_warps();
+cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                            const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
+                            int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
+                            int* launches);
+cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                                const int64_t* d_eoff, int max_reads, const int8_t* spins, double* out,
+                                cudaStream_t st);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,

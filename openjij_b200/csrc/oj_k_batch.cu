@@ -1,0 +1,262 @@
+// Batched dense SA over many instances of uneven size in one persistent launch.
+//
+// Work item = (instance m, group of up to kBatchWarps replicas of m).  Items
+// are ordered by decreasing n (longest first) and handed out through an atomic
+// counter, so the CTAs resident on the SMs keep pulling the next largest item
+// until the queue is empty.  One warp runs one replica: its FP32 local fields
+// live in the warp's slice of shared memory, laid out in 128-site chunks with
+// lane l owning sites 4l..4l+3 of every chunk (one float4 per lane), and its
+// spins are bits of one register per lane (bit 4c+e = site 128c+4l+e is -1).
+//
+// Update order and acceptance are the reference's sequential single-spin flip
+// (include/openjij/updater/single_spin_flip.hpp:66-95): sites 0..n-1 in order,
+// accept when dE <= 0 or beta*dE < -ln(u), dE = -2 s_i f_i, and on a flip every
+// field moves by -2 s_i J_ij (f_j = fma(c, J_ij, f_j), c = -2 s_i: the product
+// is exact, so this is the reference's dE += 4 s_i J_ij s_j rounded once).
+// Within a chunk the warp evaluates the acceptance of all 128 sites at once from
+// the current fields, jumps to the first accepted site, applies that flip and
+// re-evaluates the sites after it: sites that do not flip leave the state
+// unchanged, so this is the sequential sweep, with one step per flip instead
+// of one per site.  The uniform of site i, sweep k, replica r of instance m is
+// Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3].
+//
+// J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
+// read through L1 one float4 per lane on every accepted flip; h likewise.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "oj_device.cuh"
+#include "oj_internal.h"
+
+namespace oj {
+namespace {
+
+constexpr int kBatchWarps = 8;
+constexpr int kBatchMaxN = 1024;
+
+struct BatchArgs {
+  const float* J;          // concatenated padded rows
+  const float* h;          // concatenated padded fields
+  const int64_t* joff;     // [count] offset of instance m's J (floats)
+  const int64_t* hoff;     // [count] offset of instance m's h (floats)
+  const int32_t* n;        // [count]
+  const int32_t* reads;    // [count]
+  const int64_t* soff;     // [count] offset of instance m's spins (bytes)
+  const int32_t* items;    // [nitems][2] (instance, replica group), longest instance first
+  int nitems;
+  int* counter;            // work-queue head, zero at launch
+  int8_t* spins;
+  const float* betas;
+  int64_t nsweeps;
+  ojd::Keys keys;
+  uint32_t sweep0;
+  uint32_t inst0;          // global index of instance 0
+};
+
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+__global__ void __launch_bounds__(kBatchWarps * 32) sa_batch_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) float shb[];
+  __shared__ int item_sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* f = shb + (size_t)warp * kBatchMaxN;  // this warp's fields, float4 per lane per chunk
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int item = item_sh;
+    if (item >= a.nitems) break;
+    const int m = a.items[2 * item];
+    const int r = a.items[2 * item + 1] * kBatchWarps + warp;
+    const int n = a.n[m];
+    if (r >= a.reads[m]) continue;  // no block-wide barrier until the next item
+    const int nch = (n + 127) >> 7;
+    const int npad = nch << 7;
+    const float* J = a.J + a.joff[m];
+    const float* h = a.h + a.hoff[m];
+    int8_t* gs = a.spins + a.soff[m] + (size_t)r * n;
+    // spins -> bits
+    uint32_t sb = 0u;
+    for (int c = 0; c < nch; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int i = 128 * c + 4 * lane + e;
+        if (i < n && gs[i] < 0) sb |= 1u << (4 * c + e);
+      }
+    // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j)
+    for (int c = 0; c < nch; ++c) {
+      float4 acc = ldg4(h + 128 * c + 4 * lane);
+      for (int i = 0; i < n; ++i) {
+        const uint32_t wi = __shfl_sync(0xffffffffu, sb, (i & 127) >> 2);
+        const bool neg = (wi >> (4 * (i >> 7) + (i & 3))) & 1u;
+        const float4 v = ldg4(J + (size_t)i * npad + 128 * c + 4 * lane);
+        acc.x = __fadd_rn(acc.x, neg ? -v.x : v.x);
+        acc.y = __fadd_rn(acc.y, neg ? -v.y : v.y);
+        acc.z = __fadd_rn(acc.z, neg ? -v.z : v.z);
+        acc.w = __fadd_rn(acc.w, neg ? -v.w : v.w);
+      }
+      reinterpret_cast<float4*>(f)[32 * c + lane] = acc;
+    }
+    __syncwarp();
+    const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
+    for (int64_t k = 0; k < a.nsweeps; ++k) {
+      const float beta = __ldg(a.betas + k);
+      const uint32_t kk = a.sweep0 + (uint32_t)k;
+      for (int c = 0; c < nch; ++c) {
+        const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, (uint32_t)r, tag, a.keys);
+        float L[4];
+        L[0] = ojd::neglog(x.x);
+        L[1] = ojd::neglog(x.y);
+        L[2] = ojd::neglog(x.z);
+        L[3] = ojd::neglog(x.w);
+        int pos = 0;  // chunk-local index of the first site not yet decided
+        for (;;) {
+          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
+          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
+          uint32_t mask = 0u;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int t = 4 * lane + e;
+            const bool neg = (sb >> (4 * c + e)) & 1u;
+            const float dE = neg ? 2.0f * fv[e] : -2.0f * fv[e];
+            const bool acc = dE <= 0.0f || __fmul_rn(beta, dE) < L[e];
+            if (acc && t >= pos && 128 * c + t < n) mask |= 1u << e;
+          }
+          const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
+          if (!lanes) break;
+          const int ls = __ffs(lanes) - 1;
+          const uint32_t ms = __shfl_sync(0xffffffffu, mask, ls);
+          const int es = __ffs(ms) - 1;
+          const uint32_t ws = __shfl_sync(0xffffffffu, sb, ls);
+          const bool neg = (ws >> (4 * c + es)) & 1u;
+          const float coef = neg ? 2.0f : -2.0f;
+          const int i = 128 * c + 4 * ls + es;
+          const float* Ji = J + (size_t)i * npad + 4 * lane;
+          for (int c2 = 0; c2 < nch; ++c2) {
+            const float4 v = ldg4(Ji + 128 * c2);
+            float4 g = reinterpret_cast<const float4*>(f)[32 * c2 + lane];
+            g.x = __fmaf_rn(coef, v.x, g.x);
+            g.y = __fmaf_rn(coef, v.y, g.y);
+            g.z = __fmaf_rn(coef, v.z, g.z);
+            g.w = __fmaf_rn(coef, v.w, g.w);
+            reinterpret_cast<float4*>(f)[32 * c2 + lane] = g;
+          }
+          if (lane == ls) sb ^= 1u << (4 * c + es);
+          pos = 4 * ls + es + 1;
+          __syncwarp();
+        }
+      }
+    }
+    for (int c = 0; c < nch; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int i = 128 * c + 4 * lane + e;
+        if (i < n) gs[i] = ((sb >> (4 * c + e)) & 1u) ? (int8_t)-1 : (int8_t)1;
+      }
+    __syncwarp();
+  }
+}
+
+// FP64 energy of every replica: E = sum_{i<j} J_ij s_i s_j + sum_i h_i s_i
+// (dense.hpp:176-192) from the FP64 augmented matrix.  One CTA per (instance,
+// 32 replicas): the spins are staged as one word per site (bit = replica), a
+// lane accumulates its replica, warps take rows round-robin and the per-warp
+// partial sums are added in warp order, so the result does not depend on timing.
+__global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restrict__ J64,
+                                                           const int64_t* __restrict__ j64off,
+                                                           const int32_t* __restrict__ n_arr,
+                                                           const int32_t* __restrict__ reads,
+                                                           const int64_t* __restrict__ soff,
+                                                           const int64_t* __restrict__ eoff,
+                                                           const int8_t* __restrict__ spins, double* __restrict__ out) {
+  __shared__ uint32_t wsh[kBatchMaxN];
+  __shared__ double part[8][32];
+  const int m = blockIdx.x;
+  const int r0 = 32 * blockIdx.y;
+  const int R = reads[m];
+  if (r0 >= R) return;
+  const int n = n_arr[m];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int8_t* s = spins + soff[m];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    uint32_t w = 0u;
+    for (int q = 0; q < 32 && r0 + q < R; ++q)
+      if (s[(size_t)(r0 + q) * n + j] < 0) w |= 1u << q;
+    wsh[j] = w;
+  }
+  __syncthreads();
+  const double* A = J64 + j64off[m];  // augmented (n+1)^2, row-major
+  double acc = 0.0;
+  for (int i = warp; i < n; i += 8) {
+    const double* Ai = A + (size_t)i * (n + 1);
+    const uint32_t wi = wsh[i];
+    double row = 0.0;
+    for (int j = i + 1; j < n; ++j) {
+      const double v = __ldg(Ai + j);
+      row += ((wi ^ wsh[j]) >> lane) & 1u ? -v : v;
+    }
+    const double hv = __ldg(Ai + n);
+    acc += row + (((wi >> lane) & 1u) ? -hv : hv);
+  }
+  part[warp][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && r0 + lane < R) {
+    double e = 0.0;
+    for (int w = 0; w < 8; ++w) e += part[w][lane];
+    out[eoff[m] + r0 + lane] = e;
+  }
+}
+
+}  // namespace
+
+int batch_max_sites() { return kBatchMaxN; }
+int batch_warps() { return kBatchWarps; }
+
+cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                            const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
+                            int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
+                            int* launches) {
+  const size_t smem = (size_t)kBatchWarps * kBatchMaxN * sizeof(float);
+  auto kern = sa_batch_kernel;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchWarps * 32, smem);
+  if (e != cudaSuccess) return e;
+  const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sm_count));
+  BatchArgs a;
+  a.J = b->d_J.as<float>();
+  a.h = b->d_h.as<float>();
+  a.joff = b->d_joff.as<int64_t>();
+  a.hoff = b->d_hoff.as<int64_t>();
+  a.n = b->d_n.as<int32_t>();
+  a.reads = d_reads;
+  a.soff = d_soff;
+  a.items = d_items;
+  a.nitems = nitems;
+  a.counter = d_counter;
+  a.spins = spins;
+  a.betas = betas;
+  a.nsweeps = nsweeps;
+  a.keys = ojd::make_keys(rb.k0, rb.k1);
+  a.sweep0 = rb.sweep0;
+  a.inst0 = inst0;
+  e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, kBatchWarps * 32, smem, st>>>(a);
+  if (launches) ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                                const int64_t* d_eoff, int max_reads, const int8_t* spins, double* out,
+                                cudaStream_t st) {
+  if (b->count == 0 || max_reads == 0) return cudaSuccess;
+  dim3 grid(b->count, (max_reads + 31) / 32);
+  batch_energy_kernel<<<grid, 256, 0, st>>>(b->d_J64.as<double>(), b->d_j64off.as<int64_t>(), b->d_n.as<int32_t>(),
+                                            d_reads, d_soff, d_eoff, spins, out);
+  return cudaGetLastError();
+}
+
+}  // namespace oj

@@ -203,6 +203,7 @@ constexpr uint32_t TAG_SQA = 0xA5u;      // low byte of c3 of the SQA stream
 constexpr uint32_t TAG_SA_MSC = 0x3Cu;   // low byte of c3 of the bit-packed SA stream
 constexpr uint32_t TAG_SQA_MSC = 0xC3u;    // low byte of c3 of the bit-packed SQA stream
 constexpr uint32_t TAG_SQA_SPLIT = 0x69u;  // low byte of c3 of the slice-split SQA stream
+constexpr uint32_t TAG_BATCH = 0x96u;      // low byte of c3 of the batched dense SA stream
 
 inline float f_of(uint32_t b) {
   float f;
@@ -876,6 +877,62 @@ void orc_replay_sqa_split(int n, const int64_t* indptr, const int32_t* indices, 
               }
             }
           }
+    }
+  });
+}
+
+// Batched dense SA replay.  Instance m has n[m] spins and its augmented
+// (n+1)^2 FP64 matrix at J_aug + offset[m]; the dynamics use FP32 J and h.
+// Each replica r of instance m runs the sequential sweep of mode 1 above
+// (sites 0..n-1, accept when dE <= 0 or beta*dE < -ln(u), fields moved by
+// c*J_ij with c = -2 s_i) with u(m, r, k, i) = Philox(ctr = (i >> 2, k, r,
+// (inst0 + m) << 8 | TAG_BATCH))[i & 3].  spins: the instances' [reads[m]][n[m]]
+// blocks concatenated.
+void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset, const double* J_aug,
+                         const int32_t* reads, int8_t* spins, const float* betas_f, int64_t nsweeps,
+                         uint64_t seed, uint32_t inst0, int threads) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  std::vector<int64_t> soff(count + 1, 0);
+  std::vector<int> rm, rr;  // flattened (instance, replica)
+  for (int m = 0; m < count; ++m) {
+    soff[m + 1] = soff[m] + (int64_t)reads[m] * n_arr[m];
+    for (int r = 0; r < reads[m]; ++r) {
+      rm.push_back(m);
+      rr.push_back(r);
+    }
+  }
+  parallel_for((int)rm.size(), threads, [&](int q) {
+    const int m = rm[q], r = rr[q], n = n_arr[m];
+    const int64_t n1 = n + 1;
+    const double* A = J_aug + offset[m];
+    std::vector<float> J((size_t)n * n), h(n), f(n);
+    for (int i = 0; i < n; ++i) {
+      for (int j = 0; j < n; ++j) J[(size_t)i * n + j] = (float)A[i * n1 + j];
+      h[i] = (float)A[i * n1 + n];
+    }
+    int8_t* s = spins + soff[m] + (size_t)r * n;
+    for (int j = 0; j < n; ++j) {
+      float acc = h[j];
+      for (int i = 0; i < n; ++i) {
+        const float v = J[(size_t)i * n + j];
+        acc = acc + (s[i] > 0 ? v : -v);
+      }
+      f[j] = acc;
+    }
+    const uint32_t tag = ((inst0 + (uint32_t)m) << 8) | TAG_BATCH;
+    for (int64_t k = 0; k < nsweeps; ++k) {
+      const float beta = betas_f[k];
+      for (int i = 0; i < n; ++i) {
+        const float dE = s[i] > 0 ? -2.0f * f[i] : 2.0f * f[i];
+        const P4 u = philox((uint32_t)(i >> 2), (uint32_t)k, (uint32_t)r, tag, k0, k1);
+        const float L = neglog(u.v[i & 3]);
+        if (dE <= 0.0f || beta * dE < L) {
+          const float c = s[i] > 0 ? -2.0f : 2.0f;
+          const float* Ji = &J[(size_t)i * n];
+          for (int j = 0; j < n; ++j) f[j] = f[j] + c * Ji[j];
+          s[i] = (int8_t)-s[i];
+        }
+      }
     }
   });
 }

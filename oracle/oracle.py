@@ -76,6 +76,8 @@ def lib():
         L.orc_sqa_msc_thresholds.argtypes = [_f32p, _f32p, C.c_int64, C.c_double, C.c_int, _u32p, _u32p]
         L.orc_replay_sqa_split.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _u32p,
                                            _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
+        L.orc_replay_sa_batch.argtypes = [C.c_int, _i32p, _i64p, _f64p, _i32p, _i8p, _f32p, C.c_int64,
+                                          C.c_uint64, C.c_uint32, C.c_int]
         L.orc_gen_spin_seq.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _i8p]
         _lib = L
     return _lib
@@ -357,3 +359,17 @@ def replay_sqa_split(g: AugCSR, init3d, thr, mode, seed, threads=None):
     dmax = thr.shape[1] // 3 - 1
     lib().orc_replay_sqa_split(*g.args(), R, T, S, thr, mode, dmax, thr.shape[0], int(seed), _threads(threads))
     return S
+
+
+def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, threads=None):
+    """Batched dense SA replay; mats: augmented (n+1)x(n+1) FP64 matrices,
+    spins_flat: the instances' [reads[m]][n[m]] int8 blocks concatenated."""
+    n = np.array([m.shape[0] - 1 for m in mats], np.int32)
+    sizes = np.array([(k + 1) * (k + 1) for k in n], np.int64)
+    offset = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    flat = np.ascontiguousarray(np.concatenate([np.asarray(m, np.float64).ravel() for m in mats]))
+    s = np.array(spins_flat, np.int8, copy=True)
+    b = np.ascontiguousarray(betas_per_sweep, np.float32)
+    lib().orc_replay_sa_batch(len(mats), n, offset, flat, np.ascontiguousarray(reads, np.int32), s, b, len(b),
+                              int(seed), int(inst0), _threads(threads))
+    return s

@@ -1,0 +1,110 @@
+"""Batched uneven-size dense SA (oj_sa_run_batched) against its CPU replay,
+spin for spin, through the C ABI."""
+import numpy as np
+import pytest
+
+from openjij_b200 import _native as N
+from openjij_b200 import instances as I
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _int_batch(sizes, seed):
+    return [I.dense_qubo_int(int(n), seed=seed + k)[0].toarray() for k, n in enumerate(sizes)]
+
+
+def _normal_batch(sizes, seed):
+    return [I.dense_qubo_normal(int(n), seed=seed + k)[0].toarray() for k, n in enumerate(sizes)]
+
+
+def _spins(mats, reads, seed):
+    total = sum(r * (m.shape[0] - 1) for r, m in zip(reads, mats))
+    return np.random.default_rng(seed).choice(np.array([-1, 1], np.int8), size=total)
+
+
+def _per_sweep(betas, mcs):
+    return np.repeat(np.asarray(betas, np.float64), mcs).astype(np.float32)
+
+
+def _energies(mats, reads, spins):
+    out, off = [], 0
+    for m, r in zip(mats, reads):
+        n = m.shape[0] - 1
+        g = O.AugCSR(m)
+        for q in range(r):
+            out.append(O.energy(g, spins[off + q * n: off + (q + 1) * n]))
+        off += r * n
+    return np.array(out)
+
+
+@pytest.mark.parametrize("kind", ["integer", "normal"])
+def test_batched_bit_exact(ctx, kind):
+    sizes = [1, 7, 64, 130, 300, 1024, 255, 129]
+    reads = [1, 3, 8, 9, 17, 2, 0, 33]
+    mats = _int_batch(sizes, 40) if kind == "integer" else _normal_batch(sizes, 50)
+    b = N.Batch(ctx, mats)
+    betas, mcs = I.geometric_betas(0.1, 10.0, 30)
+    s0 = _spins(mats, reads, 1)
+    s = s0.copy()
+    e = np.zeros(sum(reads))
+    st = N.sa_run_batched(b, reads, s, betas, mcs, seed=77, energies=e)
+    assert st["launches"] == 2 and st["attempts"] == sum(r * n for r, n in zip(reads, sizes)) * 30
+    ref = O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), 77)
+    np.testing.assert_array_equal(s, ref)
+    want = _energies(mats, reads, ref)
+    np.testing.assert_allclose(e, want, rtol=1e-12, atol=1e-9)
+
+
+def test_batched_split_over_calls_and_instances(ctx):
+    """Sweeps split over two calls (first_sweep) and instances split over two
+    batches (instance_offset) reproduce the single run."""
+    sizes = [90, 200, 33, 140]
+    reads = [5, 3, 8, 2]
+    mats = _int_batch(sizes, 60)
+    betas, mcs = I.geometric_betas(0.2, 5.0, 20)
+    s0 = _spins(mats, reads, 2)
+    whole = s0.copy()
+    N.sa_run_batched(N.Batch(ctx, mats), reads, whole, betas, mcs, seed=5)
+    cut = reads[0] * sizes[0] + reads[1] * sizes[1]
+    a, b = s0[:cut].copy(), s0[cut:].copy()
+    ba, bb = N.Batch(ctx, mats[:2]), N.Batch(ctx, mats[2:])
+    for part, bt, off, rd in ((a, ba, 0, reads[:2]), (b, bb, 2, reads[2:])):
+        N.sa_run_batched(bt, rd, part, betas[:7], mcs[:7], seed=5, instance_offset=off)
+        N.sa_run_batched(bt, rd, part, betas[7:], mcs[7:], seed=5, instance_offset=off,
+                         first_sweep=int(np.sum(mcs[:7])))
+    np.testing.assert_array_equal(np.concatenate([a, b]), whole)
+
+
+def test_batched_device_pointers(ctx):
+    import torch
+    sizes, reads = [100, 260], [4, 6]
+    mats = _normal_batch(sizes, 70)
+    b = N.Batch(ctx, mats)
+    betas, mcs = I.geometric_betas(0.1, 3.0, 10)
+    s0 = _spins(mats, reads, 3)
+    sd = torch.from_numpy(s0.copy()).cuda()
+    ed = torch.zeros(sum(reads), dtype=torch.float64, device="cuda")
+    N.sa_run_batched(b, reads, sd, betas, mcs, seed=9, energies=ed, device=True)
+    ctx.synchronize()
+    ref = O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), 9)
+    np.testing.assert_array_equal(sd.cpu().numpy(), ref)
+    np.testing.assert_allclose(ed.cpu().numpy(), _energies(mats, reads, ref), rtol=1e-12, atol=1e-9)
+
+
+def test_batched_rejects_bad_input(ctx):
+    big = np.zeros((1026, 1026))
+    big[-1, -1] = 1.0
+    with pytest.raises(N.OJError) as ei:
+        N.Batch(ctx, [big])
+    assert ei.value.status == N.OJ_ERR_ARG
+    asym = _int_batch([5], 1)[0]
+    asym[0, 1] += 1.0
+    with pytest.raises(N.OJError) as ei:
+        N.Batch(ctx, [asym])
+    assert ei.value.status == N.OJ_ERR_ARG
+    b = N.Batch(ctx, _int_batch([5], 1))
+    with pytest.raises(N.OJError):
+        N.sa_run_batched(b, [-1], np.zeros(5, np.int8), [1.0], [1], seed=1)
+    # no replicas at all: nothing runs
+    N.sa_run_batched(b, [0], np.zeros(0, np.int8), [1.0], [1], seed=1)

@@ -227,3 +227,50 @@ def test_slice_split_sqa_replay_matches_python_restatement(T, R):
     got = O.replay_sqa_split(g, init, thr, mode, seed=0x9_0000_0003)
     want = _py_replay_sqa_split(g, init, thr, mode, seed=0x9_0000_0003)
     np.testing.assert_array_equal(got, want)
+
+
+def _py_replay_sa_batch(mats, reads, spins, betas, seed, inst0=0):
+    """Python restatement of the batched dense SA replay (tiny sizes)."""
+    out = np.array(spins, np.int64)
+    k0, k1 = seed & 0xFFFFFFFF, seed >> 32
+    off = 0
+    for m, A in enumerate(mats):
+        n = A.shape[0] - 1
+        J = A[:n, :n].astype(np.float32)
+        h = A[:n, n].astype(np.float32)
+        for r in range(reads[m]):
+            s = out[off + r * n: off + (r + 1) * n]
+            f = np.zeros(n, np.float32)
+            for j in range(n):
+                acc = np.float32(h[j])
+                for i in range(n):
+                    acc = np.float32(acc + (J[i, j] if s[i] > 0 else -J[i, j]))
+                f[j] = acc
+            for k, beta in enumerate(np.asarray(betas, np.float32)):
+                for i in range(n):
+                    dE = np.float32(-2.0) * f[i] if s[i] > 0 else np.float32(2.0) * f[i]
+                    u = O.philox4x32_10([i >> 2, k, r, ((inst0 + m) << 8) | 0x96], [k0, k1])[i & 3]
+                    if dE <= 0 or np.float32(beta * dE) < np.float32(O.neglog(int(u))):
+                        c = np.float32(-2.0 if s[i] > 0 else 2.0)
+                        f = (f + c * J[i]).astype(np.float32)
+                        s[i] = -s[i]
+        off += reads[m] * n
+    return out.astype(np.int8)
+
+
+def test_batched_replay_matches_python_restatement():
+    rng = np.random.default_rng(7)
+    mats = []
+    for n in (5, 3, 6):
+        Q = np.triu(rng.standard_normal((n, n)).astype(np.float32).astype(np.float64))
+        A = np.zeros((n + 1, n + 1))
+        A[:n, :n] = np.triu(Q, 1) + np.triu(Q, 1).T
+        A[:n, n] = A[n, :n] = np.diag(Q)
+        A[n, n] = 1.0
+        mats.append(A)
+    reads = [2, 3, 1]
+    spins = rng.choice(np.array([-1, 1], np.int8), size=sum(r * (m.shape[0] - 1) for r, m in zip(reads, mats)))
+    betas = np.array([0.3, 1.0, 2.0, 4.0])
+    got = O.replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4)
+    want = _py_replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4)
+    np.testing.assert_array_equal(got, want)
