@@ -752,11 +752,12 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   } else if (sbytes > 0 && !is_device_ptr(spins)) {
     return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
   }
-  // one staging buffer: reads | soff | eoff | items | counter | betas
+  // one staging buffer: reads | soff | eoff | items | counter | betas | order
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t b_reads = al((size_t)count * 4), b_soff = al((size_t)count * 8), b_eoff = al((size_t)count * 8),
-               b_items = al(items.size() * 4 + 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4);
-  OJ_CK(ctx->batch.ensure(b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta), "alloc batch tables");
+               b_items = al(items.size() * 4 + 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4),
+               b_order = al((size_t)count * 4);
+  OJ_CK(ctx->batch.ensure(b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta + b_order), "alloc batch tables");
   char* base = ctx->batch.as<char>();
   int32_t* d_reads = reinterpret_cast<int32_t*>(base);
   int64_t* d_soff = reinterpret_cast<int64_t*>(base + b_reads);
@@ -764,6 +765,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   int32_t* d_items = reinterpret_cast<int32_t*>(base + b_reads + b_soff + b_eoff);
   int* d_counter = reinterpret_cast<int*>(base + b_reads + b_soff + b_eoff + b_items);
   float* d_beta = reinterpret_cast<float*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt);
+  int32_t* d_order = reinterpret_cast<int32_t*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta);
   int launches = 0;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(d_spins, spins, sbytes, cudaMemcpyHostToDevice, st), "H2D spins");
@@ -772,6 +774,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   OJ_CK(cudaMemcpyAsync(d_eoff, eoff.data(), (size_t)count * 8, cudaMemcpyHostToDevice, st), "H2D offsets");
   if (nitems) OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
   if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+  if (count) OJ_CK(cudaMemcpyAsync(d_order, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st), "H2D order");
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
   if (S > 0 && nitems > 0)
     OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
@@ -784,7 +787,8 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
       OJ_CK(ctx->energies.ensure((size_t)nrep * 8), "alloc energies");
       d_e = ctx->energies.as<double>();
     }
-    OJ_CK(launch_batch_energy(b, d_reads, d_soff, d_eoff, max_reads, d_spins, d_e, st), "batch energy kernel");
+    OJ_CK(launch_batch_energy(b, d_reads, d_soff, d_eoff, d_order, max_reads, d_spins, d_e, st),
+          "batch energy kernel");
     ++launches;
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)nrep * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
   }

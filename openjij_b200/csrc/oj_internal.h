@@ -167,8 +167,8 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
                             int* launches);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
-                                const int64_t* d_eoff, int max_reads, const int8_t* spins, double* out,
-                                cudaStream_t st);
+                                const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
+                                double* out, cudaStream_t st);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,

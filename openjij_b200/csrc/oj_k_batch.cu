@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "oj_device.cuh"
 #include "oj_internal.h"
@@ -56,7 +57,8 @@ struct BatchArgs {
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
-__global__ void __launch_bounds__(kBatchWarps * 32) sa_batch_kernel(BatchArgs a) {
+template <int MINB>
+__global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -87,14 +89,24 @@ __global__ void __launch_bounds__(kBatchWarps * 32) sa_batch_kernel(BatchArgs a)
     // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j)
     for (int c = 0; c < nch; ++c) {
       float4 acc = ldg4(h + 128 * c + 4 * lane);
-      for (int i = 0; i < n; ++i) {
-        const uint32_t wi = __shfl_sync(0xffffffffu, sb, (i & 127) >> 2);
-        const bool neg = (wi >> (4 * (i >> 7) + (i & 3))) & 1u;
-        const float4 v = ldg4(J + (size_t)i * npad + 128 * c + 4 * lane);
-        acc.x = __fadd_rn(acc.x, neg ? -v.x : v.x);
-        acc.y = __fadd_rn(acc.y, neg ? -v.y : v.y);
-        acc.z = __fadd_rn(acc.z, neg ? -v.z : v.z);
-        acc.w = __fadd_rn(acc.w, neg ? -v.w : v.w);
+      const float* Jc = J + 128 * c + 4 * lane;
+      for (int i0 = 0; i0 < n; i0 += 4) {
+        float4 v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (i0 + q < n) v[q] = ldg4(Jc + (size_t)(i0 + q) * npad);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = i0 + q;
+          const uint32_t wi = __shfl_sync(0xffffffffu, sb, (i & 127) >> 2);
+          if (i < n) {
+            const bool neg = (wi >> (4 * (i >> 7) + (i & 3))) & 1u;
+            acc.x = __fadd_rn(acc.x, neg ? -v[q].x : v[q].x);
+            acc.y = __fadd_rn(acc.y, neg ? -v[q].y : v[q].y);
+            acc.z = __fadd_rn(acc.z, neg ? -v[q].z : v[q].z);
+            acc.w = __fadd_rn(acc.w, neg ? -v[q].w : v[q].w);
+          }
+        }
       }
       reinterpret_cast<float4*>(f)[32 * c + lane] = acc;
     }
@@ -133,14 +145,24 @@ __global__ void __launch_bounds__(kBatchWarps * 32) sa_batch_kernel(BatchArgs a)
           const float coef = neg ? 2.0f : -2.0f;
           const int i = 128 * c + 4 * ls + es;
           const float* Ji = J + (size_t)i * npad + 4 * lane;
-          for (int c2 = 0; c2 < nch; ++c2) {
-            const float4 v = ldg4(Ji + 128 * c2);
-            float4 g = reinterpret_cast<const float4*>(f)[32 * c2 + lane];
-            g.x = __fmaf_rn(coef, v.x, g.x);
-            g.y = __fmaf_rn(coef, v.y, g.y);
-            g.z = __fmaf_rn(coef, v.z, g.z);
-            g.w = __fmaf_rn(coef, v.w, g.w);
-            reinterpret_cast<float4*>(f)[32 * c2 + lane] = g;
+          // the row in groups of four chunks whose loads are in flight together
+#pragma unroll
+          for (int c0 = 0; c0 < kBatchMaxN / 128; c0 += 4) {
+            if (c0 >= nch) break;
+            float4 v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (c0 + q < nch) v[q] = ldg4(Ji + 128 * (c0 + q));
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (c0 + q < nch) {
+                float4 g = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
+                g.x = __fmaf_rn(coef, v[q].x, g.x);
+                g.y = __fmaf_rn(coef, v[q].y, g.y);
+                g.z = __fmaf_rn(coef, v[q].z, g.z);
+                g.w = __fmaf_rn(coef, v[q].w, g.w);
+                reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g;
+              }
           }
           if (lane == ls) sb ^= 1u << (4 * c + es);
           pos = 4 * ls + es + 1;
@@ -160,29 +182,35 @@ __global__ void __launch_bounds__(kBatchWarps * 32) sa_batch_kernel(BatchArgs a)
 
 // FP64 energy of every replica: E = sum_{i<j} J_ij s_i s_j + sum_i h_i s_i
 // (dense.hpp:176-192) from the FP64 augmented matrix.  One CTA per (instance,
-// 32 replicas): the spins are staged as one word per site (bit = replica), a
-// lane accumulates its replica, warps take rows round-robin and the per-warp
-// partial sums are added in warp order, so the result does not depend on timing.
+// 32 replicas), instances largest first: the spins are staged as one word per
+// site (bit = replica), a lane accumulates its replica, warps take rows
+// round-robin, read each row segment once (coalesced, through a per-warp
+// shared buffer, next segment prefetched) and apply it to all 32 replicas;
+// partial sums are combined in a fixed order, so the result does not depend on
+// timing.
 __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restrict__ J64,
                                                            const int64_t* __restrict__ j64off,
                                                            const int32_t* __restrict__ n_arr,
                                                            const int32_t* __restrict__ reads,
                                                            const int64_t* __restrict__ soff,
                                                            const int64_t* __restrict__ eoff,
+                                                           const int32_t* __restrict__ order,
                                                            const int8_t* __restrict__ spins, double* __restrict__ out) {
-  __shared__ uint32_t wsh[kBatchMaxN];
+  __shared__ uint32_t wsh[kBatchMaxN + 32];
+  __shared__ double rowbuf[8][32];
   __shared__ double part[8][32];
-  const int m = blockIdx.x;
+  const int m = order[blockIdx.x];
   const int r0 = 32 * blockIdx.y;
   const int R = reads[m];
   if (r0 >= R) return;
   const int n = n_arr[m];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int8_t* s = spins + soff[m];
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+  for (int j = threadIdx.x; j < n + 32; j += blockDim.x) {
     uint32_t w = 0u;
-    for (int q = 0; q < 32 && r0 + q < R; ++q)
-      if (s[(size_t)(r0 + q) * n + j] < 0) w |= 1u << q;
+    if (j < n)
+      for (int q = 0; q < 32 && r0 + q < R; ++q)
+        if (s[(size_t)(r0 + q) * n + j] < 0) w |= 1u << q;
     wsh[j] = w;
   }
   __syncthreads();
@@ -191,13 +219,24 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
   for (int i = warp; i < n; i += 8) {
     const double* Ai = A + (size_t)i * (n + 1);
     const uint32_t wi = wsh[i];
-    double row = 0.0;
-    for (int j = i + 1; j < n; ++j) {
-      const double v = __ldg(Ai + j);
-      row += ((wi ^ wsh[j]) >> lane) & 1u ? -v : v;
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
+    int j0 = i + 1;
+    double a = j0 + lane < n ? __ldg(Ai + j0 + lane) : 0.0;
+    for (; j0 < n; j0 += 32) {
+      const double an = j0 + 32 + lane < n ? __ldg(Ai + j0 + 32 + lane) : 0.0;  // next segment
+      __syncwarp();
+      rowbuf[warp][lane] = a;  // zero past the end of the row
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        const double v = rowbuf[warp][q];
+        const uint32_t flip = ((wi ^ wsh[j0 + q]) >> lane) & 1u;  // s_i != s_j in this replica
+        p[q & 3] += flip ? -v : v;
+      }
+      a = an;
     }
     const double hv = __ldg(Ai + n);
-    acc += row + (((wi >> lane) & 1u) ? -hv : hv);
+    acc += ((p[0] + p[1]) + (p[2] + p[3])) + (((wi >> lane) & 1u) ? -hv : hv);
   }
   part[warp][lane] = acc;
   __syncthreads();
@@ -218,7 +257,10 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
                             int* launches) {
   const size_t smem = (size_t)kBatchWarps * kBatchMaxN * sizeof(float);
-  auto kern = sa_batch_kernel;
+  // two register budgets: 80 per thread (3 CTAs per SM) or 64 (4 CTAs per SM)
+  int variant = 3;
+  if (const char* env = std::getenv("OJ_BATCH_MINB")) variant = std::atoi(env) == 4 ? 4 : 3;
+  auto kern = variant == 4 ? sa_batch_kernel<4> : sa_batch_kernel<3>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -250,12 +292,12 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
 }
 
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
-                                const int64_t* d_eoff, int max_reads, const int8_t* spins, double* out,
-                                cudaStream_t st) {
+                                const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
+                                double* out, cudaStream_t st) {
   if (b->count == 0 || max_reads == 0) return cudaSuccess;
   dim3 grid(b->count, (max_reads + 31) / 32);
   batch_energy_kernel<<<grid, 256, 0, st>>>(b->d_J64.as<double>(), b->d_j64off.as<int64_t>(), b->d_n.as<int32_t>(),
-                                            d_reads, d_soff, d_eoff, spins, out);
+                                            d_reads, d_soff, d_eoff, d_order, spins, out);
   return cudaGetLastError();
 }
 
