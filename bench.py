@@ -544,6 +544,130 @@ def run_ours(args):
     return 0
 
 
+def _t99(tau_ms, p):
+    """OpenJij's TTS formula (openjij/utils/benchmark.py:205-224): tau*ln(1-0.99)/ln(1-p_s)."""
+    if p <= 0.0:
+        return float("inf")
+    if p >= 1.0:
+        return tau_ms
+    return tau_ms * np.log(1.0 - 0.99) / np.log(1.0 - p)
+
+
+def _csr_of(A):
+    import scipy.sparse as sp
+    m = sp.csr_matrix(A)
+    m.sort_indices()
+    return (np.ascontiguousarray(m.indptr, np.int64), np.ascontiguousarray(m.indices, np.int32),
+            np.ascontiguousarray(m.data, np.float64))
+
+
+def _best_of(cands):
+    return dict(min(cands, key=lambda c: c["t99_ms"]), ladder=cands)
+
+
+def run_tts(args):
+    """Time-to-1%-energy on configs 3-5: the batched / mixed-precision kernel
+    against the plain single-instance FP32 kernel, each over a ladder of
+    num_sweeps {S/16, S/8, S/4, S/2, S}.  E* is the best energy found by any
+    run of any method (per instance for config 5); a read succeeds when
+    E <= E* + 0.01|E*|; tau is the call's device time with host buffers in and
+    out.  Config 5: plain = one call per instance, T99 = sum over instances of
+    tau_m * R99(p_m); batched = one call for all, T99 = tau * max_m R99(p_m),
+    R99(p) = ln(0.01)/ln(1-p) repetitions."""
+    import torch
+    from openjij_b200 import _native as N
+    from openjij_b200 import instances as I
+    torch.cuda.set_device(0)
+    ctx = N.Context(0)
+    w = _workload(args.config, None, None)
+    S = int(w["sweeps"]) if w["kind"] == "batch" else int(np.sum(w["mcs"]))
+    ladder = sorted({max(1, S // d) for d in (16, 8, 4, 2, 1)})
+    runs = []  # (method, S_l, tau_ms, energies, per-instance taus)
+    best = None
+    if w["kind"] == "batch":
+        mats, reads = w["mats"], w["reads"]
+        batch = N.Batch(ctx, mats)
+        graphs = [N.Graph(ctx, A.shape[0] - 1, *_csr_of(A)) for A in mats]
+        sizes = [A.shape[0] - 1 for A in mats]
+        rng = np.random.default_rng(7)
+        init = [rng.choice(np.array([-1, 1], np.int8), size=(int(r), n)) for r, n in zip(reads, sizes)]
+        off = np.concatenate([[0], np.cumsum(reads)])
+        for Sl in ladder:
+            betas, mcs = I.geometric_betas(0.1, 10.0, Sl)
+            flat = np.concatenate([x.ravel() for x in init])
+            e = np.zeros(int(np.sum(reads)))
+            N.sa_run_batched(batch, reads, flat.copy(), betas, mcs, seed=3, energies=e)  # warm-up
+            st = N.sa_run_batched(batch, reads, flat, betas, mcs, seed=3, energies=e)
+            runs.append(("batched", Sl, st["total_ms"], [e[off[m]:off[m + 1]] for m in range(len(mats))], None))
+            taus, es = [], []
+            for m, g in enumerate(graphs):
+                em = np.zeros(int(reads[m]))
+                st = N.sa_run(g, init[m].copy(), betas, mcs, seed=3, kernel="dense_plain", energies=em)
+                taus.append(st["total_ms"])
+                es.append(em)
+            runs.append(("plain", Sl, float(np.sum(taus)), es, taus))
+        emin = [min(float(np.min(r[3][m])) for r in runs) for m in range(len(mats))]
+        out = {}
+        for meth in ("batched", "plain"):
+            cands = []
+            for r in runs:
+                if r[0] != meth:
+                    continue
+                ps = [float(np.mean(r[3][m] <= emin[m] + 0.01 * abs(emin[m]))) for m in range(len(mats))]
+                if meth == "batched":
+                    t = r[2] * max(_t99(1.0, p) for p in ps)
+                else:
+                    t = float(np.sum([tau * _t99(1.0, p) for tau, p in zip(r[4], ps)]))
+                cands.append({"num_sweeps": r[1], "tau_ms": r[2], "t99_ms": t,
+                              "min_p_success": float(np.min(ps)), "mean_p_success": float(np.mean(ps))})
+            out[meth] = _best_of(cands)
+    else:
+        from oracle import oracle as O  # only for the CSR arrays of the instance
+        g = O.AugCSR(w["matrix"])
+        graph = N.Graph(ctx, g.n, g.indptr, g.indices, g.data)
+        R, T = w["replicas"], w["T"]
+        rng = np.random.default_rng(7)
+        shape = (R, g.n) if w["kind"] == "sa" else (R, T, g.n)
+        init = rng.choice(np.array([-1, 1], np.int8), size=shape)
+        methods = {"batched": "dense_tc" if args.config == 3 else "bitpacked",
+                   "plain": "dense_plain" if args.config == 3 else "colour"}
+        for Sl in ladder:
+            for meth, kern in methods.items():
+                sp = init.copy()
+                if w["kind"] == "sa":
+                    betas, mcs = I.geometric_betas(0.05, 5.0, Sl)
+                    e = np.zeros(R)
+                    N.sa_run(graph, sp.copy(), betas, mcs, seed=3, kernel=kern)  # warm-up
+                    st = N.sa_run(graph, sp, betas, mcs, seed=3, kernel=kern, energies=e)
+                else:
+                    ss = np.linspace(0.0, 1.0, Sl)
+                    betas = np.full(Sl, w["beta"])
+                    mcs = np.ones(Sl, np.int32)
+                    et = np.zeros((R, T))
+                    N.sqa_run(graph, sp.copy(), w["gamma"], betas, ss, mcs, seed=3, kernel=kern)
+                    st = N.sqa_run(graph, sp, w["gamma"], betas, ss, mcs, seed=3, kernel=kern, energies=et)
+                    e = et.min(axis=1)  # get_solution: the best slice of each replica
+                runs.append((meth, Sl, st["total_ms"], e, None))
+        best = min(float(np.min(r[3])) for r in runs)
+        out = {}
+        for meth in methods:
+            cands = []
+            for r in runs:
+                if r[0] != meth:
+                    continue
+                p = float(np.mean(r[3] <= best + 0.01 * abs(best)))
+                cands.append({"num_sweeps": r[1], "tau_ms": r[2], "p_success": p, "t99_ms": _t99(r[2], p),
+                              "mean_energy": float(np.mean(r[3]))})
+            out[meth] = _best_of(cands)
+        out["batched"]["kernel"], out["plain"]["kernel"] = methods["batched"], methods["plain"]
+    line = {"metric": "time-to-1%-energy (T99)", "unit": "ms", "higher_is_better": False,
+            "config": {"workload": w["name"], "ladder": ladder}, "best_energy": best,
+            "batched": out["batched"], "plain": out["plain"],
+            "plain_over_batched": out["plain"]["t99_ms"] / out["batched"]["t99_ms"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -558,7 +682,11 @@ def main():
                     help="benchmark configuration 1-5 (default 2: the L=128 +-J lattice)")
     ap.add_argument("--kernel", default=None,
                     help="force a kernel: colour, dense_plain, bitpacked, dense_tc (default: planner)")
+    ap.add_argument("--tts", action="store_true",
+                    help="time-to-1%%-energy of the batched/mixed kernel vs the plain kernel (configs 3-5)")
     args = ap.parse_args()
+    if args.tts:
+        return run_tts(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.config == 5:

@@ -332,12 +332,17 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   uint32_t kernel = flags & OJ_KERNEL_MASK;
   const oj_graph_info& inf = g->info;
   if (kernel == OJ_KERNEL_AUTO) {
-    if (inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1)
+    if (inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1) {
       kernel = OJ_KERNEL_BITPACKED;
-    else if (inf.num_colours > 64 && (int64_t)n * n * 4 <= ((int64_t)8 << 30))
-      kernel = OJ_KERNEL_DENSE_PLAIN;
-    else
+    } else if (inf.num_colours > 64 && (int64_t)n * n * 4 <= ((int64_t)8 << 30)) {
+      // dense: delayed tensor-core field updates when there are enough 128-replica
+      // tiles to occupy the GPU, else the sequential warp-per-replica kernel
+      std::string why;
+      kernel = (R >= 512 && n >= 256 && dense_tc_prepare(g, &why) == cudaSuccess) ? OJ_KERNEL_DENSE_TC
+                                                                                  : OJ_KERNEL_DENSE_PLAIN;
+    } else {
       kernel = OJ_KERNEL_COLOUR;
+    }
   }
   if (kernel == OJ_KERNEL_BITPACKED &&
       !(inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1)) {
