@@ -167,12 +167,13 @@ __device__ __forceinline__ void split_range(int lo, int hi, uint32_t* __restrict
 }
 
 // Shared memory: E[slots] | O[slots] | gid[nlocmax] | jm[nlocmax] | nbr[nlocmax][D]
-template <int D>
+// CL: the group's sites are split over a cluster of CTAs (halo exchange);
+// without it one CTA owns all sites and a phase ends with one block barrier.
+template <int D, bool CL>
 __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a) {
   extern __shared__ __align__(16) uint32_t sh[];
   constexpr int NC = SplitSweep<D>::NC;
-  cg::cluster_group cl = cg::this_cluster();
-  const int p = (int)cl.block_rank();
+  const int p = CL ? (int)cg::this_cluster().block_rank() : 0;
   const int g = blockIdx.y;
   const int32_t* gid_g = a.gidx + (size_t)p * a.slots;
   const int32_t* co = a.coff + (size_t)p * (a.ncol + 1);
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
   }
   for (int s = threadIdx.x; s < nloc * D; s += blockDim.x) nbr[s] = nbr_g[s];
   __syncthreads();
-  cluster_arrive();
+  if constexpr (CL) cluster_arrive();
   int prev_c = -1, prev_q = 0;  // colour class and half updated by the previous phase
   const uint32_t gg = a.group0 + (uint32_t)g;
   for (int64_t k = 0; k < a.nsweeps; ++k) {
@@ -216,27 +217,33 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
       uint32_t* X = q ? WO : WE;
       const uint32_t* Y = q ? WE : WO;
       for (int c = 0; c < a.ncol; ++c) {
-        split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
-        cluster_wait();
-        if (prev_c >= 0) {
-          uint32_t* P = prev_q ? WO : WE;
-          const int hlo = ho[prev_c], hhi = ho[prev_c + 1];
-          for (int e = hlo + threadIdx.x; e < hhi; e += blockDim.x) {
-            const uint32_t src = hs[e];
-            const uint32_t* remote = cl.map_shared_rank(P, (int)(src >> 16));
-            P[hd[e]] = remote[src & 0xFFFFu];
+        if constexpr (CL) {
+          cg::cluster_group cl = cg::this_cluster();
+          split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          cluster_wait();
+          if (prev_c >= 0) {
+            uint32_t* P = prev_q ? WO : WE;
+            const int hlo = ho[prev_c], hhi = ho[prev_c + 1];
+            for (int e = hlo + threadIdx.x; e < hhi; e += blockDim.x) {
+              const uint32_t src = hs[e];
+              const uint32_t* remote = cl.map_shared_rank(P, (int)(src >> 16));
+              P[hd[e]] = remote[src & 0xFFFFu];
+            }
           }
+          __syncthreads();
+          split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          cluster_arrive();
+          __syncthreads();
+          prev_c = c;
+          prev_q = q;
+        } else {
+          split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          __syncthreads();
         }
-        __syncthreads();
-        split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
-        cluster_arrive();
-        __syncthreads();
-        prev_c = c;
-        prev_q = q;
       }
     }
   }
-  cluster_wait();
+  if constexpr (CL) cluster_wait();
   for (int s = threadIdx.x; s < nloc; s += blockDim.x) {
     const int i = gid[s];
     gE[i] = WE[s];
@@ -298,9 +305,16 @@ int split_threads() {
 
 template <int D>
 cudaError_t launch_d(const MscPlan& pl, const SplitArgs& a, int G, cudaStream_t st) {
-  auto kern = sqa_split_kernel<D>;
   const size_t smem = split_smem_bytes(pl);
   if (smem > kSplitSmemBytes) return cudaErrorInvalidValue;
+  if (pl.P == 1) {
+    auto k1 = sqa_split_kernel<D, false>;
+    cudaError_t e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k1<<<dim3(1, G, 1), split_threads(), smem, st>>>(a);
+    return cudaGetLastError();
+  }
+  auto kern = sqa_split_kernel<D, true>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (pl.P > 8) {
