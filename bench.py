@@ -412,17 +412,16 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from openjij_b200 import _native as N
-    from oracle import oracle as O  # CPU baseline only
+    from openjij_b200 import instances as I
     w = _workload(args.config, args.sweeps, args.replicas)
     kernel = args.kernel or w["kernel"]
-    g_or = O.AugCSR(w["matrix"])
-    n = g_or.n
+    n, indptr, indices, data = I.augmented_csr(w["matrix"])
     R, T = w["replicas"], w["T"]
     betas, mcs = w["betas"], w["mcs"]
     stream = torch.cuda.current_stream()
     ctx = N.Context(local)
     ctx.set_stream(stream.cuda_stream)
-    graph = N.Graph(ctx, n, g_or.indptr, g_or.indices, g_or.data)
+    graph = N.Graph(ctx, n, indptr, indices, data)
     rng = np.random.default_rng(1000 + rank)
     shape = (R, n) if w["kind"] == "sa" else (R, T, n)
     init_host = rng.choice(np.array([-1, 1], np.int8), size=shape)
@@ -553,14 +552,6 @@ def _t99(tau_ms, p):
     return tau_ms * np.log(1.0 - 0.99) / np.log(1.0 - p)
 
 
-def _csr_of(A):
-    import scipy.sparse as sp
-    m = sp.csr_matrix(A)
-    m.sort_indices()
-    return (np.ascontiguousarray(m.indptr, np.int64), np.ascontiguousarray(m.indices, np.int32),
-            np.ascontiguousarray(m.data, np.float64))
-
-
 def _best_of(cands):
     return dict(min(cands, key=lambda c: c["t99_ms"]), ladder=cands)
 
@@ -587,7 +578,7 @@ def run_tts(args):
     if w["kind"] == "batch":
         mats, reads = w["mats"], w["reads"]
         batch = N.Batch(ctx, mats)
-        graphs = [N.Graph(ctx, A.shape[0] - 1, *_csr_of(A)) for A in mats]
+        graphs = [N.Graph(ctx, *I.augmented_csr(A)) for A in mats]
         sizes = [A.shape[0] - 1 for A in mats]
         rng = np.random.default_rng(7)
         init = [rng.choice(np.array([-1, 1], np.int8), size=(int(r), n)) for r, n in zip(reads, sizes)]
@@ -622,12 +613,11 @@ def run_tts(args):
                               "min_p_success": float(np.min(ps)), "mean_p_success": float(np.mean(ps))})
             out[meth] = _best_of(cands)
     else:
-        from oracle import oracle as O  # only for the CSR arrays of the instance
-        g = O.AugCSR(w["matrix"])
-        graph = N.Graph(ctx, g.n, g.indptr, g.indices, g.data)
+        n, indptr, indices, data = I.augmented_csr(w["matrix"])
+        graph = N.Graph(ctx, n, indptr, indices, data)
         R, T = w["replicas"], w["T"]
         rng = np.random.default_rng(7)
-        shape = (R, g.n) if w["kind"] == "sa" else (R, T, g.n)
+        shape = (R, n) if w["kind"] == "sa" else (R, T, n)
         init = rng.choice(np.array([-1, 1], np.int8), size=shape)
         methods = {"batched": "dense_tc" if args.config == 3 else "bitpacked",
                    "plain": "dense_plain" if args.config == 3 else "colour"}

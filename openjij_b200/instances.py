@@ -13,6 +13,15 @@ import numpy as np
 import scipy.sparse as sp
 
 
+def augmented_csr(mat):
+    """(n, indptr int64, indices int32, data float64) of a symmetric augmented
+    (n+1)x(n+1) matrix, sorted column indices: the arrays oj_graph_create_csr takes."""
+    m = sp.csr_matrix(mat, dtype=np.float64)
+    m.sort_indices()
+    return (m.shape[0] - 1, np.ascontiguousarray(m.indptr, np.int64), np.ascontiguousarray(m.indices, np.int32),
+            np.ascontiguousarray(m.data, np.float64))
+
+
 def augmented_from_ising(h, J_upper_coo, n):
     """h: [n]; J_upper_coo: (rows, cols, vals) with rows < cols (summed)."""
     r, c, v = (np.asarray(x) for x in J_upper_coo)
