@@ -11,13 +11,16 @@ Same parameters, defaults and schedule construction as the reference's
 """
 from __future__ import annotations
 
+import time
 from typing import Optional, Union
 
 import numpy as np
 
 import openjij_b200.cxxjij as cxxjij
 from openjij_b200.model.model import BinaryQuadraticModel
+from openjij_b200.sampler.response import Response
 from openjij_b200.sampler.sampler import BaseSampler, _as_bqm, spins_from_initial_state
+from openjij_b200.variable_type import BINARY
 
 
 class SASampler(BaseSampler):
@@ -115,6 +118,80 @@ class SASampler(BaseSampler):
                                          seed, offset)
         response.info["schedule"] = self.schedule_info
         return response
+
+
+    def sample_batch(self, models, beta_min: Optional[float] = None, beta_max: Optional[float] = None,
+                     num_sweeps: Optional[int] = None, num_reads: Optional[int] = None, seed: Optional[int] = None,
+                     device: int = 0):
+        """Anneals many dense models of uneven size in one GPU launch (an
+        extension: the reference samples one model per ``sample`` call).
+
+        ``models``: BinaryQuadraticModels (or dimod-like models, or QUBO dicts),
+        each with at most 1024 variables.  All models share one geometric
+        schedule; a missing end of the beta range is estimated per model as in
+        ``sample`` and the widest range over the models is used.  Returns one
+        Response per model, in order.
+        """
+        from openjij_b200 import _native as N
+        self._set_params(beta_min=beta_min, beta_max=beta_max, num_sweeps=num_sweeps, num_reads=num_reads)
+        R = int(self._params["num_reads"])
+        S = int(self._params["num_sweeps"])
+        bqms, mats, offsets = [], [], []
+        for mdl in models:
+            b = BinaryQuadraticModel.from_qubo(mdl) if isinstance(mdl, dict) else _as_bqm(mdl, False)
+            graph, off = b.get_cxxjij_ising_graph()
+            bqms.append(b)
+            mats.append(np.ascontiguousarray(graph.get_interactions(), np.float64))
+            offsets.append(off)
+        bmin, bmax = self._params["beta_min"], self._params["beta_max"]
+        if bmin is None or bmax is None:
+            lo, hi = [], []
+            for b in bqms:
+                graph, _ = b.get_cxxjij_ising_graph()
+                _, (b1, b0) = geometric_ising_beta_schedule(graph, beta_max=bmax, beta_min=bmin, num_sweeps=S,
+                                                            seed=seed)
+                lo.append(b0)
+                hi.append(b1)
+            bmin = min(lo) if bmin is None else bmin
+            bmax = max(hi) if bmax is None else bmax
+        m = max(1, S // 1000)
+        count = S // m
+        betas = cxxjij.utility.make_classical_schedule_list(float(bmin), float(bmax), m, count)
+        beta_arr = np.array([e.updater_parameter.beta for e in betas], np.float64)
+        mcs = np.array([e.one_mc_step for e in betas], np.int32)
+        sizes = [a.shape[0] - 1 for a in mats]
+        rng = np.random.default_rng(seed)
+        spins = rng.choice(np.array([-1, 1], np.int8), size=int(R * sum(sizes)))
+        reads = np.full(len(mats), R, np.int32)
+        energies = np.zeros(R * len(mats))
+        ctx = _batch_context(device)
+        t0 = time.perf_counter()
+        st = N.sa_run_batched(N.Batch(ctx, mats), reads, spins, beta_arr, mcs,
+                              seed=(rng.integers(0, 2 ** 63) if seed is None else int(seed)), energies=energies)
+        elapsed = time.perf_counter() - t0
+        out, off = [], 0
+        for k, b in enumerate(bqms):
+            n = sizes[k]
+            st_k = spins[off: off + R * n].reshape(R, n)
+            off += R * n
+            if b.vartype == BINARY:
+                st_k = (st_k + 1) // 2
+            resp = Response(st_k.astype(np.int8), energies[k * R:(k + 1) * R] + offsets[k], b.variables, b.vartype)
+            resp.info["schedule"] = {"beta_min": bmin, "beta_max": bmax, "num_sweeps": S}
+            resp.info["sampling_time"] = elapsed * 1e6
+            resp.info["run"] = st
+            out.append(resp)
+        return out
+
+
+_BATCH_CTX = {}
+
+
+def _batch_context(device):
+    from openjij_b200 import _native as N
+    if device not in _BATCH_CTX:
+        _BATCH_CTX[device] = N.Context(device)
+    return _BATCH_CTX[device]
 
 
 def geometric_ising_beta_schedule(cxxgraph, beta_max=None, beta_min=None, num_sweeps=1000, seed=None):

@@ -220,3 +220,22 @@ def test_reverse_annealing_chains_reads():
 def test_unknown_parameter_and_updater():
     with pytest.raises(ValueError):
         oj.SASampler().sample_ising(NUM_H, NUM_J, updater="swendsen wang")
+
+
+def test_sa_sample_batch():
+    """SASampler.sample_batch: many models of uneven size in one GPU launch, one
+    Response per model, energies equal to the models' own."""
+    rng = np.random.default_rng(11)
+    rand_q = {(i, j): float(rng.standard_normal()) for i in range(40) for j in range(i, 40)}
+    models = [oj.BinaryQuadraticModel.from_ising(NUM_H, NUM_J), QUBO, rand_q,
+              oj.BinaryQuadraticModel.from_ising({0: -10}, {(i, i + 1): 1 for i in range(29)})]
+    out = oj.SASampler().sample_batch(models, num_reads=16, num_sweeps=300, seed=5)
+    assert len(out) == 4
+    for mdl, res in zip(models, out):
+        bqm = mdl if isinstance(mdl, oj.BinaryQuadraticModel) else oj.BinaryQuadraticModel.from_qubo(mdl)
+        assert len(res.states) == 16
+        for st, e in zip(res.samples(), res.energies):
+            assert e == pytest.approx(bqm.energy(st), abs=1e-9)
+    assert list(out[0].first.sample.values()) == GROUND5 and out[0].first.energy == -6
+    assert list(out[1].first.sample.values()) == [1, 1, 0, 0, 0] and out[1].first.energy == -3
+    assert out[3].first.sample == {i: (-1) ** i for i in range(30)}
