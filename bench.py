@@ -321,7 +321,7 @@ def run_ours_batch(args, w):
 
     def step(k, spins, en, device):
         return N.sa_run_batched(batch, reads, spins, betas, mcs, seed=seed0 + k, energies=en, device=device,
-                                instance_offset=inst0)
+                                instance_offset=inst0, tune=True)
 
     for k in range(args.warmup):
         flush.zero_()
@@ -383,6 +383,8 @@ def run_ours_batch(args, w):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded instances)",
             "config": {"workload": w["name"], "instances": len(mats), "spins_total": int(np.sum(sizes)),
                        "replicas_per_instance": int(w["replicas"]), "num_sweeps": S, "kernel": "batched",
+                       "launch_shape": {"threads": st["threads"], "register_variant": st["variant"],
+                                        "autotuned": True},
                        "l2": "flushed between steps (256 MB write)", "attempts_per_step": attempts_per_step},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "kernel_ms": kms,
@@ -436,9 +438,9 @@ def run_ours(args):
     def run(spins, seed, device, en):
         if w["kind"] == "sa":
             return N.sa_run(graph, spins, betas, mcs, seed=seed, energies=en, device=device, kernel=kernel,
-                            replica_offset=rep0)
+                            replica_offset=rep0, tune=True)
         return N.sqa_run(graph, spins, w["gamma"], betas, w["s"], mcs, seed=seed, energies=en,
-                         device=device, kernel=kernel, replica_offset=rep0)
+                         device=device, kernel=kernel, replica_offset=rep0, tune=True)
 
     def step(k):
         work.copy_(init_dev)
@@ -521,6 +523,7 @@ def run_ours(args):
             "data": "synthetic (seeded instance)",
             "config": {"workload": w["name"], "spins": n, "replicas": R, "trotter": T,
                        "num_sweeps": int(np.sum(mcs)), "kernel": used_kernel,
+                       "launch_shape": {"cluster": st["cluster"], "threads": st["threads"], "autotuned": True},
                        "l2": "flushed between steps (256 MB write)",
                        "attempts_per_step": attempts_per_step},
             "roofline": {"bound": w["bound"], "achieved": achieved, "peak": peak, "unit": unit,

@@ -41,6 +41,13 @@ enum {
 
 /* flags */
 #define OJ_DEVICE_POINTERS 0x1u
+/* Autotune: on the first call for a (graph or batch, kernel, replicas, slices)
+ * the tunable kernels (bit-packed SA, slice-split SQA, batched SA) time their
+ * candidate launch shapes (cluster size, threads per CTA, register budget)
+ * for a few sweeps on a copy of the call's own state and keep the fastest for
+ * later calls.  Every shape gives the same spins; only the time differs.
+ * Also enabled by the environment variable OJ_AUTOTUNE=1. */
+#define OJ_AUTOTUNE 0x2u
 /* kernel selection (bits 4..7) */
 #define OJ_KERNEL_SHIFT 4
 #define OJ_KERNEL_MASK (0xFu << OJ_KERNEL_SHIFT)
@@ -73,6 +80,10 @@ typedef struct oj_run_stats {
   double attempts;       /* spin-flip attempts = R * T * n * sweeps */
   float anneal_ms;       /* device time of the annealing kernel(s) */
   float total_ms;        /* device time of the whole call incl. copies */
+  int32_t cluster;       /* CTAs per cluster of the annealing launch (tunable kernels, else 0) */
+  int32_t threads;       /* threads per CTA of the annealing launch (tunable kernels, else 0) */
+  int32_t variant;       /* register-budget variant (batched kernel, else 0) */
+  int32_t tuned;         /* 1 when this call ran the autotuner */
 } oj_run_stats;
 
 const char* oj_version(void);
@@ -179,7 +190,7 @@ oj_status oj_batch_destroy(oj_batch* b);
  * mcs[j]) for all instances.  first_sweep as in oj_sa_run; instance_offset is
  * the global index of instance 0 (random numbers are a pure function of seed,
  * global instance, replica, sweep and site, so a batch split over calls or
- * GPUs reproduces the whole).  flags: OJ_DEVICE_POINTERS only. */
+ * GPUs reproduces the whole).  flags: OJ_DEVICE_POINTERS, OJ_AUTOTUNE. */
 oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads, int8_t* spins,
                             const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
                             int64_t first_sweep, int64_t instance_offset, uint32_t flags, double* energies,

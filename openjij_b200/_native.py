@@ -24,6 +24,7 @@ OJ_ERR_UNSUPPORTED = 6
 OJ_ERR_NODEVICE = 7
 
 OJ_DEVICE_POINTERS = 0x1
+OJ_AUTOTUNE = 0x2
 KERNEL_SHIFT = 4
 KERNELS = {"auto": 0, "colour": 1, "dense_plain": 2, "bitpacked": 3, "dense_tc": 4}
 KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
@@ -45,7 +46,8 @@ class GraphInfo(C.Structure):
 
 class RunStats(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("launches", C.c_int32), ("sweeps", C.c_int64),
-                ("attempts", C.c_double), ("anneal_ms", C.c_float), ("total_ms", C.c_float)]
+                ("attempts", C.c_double), ("anneal_ms", C.c_float), ("total_ms", C.c_float),
+                ("cluster", C.c_int32), ("threads", C.c_int32), ("variant", C.c_int32), ("tuned", C.c_int32)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -186,15 +188,17 @@ class Graph:
             pass
 
 
-def _flags(kernel, device):
+def _flags(kernel, device, tune=False):
     f = KERNELS[kernel] << KERNEL_SHIFT
     if device:
         f |= OJ_DEVICE_POINTERS
+    if tune:
+        f |= OJ_AUTOTUNE
     return f
 
 
 def sa_run(g: Graph, spins, betas, mcs, seed, kernel="auto", energies=None, device=False,
-           first_sweep=0, replica_offset=0):
+           first_sweep=0, replica_offset=0, tune=False):
     """spins: int8 [R][n] numpy (in/out) or device tensor/pointer with device=True."""
     R = spins.shape[0] if hasattr(spins, "shape") else None
     b = np.ascontiguousarray(betas, np.float64)
@@ -202,12 +206,12 @@ def sa_run(g: Graph, spins, betas, mcs, seed, kernel="auto", energies=None, devi
     st = RunStats()
     g.ctx.check(lib().oj_sa_run(g.ctx._h, g._h, int(R), _ptr(spins), _ptr(b), _ptr(m), len(b),
                                 int(seed) & 0xFFFFFFFFFFFFFFFF, int(first_sweep), int(replica_offset),
-                                _flags(kernel, device), _ptr(energies), C.byref(st)), "oj_sa_run")
+                                _flags(kernel, device, tune), _ptr(energies), C.byref(st)), "oj_sa_run")
     return st.as_dict()
 
 
 def sqa_run(g: Graph, spins, gamma, betas, s, mcs, seed, energies=None, best=None, kernel="auto",
-            device=False, first_sweep=0, replica_offset=0):
+            device=False, first_sweep=0, replica_offset=0, tune=False):
     """spins: int8 [R][T][n]."""
     R, T = spins.shape[0], spins.shape[1]
     b = np.ascontiguousarray(betas, np.float64)
@@ -216,7 +220,7 @@ def sqa_run(g: Graph, spins, gamma, betas, s, mcs, seed, energies=None, best=Non
     st = RunStats()
     g.ctx.check(lib().oj_sqa_run(g.ctx._h, g._h, int(R), int(T), _ptr(spins), float(gamma), _ptr(b),
                                  _ptr(sv), _ptr(m), len(b), int(seed) & 0xFFFFFFFFFFFFFFFF,
-                                 int(first_sweep), int(replica_offset), _flags(kernel, device),
+                                 int(first_sweep), int(replica_offset), _flags(kernel, device, tune),
                                  _ptr(energies), _ptr(best), C.byref(st)),
                 "oj_sqa_run")
     return st.as_dict()
@@ -269,7 +273,7 @@ class Batch:
 
 
 def sa_run_batched(b: Batch, reads, spins, betas, mcs, seed, energies=None, device=False, first_sweep=0,
-                   instance_offset=0):
+                   instance_offset=0, tune=False):
     """spins: int8, the instances' [reads[k]][n[k]] blocks concatenated."""
     r = np.ascontiguousarray(reads, np.int32)
     bb = np.ascontiguousarray(betas, np.float64)
@@ -277,7 +281,7 @@ def sa_run_batched(b: Batch, reads, spins, betas, mcs, seed, energies=None, devi
     st = RunStats()
     b.ctx.check(lib().oj_sa_run_batched(b.ctx._h, b._h, _ptr(r), _ptr(spins), _ptr(bb), _ptr(m), len(bb),
                                         int(seed) & 0xFFFFFFFFFFFFFFFF, int(first_sweep), int(instance_offset),
-                                        _flags("auto", device), _ptr(energies), C.byref(st)),
+                                        _flags("auto", device, tune), _ptr(energies), C.byref(st)),
                 "oj_sa_run_batched")
     d = st.as_dict()
     d["kernel"] = "batched"

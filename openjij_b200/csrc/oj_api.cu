@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -143,6 +144,55 @@ void sqa_msc_thresholds(const std::vector<float2>& coef, double c, int D, std::v
     mode[2 * k] = always;
     mode[2 * k + 1] = live;
   }
+}
+
+bool autotune_requested(uint32_t flags) {
+  if (flags & OJ_AUTOTUNE) return true;
+  const char* e = std::getenv("OJ_AUTOTUNE");
+  return e && e[0] == '1';
+}
+
+// Autotuner core: for each candidate, restore() puts the call's own initial
+// state into a scratch copy and enqueue(i) runs candidate i on it for a few
+// sweeps; each candidate runs twice and its second time counts.  Returns the
+// fastest candidate, -1 when none launched, or -2 on a device error (which
+// the caller reports).  Candidates that cannot launch (cluster or shared-memory
+// limits) are skipped.
+template <class Restore, class Enqueue>
+int time_candidates(cudaStream_t st, int count, Restore restore, Enqueue enqueue, cudaError_t* err) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if ((*err = cudaEventCreate(&e0)) != cudaSuccess) return -2;
+  if ((*err = cudaEventCreate(&e1)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return -2;
+  }
+  float best = 0.0f;
+  int bi = -1;
+  for (int i = 0; i < count && *err == cudaSuccess; ++i) {
+    float ms = 0.0f;
+    bool ok = true;
+    for (int rep = 0; rep < 2 && ok; ++rep) {
+      if ((*err = restore()) != cudaSuccess) break;
+      cudaEventRecord(e0, st);
+      const cudaError_t le = enqueue(i);
+      cudaEventRecord(e1, st);
+      if (le != cudaSuccess) {
+        cudaGetLastError();  // launch-configuration errors are not sticky
+        ok = false;
+        break;
+      }
+      if ((*err = cudaStreamSynchronize(st)) != cudaSuccess) break;
+      cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (*err != cudaSuccess) break;
+    if (ok && (bi < 0 || ms < best)) {
+      best = ms;
+      bi = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return *err != cudaSuccess ? -2 : bi;
 }
 
 }  // namespace
@@ -367,6 +417,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
   }
   int launches = 0;
+  int P_used = 0, threads_used = 0;
+  bool tuned_now = false;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED) {
@@ -393,8 +445,46 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     uint32_t* d_words = ctx->words.as<uint32_t>();
     OJ_CK(launch_pack(d_spins, R, n, d_words, st), "pack");
     ++launches;
+    // launch shape: cached, autotuned now, or the default heuristic
+    const uint64_t key = ((uint64_t)OJ_KERNEL_BITPACKED << 40) | (uint64_t)R;
+    Shape shp;
+    auto it = g->tuned.find(key);
+    if (it != g->tuned.end()) {
+      shp = it->second;
+    } else if (autotune_requested(flags) && S > 0) {
+      std::vector<Shape> cand;
+      for (int Pc : {1, 2, 4, 8, 16})
+        if (Pc == 1 || n / Pc >= 64)
+          for (int th : {256, 512, 1024}) cand.push_back(Shape{Pc, th, 0});
+      OJ_CK(ctx->aux.ensure((size_t)G * n * 4), "alloc tuning scratch");
+      uint32_t* scratch = ctx->aux.as<uint32_t>();
+      const int64_t Ssub = std::min<int64_t>(S, 16);
+      cudaError_t terr = cudaSuccess;
+      const int bi = time_candidates(
+          st, (int)cand.size(),
+          [&] { return cudaMemcpyAsync(scratch, d_words, (size_t)G * n * 4, cudaMemcpyDeviceToDevice, st); },
+          [&](int i) {
+            std::string w;
+            const cudaError_t e = msc_prepare(g, cand[i].cluster, &w);
+            if (e != cudaSuccess) return e;
+            return launch_sa_msc(g, G, scratch, d_thr, d_alw, Ssub, rb, st, nullptr, cand[i].threads);
+          },
+          &terr);
+      if (bi == -2) return cuda_fail(ctx, terr, "autotune");
+      if (bi >= 0) shp = cand[bi];
+      g->tuned[key] = shp;
+      tuned_now = true;
+    }
+    P_used = shp.cluster ? shp.cluster : msc_choose_cluster(g, G, ctx->sm_count);
+    threads_used = shp.threads ? shp.threads : msc_default_threads();
+    pe = msc_prepare(g, P_used, &why);
+    if (pe != cudaSuccess) {
+      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
+      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+    }
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-    if (S > 0) OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, rb, st, &launches), "sa bit-packed kernel");
+    if (S > 0)
+      OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, rb, st, &launches, threads_used), "sa bit-packed kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_unpack(d_words, R, n, d_spins, st), "unpack");
     ++launches;
@@ -441,6 +531,9 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     stats->launches = launches;
     stats->sweeps = S;
     stats->attempts = (double)R * n * (double)S;
+    stats->cluster = P_used;
+    stats->threads = threads_used;
+    stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
   }
@@ -499,6 +592,8 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
   }
   int launches = 0;
+  int P_used = 0, threads_used = 0;
+  bool tuned_now = false;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED && split_ok) {
@@ -523,9 +618,48 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     uint32_t* d_words = ctx->words.as<uint32_t>();
     OJ_CK(launch_sqa_split_pack(d_spins, R, T, n, G, d_words, st), "pack");
     ++launches;
+    const uint64_t key = ((uint64_t)0x80 << 40) | ((uint64_t)T << 32) | (uint64_t)R;
+    Shape shp;
+    auto it = g->tuned.find(key);
+    if (it != g->tuned.end()) {
+      shp = it->second;
+    } else if (autotune_requested(flags) && S > 0) {
+      std::vector<Shape> cand;
+      for (int Pc : {1, 2, 4})
+        if (Pc == 1 || n / Pc >= 64)
+          for (int th : {256, 512}) cand.push_back(Shape{Pc, th, 0});
+      OJ_CK(ctx->aux.ensure((size_t)G * 2 * n * 4), "alloc tuning scratch");
+      uint32_t* scratch = ctx->aux.as<uint32_t>();
+      const int64_t Ssub = std::min<int64_t>(S, 16);
+      cudaError_t terr = cudaSuccess;
+      const int bi = time_candidates(
+          st, (int)cand.size(),
+          [&] { return cudaMemcpyAsync(scratch, d_words, (size_t)G * 2 * n * 4, cudaMemcpyDeviceToDevice, st); },
+          [&](int i) {
+            std::string w;
+            const cudaError_t e = sqa_split_prepare(g, G, ctx->sm_count, &w, cand[i].cluster);
+            if (e != cudaSuccess || g->msc->P != cand[i].cluster) return e != cudaSuccess ? e : cudaErrorInvalidValue;
+            return launch_sqa_split(g, G, T, scratch, d_thr, d_mode, Ssub, rb, st, nullptr, cand[i].threads);
+          },
+          &terr);
+      if (bi == -2) return cuda_fail(ctx, terr, "autotune");
+      if (bi >= 0) shp = cand[bi];
+      g->tuned[key] = shp;
+      tuned_now = true;
+    }
+    {
+      const cudaError_t pe2 = sqa_split_prepare(g, G, ctx->sm_count, &why, shp.cluster);
+      if (pe2 != cudaSuccess) {
+        ctx->last_error = why.empty() ? cudaGetErrorString(pe2) : why;
+        return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+      }
+    }
+    P_used = g->msc->P;
+    threads_used = shp.threads ? shp.threads : split_default_threads();
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
-      OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rb, st, &launches), "sqa slice-split kernel");
+      OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rb, st, &launches, threads_used),
+            "sqa slice-split kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_sqa_split_unpack(d_words, R, T, n, G, d_spins, st), "unpack");
     ++launches;
@@ -588,6 +722,9 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     stats->launches = launches;
     stats->sweeps = S;
     stats->attempts = (double)R * T * n * (double)S;
+    stats->cluster = P_used;
+    stats->threads = threads_used;
+    stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
   }
@@ -780,10 +917,36 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (nitems) OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
   if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
   if (count) OJ_CK(cudaMemcpyAsync(d_order, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st), "H2D order");
+  oj_batch* bm = const_cast<oj_batch*>(b);
+  bool tuned_now = false;
+  if (bm->tuned_variant == 0 && autotune_requested(flags) && S > 0 && nitems > 0) {
+    // the work per sweep follows the acceptance rate, so the candidates run 16
+    // sweeps whose betas are spread over the whole schedule
+    const int cand[2] = {3, 4};
+    const int64_t Ssub = std::min<int64_t>(S, 16);
+    std::vector<float> tb(Ssub);
+    for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
+    const size_t sb_al = ((size_t)std::max<int64_t>(sbytes, 16) + 255) & ~(size_t)255;
+    OJ_CK(ctx->aux.ensure(sb_al + tb.size() * 4), "alloc tuning scratch");
+    int8_t* scratch = ctx->aux.as<int8_t>();
+    float* d_tb = reinterpret_cast<float*>(ctx->aux.as<char>() + sb_al);
+    OJ_CK(cudaMemcpyAsync(d_tb, tb.data(), tb.size() * 4, cudaMemcpyHostToDevice, st), "H2D tuning betas");
+    cudaError_t terr = cudaSuccess;
+    const int bi = time_candidates(
+        st, 2, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
+        [&](int i) {
+          return launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, scratch, d_tb, Ssub, rb,
+                                 (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i]);
+        },
+        &terr);
+    if (bi == -2) return cuda_fail(ctx, terr, "autotune");
+    bm->tuned_variant = bi >= 0 ? cand[bi] : 3;
+    tuned_now = true;
+  }
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
   if (S > 0 && nitems > 0)
     OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
-                          (uint32_t)instance_offset, ctx->sm_count, st, &launches),
+                          (uint32_t)instance_offset, ctx->sm_count, st, &launches, bm->tuned_variant),
           "sa batched kernel");
   OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   if (energies) {
@@ -803,6 +966,9 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (stats) {
     stats->kernel = 0;
     stats->launches = launches;
+    stats->threads = batch_warps() * 32;
+    stats->variant = bm->tuned_variant;
+    stats->tuned = tuned_now ? 1 : 0;
     stats->sweeps = S;
     stats->attempts = attempts_per_sweep * (double)S;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);

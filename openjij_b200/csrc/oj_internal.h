@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -62,6 +63,13 @@ struct MscPlan {
   uint16_t* jm = nullptr;    // [P][nlocmax] bit l set when J(site, nbr l) > 0
 };
 
+// Launch shape of a tunable kernel; 0 = the kernel's default choice.
+struct Shape {
+  int cluster = 0;  // CTAs per thread block cluster
+  int threads = 0;  // threads per CTA
+  int variant = 0;  // register-budget variant (batched kernel)
+};
+
 // Tiled couplings of the tensor-core dense kernel: J in BF16 (and the BF16
 // remainder J - bf16(J) for non-exact couplings) as the MMA B tiles of every
 // (32-spin block, CTA column range), FP32 32x32 in-block tiles and padded h.
@@ -95,6 +103,7 @@ struct oj_graph {
   std::unique_ptr<oj::MscPlan> msc;
   std::unique_ptr<oj::TcPlan> tc;
   oj::DevBuf sqa_nbr, sqa_jm;  // bit-packed SQA tables: [n][D] neighbours (u16), [n] J>0 masks
+  std::map<uint64_t, oj::Shape> tuned;  // autotuned launch shapes by (kernel, replicas, slices)
   ~oj_graph();
 };
 
@@ -107,6 +116,7 @@ struct oj_batch {
   int max_n = 0;
   std::vector<int32_t> n;
   oj::DevBuf d_J, d_h, d_J64, d_joff, d_hoff, d_j64off, d_n;
+  int tuned_variant = 0;  // autotuned register-budget variant, 0 = not tuned
   ~oj_batch();
 };
 
@@ -141,7 +151,7 @@ cudaError_t launch_sa_dense_plain(const oj_graph* g, int R, int8_t* spins, const
                                   int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
 cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
                           const uint32_t* always, int64_t nsweeps, RngBase rb, cudaStream_t st,
-                          int* launches);
+                          int* launches, int threads = 0);
 cudaError_t launch_sa_dense_tc(const oj_graph* g, int R, int8_t* spins, const float* betas, int64_t nsweeps,
                                RngBase rb, int recompute, cudaStream_t st, int* launches);
 cudaError_t dense_tc_prepare(oj_graph* g, std::string* why);
@@ -153,9 +163,10 @@ cudaError_t launch_sqa_pack(const int8_t* spins, int R, int T, int n, uint32_t* 
 cudaError_t launch_sqa_unpack(const uint32_t* words, int R, int T, int n, int8_t* spins, cudaStream_t st);
 int sqa_split_replicas_per_group(int T);
 bool sqa_split_applies(const oj_graph* g, int T);
-cudaError_t sqa_split_prepare(oj_graph* g, int G, int sm_count, std::string* why);
+cudaError_t sqa_split_prepare(oj_graph* g, int G, int sm_count, std::string* why, int cluster = 0);
 cudaError_t launch_sqa_split(const oj_graph* g, int G, int T, uint32_t* words, const uint32_t* thr,
-                             const uint32_t* mode, int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches);
+                             const uint32_t* mode, int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches,
+                             int threads = 0);
 cudaError_t launch_sqa_split_pack(const int8_t* spins, int R, int T, int n, int G, uint32_t* words,
                                   cudaStream_t st);
 cudaError_t launch_sqa_split_unpack(const uint32_t* words, int R, int T, int n, int G, int8_t* spins,
@@ -165,7 +176,7 @@ int batch_warps();
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches);
+                            int* launches, int variant = 0);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st);
@@ -178,6 +189,8 @@ cudaError_t launch_best_slice(const double* energies, int R, int T, int32_t* bes
 // Kernel limits used by the planner.
 int sa_colour_max_smem_sites();
 int msc_max_degree();
+int msc_default_threads();
+int split_default_threads();
 cudaError_t msc_prepare(oj_graph* g, int P, std::string* why);
 int msc_choose_cluster(const oj_graph* g, int G, int sm_count);
 

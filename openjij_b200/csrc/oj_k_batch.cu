@@ -255,11 +255,14 @@ int batch_warps() { return kBatchWarps; }
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches) {
+                            int* launches, int variant) {
   const size_t smem = (size_t)kBatchWarps * kBatchMaxN * sizeof(float);
   // two register budgets: 80 per thread (3 CTAs per SM) or 64 (4 CTAs per SM)
-  int variant = 3;
-  if (const char* env = std::getenv("OJ_BATCH_MINB")) variant = std::atoi(env) == 4 ? 4 : 3;
+  if (variant == 0) {
+    variant = 3;
+    if (const char* env = std::getenv("OJ_BATCH_MINB")) variant = std::atoi(env) == 4 ? 4 : 3;
+  }
+  if (variant != 3 && variant != 4) return cudaErrorInvalidValue;
   auto kern = variant == 4 ? sa_batch_kernel<4> : sa_batch_kernel<3>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

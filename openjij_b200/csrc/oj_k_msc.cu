@@ -246,7 +246,7 @@ int msc_threads() {
 }
 
 template <int D>
-cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st) {
+cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st, int threads) {
   auto kern = sa_msc_kernel<D>;
   const size_t smem = msc_smem_bytes(pl);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -257,7 +257,7 @@ cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(pl.P, G, 1);
-  cfg.blockDim = dim3(msc_threads(), 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -273,6 +273,7 @@ cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st
 }  // namespace
 
 int msc_max_degree() { return kMscMaxDegree; }
+int msc_default_threads() { return msc_threads(); }
 
 // Cluster size: the number of CTAs per replica group.  One CTA per SM, as
 // many CTAs as fit on the SMs (measured on the L=128 lattice: one 512-thread
@@ -430,7 +431,9 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
 
 cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint32_t* thr,
                           const uint32_t* always, int64_t nsweeps, RngBase rb, cudaStream_t st,
-                          int* launches) {
+                          int* launches, int threads) {
+  if (threads == 0) threads = msc_threads();
+  if (threads < 32 || threads > kMscMaxThreads || threads % 32) return cudaErrorInvalidValue;
   const MscPlan& pl = *g->msc;
   MscArgs a;
   a.gidx = pl.gidx;
@@ -455,14 +458,14 @@ cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint3
   a.group0 = rb.rep0 >> 5;
   if (launches) ++*launches;
   switch (pl.D) {
-    case 1: return launch_d<1>(pl, a, G, st);
-    case 2: return launch_d<2>(pl, a, G, st);
-    case 3: return launch_d<3>(pl, a, G, st);
-    case 4: return launch_d<4>(pl, a, G, st);
-    case 5: return launch_d<5>(pl, a, G, st);
-    case 6: return launch_d<6>(pl, a, G, st);
-    case 7: return launch_d<7>(pl, a, G, st);
-    case 8: return launch_d<8>(pl, a, G, st);
+    case 1: return launch_d<1>(pl, a, G, st, threads);
+    case 2: return launch_d<2>(pl, a, G, st, threads);
+    case 3: return launch_d<3>(pl, a, G, st, threads);
+    case 4: return launch_d<4>(pl, a, G, st, threads);
+    case 5: return launch_d<5>(pl, a, G, st, threads);
+    case 6: return launch_d<6>(pl, a, G, st, threads);
+    case 7: return launch_d<7>(pl, a, G, st, threads);
+    case 8: return launch_d<8>(pl, a, G, st, threads);
     default: return cudaErrorInvalidValue;
   }
 }

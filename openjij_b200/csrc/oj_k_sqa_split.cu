@@ -304,14 +304,14 @@ int split_threads() {
 }
 
 template <int D>
-cudaError_t launch_d(const MscPlan& pl, const SplitArgs& a, int G, cudaStream_t st) {
+cudaError_t launch_d(const MscPlan& pl, const SplitArgs& a, int G, cudaStream_t st, int threads) {
   const size_t smem = split_smem_bytes(pl);
   if (smem > kSplitSmemBytes) return cudaErrorInvalidValue;
   if (pl.P == 1) {
     auto k1 = sqa_split_kernel<D, false>;
     cudaError_t e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k1<<<dim3(1, G, 1), split_threads(), smem, st>>>(a);
+    k1<<<dim3(1, G, 1), threads, smem, st>>>(a);
     return cudaGetLastError();
   }
   auto kern = sqa_split_kernel<D, true>;
@@ -323,7 +323,7 @@ cudaError_t launch_d(const MscPlan& pl, const SplitArgs& a, int G, cudaStream_t 
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(pl.P, G, 1);
-  cfg.blockDim = dim3(split_threads(), 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -337,6 +337,8 @@ cudaError_t launch_d(const MscPlan& pl, const SplitArgs& a, int G, cudaStream_t 
 }
 
 }  // namespace
+
+int split_default_threads() { return split_threads(); }
 
 int sqa_split_replicas_per_group(int T) {
   const int H = T / 2;
@@ -353,13 +355,14 @@ bool sqa_split_applies(const oj_graph* g, int T) {
 // Cluster size for G replica groups: as many CTAs per group as the SMs allow
 // (one CTA per SM), at least 256 sites per CTA, and a partition whose two
 // halves, halo and tables fit the shared-memory budget.
-cudaError_t sqa_split_prepare(oj_graph* g, int G, int sm_count, std::string* why) {
+cudaError_t sqa_split_prepare(oj_graph* g, int G, int sm_count, std::string* why, int cluster) {
   int P = std::max(1, std::min(kSplitMaxCluster, sm_count / std::max(G, 1)));
   while (P > 1 && g->n / P < 256) --P;
   if (const char* env = std::getenv("OJ_SQA_CLUSTER")) {
     const int v = std::atoi(env);
     if (v >= 1 && v <= kSplitMaxCluster && v <= g->n) P = v;
   }
+  if (cluster >= 1 && cluster <= kSplitMaxCluster && cluster <= g->n) P = cluster;
   for (; P <= kSplitMaxCluster; ++P) {
     std::string w;
     const cudaError_t e = msc_prepare(g, P, &w);
@@ -371,7 +374,10 @@ cudaError_t sqa_split_prepare(oj_graph* g, int G, int sm_count, std::string* why
 }
 
 cudaError_t launch_sqa_split(const oj_graph* g, int G, int T, uint32_t* words, const uint32_t* thr,
-                             const uint32_t* mode, int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches) {
+                             const uint32_t* mode, int64_t nsweeps, RngBase rb, cudaStream_t st, int* launches,
+                             int threads) {
+  if (threads == 0) threads = split_threads();
+  if (threads < 32 || threads > kSplitMaxThreads || threads % 32) return cudaErrorInvalidValue;
   const MscPlan& pl = *g->msc;
   SplitArgs a;
   a.gidx = pl.gidx;
@@ -405,14 +411,14 @@ cudaError_t launch_sqa_split(const oj_graph* g, int G, int T, uint32_t* words, c
   a.group0 = rb.rep0 / (uint32_t)P;
   if (launches) ++*launches;
   switch (pl.D) {
-    case 1: return launch_d<1>(pl, a, G, st);
-    case 2: return launch_d<2>(pl, a, G, st);
-    case 3: return launch_d<3>(pl, a, G, st);
-    case 4: return launch_d<4>(pl, a, G, st);
-    case 5: return launch_d<5>(pl, a, G, st);
-    case 6: return launch_d<6>(pl, a, G, st);
-    case 7: return launch_d<7>(pl, a, G, st);
-    case 8: return launch_d<8>(pl, a, G, st);
+    case 1: return launch_d<1>(pl, a, G, st, threads);
+    case 2: return launch_d<2>(pl, a, G, st, threads);
+    case 3: return launch_d<3>(pl, a, G, st, threads);
+    case 4: return launch_d<4>(pl, a, G, st, threads);
+    case 5: return launch_d<5>(pl, a, G, st, threads);
+    case 6: return launch_d<6>(pl, a, G, st, threads);
+    case 7: return launch_d<7>(pl, a, G, st, threads);
+    case 8: return launch_d<8>(pl, a, G, st, threads);
     default: return cudaErrorInvalidValue;
   }
 }
