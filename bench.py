@@ -622,8 +622,10 @@ def run_tts(args):
         rng = np.random.default_rng(7)
         shape = (R, n) if w["kind"] == "sa" else (R, T, n)
         init = rng.choice(np.array([-1, 1], np.int8), size=shape)
-        methods = {"batched": "dense_tc" if args.config == 3 else "bitpacked",
+        methods = {"batched": "dense_jump" if args.config == 3 else "bitpacked",
                    "plain": "dense_plain" if args.config == 3 else "colour"}
+        if args.kernel:
+            methods["batched"] = args.kernel
         for Sl in ladder:
             for meth, kern in methods.items():
                 sp = init.copy()

@@ -56,6 +56,9 @@ enum {
 #define OJ_KERNEL_DENSE_PLAIN (2u << OJ_KERNEL_SHIFT) /* sequential dense, one warp per replica, FP32 */
 #define OJ_KERNEL_BITPACKED (3u << OJ_KERNEL_SHIFT)  /* 32 replicas per word, couplings +-c, h = 0 */
 #define OJ_KERNEL_DENSE_TC (4u << OJ_KERNEL_SHIFT)   /* sequential dense, delayed tensor-core field updates */
+#define OJ_KERNEL_DENSE_JUMP (5u << OJ_KERNEL_SHIFT) /* sequential dense, one warp per replica evaluating 128
+                                                        sites at once and jumping between accepted flips
+                                                        (the batched kernel on one instance), n <= 4096 */
 
 typedef struct oj_ctx oj_ctx;
 typedef struct oj_graph oj_graph;

@@ -26,7 +26,7 @@ OJ_ERR_NODEVICE = 7
 OJ_DEVICE_POINTERS = 0x1
 OJ_AUTOTUNE = 0x2
 KERNEL_SHIFT = 4
-KERNELS = {"auto": 0, "colour": 1, "dense_plain": 2, "bitpacked": 3, "dense_tc": 4}
+KERNELS = {"auto": 0, "colour": 1, "dense_plain": 2, "bitpacked": 3, "dense_tc": 4, "dense_jump": 5}
 KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
 
 # every symbol the header declares

@@ -146,6 +146,46 @@ void sqa_msc_thresholds(const std::vector<float2>& coef, double c, int D, std::v
   }
 }
 
+oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset, const double* J_aug,
+                      oj_batch** out);
+
+// The graph's augmented matrix as a one-instance batch: FP32 padded rows for
+// the dense jump kernel and the FP64 matrix for the replica-parallel energies.
+oj_status ensure_single(oj_ctx* ctx, oj_graph* g) {
+  if (g->single) return OJ_OK;
+  const int n = g->n;
+  const int64_t n1 = (int64_t)n + 1;
+  std::vector<double> A;
+  try {
+    A.assign((size_t)(n1 * n1), 0.0);
+  } catch (...) {
+    return OJ_ERR_OOM;
+  }
+  for (int64_t i = 0; i < n1; ++i)
+    for (int64_t q = g->aug_indptr[i]; q < g->aug_indptr[i + 1]; ++q)
+      A[(size_t)(i * n1 + g->aug_indices[q])] = g->aug_data[q];
+  const int32_t nn = n;
+  const int64_t off = 0;
+  oj_batch* b1 = nullptr;
+  if (oj_status bs = build_batch(ctx, 1, &nn, &off, A.data(), &b1)) return bs;
+  g->single.reset(b1);
+  return OJ_OK;
+}
+
+// FP64 energies of R replicas of a dense graph with the batched energy kernel
+// (the coupling matrix is read once per 32 replicas).
+cudaError_t single_energy(oj_graph* g, int R, const int8_t* spins, double* out, cudaStream_t st) {
+  struct Tab {
+    int32_t reads, order;
+    int64_t soff, eoff;
+  } h{R, 0, 0, 0};
+  cudaError_t e = g->single_tab.ensure(sizeof(Tab));
+  if (e != cudaSuccess) return e;
+  Tab* d = g->single_tab.as<Tab>();
+  if ((e = cudaMemcpyAsync(d, &h, sizeof(Tab), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  return launch_batch_energy(g->single.get(), &d->reads, &d->soff, &d->eoff, &d->order, R, spins, out, st);
+}
+
 bool autotune_requested(uint32_t flags) {
   if (flags & OJ_AUTOTUNE) return true;
   const char* e = std::getenv("OJ_AUTOTUNE");
@@ -385,11 +425,14 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     if (inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1) {
       kernel = OJ_KERNEL_BITPACKED;
     } else if (inf.num_colours > 64 && (int64_t)n * n * 4 <= ((int64_t)8 << 30)) {
-      // dense: delayed tensor-core field updates when there are enough 128-replica
-      // tiles to occupy the GPU, else the sequential warp-per-replica kernel
+      // dense: one warp per replica jumping between accepted flips (fastest
+      // measured on dense QUBOs), else the tensor-core kernel for many replicas,
+      // else the plain sequential kernel
       std::string why;
-      kernel = (R >= 512 && n >= 256 && dense_tc_prepare(g, &why) == cudaSuccess) ? OJ_KERNEL_DENSE_TC
-                                                                                  : OJ_KERNEL_DENSE_PLAIN;
+      if (n <= batch_max_sites())
+        kernel = OJ_KERNEL_DENSE_JUMP;
+      else
+        kernel = (R >= 512 && dense_tc_prepare(g, &why) == cudaSuccess) ? OJ_KERNEL_DENSE_TC : OJ_KERNEL_DENSE_PLAIN;
     } else {
       kernel = OJ_KERNEL_COLOUR;
     }
@@ -397,6 +440,11 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   if (kernel == OJ_KERNEL_BITPACKED &&
       !(inf.bimodal && g->regular && inf.max_degree <= msc_max_degree() && inf.max_degree >= 1)) {
     ctx->last_error = "bit-packed kernel needs a regular graph with couplings +-c (degree <= 8) and h = 0";
+    return OJ_ERR_UNSUPPORTED;
+  }
+  if (kernel > OJ_KERNEL_DENSE_JUMP) return arg_fail(ctx, "unknown kernel");
+  if (kernel == OJ_KERNEL_DENSE_JUMP && n > batch_max_sites()) {
+    ctx->last_error = "dense jump kernel supports n <= 4096";
     return OJ_ERR_UNSUPPORTED;
   }
   if (kernel == OJ_KERNEL_DENSE_TC) {
@@ -488,6 +536,37 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_unpack(d_words, R, n, d_spins, st), "unpack");
     ++launches;
+  } else if (kernel == OJ_KERNEL_DENSE_JUMP) {
+    if (oj_status bs = ensure_single(ctx, g)) return bs;
+    const int W = batch_warps();
+    std::vector<int32_t> items;
+    for (int gq = 0; gq * W < R; ++gq) {
+      items.push_back(0);
+      items.push_back(gq);
+    }
+    const int nitems = (int)(items.size() / 2);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t b_hdr = al(4 + 8), b_items = al(items.size() * 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4);
+    OJ_CK(ctx->batch.ensure(b_hdr + b_items + b_cnt + b_beta), "alloc tables");
+    char* base = ctx->batch.as<char>();
+    int32_t* d_reads = reinterpret_cast<int32_t*>(base);
+    int64_t* d_soff = reinterpret_cast<int64_t*>(base + 8);
+    int32_t* d_items = reinterpret_cast<int32_t*>(base + b_hdr);
+    int* d_counter = reinterpret_cast<int*>(base + b_hdr + b_items);
+    float* d_beta = reinterpret_cast<float*>(base + b_hdr + b_items + b_cnt);
+    const int32_t hreads = R;
+    const int64_t hsoff = 0;
+    OJ_CK(cudaMemcpyAsync(d_reads, &hreads, 4, cudaMemcpyHostToDevice, st), "H2D reads");
+    OJ_CK(cudaMemcpyAsync(d_soff, &hsoff, 8, cudaMemcpyHostToDevice, st), "H2D offsets");
+    OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
+    if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+    if (S > 0)
+      OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb, 0,
+                            ctx->sm_count, st, &launches),
+            "sa dense jump kernel");
+    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+    threads_used = W * 32;
   } else {
     OJ_CK(ctx->params.ensure(std::max<size_t>(bf.size() * 4, 16)), "alloc params");
     float* d_beta = ctx->params.as<float>();
@@ -511,7 +590,11 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
       d_e = ctx->energies.as<double>();
     }
-    OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+    const bool dense = kernel == OJ_KERNEL_DENSE_PLAIN || kernel == OJ_KERNEL_DENSE_TC || kernel == OJ_KERNEL_DENSE_JUMP;
+    if (dense && n <= batch_max_sites() && ensure_single(ctx, g) == OJ_OK)
+      OJ_CK(single_energy(g, R, d_spins, d_e, st), "energy kernel");
+    else
+      OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
     ++launches;
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
   }
@@ -761,6 +844,14 @@ oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t R, const int8_t* spi
 
 oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset,
                                 const double* J_aug, oj_batch** out) {
+  return build_batch(ctx, count, n, offset, J_aug, out);
+}
+
+}  // extern "C"
+
+namespace {
+oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset, const double* J_aug,
+                      oj_batch** out) {
   if (!ctx || !out || count < 0 || (count > 0 && (!n || !offset || !J_aug)))
     return arg_fail(ctx, "null argument or negative size");
   *out = nullptr;
@@ -769,7 +860,7 @@ oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, co
   int64_t tot32 = 0, toth = 0, tot64 = 0;
   int max_n = 0;
   for (int32_t k = 0; k < count; ++k) {
-    if (n[k] < 0 || n[k] > nmax) return arg_fail(ctx, "batched instances need 0 <= n <= 1024");
+    if (n[k] < 0 || n[k] > nmax) return arg_fail(ctx, "batched instances need 0 <= n <= 4096");
     if (offset[k] < 0) return arg_fail(ctx, "negative instance offset");
     const int64_t npad = ((int64_t)n[k] + 127) / 128 * 128;
     joff[k] = tot32;
@@ -826,6 +917,9 @@ oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, co
   *out = b.release();
   return OJ_OK;
 }
+}  // namespace
+
+extern "C" {
 
 oj_status oj_batch_destroy(oj_batch* b) {
   delete b;

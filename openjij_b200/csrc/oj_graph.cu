@@ -45,6 +45,8 @@ oj_graph::~oj_graph() {
   d_dense.release();
   sqa_nbr.release();
   sqa_jm.release();
+  single.reset();
+  single_tab.release();
   if (msc) msc->tables.release();
   if (tc) {
     tc->bt_hi.release();

@@ -104,6 +104,8 @@ struct oj_graph {
   std::unique_ptr<oj::TcPlan> tc;
   oj::DevBuf sqa_nbr, sqa_jm;  // bit-packed SQA tables: [n][D] neighbours (u16), [n] J>0 masks
   std::map<uint64_t, oj::Shape> tuned;  // autotuned launch shapes by (kernel, replicas, slices)
+  std::unique_ptr<oj_batch> single;     // this graph as a one-instance batch (dense jump kernel, energies)
+  oj::DevBuf single_tab;                // its per-call tables: reads, order, replica and energy offsets
   ~oj_graph();
 };
 

@@ -6,7 +6,8 @@
 // until the queue is empty.  One warp runs one replica: its FP32 local fields
 // live in the warp's slice of shared memory, laid out in 128-site chunks with
 // lane l owning sites 4l..4l+3 of every chunk (one float4 per lane), and its
-// spins are bits of one register per lane (bit 4c+e = site 128c+4l+e is -1).
+// spins are bits in shared memory, one word per (chunk c, lane l) with bit e set
+// when site 128c+4l+e is -1.
 //
 // Update order and acceptance are the reference's sequential single-spin flip
 // (include/openjij/updater/single_spin_flip.hpp:66-95): sites 0..n-1 in order,
@@ -18,7 +19,8 @@
 // re-evaluates the sites after it: sites that do not flip leave the state
 // unchanged, so this is the sequential sweep, with one step per flip instead
 // of one per site.  The uniform of site i, sweep k, replica r of instance m is
-// Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3].
+// Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3], r the replica's global
+// index (rep0 + index within the instance).
 //
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
 // read through L1 one float4 per lane on every accepted flip; h likewise.
@@ -34,7 +36,8 @@ namespace oj {
 namespace {
 
 constexpr int kBatchWarps = 8;
-constexpr int kBatchMaxN = 1024;
+constexpr int kBatchMaxN = 4096;
+constexpr int kMaxChunks = kBatchMaxN / 128;
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -53,6 +56,8 @@ struct BatchArgs {
   ojd::Keys keys;
   uint32_t sweep0;
   uint32_t inst0;          // global index of instance 0
+  uint32_t rep0;           // global index of each instance's replica 0
+  int fstride;             // fields per warp in shared memory (multiple of 128)
 };
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
@@ -62,7 +67,9 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* f = shb + (size_t)warp * kBatchMaxN;  // this warp's fields, float4 per lane per chunk
+  float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
+  uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)kBatchWarps * a.fstride) +
+                 (size_t)warp * (a.fstride / 4);  // spin words [chunk][lane]
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
@@ -79,13 +86,16 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
     const float* h = a.h + a.hoff[m];
     int8_t* gs = a.spins + a.soff[m] + (size_t)r * n;
     // spins -> bits
-    uint32_t sb = 0u;
-    for (int c = 0; c < nch; ++c)
+    for (int c = 0; c < nch; ++c) {
+      uint32_t w = 0u;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int i = 128 * c + 4 * lane + e;
-        if (i < n && gs[i] < 0) sb |= 1u << (4 * c + e);
+        if (i < n && gs[i] < 0) w |= 1u << e;
       }
+      sw[32 * c + lane] = w;
+    }
+    __syncwarp();
     // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j)
     for (int c = 0; c < nch; ++c) {
       float4 acc = ldg4(h + 128 * c + 4 * lane);
@@ -98,9 +108,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int i = i0 + q;
-          const uint32_t wi = __shfl_sync(0xffffffffu, sb, (i & 127) >> 2);
           if (i < n) {
-            const bool neg = (wi >> (4 * (i >> 7) + (i & 3))) & 1u;
+            const bool neg = (sw[32 * (i >> 7) + ((i & 127) >> 2)] >> (i & 3)) & 1u;
             acc.x = __fadd_rn(acc.x, neg ? -v[q].x : v[q].x);
             acc.y = __fadd_rn(acc.y, neg ? -v[q].y : v[q].y);
             acc.z = __fadd_rn(acc.z, neg ? -v[q].z : v[q].z);
@@ -112,11 +121,12 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
     }
     __syncwarp();
     const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
+    const uint32_t rg = a.rep0 + (uint32_t)r;
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta = __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
       for (int c = 0; c < nch; ++c) {
-        const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, (uint32_t)r, tag, a.keys);
+        const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
         float L[4];
         L[0] = ojd::neglog(x.x);
         L[1] = ojd::neglog(x.y);
@@ -126,11 +136,12 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
         for (;;) {
           const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
           const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
+          const uint32_t myw = sw[32 * c + lane];
           uint32_t mask = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int t = 4 * lane + e;
-            const bool neg = (sb >> (4 * c + e)) & 1u;
+            const bool neg = (myw >> e) & 1u;
             const float dE = neg ? 2.0f * fv[e] : -2.0f * fv[e];
             const bool acc = dE <= 0.0f || __fmul_rn(beta, dE) < L[e];
             if (acc && t >= pos && 128 * c + t < n) mask |= 1u << e;
@@ -140,14 +151,14 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
           const int ls = __ffs(lanes) - 1;
           const uint32_t ms = __shfl_sync(0xffffffffu, mask, ls);
           const int es = __ffs(ms) - 1;
-          const uint32_t ws = __shfl_sync(0xffffffffu, sb, ls);
-          const bool neg = (ws >> (4 * c + es)) & 1u;
+          const uint32_t ws = sw[32 * c + ls];
+          const bool neg = (ws >> es) & 1u;
           const float coef = neg ? 2.0f : -2.0f;
           const int i = 128 * c + 4 * ls + es;
           const float* Ji = J + (size_t)i * npad + 4 * lane;
           // the row in groups of four chunks whose loads are in flight together
 #pragma unroll
-          for (int c0 = 0; c0 < kBatchMaxN / 128; c0 += 4) {
+          for (int c0 = 0; c0 < kMaxChunks; c0 += 4) {
             if (c0 >= nch) break;
             float4 v[4];
 #pragma unroll
@@ -164,18 +175,21 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
                 reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g;
               }
           }
-          if (lane == ls) sb ^= 1u << (4 * c + es);
+          __syncwarp();
+          if (lane == ls) sw[32 * c + ls] = ws ^ (1u << es);
           pos = 4 * ls + es + 1;
           __syncwarp();
         }
       }
     }
-    for (int c = 0; c < nch; ++c)
+    for (int c = 0; c < nch; ++c) {
+      const uint32_t w = sw[32 * c + lane];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int i = 128 * c + 4 * lane + e;
-        if (i < n) gs[i] = ((sb >> (4 * c + e)) & 1u) ? (int8_t)-1 : (int8_t)1;
+        if (i < n) gs[i] = ((w >> e) & 1u) ? (int8_t)-1 : (int8_t)1;
       }
+    }
     __syncwarp();
   }
 }
@@ -256,7 +270,8 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
                             int* launches, int variant) {
-  const size_t smem = (size_t)kBatchWarps * kBatchMaxN * sizeof(float);
+  const int fstride = std::max(128, (b->max_n + 127) / 128 * 128);
+  const size_t smem = (size_t)kBatchWarps * fstride * 5;  // FP32 fields + spin words
   // two register budgets: 80 per thread (3 CTAs per SM) or 64 (4 CTAs per SM)
   if (variant == 0) {
     variant = 3;
@@ -287,6 +302,8 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.keys = ojd::make_keys(rb.k0, rb.k1);
   a.sweep0 = rb.sweep0;
   a.inst0 = inst0;
+  a.rep0 = rb.rep0;
+  a.fstride = fstride;
   e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   kern<<<grid, kBatchWarps * 32, smem, st>>>(a);

@@ -93,7 +93,7 @@ def test_batched_device_pointers(ctx):
 
 
 def test_batched_rejects_bad_input(ctx):
-    big = np.zeros((1026, 1026))
+    big = np.zeros((4098, 4098))  # n = 4097 > 4096
     big[-1, -1] = 1.0
     with pytest.raises(N.OJError) as ei:
         N.Batch(ctx, [big])
@@ -108,3 +108,33 @@ def test_batched_rejects_bad_input(ctx):
         N.sa_run_batched(b, [-1], np.zeros(5, np.int8), [1.0], [1], seed=1)
     # no replicas at all: nothing runs
     N.sa_run_batched(b, [0], np.zeros(0, np.int8), [1.0], [1], seed=1)
+
+
+@pytest.mark.parametrize("n,R,kind", [(50, 3, "integer"), (300, 17, "normal"), (2048, 8, "integer"),
+                                      (4096, 2, "normal")])
+def test_dense_jump_kernel_bit_exact(ctx, n, R, kind):
+    """oj_sa_run with OJ_KERNEL_DENSE_JUMP (the batched kernel on one graph)
+    against the batched replay of that single instance."""
+    A = (I.dense_qubo_int(n, seed=n) if kind == "integer" else I.dense_qubo_normal(n, seed=n))[0].toarray()
+    g = N.Graph(ctx, *I.augmented_csr(A))
+    betas, mcs = I.geometric_betas(0.1, 5.0, 4 if n >= 2048 else 20)
+    s0 = np.random.default_rng(n).choice(np.array([-1, 1], np.int8), size=(R, n))
+    s = s0.copy()
+    e = np.zeros(R)
+    st = N.sa_run(g, s, betas, mcs, seed=31, kernel="dense_jump", energies=e)
+    assert st["kernel"] == "dense_jump"
+    ref = O.replay_sa_batch([A], [R], s0.ravel(), _per_sweep(betas, mcs), 31).reshape(R, n)
+    np.testing.assert_array_equal(s, ref)
+    np.testing.assert_allclose(e, _energies([A], [R], ref.ravel()), rtol=1e-12, atol=1e-9)
+
+
+def test_dense_jump_replica_shards(ctx):
+    A = I.dense_qubo_normal(200, seed=5)[0].toarray()
+    g = N.Graph(ctx, *I.augmented_csr(A))
+    betas, mcs = I.geometric_betas(0.1, 5.0, 15)
+    s0 = np.random.default_rng(9).choice(np.array([-1, 1], np.int8), size=(64, 200))
+    whole = s0.copy()
+    N.sa_run(g, whole, betas, mcs, seed=3, kernel="dense_jump")
+    part = s0[32:].copy()
+    N.sa_run(g, part, betas, mcs, seed=3, kernel="dense_jump", replica_offset=32)
+    np.testing.assert_array_equal(part, whole[32:])
