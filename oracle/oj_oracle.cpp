@@ -496,7 +496,7 @@ void orc_ref_sqa_many(int n, const int64_t* indptr, const int32_t* indices, cons
 // betas_f: one FP32 beta per sweep (schedule already expanded).
 void orc_replay_sa(int n, const int64_t* indptr, const int32_t* indices, const double* data,
                    int R, int8_t* spins, const float* betas_f, int64_t nsweeps, uint64_t seed,
-                   int mode, int threads) {
+                   int mode, int threads, uint32_t rep0, uint32_t sweep0) {
   Aug g{n, indptr, indices, data};
   Nbr b = make_nbr(g);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
@@ -514,9 +514,10 @@ void orc_replay_sa(int n, const int64_t* indptr, const int32_t* indices, const d
   }
   parallel_for(R, threads, [&](int r) {
     int8_t* s = spins + (size_t)r * n;
+    const uint32_t rg = rep0 + (uint32_t)r;  // global replica index
     auto draw = [&](int i, int64_t k) {
-      P4 q = philox((uint32_t)i, (uint32_t)k, (uint32_t)(r >> 2), TAG_SA, k0, k1);
-      return q.v[r & 3];
+      P4 q = philox((uint32_t)i, sweep0 + (uint32_t)k, rg >> 2, TAG_SA, k0, k1);
+      return q.v[rg & 3];
     };
     if (mode == 0) {
       for (int64_t k = 0; k < nsweeps; ++k) {

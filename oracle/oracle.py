@@ -64,7 +64,7 @@ def lib():
         L.orc_ref_sqa_many.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p,
                                        C.c_double, _f64p, _f64p, _i64p, C.c_int64, _u64p, C.c_int]
         L.orc_replay_sa.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f32p, C.c_int64,
-                                    C.c_uint64, C.c_int, C.c_int]
+                                    C.c_uint64, C.c_int, C.c_int, C.c_uint32, C.c_uint32]
         L.orc_replay_sqa.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _f32p,
                                      _f32p, C.c_int64, C.c_uint64, C.c_int]
         L.orc_replay_sa_msc.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _u32p, _u32p,
@@ -246,11 +246,12 @@ def ref_sqa_many(g: AugCSR, init3d, gamma, betas, ss, mcs, seeds, threads=None):
 # replays of the B200 kernels
 # ---------------------------------------------------------------------------
 
-def replay_sa(g: AugCSR, init2d, betas_per_sweep, seed, mode="colour", threads=None):
+def replay_sa(g: AugCSR, init2d, betas_per_sweep, seed, mode="colour", threads=None, rep0=0, sweep0=0):
+    """rep0 / sweep0: global index of replica 0 and of the first sweep (shards, split runs)."""
     s = np.array(init2d, np.int8, copy=True, order="C")
     b = np.ascontiguousarray(betas_per_sweep, np.float32)
     lib().orc_replay_sa(*g.args(), s.shape[0], s, b, len(b), int(seed),
-                        0 if mode == "colour" else 1, _threads(threads))
+                        0 if mode == "colour" else 1, _threads(threads), int(rep0), int(sweep0))
     return s
 
 
