@@ -83,6 +83,37 @@ std::vector<int32_t> greedy_colouring(int n, const std::vector<int32_t>& rp, con
   return col;
 }
 
+// Evens out the classes of a proper colouring (the colour-class kernels run
+// one class per phase with a barrier between phases, so the largest class
+// sets the phase time).  target = ceil(n / ncol); a pass visits the sites in
+// index order and moves a site whose class is above the target into the
+// lowest colour whose class is below the target and holds none of its
+// neighbours; passes repeat until one moves nothing (at most 8).  The
+// colouring stays proper and keeps ncol classes.
+void balance_colouring(int n, const std::vector<int32_t>& rp, const std::vector<int32_t>& ci, int ncol,
+                       std::vector<int32_t>& col) {
+  if (ncol < 2 || n == 0) return;
+  const int target = (n + ncol - 1) / ncol;
+  std::vector<int> size(ncol, 0), mark(ncol, -1);
+  for (int i = 0; i < n; ++i) size[col[i]]++;
+  for (int pass = 0; pass < 8; ++pass) {
+    bool moved = false;
+    for (int i = 0; i < n; ++i) {
+      if (size[col[i]] <= target) continue;
+      for (int q = rp[i]; q < rp[i + 1]; ++q) mark[col[ci[q]]] = i;
+      for (int c = 0; c < ncol; ++c)
+        if (size[c] < target && mark[c] != i) {
+          size[col[i]]--;
+          size[c]++;
+          col[i] = c;
+          moved = true;
+          break;
+        }
+    }
+    if (!moved) break;
+  }
+}
+
 template <class T>
 static cudaError_t upload(DevBuf& b, const std::vector<T>& v) {
   const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
@@ -161,6 +192,7 @@ oj_status finish_graph(oj_ctx* ctx, oj_graph* g) {
   inf.nnz = (int64_t)g->ci.size();
   int ncol = 0;
   g->colour = greedy_colouring(n, g->rp, g->ci, &ncol);
+  balance_colouring(n, g->rp, g->ci, ncol, g->colour);
   inf.num_colours = ncol;
   int dmax = 0, dmin = n > 0 ? 1 << 30 : 0;
   for (int i = 0; i < n; ++i) {

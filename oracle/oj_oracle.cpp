@@ -265,6 +265,39 @@ std::vector<int> greedy_colour(int n, const int64_t* rp, const int32_t* ci) {
   return col;
 }
 
+// The colouring the colour-class kernels use: the greedy colouring above with
+// its classes evened out.  With target t = ceil(n / ncol), each pass goes over
+// the sites 0..n-1 and puts a site whose class holds more than t sites into
+// the smallest-index colour whose class holds fewer than t sites and none of
+// the site's neighbours; passes stop after one without a move, or after 8.
+std::vector<int> kernel_colour(int n, const int64_t* rp, const int32_t* ci) {
+  std::vector<int> col = greedy_colour(n, rp, ci);
+  int ncol = 0;
+  for (int c : col) ncol = std::max(ncol, c + 1);
+  if (ncol < 2) return col;
+  const int t = (n + ncol - 1) / ncol;
+  std::vector<int> cnt(ncol, 0);
+  for (int c : col) ++cnt[c];
+  for (int pass = 0; pass < 8; ++pass) {
+    int moves = 0;
+    for (int i = 0; i < n; ++i) {
+      if (cnt[col[i]] <= t) continue;
+      std::vector<char> used(ncol, 0);
+      for (int64_t p = rp[i]; p < rp[i + 1]; ++p) used[col[ci[p]]] = 1;
+      for (int c = 0; c < ncol; ++c) {
+        if (cnt[c] >= t || used[c]) continue;
+        --cnt[col[i]];
+        ++cnt[c];
+        col[i] = c;
+        ++moves;
+        break;
+      }
+    }
+    if (moves == 0) break;
+  }
+  return col;
+}
+
 // Site neighbour lists (excluding the diagonal and the dummy column n) in CSR
 // column order, and h_i, both rounded to FP32 — the data the kernels hold.
 struct Nbr {
@@ -324,6 +357,11 @@ float orc_neglog(uint32_t x) { return neglog(x); }
 
 void orc_greedy_colour(int n, const int64_t* rp, const int32_t* ci, int32_t* out) {
   auto c = greedy_colour(n, rp, ci);
+  for (int i = 0; i < n; ++i) out[i] = c[i];
+}
+
+void orc_kernel_colour(int n, const int64_t* rp, const int32_t* ci, int32_t* out) {
+  auto c = kernel_colour(n, rp, ci);
   for (int i = 0; i < n; ++i) out[i] = c[i];
 }
 
@@ -500,7 +538,7 @@ void orc_replay_sa(int n, const int64_t* indptr, const int32_t* indices, const d
   Aug g{n, indptr, indices, data};
   Nbr b = make_nbr(g);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  std::vector<int> col = kernel_colour(n, b.rp.data(), b.ci.data());
   int ncol = 0;
   for (int c : col) ncol = std::max(ncol, c + 1);
   std::vector<std::vector<int>> by_col(ncol);
@@ -571,7 +609,7 @@ void orc_replay_sqa(int n, const int64_t* indptr, const int32_t* indices, const 
   Aug g{n, indptr, indices, data};
   Nbr b = make_nbr(g);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  std::vector<int> col = kernel_colour(n, b.rp.data(), b.ci.data());
   int ncol = 0;
   for (int c : col) ncol = std::max(ncol, c + 1);
   std::vector<std::vector<int>> by_col(ncol);
@@ -623,7 +661,7 @@ void orc_replay_sa_msc(int n, const int64_t* indptr, const int32_t* indices, con
   Aug g{n, indptr, indices, data};
   Nbr b = make_nbr(g);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  std::vector<int> col = kernel_colour(n, b.rp.data(), b.ci.data());
   int ncol = 0;
   for (int c : col) ncol = std::max(ncol, c + 1);
   std::vector<std::vector<int>> by_col(ncol);
@@ -722,7 +760,7 @@ void orc_replay_sqa_msc(int n, const int64_t* indptr, const int32_t* indices, co
   Aug g{n, indptr, indices, data};
   Nbr b = make_nbr(g);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  std::vector<int> col = kernel_colour(n, b.rp.data(), b.ci.data());
   int ncol = 0;
   for (int c : col) ncol = std::max(ncol, c + 1);
   std::vector<std::vector<int>> by_col(ncol);
@@ -830,7 +868,7 @@ void orc_replay_sqa_split(int n, const int64_t* indptr, const int32_t* indices, 
   Aug g{n, indptr, indices, data};
   Nbr b = make_nbr(g);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int> col = greedy_colour(n, b.rp.data(), b.ci.data());
+  std::vector<int> col = kernel_colour(n, b.rp.data(), b.ci.data());
   int ncol = 0;
   for (int c : col) ncol = std::max(ncol, c + 1);
   std::vector<std::vector<int>> by_col(ncol);

@@ -50,6 +50,7 @@ def lib():
         L.orc_neglog.argtypes = [C.c_uint32]
         L.orc_neglog.restype = C.c_float
         L.orc_greedy_colour.argtypes = [C.c_int, _i64p, _i32p, _i32p]
+        L.orc_kernel_colour.argtypes = [C.c_int, _i64p, _i32p, _i32p]
         L.orc_gen_spin.argtypes = [C.c_uint64, C.c_int, C.c_int, _i8p]
         L.orc_classical_schedule.argtypes = [C.c_double, C.c_double, C.c_int64, _f64p]
         L.orc_transverse_schedule.argtypes = [C.c_int64, _f64p]
@@ -150,6 +151,14 @@ def greedy_colour(g: AugCSR):
     nb = neighbour_csr(g)
     out = np.zeros(g.n, np.int32)
     lib().orc_greedy_colour(g.n, nb[0], nb[1], out)
+    return out
+
+
+def kernel_colour(g: AugCSR):
+    """The colouring the colour-class kernels sweep by: greedy, classes evened out."""
+    nb = neighbour_csr(g)
+    out = np.zeros(g.n, np.int32)
+    lib().orc_kernel_colour(g.n, nb[0], nb[1], out)
     return out
 
 

@@ -108,7 +108,7 @@ def _py_replay_sqa_msc(g, init3d, thr, mode, seed):
     S = init3d.astype(np.int64).copy()
     nb = [[(int(g.indices[p]), g.data[p]) for p in range(g.indptr[i], g.indptr[i + 1])
            if g.indices[p] != i and g.indices[p] != n and g.data[p] != 0] for i in range(n)]
-    col = O.greedy_colour(g)
+    col = O.kernel_colour(g)
     classes = [[i for i in range(n) if col[i] == c] for c in range(max(col) + 1)]
     upper = T - 1 if T % 2 else T
     groups = [list(range(0, upper, 2)), list(range(1, T, 2)), [T - 1] if T % 2 else []]
@@ -185,7 +185,7 @@ def _py_replay_sqa_split(g, init3d, thr, mode, seed):
     S = init3d.astype(np.int64).copy()
     nb = [[(int(g.indices[p]), g.data[p]) for p in range(g.indptr[i], g.indptr[i + 1])
            if g.indices[p] != i and g.indices[p] != n and g.data[p] != 0] for i in range(n)]
-    col = O.greedy_colour(g)
+    col = O.kernel_colour(g)
     classes = [[i for i in range(n) if col[i] == c] for c in range(max(col) + 1)]
     k0, k1 = seed & 0xFFFFFFFF, seed >> 32
     for r in range(R):
@@ -274,3 +274,20 @@ def test_batched_replay_matches_python_restatement():
     got = O.replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4)
     want = _py_replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4)
     np.testing.assert_array_equal(got, want)
+
+
+def test_kernel_colouring_is_proper_and_even():
+    from openjij_b200 import instances as I
+    for m in (I.random_regular_pm_j(4096, 3, seed=4)[0], I.lattice_pm_j(16, seed=1)[0],
+              I.random_regular_pm_j(500, 5, seed=2)[0]):
+        g = O.AugCSR(m)
+        col = O.kernel_colour(g)
+        greedy = O.greedy_colour(g)
+        rp, ci = O.neighbour_csr(g)[:2]
+        for i in range(g.n):
+            assert all(col[i] != col[j] for j in ci[rp[i]:rp[i + 1]])
+        sizes = np.bincount(col)
+        assert len(sizes) == greedy.max() + 1
+        assert sizes.max() <= max(np.bincount(greedy).max(), -(-g.n // len(sizes)))
+    sizes = np.bincount(O.kernel_colour(O.AugCSR(I.random_regular_pm_j(4096, 3, seed=4)[0])))
+    assert sizes.max() == 1024  # four classes of 1024 (greedy gives 1526/1506/968/96)
