@@ -929,7 +929,7 @@ void orc_replay_sqa_split(int n, const int64_t* indptr, const int32_t* indices, 
 // blocks concatenated.
 void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset, const double* J_aug,
                          const int32_t* reads, int8_t* spins, const float* betas_f, int64_t nsweeps,
-                         uint64_t seed, uint32_t inst0, int threads) {
+                         uint64_t seed, uint32_t inst0, int threads, float* fields_out) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   std::vector<int64_t> soff(count + 1, 0);
   std::vector<int> rm, rr;  // flattened (instance, replica)
@@ -973,6 +973,9 @@ void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset,
         }
       }
     }
+    // the incrementally updated FP32 fields at the end (same layout as spins)
+    if (fields_out)
+      for (int j = 0; j < n; ++j) fields_out[soff[m] + (size_t)r * n + j] = f[j];
   });
 }
 

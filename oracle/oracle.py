@@ -78,7 +78,7 @@ def lib():
         L.orc_replay_sqa_split.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _u32p,
                                            _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
         L.orc_replay_sa_batch.argtypes = [C.c_int, _i32p, _i64p, _f64p, _i32p, _i8p, _f32p, C.c_int64,
-                                          C.c_uint64, C.c_uint32, C.c_int]
+                                          C.c_uint64, C.c_uint32, C.c_int, C.c_void_p]
         L.orc_gen_spin_seq.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _i8p]
         _lib = L
     return _lib
@@ -371,15 +371,18 @@ def replay_sqa_split(g: AugCSR, init3d, thr, mode, seed, threads=None):
     return S
 
 
-def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, threads=None):
+def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, threads=None, fields=False):
     """Batched dense SA replay; mats: augmented (n+1)x(n+1) FP64 matrices,
-    spins_flat: the instances' [reads[m]][n[m]] int8 blocks concatenated."""
+    spins_flat: the instances' [reads[m]][n[m]] int8 blocks concatenated.
+    fields=True also returns the final incrementally updated FP32 fields."""
     n = np.array([m.shape[0] - 1 for m in mats], np.int32)
     sizes = np.array([(k + 1) * (k + 1) for k in n], np.int64)
     offset = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
     flat = np.ascontiguousarray(np.concatenate([np.asarray(m, np.float64).ravel() for m in mats]))
     s = np.array(spins_flat, np.int8, copy=True)
     b = np.ascontiguousarray(betas_per_sweep, np.float32)
+    fo = np.zeros(s.shape, np.float32) if fields else None
     lib().orc_replay_sa_batch(len(mats), n, offset, flat, np.ascontiguousarray(reads, np.int32), s, b, len(b),
-                              int(seed), int(inst0), _threads(threads))
-    return s
+                              int(seed), int(inst0), _threads(threads),
+                              None if fo is None else fo.ctypes.data)
+    return (s, fo) if fields else s

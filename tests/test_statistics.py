@@ -163,3 +163,30 @@ def test_sqa_annealing_ground_state_rate(scheme):
     ok, rates = _two_prop_ok(np.sum(np.isclose(bg, e0)), R, np.sum(np.isclose(br, e0)), R, 0.05)
     assert ok, rates
     assert 0.02 < rates[1] < 0.98
+
+
+def test_batched_fp32_field_drift_is_stated():
+    """The batched / dense-jump kernels update FP32 fields incrementally (one
+    rounding per accepted flip, no periodic recompute).  Their replay performs
+    the same FP32 operations, so its final fields are the kernel's; against the
+    FP64 fields of the final spins the drift on N(0,1) QUBOs (n = 512 and 1024,
+    500 sweeps, beta 0.1 -> 10) stays below 1e-5 relative to the field scale,
+    and is zero for integer couplings."""
+    from openjij_b200 import instances as I
+    betas, mcs = I.geometric_betas(0.1, 10.0, 500)
+    per = np.repeat(betas, mcs).astype(np.float32)
+    for maker, tol in ((lambda n: I.dense_qubo_normal(n, seed=n), 1e-5), (lambda n: I.dense_qubo_int(n, seed=n), 0.0)):
+        for n in (512, 1024):
+            A = maker(n)[0].toarray()
+            R = 4
+            s0 = _init(R, n, n)
+            s, f32 = O.replay_sa_batch([A], [R], s0.ravel(), per, 7, fields=True)
+            S = s.reshape(R, n).astype(np.float64)
+            f64 = A[:n, n][None, :] + S @ A[:n, :n]
+            f32 = f32.reshape(R, n).astype(np.float64)
+            # FP64 fields of the FP32-rounded couplings: the kernel's own inputs
+            A32 = A.astype(np.float32).astype(np.float64)
+            f64r = A32[:n, n][None, :] + S @ A32[:n, :n]
+            scale = np.abs(f64).max()
+            drift = np.abs(f32 - f64r).max() / scale
+            assert drift <= tol, (n, drift)
