@@ -383,7 +383,7 @@ def run_ours_batch(args, w):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded instances)",
             "config": {"workload": w["name"], "instances": len(mats), "spins_total": int(np.sum(sizes)),
                        "replicas_per_instance": int(w["replicas"]), "num_sweeps": S, "kernel": "batched",
-                       "launch_shape": {"threads": st["threads"], "register_variant": st["variant"],
+                       "launch_shape": {"threads": st["threads"], "variant": st["variant"],
                                         "autotuned": True},
                        "l2": "flushed between steps (256 MB write)", "attempts_per_step": attempts_per_step},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

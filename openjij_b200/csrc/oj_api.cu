@@ -465,7 +465,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
   }
   int launches = 0;
-  int P_used = 0, threads_used = 0;
+  int P_used = 0, threads_used = 0, variant_used = 0;
   bool tuned_now = false;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
@@ -538,15 +538,21 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     ++launches;
   } else if (kernel == OJ_KERNEL_DENSE_JUMP) {
     if (oj_status bs = ensure_single(ctx, g)) return bs;
-    const int W = batch_warps();
-    std::vector<int32_t> items;
-    for (int gq = 0; gq * W < R; ++gq) {
-      items.push_back(0);
-      items.push_back(gq);
-    }
-    const int nitems = (int)(items.size() / 2);
+    auto make_items = [&](int W) {
+      std::vector<int32_t> it;
+      for (int gq = 0; gq * W < R; ++gq) {
+        it.push_back(0);
+        it.push_back(gq);
+      }
+      return it;
+    };
+    const uint64_t key = ((uint64_t)OJ_KERNEL_DENSE_JUMP << 40) | (uint64_t)R;
+    auto tit = g->tuned.find(key);
+    int variant = tit != g->tuned.end() ? tit->second.variant : batch_default_variant();
+    std::vector<int32_t> items = make_items(batch_variant_warps(variant));
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t b_hdr = al(4 + 8), b_items = al(items.size() * 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4);
+    const size_t b_hdr = al(4 + 8), b_items = al(make_items(batch_warps()).size() * 4 + 4), b_cnt = al(4),
+                 b_beta = al(bf.size() * 4 + 4);
     OJ_CK(ctx->batch.ensure(b_hdr + b_items + b_cnt + b_beta), "alloc tables");
     char* base = ctx->batch.as<char>();
     int32_t* d_reads = reinterpret_cast<int32_t*>(base);
@@ -558,15 +564,49 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     const int64_t hsoff = 0;
     OJ_CK(cudaMemcpyAsync(d_reads, &hreads, 4, cudaMemcpyHostToDevice, st), "H2D reads");
     OJ_CK(cudaMemcpyAsync(d_soff, &hsoff, 8, cudaMemcpyHostToDevice, st), "H2D offsets");
-    OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
     if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+    if (tit == g->tuned.end() && autotune_requested(flags) && S > 0) {
+      // candidates run 16 sweeps with betas spread over the schedule on a copy of the spins
+      const int cand[4] = {83, 84, 162, 321};
+      const int64_t Ssub = std::min<int64_t>(S, 16);
+      std::vector<float> tb(Ssub);
+      for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
+      const size_t sb_al = al(spin_bytes);
+      OJ_CK(ctx->aux.ensure(sb_al + tb.size() * 4), "alloc tuning scratch");
+      int8_t* scratch = ctx->aux.as<int8_t>();
+      float* d_tb = reinterpret_cast<float*>(ctx->aux.as<char>() + sb_al);
+      OJ_CK(cudaMemcpyAsync(d_tb, tb.data(), tb.size() * 4, cudaMemcpyHostToDevice, st), "H2D tuning betas");
+      cudaError_t terr = cudaSuccess;
+      std::vector<int32_t> it;
+      int loaded = -1;
+      const int bi = time_candidates(
+          st, 4, [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
+          [&](int i) {
+            if (loaded != i) {
+              it = make_items(batch_variant_warps(cand[i]));
+              const cudaError_t e = cudaMemcpyAsync(d_items, it.data(), it.size() * 4, cudaMemcpyHostToDevice, st);
+              if (e != cudaSuccess) return e;
+              loaded = i;
+            }
+            return launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter,
+                                   scratch, d_tb, Ssub, rb, 0, ctx->sm_count, st, nullptr, cand[i]);
+          },
+          &terr);
+      if (bi == -2) return cuda_fail(ctx, terr, "autotune");
+      variant = bi >= 0 ? cand[bi] : 83;
+      g->tuned[key] = Shape{0, 0, variant};
+      tuned_now = true;
+      items = make_items(batch_variant_warps(variant));
+    }
+    OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
-      OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb, 0,
-                            ctx->sm_count, st, &launches),
+      OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(items.size() / 2), d_counter, d_spins,
+                            d_beta, S, rb, 0, ctx->sm_count, st, &launches, variant),
             "sa dense jump kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
-    threads_used = W * 32;
+    threads_used = batch_variant_warps(variant) * 32;
+    variant_used = variant;
   } else {
     OJ_CK(ctx->params.ensure(std::max<size_t>(bf.size() * 4, 16)), "alloc params");
     float* d_beta = ctx->params.as<float>();
@@ -616,6 +656,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     stats->attempts = (double)R * n * (double)S;
     stats->cluster = P_used;
     stats->threads = threads_used;
+    stats->variant = variant_used;
     stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
@@ -947,8 +988,6 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   int64_t sbytes = 0, nrep = 0;
   int max_reads = 0;
   double attempts_per_sweep = 0.0;
-  std::vector<int32_t> items;
-  const int W = batch_warps();
   for (int k = 0; k < count; ++k) {
     if (reads[k] < 0) return arg_fail(ctx, "negative read count");
     soff[k] = sbytes;
@@ -960,18 +999,27 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   }
   if (nrep == 0) return OJ_OK;
   if (!spins && sbytes > 0) return arg_fail(ctx, "null spins");
-  // work items (instance, group of W replicas), longest instance first
+  // work items (instance, group of W replicas), longest instance first; W is
+  // the warps per CTA of the launch variant
   std::vector<int> order(count);
   for (int k = 0; k < count; ++k) order[k] = k;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->n[x] > b->n[y]; });
-  for (int k : order) {
-    if (b->n[k] == 0) continue;
-    for (int gq = 0; gq * W < reads[k]; ++gq) {
-      items.push_back(k);
-      items.push_back(gq);
+  auto make_items = [&](int W) {
+    std::vector<int32_t> it;
+    for (int k : order) {
+      if (b->n[k] == 0) continue;
+      for (int gq = 0; gq * W < reads[k]; ++gq) {
+        it.push_back(k);
+        it.push_back(gq);
+      }
     }
-  }
-  const int nitems = (int)(items.size() / 2);
+    return it;
+  };
+  oj_batch* bm = const_cast<oj_batch*>(b);
+  const int variant0 = bm->tuned_variant ? bm->tuned_variant : batch_default_variant();
+  std::vector<int32_t> items = make_items(batch_variant_warps(variant0));
+  const size_t items_cap = make_items(batch_warps()).size();  // the most items of any variant
+  int nitems = (int)(items.size() / 2);
   RngBase rb;
   if (oj_status st_ = rng_base(ctx, seed, first_sweep, 0, &rb)) return st_;
   DeviceGuard dg(ctx->device);
@@ -991,7 +1039,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   // one staging buffer: reads | soff | eoff | items | counter | betas | order
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t b_reads = al((size_t)count * 4), b_soff = al((size_t)count * 8), b_eoff = al((size_t)count * 8),
-               b_items = al(items.size() * 4 + 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4),
+               b_items = al(items_cap * 4 + 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4),
                b_order = al((size_t)count * 4);
   OJ_CK(ctx->batch.ensure(b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta + b_order), "alloc batch tables");
   char* base = ctx->batch.as<char>();
@@ -1011,12 +1059,11 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (nitems) OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
   if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
   if (count) OJ_CK(cudaMemcpyAsync(d_order, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st), "H2D order");
-  oj_batch* bm = const_cast<oj_batch*>(b);
   bool tuned_now = false;
   if (bm->tuned_variant == 0 && autotune_requested(flags) && S > 0 && nitems > 0) {
     // the work per sweep follows the acceptance rate, so the candidates run 16
     // sweeps whose betas are spread over the whole schedule
-    const int cand[2] = {3, 4};
+    const int cand[4] = {83, 84, 162, 321};
     const int64_t Ssub = std::min<int64_t>(S, 16);
     std::vector<float> tb(Ssub);
     for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
@@ -1026,21 +1073,33 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     float* d_tb = reinterpret_cast<float*>(ctx->aux.as<char>() + sb_al);
     OJ_CK(cudaMemcpyAsync(d_tb, tb.data(), tb.size() * 4, cudaMemcpyHostToDevice, st), "H2D tuning betas");
     cudaError_t terr = cudaSuccess;
+    int loaded = -1;  // variant whose items are in d_items
+    std::vector<int32_t> it;
     const int bi = time_candidates(
-        st, 2, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
+        st, 4, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
         [&](int i) {
-          return launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, scratch, d_tb, Ssub, rb,
-                                 (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i]);
+          if (loaded != i) {
+            it = make_items(batch_variant_warps(cand[i]));
+            const cudaError_t e = cudaMemcpyAsync(d_items, it.data(), it.size() * 4, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return e;
+            loaded = i;
+          }
+          return launch_sa_batch(b, d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter, scratch, d_tb, Ssub,
+                                 rb, (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i]);
         },
         &terr);
     if (bi == -2) return cuda_fail(ctx, terr, "autotune");
-    bm->tuned_variant = bi >= 0 ? cand[bi] : 3;
+    bm->tuned_variant = bi >= 0 ? cand[bi] : 83;
     tuned_now = true;
+    items = make_items(batch_variant_warps(bm->tuned_variant));
+    nitems = (int)(items.size() / 2);
+    OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
   }
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
   if (S > 0 && nitems > 0)
     OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
-                          (uint32_t)instance_offset, ctx->sm_count, st, &launches, bm->tuned_variant),
+                          (uint32_t)instance_offset, ctx->sm_count, st, &launches,
+                          bm->tuned_variant ? bm->tuned_variant : variant0),
           "sa batched kernel");
   OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   if (energies) {
@@ -1060,8 +1119,9 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (stats) {
     stats->kernel = 0;
     stats->launches = launches;
-    stats->threads = batch_warps() * 32;
-    stats->variant = bm->tuned_variant;
+    const int v = bm->tuned_variant ? bm->tuned_variant : variant0;
+    stats->threads = batch_variant_warps(v) * 32;
+    stats->variant = v;
     stats->tuned = tuned_now ? 1 : 0;
     stats->sweeps = S;
     stats->attempts = attempts_per_sweep * (double)S;

@@ -1,6 +1,8 @@
 // Batched dense SA over many instances of uneven size in one persistent launch.
 //
-// Work item = (instance m, group of up to kBatchWarps replicas of m).  Items
+// Work item = (instance m, group of up to W replicas of m, W = warps per CTA
+// of the launch variant: 8, 16 or 32; with 32 all reads of a 32-read instance
+// share one SM and its L1 for the J rows).  Items
 // are ordered by decreasing n (longest first) and handed out through an atomic
 // counter, so the CTAs resident on the SMs keep pulling the next largest item
 // until the queue is empty.  One warp runs one replica: its FP32 local fields
@@ -62,13 +64,13 @@ struct BatchArgs {
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
-template <int MINB>
-__global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchArgs a) {
+template <int W, int MINB>
+__global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
-  uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)kBatchWarps * a.fstride) +
+  uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
                  (size_t)warp * (a.fstride / 4);  // spin words [chunk][lane]
   for (;;) {
     __syncthreads();
@@ -77,7 +79,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) sa_batch_kernel(BatchA
     const int item = item_sh;
     if (item >= a.nitems) break;
     const int m = a.items[2 * item];
-    const int r = a.items[2 * item + 1] * kBatchWarps + warp;
+    const int r = a.items[2 * item + 1] * W + warp;
     const int n = a.n[m];
     if (r >= a.reads[m]) continue;  // no block-wide barrier until the next item
     const int nch = (n + 127) >> 7;
@@ -266,25 +268,42 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
 int batch_max_sites() { return kBatchMaxN; }
 int batch_warps() { return kBatchWarps; }
 
+// Launch variants: warps per CTA x minimum CTAs per SM (register budget).
+// 83 = 8 warps, 80 registers; 84 = 8 warps, 64; 162 = 16 warps, 64; 321 = 32 warps, 64.
+int batch_variant_warps(int variant) { return variant / 10 >= 8 ? variant / 10 : kBatchWarps; }
+
+bool batch_variant_valid(int variant) { return variant == 83 || variant == 84 || variant == 162 || variant == 321; }
+
+int batch_default_variant() {
+  if (const char* env = std::getenv("OJ_BATCH_VARIANT")) {
+    const int v = std::atoi(env);
+    if (batch_variant_valid(v)) return v;
+  }
+  return 83;
+}
+
+template <int W, int MINB>
+cudaError_t launch_variant(const BatchArgs& a, int nitems, int fstride, int sm_count, cudaStream_t st) {
+  auto kern = sa_batch_kernel<W, MINB>;
+  const size_t smem = (size_t)W * fstride * 5;  // FP32 fields + spin words
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = std::max(1, std::min(nitems, per_sm * sm_count));
+  kern<<<grid, W * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
                             int* launches, int variant) {
+  if (variant == 0) variant = batch_default_variant();
+  if (!batch_variant_valid(variant)) return cudaErrorInvalidValue;
   const int fstride = std::max(128, (b->max_n + 127) / 128 * 128);
-  const size_t smem = (size_t)kBatchWarps * fstride * 5;  // FP32 fields + spin words
-  // two register budgets: 80 per thread (3 CTAs per SM) or 64 (4 CTAs per SM)
-  if (variant == 0) {
-    variant = 3;
-    if (const char* env = std::getenv("OJ_BATCH_MINB")) variant = std::atoi(env) == 4 ? 4 : 3;
-  }
-  if (variant != 3 && variant != 4) return cudaErrorInvalidValue;
-  auto kern = variant == 4 ? sa_batch_kernel<4> : sa_batch_kernel<3>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchWarps * 32, smem);
-  if (e != cudaSuccess) return e;
-  const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sm_count));
   BatchArgs a;
   a.J = b->d_J.as<float>();
   a.h = b->d_h.as<float>();
@@ -304,11 +323,16 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.inst0 = inst0;
   a.rep0 = rb.rep0;
   a.fstride = fstride;
-  e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
-  kern<<<grid, kBatchWarps * 32, smem, st>>>(a);
-  if (launches) ++*launches;
-  return cudaGetLastError();
+  switch (variant) {
+    case 83: e = launch_variant<8, 3>(a, nitems, fstride, sm_count, st); break;
+    case 84: e = launch_variant<8, 4>(a, nitems, fstride, sm_count, st); break;
+    case 162: e = launch_variant<16, 2>(a, nitems, fstride, sm_count, st); break;
+    default: e = launch_variant<32, 1>(a, nitems, fstride, sm_count, st); break;
+  }
+  if (e == cudaSuccess && launches) ++*launches;
+  return e;
 }
 
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
