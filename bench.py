@@ -523,7 +523,8 @@ def run_ours(args):
             "data": "synthetic (seeded instance)",
             "config": {"workload": w["name"], "spins": n, "replicas": R, "trotter": T,
                        "num_sweeps": int(np.sum(mcs)), "kernel": used_kernel,
-                       "launch_shape": {"cluster": st["cluster"], "threads": st["threads"], "autotuned": True},
+                       "launch_shape": {"cluster": st["cluster"], "threads": st["threads"],
+                                        "variant": st["variant"], "autotuned": True},
                        "l2": "flushed between steps (256 MB write)",
                        "attempts_per_step": attempts_per_step},
             "roofline": {"bound": w["bound"], "achieved": achieved, "peak": peak, "unit": unit,

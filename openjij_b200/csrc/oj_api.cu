@@ -194,7 +194,7 @@ bool autotune_requested(uint32_t flags) {
 
 // Autotuner core: for each candidate, restore() puts the call's own initial
 // state into a scratch copy and enqueue(i) runs candidate i on it for a few
-// sweeps; each candidate runs twice and its second time counts.  Returns the
+// sweeps; each candidate runs twice and the faster run counts.  Returns the
 // fastest candidate, -1 when none launched, or -2 on a device error (which
 // the caller reports).  Candidates that cannot launch (cluster or shared-memory
 // limits) are skipped.
@@ -222,7 +222,9 @@ int time_candidates(cudaStream_t st, int count, Restore restore, Enqueue enqueue
         break;
       }
       if ((*err = cudaStreamSynchronize(st)) != cudaSuccess) break;
-      cudaEventElapsedTime(&ms, e0, e1);
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, e0, e1);
+      ms = rep == 0 ? t : std::min(ms, t);
     }
     if (*err != cudaSuccess) break;
     if (ok && (bi < 0 || ms < best)) {
@@ -567,8 +569,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
     if (tit == g->tuned.end() && autotune_requested(flags) && S > 0) {
       // candidates run 16 sweeps with betas spread over the schedule on a copy of the spins
-      const int cand[4] = {83, 84, 162, 321};
-      const int64_t Ssub = std::min<int64_t>(S, 16);
+      const int cand[5] = {82, 83, 84, 162, 321};
+      const int64_t Ssub = std::min<int64_t>(S, 32);
       std::vector<float> tb(Ssub);
       for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
       const size_t sb_al = al(spin_bytes);
@@ -580,7 +582,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       std::vector<int32_t> it;
       int loaded = -1;
       const int bi = time_candidates(
-          st, 4, [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
+          st, 5, [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
           [&](int i) {
             if (loaded != i) {
               it = make_items(batch_variant_warps(cand[i]));
@@ -1063,8 +1065,8 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (bm->tuned_variant == 0 && autotune_requested(flags) && S > 0 && nitems > 0) {
     // the work per sweep follows the acceptance rate, so the candidates run 16
     // sweeps whose betas are spread over the whole schedule
-    const int cand[4] = {83, 84, 162, 321};
-    const int64_t Ssub = std::min<int64_t>(S, 16);
+    const int cand[5] = {82, 83, 84, 162, 321};
+    const int64_t Ssub = std::min<int64_t>(S, 32);
     std::vector<float> tb(Ssub);
     for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
     const size_t sb_al = ((size_t)std::max<int64_t>(sbytes, 16) + 255) & ~(size_t)255;
@@ -1076,7 +1078,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     int loaded = -1;  // variant whose items are in d_items
     std::vector<int32_t> it;
     const int bi = time_candidates(
-        st, 4, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
+        st, 5, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
         [&](int i) {
           if (loaded != i) {
             it = make_items(batch_variant_warps(cand[i]));

@@ -40,6 +40,8 @@ namespace {
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
 constexpr int kMaxChunks = kBatchMaxN / 128;
+constexpr int kInitRows = 16;                          // J rows per staged initialisation tile
+constexpr int kInitLoads = (kInitRows * 32 + 255) / 256;  // float4 loads per thread and tile (>= 256 threads)
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -64,10 +66,13 @@ struct BatchArgs {
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
-template <int W, int MINB>
+// GROUP: chunks of a flipped site's J row loaded before any is used (the
+// flip's L2 round trips are ceil(chunks / GROUP)); more costs registers.
+template <int W, int MINB, int GROUP>
 __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
+  __shared__ float4 jtile[2 * kInitRows * 32];  // J tiles of the field initialisation
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
@@ -81,46 +86,71 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     const int m = a.items[2 * item];
     const int r = a.items[2 * item + 1] * W + warp;
     const int n = a.n[m];
-    if (r >= a.reads[m]) continue;  // no block-wide barrier until the next item
+    const bool active = r < a.reads[m];  // every warp takes part in the field initialisation
     const int nch = (n + 127) >> 7;
     const int npad = nch << 7;
     const float* J = a.J + a.joff[m];
     const float* h = a.h + a.hoff[m];
-    int8_t* gs = a.spins + a.soff[m] + (size_t)r * n;
+    int8_t* gs = a.spins + a.soff[m] + (size_t)(active ? r : 0) * n;
     // spins -> bits
-    for (int c = 0; c < nch; ++c) {
-      uint32_t w = 0u;
+    if (active)
+      for (int c = 0; c < nch; ++c) {
+        uint32_t w = 0u;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int i = 128 * c + 4 * lane + e;
-        if (i < n && gs[i] < 0) w |= 1u << e;
+        for (int e = 0; e < 4; ++e) {
+          const int i = 128 * c + 4 * lane + e;
+          if (i < n && gs[i] < 0) w |= 1u << e;
+        }
+        sw[32 * c + lane] = w;
       }
-      sw[32 * c + lane] = w;
-    }
     __syncwarp();
-    // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j)
-    for (int c = 0; c < nch; ++c) {
-      float4 acc = ldg4(h + 128 * c + 4 * lane);
-      const float* Jc = J + 128 * c + 4 * lane;
-      for (int i0 = 0; i0 < n; i0 += 4) {
-        float4 v[4];
+    // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j).
+    // The CTA's warps share each tile of kInitRows rows x 128 columns of J,
+    // staged in shared memory (double-buffered, the next tile's loads in flight
+    // while the current one is summed), so J is read once per CTA, not per warp.
+    {
+      const int ntr = (n + kInitRows - 1) / kInitRows;  // row tiles per chunk
+      const int ntiles = nch * ntr;
+      float4 pre[kInitLoads];
+      auto load_tile = [&](int t) {
+        const int c = t / ntr, i0 = (t - c * ntr) * kInitRows;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (i0 + q < n) v[q] = ldg4(Jc + (size_t)(i0 + q) * npad);
+        for (int q = 0; q < kInitLoads; ++q) {
+          const int idx = threadIdx.x + q * W * 32;
+          const int row = idx >> 5, col = idx & 31;
+          pre[q] = (row < kInitRows && i0 + row < n) ? ldg4(J + (size_t)(i0 + row) * npad + 128 * c + 4 * col)
+                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      };
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (ntiles > 0) load_tile(0);
+      for (int t = 0; t < ntiles; ++t) {
+        const int c = t / ntr, i0 = (t - c * ntr) * kInitRows;
+        float4* buf = jtile + (t & 1) * (kInitRows * 32);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int i = i0 + q;
-          if (i < n) {
+        for (int q = 0; q < kInitLoads; ++q) {
+          const int idx = threadIdx.x + q * W * 32;
+          if (idx < kInitRows * 32) buf[idx] = pre[q];
+        }
+        __syncthreads();
+        if (t + 1 < ntiles) load_tile(t + 1);
+        if (active) {
+          if (i0 == 0) acc = ldg4(h + 128 * c + 4 * lane);
+          for (int q = 0; q < kInitRows; ++q) {
+            const int i = i0 + q;
+            if (i >= n) break;
+            const float4 v = buf[q * 32 + lane];
             const bool neg = (sw[32 * (i >> 7) + ((i & 127) >> 2)] >> (i & 3)) & 1u;
-            acc.x = __fadd_rn(acc.x, neg ? -v[q].x : v[q].x);
-            acc.y = __fadd_rn(acc.y, neg ? -v[q].y : v[q].y);
-            acc.z = __fadd_rn(acc.z, neg ? -v[q].z : v[q].z);
-            acc.w = __fadd_rn(acc.w, neg ? -v[q].w : v[q].w);
+            acc.x = __fadd_rn(acc.x, neg ? -v.x : v.x);
+            acc.y = __fadd_rn(acc.y, neg ? -v.y : v.y);
+            acc.z = __fadd_rn(acc.z, neg ? -v.z : v.z);
+            acc.w = __fadd_rn(acc.w, neg ? -v.w : v.w);
           }
+          if (i0 + kInitRows >= n) reinterpret_cast<float4*>(f)[32 * c + lane] = acc;
         }
       }
-      reinterpret_cast<float4*>(f)[32 * c + lane] = acc;
     }
+    if (!active) continue;  // no block-wide barrier until the next item
     __syncwarp();
     const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
     const uint32_t rg = a.rep0 + (uint32_t)r;
@@ -160,14 +190,14 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const float* Ji = J + (size_t)i * npad + 4 * lane;
           // the row in groups of four chunks whose loads are in flight together
 #pragma unroll
-          for (int c0 = 0; c0 < kMaxChunks; c0 += 4) {
+          for (int c0 = 0; c0 < kMaxChunks; c0 += GROUP) {
             if (c0 >= nch) break;
-            float4 v[4];
+            float4 v[GROUP];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < GROUP; ++q)
               if (c0 + q < nch) v[q] = ldg4(Ji + 128 * (c0 + q));
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < GROUP; ++q)
               if (c0 + q < nch) {
                 float4 g = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
                 g.x = __fmaf_rn(coef, v[q].x, g.x);
@@ -269,10 +299,14 @@ int batch_max_sites() { return kBatchMaxN; }
 int batch_warps() { return kBatchWarps; }
 
 // Launch variants: warps per CTA x minimum CTAs per SM (register budget).
-// 83 = 8 warps, 80 registers; 84 = 8 warps, 64; 162 = 16 warps, 64; 321 = 32 warps, 64.
+// 82 = 8 warps, 128 registers, a flip row's loads 16 chunks at a time;
+// 83 = 8 warps, 80 registers; 84 = 8 warps, 64; 162 = 16 warps, 64; 321 = 32 warps, 64
+// (4 chunks at a time).
 int batch_variant_warps(int variant) { return variant / 10 >= 8 ? variant / 10 : kBatchWarps; }
 
-bool batch_variant_valid(int variant) { return variant == 83 || variant == 84 || variant == 162 || variant == 321; }
+bool batch_variant_valid(int variant) {
+  return variant == 82 || variant == 83 || variant == 84 || variant == 162 || variant == 321;
+}
 
 int batch_default_variant() {
   if (const char* env = std::getenv("OJ_BATCH_VARIANT")) {
@@ -282,9 +316,9 @@ int batch_default_variant() {
   return 83;
 }
 
-template <int W, int MINB>
+template <int W, int MINB, int GROUP>
 cudaError_t launch_variant(const BatchArgs& a, int nitems, int fstride, int sm_count, cudaStream_t st) {
-  auto kern = sa_batch_kernel<W, MINB>;
+  auto kern = sa_batch_kernel<W, MINB, GROUP>;
   const size_t smem = (size_t)W * fstride * 5;  // FP32 fields + spin words
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -326,10 +360,11 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   switch (variant) {
-    case 83: e = launch_variant<8, 3>(a, nitems, fstride, sm_count, st); break;
-    case 84: e = launch_variant<8, 4>(a, nitems, fstride, sm_count, st); break;
-    case 162: e = launch_variant<16, 2>(a, nitems, fstride, sm_count, st); break;
-    default: e = launch_variant<32, 1>(a, nitems, fstride, sm_count, st); break;
+    case 82: e = launch_variant<8, 2, 16>(a, nitems, fstride, sm_count, st); break;
+    case 83: e = launch_variant<8, 3, 4>(a, nitems, fstride, sm_count, st); break;
+    case 84: e = launch_variant<8, 4, 4>(a, nitems, fstride, sm_count, st); break;
+    case 162: e = launch_variant<16, 2, 4>(a, nitems, fstride, sm_count, st); break;
+    default: e = launch_variant<32, 1, 4>(a, nitems, fstride, sm_count, st); break;
   }
   if (e == cudaSuccess && launches) ++*launches;
   return e;
