@@ -528,6 +528,11 @@ def run_ours(args):
                        "l2": "flushed between steps (256 MB write)",
                        "attempts_per_step": attempts_per_step},
             "roofline": {"bound": w["bound"], "achieved": achieved, "peak": peak, "unit": unit,
+                         "note": ("algorithmic state bytes against the HBM copy peak; the state lives in "
+                                  "shared memory and the kernel is integer-issue bound (profiles/)")
+                         if unit == "GB/s" else
+                         ("algorithmic 2n flop per attempt against the BF16 tensor peak; the dense "
+                          "kernels update a field row only on accepted flips (profiles/)"),
                          "frac": achieved / peak,
                          "traffic": _traffic_from_profiles() if args.config == 2 else None,
                          "peak_kind": peak_kind, "kernel_ms": kms,

@@ -428,13 +428,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       kernel = OJ_KERNEL_BITPACKED;
     } else if (inf.num_colours > 64 && (int64_t)n * n * 4 <= ((int64_t)8 << 30)) {
       // dense: one warp per replica jumping between accepted flips (fastest
-      // measured on dense QUBOs), else the tensor-core kernel for many replicas,
-      // else the plain sequential kernel
-      std::string why;
-      if (n <= batch_max_sites())
-        kernel = OJ_KERNEL_DENSE_JUMP;
-      else
-        kernel = (R >= 512 && dense_tc_prepare(g, &why) == cudaSuccess) ? OJ_KERNEL_DENSE_TC : OJ_KERNEL_DENSE_PLAIN;
+      // measured on dense QUBOs) up to its size limit, else the plain kernel
+      kernel = n <= batch_max_sites() ? OJ_KERNEL_DENSE_JUMP : OJ_KERNEL_DENSE_PLAIN;
     } else {
       kernel = OJ_KERNEL_COLOUR;
     }
