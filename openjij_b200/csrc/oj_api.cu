@@ -470,7 +470,11 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     const int D = inf.max_degree;
     const int G = (R + 31) / 32;
     std::string why;
-    const int P = msc_choose_cluster(g, G, ctx->sm_count);
+    // the cached shape's cluster when there is one, so the plan is built once
+    const uint64_t key = ((uint64_t)OJ_KERNEL_BITPACKED << 40) | (uint64_t)R;
+    const auto cached = g->tuned.find(key);
+    const int P = (cached != g->tuned.end() && cached->second.cluster) ? cached->second.cluster
+                                                                       : msc_choose_cluster(g, G, ctx->sm_count);
     cudaError_t pe = msc_prepare(g, P, &why);
     if (pe != cudaSuccess) {
       ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
@@ -491,7 +495,6 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(launch_pack(d_spins, R, n, d_words, st), "pack");
     ++launches;
     // launch shape: cached, autotuned now, or the default heuristic
-    const uint64_t key = ((uint64_t)OJ_KERNEL_BITPACKED << 40) | (uint64_t)R;
     Shape shp;
     auto it = g->tuned.find(key);
     if (it != g->tuned.end()) {
@@ -721,7 +724,11 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     const int P = sqa_split_replicas_per_group(T);
     const int G = (R + P - 1) / P;
     std::string why;
-    const cudaError_t pe = sqa_split_prepare(g, G, ctx->sm_count, &why);
+    // the cached shape's cluster when there is one, so the plan is built once
+    const uint64_t key = ((uint64_t)0x80 << 40) | ((uint64_t)T << 32) | (uint64_t)R;
+    const auto cached = g->tuned.find(key);
+    const cudaError_t pe =
+        sqa_split_prepare(g, G, ctx->sm_count, &why, cached != g->tuned.end() ? cached->second.cluster : 0);
     if (pe != cudaSuccess) {
       ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
       return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
@@ -739,7 +746,6 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     uint32_t* d_words = ctx->words.as<uint32_t>();
     OJ_CK(launch_sqa_split_pack(d_spins, R, T, n, G, d_words, st), "pack");
     ++launches;
-    const uint64_t key = ((uint64_t)0x80 << 40) | ((uint64_t)T << 32) | (uint64_t)R;
     Shape shp;
     auto it = g->tuned.find(key);
     if (it != g->tuned.end()) {
