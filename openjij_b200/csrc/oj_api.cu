@@ -195,18 +195,18 @@ bool autotune_requested(uint32_t flags) {
 // Autotuner core: for each candidate, restore() puts the call's own initial
 // state into a scratch copy and enqueue(i) runs candidate i on it for a few
 // sweeps; each candidate runs twice and the faster run counts.  Returns the
-// fastest candidate, -1 when none launched, or -2 on a device error (which
-// the caller reports).  Candidates that cannot launch (cluster or shared-memory
-// limits) are skipped.
+// fastest candidate (the default one, def, unless another is 3 % faster),
+// -1 when none launched, or -2 on a device error (which the caller reports).
+// Candidates that cannot launch (cluster or shared-memory limits) are skipped.
 template <class Restore, class Enqueue>
-int time_candidates(cudaStream_t st, int count, Restore restore, Enqueue enqueue, cudaError_t* err) {
+int time_candidates(cudaStream_t st, int count, Restore restore, Enqueue enqueue, cudaError_t* err, int def = -1) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if ((*err = cudaEventCreate(&e0)) != cudaSuccess) return -2;
   if ((*err = cudaEventCreate(&e1)) != cudaSuccess) {
     cudaEventDestroy(e0);
     return -2;
   }
-  float best = 0.0f;
+  float best = 0.0f, def_ms = -1.0f;
   int bi = -1;
   for (int i = 0; i < count && *err == cudaSuccess; ++i) {
     float ms = 0.0f;
@@ -227,6 +227,7 @@ int time_candidates(cudaStream_t st, int count, Restore restore, Enqueue enqueue
       ms = rep == 0 ? t : std::min(ms, t);
     }
     if (*err != cudaSuccess) break;
+    if (ok && i == def) def_ms = ms;
     if (ok && (bi < 0 || ms < best)) {
       best = ms;
       bi = i;
@@ -234,7 +235,11 @@ int time_candidates(cudaStream_t st, int count, Restore restore, Enqueue enqueue
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  return *err != cudaSuccess ? -2 : bi;
+  if (*err != cudaSuccess) return -2;
+  // the default shape stays unless another is clearly (3 %) faster: short
+  // timings of a few sweeps carry that much noise
+  if (def_ms > 0.0f && best > 0.97f * def_ms) return def;
+  return bi;
 }
 
 }  // namespace
@@ -504,6 +509,10 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       for (int Pc : {1, 2, 4, 8, 16})
         if (Pc == 1 || n / Pc >= 64)
           for (int th : {256, 512, 1024}) cand.push_back(Shape{Pc, th, 0});
+      int def_msc = -1;  // the heuristic shape
+      for (size_t q = 0; q < cand.size(); ++q)
+        if (cand[q].cluster == msc_choose_cluster(g, G, ctx->sm_count) && cand[q].threads == msc_default_threads())
+          def_msc = (int)q;
       OJ_CK(ctx->aux.ensure((size_t)G * n * 4), "alloc tuning scratch");
       uint32_t* scratch = ctx->aux.as<uint32_t>();
       const int64_t Ssub = std::min<int64_t>(S, 16);
@@ -517,7 +526,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
             if (e != cudaSuccess) return e;
             return launch_sa_msc(g, G, scratch, d_thr, d_alw, Ssub, rb, st, nullptr, cand[i].threads);
           },
-          &terr);
+          &terr, def_msc);
       if (bi == -2) return cuda_fail(ctx, terr, "autotune");
       if (bi >= 0) shp = cand[bi];
       g->tuned[key] = shp;
@@ -551,7 +560,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     int variant = tit != g->tuned.end() ? tit->second.variant : batch_default_variant();
     std::vector<int32_t> items = make_items(batch_variant_warps(variant));
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t b_hdr = al(4 + 8), b_items = al(make_items(batch_warps()).size() * 4 + 4), b_cnt = al(4),
+    const size_t b_hdr = al(4 + 8), b_items = al(make_items(batch_min_warps()).size() * 4 + 4), b_cnt = al(4),
                  b_beta = al(bf.size() * 4 + 4);
     OJ_CK(ctx->batch.ensure(b_hdr + b_items + b_cnt + b_beta), "alloc tables");
     char* base = ctx->batch.as<char>();
@@ -567,7 +576,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
     if (tit == g->tuned.end() && autotune_requested(flags) && S > 0) {
       // candidates run 16 sweeps with betas spread over the schedule on a copy of the spins
-      const int cand[5] = {82, 83, 84, 162, 321};
+      const int cand[6] = {45, 82, 83, 84, 162, 321};
       const int64_t Ssub = std::min<int64_t>(S, 32);
       std::vector<float> tb(Ssub);
       for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
@@ -580,10 +589,11 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       std::vector<int32_t> it;
       int loaded = -1;
       const int bi = time_candidates(
-          st, 5, [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
+          st, 6, [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
           [&](int i) {
             if (loaded != i) {
               it = make_items(batch_variant_warps(cand[i]));
+              if (it.size() * 4 > b_items) return cudaErrorInvalidValue;  // never past the table
               const cudaError_t e = cudaMemcpyAsync(d_items, it.data(), it.size() * 4, cudaMemcpyHostToDevice, st);
               if (e != cudaSuccess) return e;
               loaded = i;
@@ -591,7 +601,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
             return launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter,
                                    scratch, d_tb, Ssub, rb, 0, ctx->sm_count, st, nullptr, cand[i]);
           },
-          &terr);
+          &terr, (int)(std::find(std::begin(cand), std::end(cand), batch_default_variant()) - std::begin(cand)));
       if (bi == -2) return cuda_fail(ctx, terr, "autotune");
       variant = bi >= 0 ? cand[bi] : 83;
       g->tuned[key] = Shape{0, 0, variant};
@@ -755,6 +765,9 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
       for (int Pc : {1, 2, 4})
         if (Pc == 1 || n / Pc >= 64)
           for (int th : {256, 512}) cand.push_back(Shape{Pc, th, 0});
+      int def_split = -1;  // the heuristic shape (the plan prepared above)
+      for (size_t q = 0; q < cand.size(); ++q)
+        if (cand[q].cluster == g->msc->P && cand[q].threads == split_default_threads()) def_split = (int)q;
       OJ_CK(ctx->aux.ensure((size_t)G * 2 * n * 4), "alloc tuning scratch");
       uint32_t* scratch = ctx->aux.as<uint32_t>();
       const int64_t Ssub = std::min<int64_t>(S, 16);
@@ -768,7 +781,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
             if (e != cudaSuccess || g->msc->P != cand[i].cluster) return e != cudaSuccess ? e : cudaErrorInvalidValue;
             return launch_sqa_split(g, G, T, scratch, d_thr, d_mode, Ssub, rb, st, nullptr, cand[i].threads);
           },
-          &terr);
+          &terr, def_split);
       if (bi == -2) return cuda_fail(ctx, terr, "autotune");
       if (bi >= 0) shp = cand[bi];
       g->tuned[key] = shp;
@@ -1021,7 +1034,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   oj_batch* bm = const_cast<oj_batch*>(b);
   const int variant0 = bm->tuned_variant ? bm->tuned_variant : batch_default_variant();
   std::vector<int32_t> items = make_items(batch_variant_warps(variant0));
-  const size_t items_cap = make_items(batch_warps()).size();  // the most items of any variant
+  const size_t items_cap = make_items(batch_min_warps()).size();  // the most items of any variant
   int nitems = (int)(items.size() / 2);
   RngBase rb;
   if (oj_status st_ = rng_base(ctx, seed, first_sweep, 0, &rb)) return st_;
@@ -1066,7 +1079,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (bm->tuned_variant == 0 && autotune_requested(flags) && S > 0 && nitems > 0) {
     // the work per sweep follows the acceptance rate, so the candidates run 16
     // sweeps whose betas are spread over the whole schedule
-    const int cand[5] = {82, 83, 84, 162, 321};
+    const int cand[6] = {45, 82, 83, 84, 162, 321};
     const int64_t Ssub = std::min<int64_t>(S, 32);
     std::vector<float> tb(Ssub);
     for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
@@ -1079,10 +1092,11 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     int loaded = -1;  // variant whose items are in d_items
     std::vector<int32_t> it;
     const int bi = time_candidates(
-        st, 5, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
+        st, 6, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
         [&](int i) {
           if (loaded != i) {
             it = make_items(batch_variant_warps(cand[i]));
+            if (it.size() > items_cap) return cudaErrorInvalidValue;  // never past the table
             const cudaError_t e = cudaMemcpyAsync(d_items, it.data(), it.size() * 4, cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) return e;
             loaded = i;
@@ -1090,7 +1104,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
           return launch_sa_batch(b, d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter, scratch, d_tb, Ssub,
                                  rb, (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i]);
         },
-        &terr);
+        &terr, (int)(std::find(std::begin(cand), std::end(cand), batch_default_variant()) - std::begin(cand)));
     if (bi == -2) return cuda_fail(ctx, terr, "autotune");
     bm->tuned_variant = bi >= 0 ? cand[bi] : 83;
     tuned_now = true;

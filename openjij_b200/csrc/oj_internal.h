@@ -176,6 +176,7 @@ cudaError_t launch_sqa_split_unpack(const uint32_t* words, int R, int T, int n, 
 int batch_max_sites();
 int batch_warps();
 int batch_variant_warps(int variant);
+int batch_min_warps();  // fewest warps per CTA of any variant (most work items)
 int batch_default_variant();
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,

@@ -41,7 +41,6 @@ constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
 constexpr int kMaxChunks = kBatchMaxN / 128;
 constexpr int kInitRows = 16;                          // J rows per staged initialisation tile
-constexpr int kInitLoads = (kInitRows * 32 + 255) / 256;  // float4 loads per thread and tile (>= 256 threads)
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -53,6 +52,7 @@ struct BatchArgs {
   const int64_t* soff;     // [count] offset of instance m's spins (bytes)
   const int32_t* items;    // [nitems][2] (instance, replica group), longest instance first
   int nitems;
+  int count;               // instances in the batch
   int* counter;            // work-queue head, zero at launch
   int8_t* spins;
   const float* betas;
@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     const int item = item_sh;
     if (item >= a.nitems) break;
     const int m = a.items[2 * item];
+    if ((unsigned)m >= (unsigned)a.count) continue;  // a corrupt table entry is skipped, never followed
     const int r = a.items[2 * item + 1] * W + warp;
     const int n = a.n[m];
     const bool active = r < a.reads[m];  // every warp takes part in the field initialisation
@@ -111,11 +112,12 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     {
       const int ntr = (n + kInitRows - 1) / kInitRows;  // row tiles per chunk
       const int ntiles = nch * ntr;
-      float4 pre[kInitLoads];
+      constexpr int NL = (kInitRows * 32 + W * 32 - 1) / (W * 32);  // float4 loads per thread and tile
+      float4 pre[NL];
       auto load_tile = [&](int t) {
         const int c = t / ntr, i0 = (t - c * ntr) * kInitRows;
 #pragma unroll
-        for (int q = 0; q < kInitLoads; ++q) {
+        for (int q = 0; q < NL; ++q) {
           const int idx = threadIdx.x + q * W * 32;
           const int row = idx >> 5, col = idx & 31;
           pre[q] = (row < kInitRows && i0 + row < n) ? ldg4(J + (size_t)(i0 + row) * npad + 128 * c + 4 * col)
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         const int c = t / ntr, i0 = (t - c * ntr) * kInitRows;
         float4* buf = jtile + (t & 1) * (kInitRows * 32);
 #pragma unroll
-        for (int q = 0; q < kInitLoads; ++q) {
+        for (int q = 0; q < NL; ++q) {
           const int idx = threadIdx.x + q * W * 32;
           if (idx < kInitRows * 32) buf[idx] = pre[q];
         }
@@ -299,13 +301,24 @@ int batch_max_sites() { return kBatchMaxN; }
 int batch_warps() { return kBatchWarps; }
 
 // Launch variants: warps per CTA x minimum CTAs per SM (register budget).
+// 45 = 4 warps, 102 registers, 8 chunks at a time (more CTAs per SM when the
+//      fields' shared memory limits residency);
 // 82 = 8 warps, 128 registers, a flip row's loads 16 chunks at a time;
 // 83 = 8 warps, 80 registers; 84 = 8 warps, 64; 162 = 16 warps, 64; 321 = 32 warps, 64
 // (4 chunks at a time).
-int batch_variant_warps(int variant) { return variant / 10 >= 8 ? variant / 10 : kBatchWarps; }
+int batch_min_warps() { return 4; }
+
+int batch_variant_warps(int variant) {
+  switch (variant) {
+    case 45: return 4;
+    case 162: return 16;
+    case 321: return 32;
+    default: return 8;
+  }
+}
 
 bool batch_variant_valid(int variant) {
-  return variant == 82 || variant == 83 || variant == 84 || variant == 162 || variant == 321;
+  return variant == 45 || variant == 82 || variant == 83 || variant == 84 || variant == 162 || variant == 321;
 }
 
 int batch_default_variant() {
@@ -348,6 +361,7 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.soff = d_soff;
   a.items = d_items;
   a.nitems = nitems;
+  a.count = b->count;
   a.counter = d_counter;
   a.spins = spins;
   a.betas = betas;
@@ -360,6 +374,7 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   switch (variant) {
+    case 45: e = launch_variant<4, 5, 8>(a, nitems, fstride, sm_count, st); break;
     case 82: e = launch_variant<8, 2, 16>(a, nitems, fstride, sm_count, st); break;
     case 83: e = launch_variant<8, 3, 4>(a, nitems, fstride, sm_count, st); break;
     case 84: e = launch_variant<8, 4, 4>(a, nitems, fstride, sm_count, st); break;
