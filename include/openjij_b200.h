@@ -56,6 +56,7 @@ enum {
 #define OJ_KERNEL_DENSE_PLAIN (2u << OJ_KERNEL_SHIFT) /* sequential dense, one warp per replica, FP32 */
 #define OJ_KERNEL_BITPACKED (3u << OJ_KERNEL_SHIFT)  /* 32 replicas per word, couplings +-c, h = 0 */
 #define OJ_KERNEL_DENSE_TC (4u << OJ_KERNEL_SHIFT)   /* sequential dense, delayed tensor-core field updates */
+#define OJ_KERNEL_SWENDSEN_WANG (6u << OJ_KERNEL_SHIFT) /* reported by oj_sw_run only */
 #define OJ_KERNEL_DENSE_JUMP (5u << OJ_KERNEL_SHIFT) /* sequential dense, one warp per replica evaluating 128
                                                         sites at once and jumping between accepted flips
                                                         (the batched kernel on one instance), n <= 4096 */
@@ -126,6 +127,21 @@ oj_status oj_graph_query(const oj_graph* g, oj_graph_info* out);
  * replica_offset (a multiple of 32) the global index of replica 0, so a run
  * split over several calls or several GPUs reproduces the unsplit run. */
 oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
+                    const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
+                    int64_t first_sweep, int64_t replica_offset, uint32_t flags, double* energies,
+                    oj_run_stats* stats);
+
+/* Swendsen-Wang cluster annealing over R replicas.  Replaces
+ * Algorithm<SwendsenWang>::run on a ClassicalIsing of a sparse graph
+ * (include/openjij/updater/swendsen_wang.hpp:43-182, binding
+ * openjij/main.cpp:144-154; SASampler's updater "swendsen wang",
+ * openjij/sampler/sa_sampler.py:98-107).  Per sweep every satisfied bond
+ * (h_i as a bond to a fixed dummy spin) is kept with probability
+ * 1 - exp(-2 beta |J|) and every cluster not holding the dummy flips with
+ * probability 1/2.  Arguments, schedule, counters and energies as oj_sa_run;
+ * flags: OJ_DEVICE_POINTERS only.  One CTA per replica holds the union-find
+ * forest in shared memory: n <= 45000. */
+oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
                     const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
                     int64_t first_sweep, int64_t replica_offset, uint32_t flags, double* energies,
                     oj_run_stats* stats);

@@ -28,6 +28,7 @@ OJ_AUTOTUNE = 0x2
 KERNEL_SHIFT = 4
 KERNELS = {"auto": 0, "colour": 1, "dense_plain": 2, "bitpacked": 3, "dense_tc": 4, "dense_jump": 5}
 KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
+KERNEL_NAMES[6] = "swendsen_wang"
 
 # every symbol the header declares
 EXPORTS = [
@@ -35,6 +36,7 @@ EXPORTS = [
     "oj_ctx_synchronize", "oj_ctx_last_error", "oj_graph_create_dense", "oj_graph_create_csr",
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
     "oj_sa_run_bitpacked_noalloc", "oj_batch_create_dense", "oj_batch_destroy", "oj_sa_run_batched",
+    "oj_sw_run",
 ]
 
 
@@ -91,6 +93,7 @@ def lib():
                                  C.POINTER(RunStats)]
         L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
         L.oj_sa_run_bitpacked_noalloc.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64]
+        L.oj_sw_run.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64, u32, vp, C.POINTER(RunStats)]
         L.oj_batch_create_dense.argtypes = [vp, i32, vp, vp, vp, C.POINTER(vp)]
         L.oj_batch_destroy.argtypes = [vp]
         L.oj_sa_run_batched.argtypes = [vp, vp, vp, vp, vp, vp, i32, u64, i64, i64, u32, vp,
@@ -207,6 +210,18 @@ def sa_run(g: Graph, spins, betas, mcs, seed, kernel="auto", energies=None, devi
     g.ctx.check(lib().oj_sa_run(g.ctx._h, g._h, int(R), _ptr(spins), _ptr(b), _ptr(m), len(b),
                                 int(seed) & 0xFFFFFFFFFFFFFFFF, int(first_sweep), int(replica_offset),
                                 _flags(kernel, device, tune), _ptr(energies), C.byref(st)), "oj_sa_run")
+    return st.as_dict()
+
+
+def sw_run(g: Graph, spins, betas, mcs, seed, energies=None, device=False, first_sweep=0, replica_offset=0):
+    """Swendsen-Wang annealing of spins [R][n] (oj_sw_run)."""
+    R = spins.shape[0]
+    b = np.ascontiguousarray(betas, np.float64)
+    m = np.ascontiguousarray(mcs, np.int32)
+    st = RunStats()
+    g.ctx.check(lib().oj_sw_run(g.ctx._h, g._h, int(R), _ptr(spins), _ptr(b), _ptr(m), len(b),
+                                int(seed) & 0xFFFFFFFFFFFFFFFF, int(first_sweep), int(replica_offset),
+                                _flags("auto", device), _ptr(energies), C.byref(st)), "oj_sw_run")
     return st.as_dict()
 
 

@@ -8,7 +8,8 @@
 //   openjij/declare.hpp:195-217  CSRSparse
 //   openjij/declare.hpp:409-438  ClassicalIsing        openjij/main.cpp:68-73
 //   openjij/declare.hpp:585-641  TransverseIsing       openjij/main.cpp:80-85
-//   openjij/declare.hpp:687-793  Algorithm_SingleSpinFlip_run (4 overloads)
+//   openjij/declare.hpp:687-793  Algorithm_SingleSpinFlip_run (4 overloads),
+//                                Algorithm_SwendsenWang_run (openjij/main.cpp:144-154)
 //   openjij/declare.hpp:795-879  updater parameters, schedules, make_*_schedule_list
 //   openjij/declare.hpp:881-888  get_solution
 // Extensions: a system may hold R replicas (2-D initial spins, or 3-D Trotter
@@ -27,6 +28,7 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -86,8 +88,9 @@ struct RunInfo {
 RunInfo g_last_run;
 
 void record(const oj_run_stats& st) {
-  static const char* names[] = {"auto", "colour", "dense_plain", "bitpacked", "dense_tc"};
-  g_last_run.kernel = (st.kernel >= 0 && st.kernel < 5) ? names[st.kernel] : "?";
+  static const char* names[] = {"auto", "colour", "dense_plain", "bitpacked", "dense_tc", "dense_jump",
+                                "swendsen_wang"};
+  g_last_run.kernel = (st.kernel >= 0 && st.kernel < 7) ? names[st.kernel] : "?";
   g_last_run.launches += st.launches;
   g_last_run.sweeps += st.sweeps;
   g_last_run.attempts += st.attempts;
@@ -570,6 +573,7 @@ uint32_t kernel_flag(const std::string& k) {
   if (k == "dense_plain") return OJ_KERNEL_DENSE_PLAIN;
   if (k == "bitpacked") return OJ_KERNEL_BITPACKED;
   if (k == "dense_tc") return OJ_KERNEL_DENSE_TC;
+  if (k == "dense_jump") return OJ_KERNEL_DENSE_JUMP;
   throw std::invalid_argument("unknown kernel " + k);
 }
 
@@ -621,6 +625,57 @@ void run_classical(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<Clas
         rc = oj_sa_run(ctx(), dg, sys.R, sys.spins.data(), &b, &one, 1, seed, sweep, 0, flags, nullptr, &st);
       }
       check(rc, "Algorithm_SingleSpinFlip_run");
+      record(st);
+      ++sweep;
+      cb(sys, b);
+    }
+  }
+}
+
+// Algorithm<SwendsenWang>::run (algorithm.hpp:26-56 with
+// updater/swendsen_wang.hpp:43-182) for R classical replicas on a sparse graph.
+template <class G>
+void run_swendsen_wang(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<ClassicalSchedule>& sched,
+                       const std::function<void(const ClassicalIsing<G>&, double)>& cb) {
+  g_last_run = RunInfo();
+  if (sys.num_spins == 0 || sched.empty()) {
+    if (cb)
+      for (auto& s : sched)
+        for (size_t m = 0; m < s.one_mc_step; ++m) cb(sys, s.updater_parameter.beta);
+    return;
+  }
+  oj_graph* dg = sys.graph->device();
+  if (!cb) {
+    std::vector<double> betas;
+    std::vector<int32_t> mcs;
+    for (auto& s : sched) {
+      if (s.updater_parameter.beta < 0) throw std::invalid_argument("beta must be >= 0");
+      betas.push_back(s.updater_parameter.beta);
+      mcs.push_back((int32_t)s.one_mc_step);
+    }
+    oj_run_stats st;
+    oj_status rc;
+    {
+      py::gil_scoped_release release;
+      rc = oj_sw_run(ctx(), dg, sys.R, sys.spins.data(), betas.data(), mcs.data(), (int32_t)betas.size(), seed, 0, 0,
+                     0, nullptr, &st);
+    }
+    check(rc, "Algorithm_SwendsenWang_run");
+    record(st);
+    return;
+  }
+  int64_t sweep = 0;
+  for (auto& s : sched) {
+    for (size_t m = 0; m < s.one_mc_step; ++m) {
+      const double b = s.updater_parameter.beta;
+      const int32_t one = 1;
+      oj_run_stats st;
+      oj_status rc;
+      {
+        py::gil_scoped_release release;
+        rc = oj_sw_run(ctx(), dg, sys.R, sys.spins.data(), &b, &one, 1, seed, sweep, 0, 0, nullptr, &st);
+      }
+      check(rc, "Algorithm_SwendsenWang_run");
       record(st);
       ++sweep;
       cb(sys, b);
@@ -766,6 +821,16 @@ void bind_graph_systems(py::module_& msys, py::module_& malg, py::module_& mres,
       "system"_a, "schedule_list"_a, "callback"_a = nullptr);
   mres.def("get_solution", [](const CI& s) { return solution(s); }, "system"_a);
   mres.def("get_solution", [](const TI& s) { return solution(s); }, "system"_a);
+  // Swendsen-Wang: sparse systems only, as the reference (openjij/main.cpp:144-154)
+  if (std::is_same<G, CSRSparse>::value) {
+    const char* sw = "Algorithm_SwendsenWang_run";
+    malg.def(
+        sw, [](CI& s, uint64_t seed, const py::list& sched, const CCb& cb) { run_swendsen_wang(s, seed, classical_from_list(sched), cb); },
+        "system"_a, "seed"_a, "schedule_list"_a, "callback"_a = nullptr);
+    malg.def(
+        sw, [](CI& s, const py::list& sched, const CCb& cb) { run_swendsen_wang(s, random_seed(), classical_from_list(sched), cb); },
+        "system"_a, "schedule_list"_a, "callback"_a = nullptr);
+  }
 }
 
 }  // namespace

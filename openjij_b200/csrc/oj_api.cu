@@ -1148,4 +1148,77 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   return OJ_OK;
 }
 
+oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, const double* betas,
+                    const int32_t* mcs, int32_t num_sched, uint64_t seed, int64_t first_sweep,
+                    int64_t replica_offset, uint32_t flags, double* energies, oj_run_stats* stats) {
+  if (!ctx || !gc || R < 0 || num_sched < 0) return arg_fail(ctx, "null argument or negative size");
+  if (num_sched > 0 && (!betas || !mcs)) return arg_fail(ctx, "null schedule");
+  oj_graph* g = const_cast<oj_graph*>(gc);
+  if (g->device != ctx->device) return arg_fail(ctx, "graph belongs to another device");
+  const int n = g->n;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (R == 0 || n == 0) return OJ_OK;
+  if (!spins) return arg_fail(ctx, "null spins");
+  if ((flags & OJ_KERNEL_MASK) != OJ_KERNEL_AUTO) {
+    ctx->last_error = "Swendsen-Wang has a single kernel; pass OJ_KERNEL_AUTO";
+    return OJ_ERR_UNSUPPORTED;
+  }
+  if (n > sw_max_sites()) {
+    ctx->last_error = "Swendsen-Wang kernel supports n <= " + std::to_string(sw_max_sites());
+    return OJ_ERR_UNSUPPORTED;
+  }
+  for (int32_t k = 0; k < num_sched; ++k)
+    if (!(betas[k] >= 0.0) || std::isinf(betas[k])) return arg_fail(ctx, "beta must be finite and >= 0");
+  RngBase rb;
+  if (oj_status st_ = rng_base(ctx, seed, first_sweep, replica_offset, &rb)) return st_;
+  DeviceGuard dg(ctx->device);
+  std::vector<double> bexp;
+  if (oj_status st_ = expand(ctx, betas, mcs, num_sched, bexp)) return st_;
+  const int64_t S = (int64_t)bexp.size();
+  std::vector<float> bf(bexp.begin(), bexp.end());
+  const bool devp = (flags & OJ_DEVICE_POINTERS) != 0;
+  cudaStream_t st = ctx->stream;
+  const size_t spin_bytes = (size_t)R * n;
+  int8_t* d_spins = spins;
+  if (!devp) {
+    OJ_CK(ctx->spins.ensure(spin_bytes), "alloc spins");
+    d_spins = ctx->spins.as<int8_t>();
+  } else if (!is_device_ptr(spins)) {
+    return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
+  }
+  OJ_CK(sw_prepare(g), "bond list");
+  int launches = 0;
+  OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
+  if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
+  OJ_CK(ctx->params.ensure(std::max<size_t>(bf.size() * 4, 16)), "alloc params");
+  float* d_beta = ctx->params.as<float>();
+  if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+  OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+  if (S > 0) OJ_CK(launch_sw(g, R, d_spins, d_beta, S, rb, st, &launches), "swendsen-wang kernel");
+  OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  if (energies) {
+    double* d_e = energies;
+    if (!devp) {
+      OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
+      d_e = ctx->energies.as<double>();
+    }
+    OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+    ++launches;
+    if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+  }
+  if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
+  OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
+  if (!devp || stats) OJ_CK(cudaStreamSynchronize(st), "run");
+  if (stats) {
+    stats->kernel = (int32_t)(OJ_KERNEL_SWENDSEN_WANG >> OJ_KERNEL_SHIFT);
+    stats->launches = launches;
+    stats->sweeps = S;
+    stats->attempts = (double)R * n * (double)S;
+    stats->threads = 512;
+    cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+  }
+  return OJ_OK;
+}
+
 }  // extern "C"

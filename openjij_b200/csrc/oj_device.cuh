@@ -12,6 +12,9 @@
 //     W_l(r, q, k, i) = Philox((i, k, r, ((l>>2)<<16) | (q<<8) | TAG_SQA_MSC))[l & 3]
 //   slice-split bit-packed SQA kernel (replica group g, half q = 0 even / 1 odd):
 //     W_l(g, q, k, i) = Philox((i, k, g, ((l>>2)<<16) | (q<<8) | TAG_SQA_SPLIT))[l & 3]
+//   Swendsen-Wang (bond e, cluster root c):
+//     u(r, k, e)   = Philox((e >> 2, k, r, TAG_SW_BOND))[e & 3]
+//     coin(r, k, c) = Philox((c >> 2, k, r, TAG_SW_FLIP))[c & 3] & 1
 //   batched dense SA kernel (instance m, replica r of that instance):
 //     u(m, r, k, i) = Philox((i >> 2, k, r, (m << 8) | TAG_BATCH))[i & 3]
 // with r the replica, t the Trotter slice, k the sweep (one_mc_step repeats
@@ -28,6 +31,8 @@ constexpr uint32_t TAG_SA_MSC = 0x3Cu;
 constexpr uint32_t TAG_SQA_MSC = 0xC3u;
 constexpr uint32_t TAG_SQA_SPLIT = 0x69u;
 constexpr uint32_t TAG_BATCH = 0x96u;
+constexpr uint32_t TAG_SW_BOND = 0xB1u;
+constexpr uint32_t TAG_SW_FLIP = 0xB2u;
 
 struct u4 {
   uint32_t x, y, z, w;

@@ -47,6 +47,7 @@ oj_graph::~oj_graph() {
   sqa_jm.release();
   single.reset();
   single_tab.release();
+  sw_tables.release();
   if (msc) msc->tables.release();
   if (tc) {
     tc->bt_hi.release();

@@ -106,6 +106,8 @@ struct oj_graph {
   std::map<uint64_t, oj::Shape> tuned;  // autotuned launch shapes by (kernel, replicas, slices)
   std::unique_ptr<oj_batch> single;     // this graph as a one-instance batch (dense jump kernel, energies)
   oj::DevBuf single_tab;                // its per-call tables: reads, order, replica and energy offsets
+  int64_t sw_ne = -1;                   // Swendsen-Wang bond count (-1: list not built)
+  oj::DevBuf sw_tables;                 // its bond list: i, j, |J|, sign
   ~oj_graph();
 };
 
@@ -173,6 +175,11 @@ cudaError_t launch_sqa_split_pack(const int8_t* spins, int R, int T, int n, int 
                                   cudaStream_t st);
 cudaError_t launch_sqa_split_unpack(const uint32_t* words, int R, int T, int n, int G, int8_t* spins,
                                     cudaStream_t st);
+size_t sw_smem_bytes(int n);
+int sw_max_sites();
+cudaError_t sw_prepare(oj_graph* g);
+cudaError_t launch_sw(const oj_graph* g, int R, int8_t* spins, const float* betas, int64_t nsweeps, RngBase rb,
+                      cudaStream_t st, int* launches);
 int batch_max_sites();
 int batch_warps();
 int batch_variant_warps(int variant);

@@ -6,8 +6,8 @@ Same parameters, defaults and schedule construction as the reference's
 * reads are replicas with their own counter-based random streams, so with a
   ``seed`` the reads start from the same initial state (as in the reference,
   sa_sampler.py:253-258) but no longer repeat each other;
-* ``updater`` accepts "single spin flip" only (Swendsen-Wang is not part of
-  this library).
+* ``updater`` "swendsen wang" runs the GPU Swendsen-Wang kernel (oj_sw_run);
+  like the reference it always uses the sparse graph.
 """
 from __future__ import annotations
 
@@ -39,8 +39,10 @@ class SASampler(BaseSampler):
             "num_reads": 1,
         }
         self._params = self._default_params.copy()
-        self._make_system = {"singlespinflip": cxxjij.system.make_classical_ising}
-        self._algorithm = {"singlespinflip": cxxjij.algorithm.Algorithm_SingleSpinFlip_run}
+        self._make_system = {"singlespinflip": cxxjij.system.make_classical_ising,
+                             "swendsenwang": cxxjij.system.make_classical_ising}
+        self._algorithm = {"singlespinflip": cxxjij.algorithm.Algorithm_SingleSpinFlip_run,
+                           "swendsenwang": cxxjij.algorithm.Algorithm_SwendsenWang_run}
         self.schedule_info = {}
 
     def _convert_validation_schedule(self, schedule):
@@ -84,7 +86,9 @@ class SASampler(BaseSampler):
             reinitialize_state = True
         name = updater.lower().replace("_", "").replace(" ", "")
         if name not in self._make_system:
-            raise ValueError('updater is one of "single spin flip"')
+            raise ValueError('updater is one of "single spin flip or swendsen wang"')
+        if name == "swendsenwang":  # runs on sparse graphs only (sa_sampler.py:195-197)
+            sparse = True
         model = _as_bqm(bqm, bool(sparse))
         ising_graph, offset = model.get_cxxjij_ising_graph()
         self._set_params(beta_min=beta_min, beta_max=beta_max, num_sweeps=num_sweeps,

@@ -33,6 +33,7 @@
 #include <random>
 #include <vector>
 #include <algorithm>
+#include <functional>
 #include <thread>
 #include <atomic>
 
@@ -204,6 +205,8 @@ constexpr uint32_t TAG_SA_MSC = 0x3Cu;   // low byte of c3 of the bit-packed SA 
 constexpr uint32_t TAG_SQA_MSC = 0xC3u;    // low byte of c3 of the bit-packed SQA stream
 constexpr uint32_t TAG_SQA_SPLIT = 0x69u;  // low byte of c3 of the slice-split SQA stream
 constexpr uint32_t TAG_BATCH = 0x96u;      // low byte of c3 of the batched dense SA stream
+constexpr uint32_t TAG_SW_BOND = 0xB1u;    // Swendsen-Wang bond draws
+constexpr uint32_t TAG_SW_FLIP = 0xB2u;    // Swendsen-Wang cluster coins
 
 inline float f_of(uint32_t b) {
   float f;
@@ -976,6 +979,160 @@ void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset,
     // the incrementally updated FP32 fields at the end (same layout as spins)
     if (fields_out)
       for (int j = 0; j < n; ++j) fields_out[soff[m] + (size_t)r * n + j] = f[j];
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Swendsen-Wang
+// ---------------------------------------------------------------------------
+
+// Reference Swendsen-Wang (include/openjij/updater/swendsen_wang.hpp:43-182 with
+// include/openjij/utility/union_find.hpp): one read, spins in/out [n], the
+// dummy spin n starts at +1, result s_i * s_n (get_solution.hpp:45-46).
+namespace {
+struct RefUnionFind {  // union_find.hpp: union by rank, path compression
+  std::vector<size_t> parent, rank;
+  explicit RefUnionFind(size_t n) : parent(n), rank(n, 0) {
+    for (size_t i = 0; i < n; ++i) parent[i] = i;
+  }
+  size_t find(size_t node) {
+    size_t base = node, p = parent[node];
+    while (p != node) {
+      node = p;
+      p = parent[node];
+    }
+    const size_t root = p;
+    node = parent[base];
+    while (root != node) {
+      parent[base] = root;
+      base = node;
+      node = parent[base];
+    }
+    return root;
+  }
+  void unite(size_t x, size_t y) {
+    size_t rx = find(x), ry = find(y);
+    if (rx == ry) return;
+    if (rank[rx] > rank[ry]) {
+      parent[ry] = rx;
+    } else {
+      parent[rx] = ry;
+      if (rank[rx] == rank[ry]) ++rank[ry];
+    }
+  }
+};
+
+template <class Eng>
+void ref_sw_update(const Aug& g, std::vector<double>& s, Eng& eng, double beta) {
+  auto urd = std::uniform_real_distribution<>(0, 1.0);
+  const size_t N = (size_t)g.n + 1;
+  RefUnionFind uf(N);
+  for (size_t node = 0; node < N; ++node)
+    for (int64_t p = g.indptr[node]; p < g.indptr[node + 1]; ++p) {
+      const size_t adj = (size_t)g.indices[p];
+      const double J = g.data[p];
+      if (node >= adj) continue;
+      if (J * s[node] * s[adj] > 0) continue;
+      const double rate = std::max(0.0, 1.0 - std::exp(-2.0 * beta * std::abs(J)));
+      if (urd(eng) < rate) uf.unite(node, adj);
+    }
+  std::vector<std::vector<size_t>> members(N);
+  for (size_t node = 0; node < N; ++node) members[uf.find(node)].push_back(node);
+  std::vector<size_t> roots = uf.parent;  // get_roots(): sorted unique parents
+  std::sort(roots.begin(), roots.end());
+  roots.erase(std::unique(roots.begin(), roots.end()), roots.end());
+  for (size_t c : roots)
+    if (urd(eng) < 0.5)
+      for (size_t i : members[c]) s[i] *= -1;
+}
+}  // namespace
+
+extern "C" {
+
+void orc_ref_sw(int n, const int64_t* indptr, const int32_t* indices, const double* data, int8_t* spins,
+                const double* betas, const int64_t* mcs, int64_t nsched, uint64_t seed) {
+  Aug g{n, indptr, indices, data};
+  std::vector<double> s(n + 1);
+  for (int i = 0; i < n; ++i) s[i] = spins[i];
+  s[n] = 1;
+  Xorshift e((unsigned)seed);
+  for (int64_t k = 0; k < nsched; ++k)
+    for (int64_t m = 0; m < mcs[k]; ++m) ref_sw_update(g, s, e, betas[k]);
+  for (int i = 0; i < n; ++i) spins[i] = (int8_t)(s[i] * s[n]);
+}
+
+void orc_ref_sw_many(int n, const int64_t* indptr, const int32_t* indices, const double* data, int num_reads,
+                     int8_t* spins, const double* betas, const int64_t* mcs, int64_t nsched, const uint64_t* seeds,
+                     int threads) {
+  parallel_for(num_reads, threads, [&](int r) {
+    orc_ref_sw(n, indptr, indices, data, spins + (size_t)r * n, betas, mcs, nsched, seeds[r]);
+  });
+}
+
+// Replay of the B200 Swendsen-Wang kernel.  Bonds: (i, j), i < j, over the
+// neighbour lists in CSR column order, then (i, n) for every h_i != 0, indexed
+// e = 0, 1, ... in that order; |J| and the sign from the FP64 couplings, |J|
+// rounded to FP32.  Per sweep k (betas_f[k] FP32): bond e is kept when it is
+// satisfied (J s_i s_j < 0, s_n = +1) and neglog(u_e) < (2*beta)*|J| (FP32
+// products), u_e = Philox(ctr = (e >> 2, k, r, TAG_SW_BOND))[e & 3]; clusters
+// of the kept bonds; a cluster's label is its smallest site; every cluster
+// other than the one holding n flips when bit 0 of Philox(ctr = (c >> 2, k, r,
+// TAG_SW_FLIP))[c & 3] is set (c the label).
+void orc_replay_sw(int n, const int64_t* indptr, const int32_t* indices, const double* data, int R,
+                   int8_t* spins, const float* betas_f, int64_t nsweeps, uint64_t seed, int threads) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  std::vector<int> bi, bj;
+  std::vector<float> bw;
+  std::vector<char> bpos;
+  for (int i = 0; i < n; ++i)
+    for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) {
+      const int j = indices[p];
+      if (j == i || j == n || data[p] == 0.0 || j < i) continue;
+      bi.push_back(i);
+      bj.push_back(j);
+      bw.push_back((float)std::fabs(data[p]));
+      bpos.push_back(data[p] > 0);
+    }
+  for (int i = 0; i < n; ++i)
+    for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p)
+      if (indices[p] == n && data[p] != 0.0) {
+        bi.push_back(i);
+        bj.push_back(n);
+        bw.push_back((float)std::fabs(data[p]));
+        bpos.push_back(data[p] > 0);
+      }
+  const size_t ne = bi.size();
+  parallel_for(R, threads, [&](int r) {
+    int8_t* s = spins + (size_t)r * n;
+    std::vector<int> comp(n + 1);
+    std::function<int(int)> root = [&](int x) {
+      while (comp[x] != x) x = comp[x];
+      return x;
+    };
+    for (int64_t k = 0; k < nsweeps; ++k) {
+      for (int i = 0; i <= n; ++i) comp[i] = i;
+      const float beta2 = 2.0f * betas_f[k];
+      for (size_t e = 0; e < ne; ++e) {
+        const int si = s[bi[e]], sj = bj[e] < n ? s[bj[e]] : 1;
+        const bool aligned = si * sj > 0;
+        if (aligned == (bool)bpos[e]) continue;  // unsatisfied (or J s_i s_j > 0)
+        const P4 q = philox((uint32_t)(e >> 2), (uint32_t)k, (uint32_t)r, TAG_SW_BOND, k0, k1);
+        if (!(neglog(q.v[e & 3]) < beta2 * bw[e])) continue;
+        int a = root(bi[e]), b = root(bj[e]);
+        if (a == b) continue;
+        if (a < b) std::swap(a, b);
+        comp[a] = b;  // the larger label under the smaller: a cluster's label is its smallest site
+      }
+      const int rn = root(n);
+      for (int i = 0; i < n; ++i) {
+        const int c = root(i);
+        if (c == rn) continue;
+        const P4 q = philox((uint32_t)c >> 2, (uint32_t)k, (uint32_t)r, TAG_SW_FLIP, k0, k1);
+        if (q.v[c & 3] & 1u) s[i] = (int8_t)-s[i];
+      }
+    }
   });
 }
 

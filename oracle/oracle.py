@@ -79,6 +79,11 @@ def lib():
                                            _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
         L.orc_replay_sa_batch.argtypes = [C.c_int, _i32p, _i64p, _f64p, _i32p, _i8p, _f32p, C.c_int64,
                                           C.c_uint64, C.c_uint32, C.c_int, C.c_void_p]
+        L.orc_ref_sw.argtypes = [C.c_int, _i64p, _i32p, _f64p, _i8p, _f64p, _i64p, C.c_int64, C.c_uint64]
+        L.orc_ref_sw_many.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f64p, _i64p, C.c_int64,
+                                      _u64p, C.c_int]
+        L.orc_replay_sw.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f32p, C.c_int64, C.c_uint64,
+                                    C.c_int]
         L.orc_gen_spin_seq.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _i8p]
         _lib = L
     return _lib
@@ -386,3 +391,20 @@ def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, thr
                               int(seed), int(inst0), _threads(threads),
                               None if fo is None else fo.ctypes.data)
     return (s, fo) if fields else s
+
+
+def ref_sw_many(g: AugCSR, init2d, betas, mcs, seeds, threads=None):
+    """Reference Swendsen-Wang reads (Xorshift seeded per read), result s_i * s_dummy."""
+    s = np.array(init2d, np.int8, copy=True, order="C")
+    lib().orc_ref_sw_many(*g.args(), s.shape[0], s, np.ascontiguousarray(betas, np.float64),
+                          np.ascontiguousarray(mcs, np.int64), len(betas),
+                          np.ascontiguousarray(seeds, np.uint64), _threads(threads))
+    return s
+
+
+def replay_sw(g: AugCSR, init2d, betas_per_sweep, seed, threads=None):
+    """Replay of the B200 Swendsen-Wang kernel."""
+    s = np.array(init2d, np.int8, copy=True, order="C")
+    b = np.ascontiguousarray(betas_per_sweep, np.float32)
+    lib().orc_replay_sw(*g.args(), s.shape[0], s, b, len(b), int(seed), _threads(threads))
+    return s

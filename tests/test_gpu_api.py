@@ -219,7 +219,22 @@ def test_reverse_annealing_chains_reads():
 
 def test_unknown_parameter_and_updater():
     with pytest.raises(ValueError):
-        oj.SASampler().sample_ising(NUM_H, NUM_J, updater="swendsen wang")
+        oj.SASampler().sample_ising(NUM_H, NUM_J, updater="heat bath")
+
+
+def test_swendsen_wang_sampler():
+    """updater="swendsen wang" (sa_sampler.py:98-107): ground states of the
+    reference's 5-spin case and the AFM chain with a field, on the GPU cluster kernel."""
+    res = oj.SASampler().sample_ising(NUM_H, NUM_J, updater="swendsen wang", num_reads=16, seed=3)
+    assert res.info["run"]["kernel"] == "swendsen_wang"
+    assert list(res.first.sample.values()) == GROUND5 and res.first.energy == -6
+    res = oj.SASampler().sample_ising({0: -10}, {(i, i + 1): 1 for i in range(29)}, updater="swendsen_wang",
+                                      num_reads=32, seed=1, sparse=False)
+    assert res.first.sample == {i: (-1) ** i for i in range(30)}
+    # the cxxjij binding exists for sparse systems only, as in the reference
+    d = G.Dense(4)
+    with pytest.raises(TypeError):
+        A.Algorithm_SwendsenWang_run(S.make_classical_ising([1, 1, 1, 1], d), 1, U.make_classical_schedule_list(0.1, 1.0, 1, 4))
 
 
 def test_sa_sample_batch():

@@ -341,3 +341,43 @@ def test_sa_dense_tc_real_couplings_statistics(ctx):
     se = np.sqrt(ea.var() / len(ea) + eb.var() / len(eb))
     assert abs(ea.mean() - eb.mean()) < 4 * se + 1e-9
     np.testing.assert_allclose(ea, O.energies(g, a), rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("which", ["lattice", "regular_h", "sparse_real"])
+def test_swendsen_wang_bit_exact(ctx, which):
+    """oj_sw_run against its replay: bonds, clusters (union-find) and cluster
+    coins; with fields (bonds to the dummy spin) and real couplings."""
+    if which == "lattice":
+        m = I.lattice_pm_j(16, seed=4)[0]
+    elif which == "regular_h":
+        m = I.random_regular_pm_j(300, 3, seed=5)[0].tolil()
+        rng = np.random.default_rng(1)
+        n = m.shape[0] - 1
+        for i in range(0, n, 3):
+            m[i, n] = m[n, i] = float(rng.choice([-0.5, 0.7]))
+        m = m.tocsr()
+    else:
+        m, _ = I.dense_ising_uniform(60, seed=9)
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.1, 3.0, 12)
+    s0 = _init(40, g.n, 7)
+    s = s0.copy()
+    e = np.zeros(40)
+    st = N.sw_run(dg, s, betas, mcs, seed=19, energies=e)
+    assert st["kernel"] == "swendsen_wang"
+    ref = O.replay_sw(g, s0, _per_sweep(betas, mcs), 19)
+    np.testing.assert_array_equal(s, ref)
+    np.testing.assert_allclose(e, O.energies(g, ref), rtol=1e-12, atol=1e-9)
+
+
+def test_swendsen_wang_split_run(ctx):
+    m = I.lattice_pm_j(8, seed=2)[0]
+    g, dg = _graph(ctx, m)
+    betas, mcs = I.geometric_betas(0.2, 2.0, 10)
+    s0 = _init(64, g.n, 3)
+    whole = s0.copy()
+    N.sw_run(dg, whole, betas, mcs, seed=4)
+    part = s0[32:].copy()
+    N.sw_run(dg, part, betas[:4], mcs[:4], seed=4, replica_offset=32)
+    N.sw_run(dg, part, betas[4:], mcs[4:], seed=4, replica_offset=32, first_sweep=int(np.sum(mcs[:4])))
+    np.testing.assert_array_equal(part, whole[32:])

@@ -190,3 +190,23 @@ def test_batched_fp32_field_drift_is_stated():
             scale = np.abs(f64).max()
             drift = np.abs(f32 - f64r).max() / scale
             assert drift <= tol, (n, drift)
+
+
+def test_swendsen_wang_equilibrium_and_annealing():
+    """Swendsen-Wang replay against the reference updater (swendsen_wang.hpp):
+    the equilibrium energy histogram at a fixed beta, and the ground-state rate
+    of a short anneal."""
+    g = _lattice4()
+    R, S, beta = 4096, 100, 0.6
+    s0 = _init(R, g.n, 11)
+    ref = O.ref_sw_many(g, s0, [beta], [S], np.arange(R, dtype=np.uint64) + 77)
+    got = O.replay_sw(g, s0, np.full(S, beta, np.float32), 5)
+    p = _chi2_p(O.energies(g, got), O.energies(g, ref))
+    assert p > P_MIN, p
+    e0 = _ground_energy(g)
+    betas, mcs = I.geometric_betas(0.1, 3.0, 8)
+    ref = O.ref_sw_many(g, s0[:2048], betas, mcs, np.arange(2048, dtype=np.uint64) + 3)
+    got = O.replay_sw(g, s0[:2048], np.repeat(betas, mcs).astype(np.float32), 6)
+    eg, er = O.energies(g, got), O.energies(g, ref)
+    ok, rates = _two_prop_ok(np.sum(np.isclose(eg, e0)), 2048, np.sum(np.isclose(er, e0)), 2048, 0.05)
+    assert ok, rates
