@@ -189,8 +189,19 @@ oj_status oj_sa_run_bitpacked_noalloc(oj_ctx* ctx, const oj_graph* g, int32_t nu
 oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, const int8_t* spins,
                     uint32_t flags, double* energies);
 
+/* Statistics behind SASampler's automatic beta range (sa_sampler.py:876-965,
+ * which forms them with a dense matrix product and np.abs over the whole
+ * augmented matrix).  For K (1..8) spin configurations spins[n][K] (+-1):
+ *   dE_quad[n][K] = -2 s_i^c sum_{j<n} J_ij s_j^c   (coupling part of a flip)
+ *   dE_lin[n][K]  = h_i s_i^c                       (field part)
+ *   *abs_min      = smallest |entry| > threshold of the augmented matrix
+ *                   (couplings, fields and the corner); +inf if there is none.
+ * Host pointers; FP64; sums in the warp's order (exact for integer couplings). */
+oj_status oj_graph_flip_stats(oj_ctx* ctx, const oj_graph* g, int32_t K, const int8_t* spins, double threshold,
+                              double* dE_quad, double* dE_lin, double* abs_min);
+
 /* A batch of dense instances of uneven size for oj_sa_run_batched.  Instance
- * k has n[k] spins (0 <= n[k] <= 1024) and its augmented (n[k]+1)^2 matrix,
+ * k has n[k] spins (0 <= n[k] <= 4096) and its augmented (n[k]+1)^2 matrix,
  * row-major exactly as graph.Dense.get_interactions() returns it (J with zero
  * diagonal, h in row/column n[k], 1 in the corner; dense.hpp:117-140), at
  * J_aug + offset[k].  Invalid matrices -> OJ_ERR_ARG.  The reference has no
@@ -198,6 +209,12 @@ oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, const 
 oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset,
                                 const double* J_aug, oj_batch** out);
 oj_status oj_batch_destroy(oj_batch* b);
+
+/* oj_graph_flip_stats for every instance of a batch: spins, dE_quad and dE_lin
+ * are the instances' [n[k]][K] blocks back to back, abs_min[count] (the
+ * minimum over instance k's augmented matrix, corner included). */
+oj_status oj_batch_flip_stats(oj_ctx* ctx, const oj_batch* b, int32_t K, const int8_t* spins, double threshold,
+                              double* dE_quad, double* dE_lin, double* abs_min);
 
 /* Simulated annealing of every instance of a batch in one persistent kernel
  * launch.  Replaces a loop of SASampler.sample calls over instances

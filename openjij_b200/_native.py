@@ -36,7 +36,7 @@ EXPORTS = [
     "oj_ctx_synchronize", "oj_ctx_last_error", "oj_graph_create_dense", "oj_graph_create_csr",
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
     "oj_sa_run_bitpacked_noalloc", "oj_batch_create_dense", "oj_batch_destroy", "oj_sa_run_batched",
-    "oj_sw_run",
+    "oj_sw_run", "oj_graph_flip_stats", "oj_batch_flip_stats",
 ]
 
 
@@ -94,6 +94,8 @@ def lib():
         L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
         L.oj_sa_run_bitpacked_noalloc.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64]
         L.oj_sw_run.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64, u32, vp, C.POINTER(RunStats)]
+        L.oj_graph_flip_stats.argtypes = [vp, vp, i32, vp, dbl, vp, vp, C.POINTER(dbl)]
+        L.oj_batch_flip_stats.argtypes = [vp, vp, i32, vp, dbl, vp, vp, vp]
         L.oj_batch_create_dense.argtypes = [vp, i32, vp, vp, vp, C.POINTER(vp)]
         L.oj_batch_destroy.argtypes = [vp]
         L.oj_sa_run_batched.argtypes = [vp, vp, vp, vp, vp, vp, i32, u64, i64, i64, u32, vp,
@@ -260,6 +262,19 @@ def energy(g: Graph, spins, out=None, device=False):
     return out
 
 
+def flip_stats(g: Graph, spins, threshold=1e-8):
+    """Single-flip energy changes of spins [n][K] and the smallest coupling
+    magnitude above threshold (oj_graph_flip_stats): (quad, lin, abs_min)."""
+    s = np.ascontiguousarray(spins, np.int8)
+    n, K = s.shape
+    quad = np.zeros((n, K), np.float64)
+    lin = np.zeros((n, K), np.float64)
+    amin = C.c_double(0.0)
+    g.ctx.check(lib().oj_graph_flip_stats(g.ctx._h, g._h, int(K), _ptr(s), float(threshold), _ptr(quad),
+                                          _ptr(lin), C.byref(amin)), "oj_graph_flip_stats")
+    return quad, lin, amin.value
+
+
 class Batch:
     """Owns an oj_batch: dense instances of uneven size, given as their
     augmented (n+1)x(n+1) matrices (numpy arrays)."""
@@ -274,6 +289,19 @@ class Batch:
         self._h = C.c_void_p()
         ctx.check(lib().oj_batch_create_dense(ctx._h, len(mats), _ptr(self.n), _ptr(self.offset), _ptr(flat),
                                               C.byref(self._h)), "oj_batch_create_dense")
+
+    def flip_stats(self, spins, threshold=1e-8):
+        """oj_batch_flip_stats: spins are the instances' [n[k]][K] blocks back
+        to back; returns (quad, lin) of the same shape and abs_min[count]."""
+        s = np.ascontiguousarray(spins, np.int8)
+        if s.ndim != 2 or s.shape[0] != int(self.n.sum()):
+            raise ValueError("spins must have shape (sum(n), K)")
+        quad = np.zeros(s.shape, np.float64)
+        lin = np.zeros(s.shape, np.float64)
+        amin = np.zeros(len(self.n), np.float64)
+        self.ctx.check(lib().oj_batch_flip_stats(self.ctx._h, self._h, int(s.shape[1]), _ptr(s), float(threshold),
+                                                 _ptr(quad), _ptr(lin), _ptr(amin)), "oj_batch_flip_stats")
+        return quad, lin, amin
 
     def close(self):
         if self._h:

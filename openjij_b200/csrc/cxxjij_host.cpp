@@ -312,6 +312,25 @@ struct CSRSparse : Graph {
   mutable std::shared_ptr<DeviceGraph> dev_;
 };
 
+// Single-flip energy changes of the configurations spins[n][K] and the smallest
+// coupling magnitude above thr (oj_graph_flip_stats): what the automatic beta
+// range of SASampler reads (sa_sampler.py:876-965).
+template <class G>
+py::tuple flip_stats(const G& g, py::array_t<int8_t, py::array::c_style | py::array::forcecast> s, double thr) {
+  if (s.ndim() != 2 || (size_t)s.shape(0) != g.n_) throw std::invalid_argument("spins must have shape (n, K)");
+  const size_t K = (size_t)s.shape(1);
+  py::array_t<double> quad({g.n_, K}), lin({g.n_, K});
+  double amin = 0.0;
+  oj_graph* dg = g.device();
+  oj_status rc;
+  {
+    py::gil_scoped_release release;
+    rc = oj_graph_flip_stats(ctx(), dg, (int32_t)K, s.data(), thr, quad.mutable_data(), lin.mutable_data(), &amin);
+  }
+  check(rc, "flip_stats");
+  return py::make_tuple(quad, lin, amin);
+}
+
 // ---------------------------------------------------------------------------
 // schedules (include/openjij/utility/schedule_list.hpp)
 // ---------------------------------------------------------------------------
@@ -857,6 +876,7 @@ PYBIND11_MODULE(_cxxjij, m) {
       .def(py::init<const Dense&>(), "other"_a)
       .def("set_interaction_matrix", &Dense::set_interaction_matrix, "interaction"_a)
       .def("get_interactions", &Dense::get_interactions)
+      .def("_flip_stats", &flip_stats<Dense>, "spins"_a, "threshold"_a)
       .def("calc_energy", [](const Dense& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
       .def("energy", [](const Dense& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
       .def("__setitem__", [](Dense& g, std::pair<size_t, size_t> k, double v) { g.set(k.first, k.second, v); }, "key"_a, "val"_a)
@@ -868,6 +888,7 @@ PYBIND11_MODULE(_cxxjij, m) {
       .def(py::init<const py::object&>(), "interaction"_a)
       .def(py::init<const CSRSparse&>(), "other"_a)
       .def("get_interactions", &CSRSparse::get_interactions)
+      .def("_flip_stats", &flip_stats<CSRSparse>, "spins"_a, "threshold"_a)
       .def("calc_energy", [](const CSRSparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
       .def("energy", [](const CSRSparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a);
 

@@ -899,6 +899,82 @@ oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t R, const int8_t* spi
   return OJ_OK;
 }
 
+oj_status oj_graph_flip_stats(oj_ctx* ctx, const oj_graph* g, int32_t K, const int8_t* spins, double threshold,
+                              double* dE_quad, double* dE_lin, double* abs_min) {
+  if (!ctx || !g || !abs_min || K < 1 || K > flip_stats_max_k() || (g->n > 0 && (!spins || !dE_quad || !dE_lin)))
+    return arg_fail(ctx, "null argument or K outside 1..8");
+  const int n = g->n;
+  for (size_t q = 0; q < (size_t)n * K; ++q)
+    if (spins[q] != 1 && spins[q] != -1) return arg_fail(ctx, "spins must be +1 or -1");
+  // the corner (n, n) of the augmented matrix is part of the reference's minimum
+  double amin = INFINITY;
+  for (int64_t p = g->aug_indptr[n]; p < g->aug_indptr[n + 1]; ++p)
+    if (g->aug_indices[p] == n && std::fabs(g->aug_data[p]) > threshold) amin = std::fabs(g->aug_data[p]);
+  if (n == 0) {
+    *abs_min = amin;
+    return OJ_OK;
+  }
+  DeviceGuard dg(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const size_t nk = (size_t)n * K;
+  OJ_CK(ctx->aux.ensure(nk), "alloc spins");
+  OJ_CK(ctx->energies.ensure(nk * 16 + 8), "alloc statistics");
+  double* d_quad = ctx->energies.as<double>();
+  double* d_lin = d_quad + nk;
+  unsigned long long* d_min = reinterpret_cast<unsigned long long*>(d_lin + nk);
+  unsigned long long m0;
+  std::memcpy(&m0, &amin, 8);
+  OJ_CK(cudaMemcpyAsync(ctx->aux.ptr, spins, nk, cudaMemcpyHostToDevice, st), "H2D spins");
+  OJ_CK(cudaMemcpyAsync(d_min, &m0, 8, cudaMemcpyHostToDevice, st), "H2D minimum");
+  OJ_CK(launch_flip_stats(g, K, ctx->aux.as<int8_t>(), threshold, d_quad, d_lin, d_min, st), "flip statistics kernel");
+  OJ_CK(cudaMemcpyAsync(dE_quad, d_quad, nk * 8, cudaMemcpyDeviceToHost, st), "D2H quad");
+  OJ_CK(cudaMemcpyAsync(dE_lin, d_lin, nk * 8, cudaMemcpyDeviceToHost, st), "D2H lin");
+  OJ_CK(cudaMemcpyAsync(&m0, d_min, 8, cudaMemcpyDeviceToHost, st), "D2H minimum");
+  OJ_CK(cudaStreamSynchronize(st), "flip statistics");
+  std::memcpy(abs_min, &m0, 8);
+  return OJ_OK;
+}
+
+oj_status oj_batch_flip_stats(oj_ctx* ctx, const oj_batch* b, int32_t K, const int8_t* spins, double threshold,
+                              double* dE_quad, double* dE_lin, double* abs_min) {
+  if (!ctx || !b || K < 1 || K > flip_stats_max_k() || (b->count > 0 && !abs_min))
+    return arg_fail(ctx, "null argument or K outside 1..8");
+  std::vector<int64_t> soff(b->count + 1, 0);
+  for (int k = 0; k < b->count; ++k) soff[k + 1] = soff[k] + b->n[k];
+  const size_t nk = (size_t)soff[b->count] * K;
+  if (nk > 0 && (!spins || !dE_quad || !dE_lin)) return arg_fail(ctx, "null argument");
+  for (size_t q = 0; q < nk; ++q)
+    if (spins[q] != 1 && spins[q] != -1) return arg_fail(ctx, "spins must be +1 or -1");
+  if (b->count == 0) return OJ_OK;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const size_t soff_bytes = (size_t)b->count * 8, spin_at = (soff_bytes + 255) & ~(size_t)255;
+  OJ_CK(ctx->aux.ensure(spin_at + std::max<size_t>(nk, 1)), "alloc spins");
+  OJ_CK(ctx->energies.ensure(nk * 16 + (size_t)b->count * 8), "alloc statistics");
+  double* d_quad = ctx->energies.as<double>();
+  double* d_lin = d_quad + nk;
+  unsigned long long* d_min = reinterpret_cast<unsigned long long*>(d_lin + nk);
+  const double inf = INFINITY;
+  unsigned long long inf_bits;
+  std::memcpy(&inf_bits, &inf, 8);
+  std::vector<unsigned long long> m(b->count, inf_bits);
+  char* aux = ctx->aux.as<char>();
+  OJ_CK(cudaMemcpyAsync(aux, soff.data(), soff_bytes, cudaMemcpyHostToDevice, st), "H2D offsets");
+  if (nk) OJ_CK(cudaMemcpyAsync(aux + spin_at, spins, nk, cudaMemcpyHostToDevice, st), "H2D spins");
+  OJ_CK(cudaMemcpyAsync(d_min, m.data(), m.size() * 8, cudaMemcpyHostToDevice, st), "H2D minima");
+  OJ_CK(launch_batch_flip_stats(b, K, reinterpret_cast<int8_t*>(aux + spin_at), reinterpret_cast<int64_t*>(aux),
+                                threshold, d_quad, d_lin, d_min, st),
+        "batch flip statistics kernel");
+  if (nk) {
+    OJ_CK(cudaMemcpyAsync(dE_quad, d_quad, nk * 8, cudaMemcpyDeviceToHost, st), "D2H quad");
+    OJ_CK(cudaMemcpyAsync(dE_lin, d_lin, nk * 8, cudaMemcpyDeviceToHost, st), "D2H lin");
+  }
+  OJ_CK(cudaMemcpyAsync(m.data(), d_min, m.size() * 8, cudaMemcpyDeviceToHost, st), "D2H minima");
+  OJ_CK(cudaStreamSynchronize(st), "batch flip statistics");
+  std::memcpy(abs_min, m.data(), m.size() * 8);
+  return OJ_OK;
+}
+
 oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset,
                                 const double* J_aug, oj_batch** out) {
   return build_batch(ctx, count, n, offset, J_aug, out);

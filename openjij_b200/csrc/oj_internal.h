@@ -194,6 +194,11 @@ cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const
                                 double* out, cudaStream_t st);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
+int flip_stats_max_k();
+cudaError_t launch_flip_stats(const oj_graph* g, int K, const int8_t* s, double thr, double* quad, double* lin,
+                              unsigned long long* amin, cudaStream_t st);
+cudaError_t launch_batch_flip_stats(const oj_batch* b, int K, const int8_t* s, const int64_t* soff, double thr,
+                                    double* quad, double* lin, unsigned long long* amin, cudaStream_t st);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,
                           cudaStream_t st);
 cudaError_t launch_best_slice(const double* energies, int R, int T, int32_t* best, cudaStream_t st);

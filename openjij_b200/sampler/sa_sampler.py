@@ -131,7 +131,7 @@ class SASampler(BaseSampler):
         extension: the reference samples one model per ``sample`` call).
 
         ``models``: BinaryQuadraticModels (or dimod-like models, or QUBO dicts),
-        each with at most 1024 variables.  All models share one geometric
+        each with at most 4096 variables.  All models share one geometric
         schedule; a missing end of the beta range is estimated per model as in
         ``sample`` and the widest range over the models is used.  Returns one
         Response per model, in order.
@@ -147,13 +147,24 @@ class SASampler(BaseSampler):
             bqms.append(b)
             mats.append(np.ascontiguousarray(graph.get_interactions(), np.float64))
             offsets.append(off)
+        ctx = _batch_context(device)
+        batch = N.Batch(ctx, mats)
         bmin, bmax = self._params["beta_min"], self._params["beta_max"]
         if bmin is None or bmax is None:
-            lo, hi = [], []
-            for b in bqms:
-                graph, _ = b.get_cxxjij_ising_graph()
-                _, (b1, b0) = geometric_ising_beta_schedule(graph, beta_max=bmax, beta_min=bmin, num_sweeps=S,
-                                                            seed=seed)
+            # each model's random configurations as its own sample() call would
+            # draw them, then the statistics of all models in one GPU call
+            draws = []
+            for a in mats:
+                if seed is not None:
+                    np.random.seed(seed)
+                draws.append(_flip_spins(a.shape[0]))
+            quad, lin, amin = batch.flip_stats(np.concatenate(draws) if draws else np.zeros((0, 2), np.int8),
+                                               _THRESHOLD)
+            lo, hi, pos = [], [], 0
+            for k, a in enumerate(mats):
+                nk = a.shape[0] - 1
+                b1, b0 = _beta_range(quad[pos:pos + nk], lin[pos:pos + nk], amin[k], a.shape[0], S, bmin, bmax)
+                pos += nk
                 lo.append(b0)
                 hi.append(b1)
             bmin = min(lo) if bmin is None else bmin
@@ -168,9 +179,8 @@ class SASampler(BaseSampler):
         spins = rng.choice(np.array([-1, 1], np.int8), size=int(R * sum(sizes)))
         reads = np.full(len(mats), R, np.int32)
         energies = np.zeros(R * len(mats))
-        ctx = _batch_context(device)
         t0 = time.perf_counter()
-        st = N.sa_run_batched(N.Batch(ctx, mats), reads, spins, beta_arr, mcs,
+        st = N.sa_run_batched(batch, reads, spins, beta_arr, mcs,
                               seed=(rng.integers(0, 2 ** 63) if seed is None else int(seed)), energies=energies)
         elapsed = time.perf_counter() - t0
         out, off = [], 0
@@ -205,34 +215,59 @@ def geometric_ising_beta_schedule(cxxgraph, beta_max=None, beta_min=None, num_sw
     beta_max, m, num_sweeps // m), m = max(1, num_sweeps // 1000).  A missing
     end is estimated from the energy changes of random spin configurations,
     by the reference's procedure (median / minimum positive dE, bisection for
-    beta_min, the 1/1000 final acceptance target for beta_max).
+    beta_min, the 1/1000 final acceptance target for beta_max).  The energy
+    changes and the smallest coupling magnitude come from the GPU
+    (``_flip_stats``, oj_graph_flip_stats) instead of a dense matrix product and
+    a pass over the whole augmented matrix; the random configurations are the
+    reference's own numpy draws.
     """
     if seed is not None:
         np.random.seed(seed)
-    THRESHOLD = 1e-8
-    dE_max, dE_min, rate_dE = 1.0, 1.0, 0.5
-    J = cxxgraph.get_interactions()
-    dense = isinstance(J, np.ndarray)
+    n = cxxgraph.size() + 1  # rows of the augmented matrix
     if beta_min is None or beta_max is None:
-        if J.shape[0] <= 1:
-            dE_max = dE_min = 1.0
+        spins = _flip_spins(n)
+        quad, lin, int_min = cxxgraph._flip_stats(spins, _THRESHOLD)
+        beta_max, beta_min = _beta_range(quad, lin, int_min, n, num_sweeps, beta_min, beta_max)
+    per_beta = max(1, num_sweeps // 1000)
+    schedule = cxxjij.utility.make_classical_schedule_list(
+        beta_min=float(beta_min), beta_max=float(beta_max), one_mc_step=per_beta,
+        num_call_updater=num_sweeps // per_beta)
+    return schedule, [beta_max, beta_min]
+
+
+_THRESHOLD = 1e-8
+
+
+def _flip_spins(n_aug):
+    """The reference's random configurations: np.random.choice([-1, 1],
+    (n+1, 2)) with the dummy row set to 1, drawn only when n > 0
+    (sa_sampler.py:886-888); returns the n spin rows as int8."""
+    if n_aug <= 1:
+        return np.zeros((0, 2), np.int8)
+    spins = np.random.choice([-1, 1], size=(n_aug, 2))
+    spins[-1, :] = 1
+    return spins[:-1].astype(np.int8)
+
+
+def _beta_range(quad, lin, int_min, n_aug, num_sweeps, beta_min, beta_max):
+    """beta_max, beta_min from the flip statistics (sa_sampler.py:880-965):
+    quad / lin the coupling and field parts of the single-flip energy changes
+    of the random configurations, int_min the smallest |entry| > 1e-8 of the
+    augmented matrix, n_aug = n + 1."""
+    THRESHOLD = _THRESHOLD
+    dE_max, dE_min, rate_dE = 1.0, 1.0, 0.5
+    if n_aug > 1:
+        quad_abs = np.abs(quad)
+        if np.any(quad_abs > THRESHOLD):
+            rate_dE = np.max(np.abs(lin[quad_abs > THRESHOLD]) /
+                             (quad_abs[quad_abs > THRESHOLD].mean() + THRESHOLD))
+        positive = quad[quad > THRESHOLD]
+        if len(positive) == 0:
+            dE_min, dE_max = 1.0, 1.1
         else:
-            spins = np.random.choice([-1, 1], size=(J.shape[0], 2))
-            spins[-1, :] = 1
-            quad = J[:-1, :-1] @ spins[:-1, :] * (-2 * spins[:-1, :])
-            hcol = J[:-1, -1][:, np.newaxis] if dense else J[:-1, -1].toarray()
-            lin = hcol * spins[:-1]
-            quad_abs = np.abs(quad)
-            if np.any(quad_abs > THRESHOLD):
-                rate_dE = np.max(np.abs(lin[quad_abs > THRESHOLD]) /
-                                 (quad_abs[quad_abs > THRESHOLD].mean() + THRESHOLD))
-            positive = quad[quad > THRESHOLD]
-            if len(positive) == 0:
-                dE_min, dE_max = 1.0, 1.1
-            else:
-                dE_max = np.median(positive, axis=0).mean()
-                dE_min = np.min(positive, axis=0).mean()
-    n = J.shape[0]
+            dE_max = np.median(positive, axis=0).mean()
+            dE_min = np.min(positive, axis=0).mean()
+    n = n_aug
     prob_init = 9 / 10 - 8 / 10 * np.tanh(rate_dE / 50) + THRESHOLD
     prob_final = 1 / 1000
     if beta_min is None:
@@ -250,8 +285,9 @@ def geometric_ising_beta_schedule(cxxgraph, beta_max=None, beta_min=None, num_sw
         floor = beta_min * 0.8
         beta_min = floor + (beta_min * 1.5 - floor) * np.tanh(num_sweeps / n)
     if beta_max is None:
-        absJ = np.abs(J) if dense else abs(J).toarray()
-        int_min = max(np.min(absJ[absJ > THRESHOLD]), dE_min / 10.0)
+        if not np.isfinite(int_min):  # np.min of an empty selection in the reference
+            raise ValueError("zero-size array to reduction operation minimum which has no identity")
+        int_min = max(int_min, dE_min / 10.0)
         b_int = -np.log(prob_final) / int_min
         b_dE = -np.log(prob_final) / dE_min
         if rate_dE < 2:
@@ -265,8 +301,4 @@ def geometric_ising_beta_schedule(cxxgraph, beta_max=None, beta_min=None, num_sw
     if rate_dE > 1:
         beta_min *= rate_dE
         beta_max *= rate_dE
-    per_beta = max(1, num_sweeps // 1000)
-    schedule = cxxjij.utility.make_classical_schedule_list(
-        beta_min=float(beta_min), beta_max=float(beta_max), one_mc_step=per_beta,
-        num_call_updater=num_sweeps // per_beta)
-    return schedule, [beta_max, beta_min]
+    return beta_max, beta_min

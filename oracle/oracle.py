@@ -408,3 +408,64 @@ def replay_sw(g: AugCSR, init2d, betas_per_sweep, seed, threads=None):
     b = np.ascontiguousarray(betas_per_sweep, np.float32)
     lib().orc_replay_sw(*g.args(), s.shape[0], s, b, len(b), int(seed), _threads(threads))
     return s
+
+
+def beta_range_reference(J_aug, beta_max=None, beta_min=None, num_sweeps=1000, seed=None):
+    """[beta_max, beta_min] of SASampler's automatic schedule, restated from
+    openjij/sampler/sa_sampler.py:872-965 on the augmented matrix J_aug (dense
+    ndarray or scipy sparse, as graph.get_interactions() returns it): random
+    configurations from np.random, their single-flip energy changes by a
+    matrix product, and the smallest |entry| above 1e-8."""
+    if seed is not None:
+        np.random.seed(seed)
+    THRESHOLD = 1e-8
+    dE_max = dE_min = 1.0
+    rate_dE = 0.5
+    dense = isinstance(J_aug, np.ndarray)
+    if beta_min is None or beta_max is None:
+        if J_aug.shape[0] > 1:
+            s = np.random.choice([-1, 1], size=(J_aug.shape[0], 2))
+            s[-1, :] = 1
+            quad = np.asarray(J_aug[:-1, :-1] @ s[:-1, :]) * (-2 * s[:-1, :])
+            hcol = J_aug[:-1, -1][:, np.newaxis] if dense else J_aug[:-1, -1].toarray()
+            lin = hcol * s[:-1]
+            qa = np.abs(quad)
+            if np.any(qa > THRESHOLD):
+                rate_dE = np.max(np.abs(lin[qa > THRESHOLD]) / (qa[qa > THRESHOLD].mean() + THRESHOLD))
+            pos = quad[quad > THRESHOLD]
+            if len(pos) == 0:
+                dE_min, dE_max = 1.0, 1.1
+            else:
+                dE_max = np.median(pos, axis=0).mean()
+                dE_min = np.min(pos, axis=0).mean()
+    n = J_aug.shape[0]
+    prob_init = 9 / 10 - 8 / 10 * np.tanh(rate_dE / 50) + THRESHOLD
+    prob_final = 1 / 1000
+    if beta_min is None:
+        lo, hi = -np.log(prob_init) / dE_max, -np.log(prob_init) / dE_min
+        for _ in range(5):
+            b = (lo + hi) / 2
+            f = 2 * b * prob_init - np.exp(-b * dE_min) + np.exp(-b * dE_max)
+            if abs(f) < 1e-8:
+                break
+            if f > 0:
+                hi = b
+            else:
+                lo = b
+        beta_min = lo * 0.8 + (lo * 1.5 - lo * 0.8) * np.tanh(num_sweeps / n)
+    if beta_max is None:
+        vals = np.abs(J_aug).ravel() if dense else np.abs(sp.csr_matrix(J_aug).data)
+        int_min = max(np.min(vals[vals > THRESHOLD]), dE_min / 10.0)
+        b_int = -np.log(prob_final) / int_min
+        b_dE = -np.log(prob_final) / dE_min
+        if rate_dE < 2:
+            lo, hi = min(b_dE, b_int), max(b_dE, b_int)
+            beta_max = lo + (hi - lo) * np.tanh(num_sweeps / (2 * n))
+        else:
+            beta_max = -np.log(prob_final) / max(dE_min, int_min) / min(100, num_sweeps // 10 + 1)
+        if beta_max < beta_min:
+            beta_max = beta_min * 10.0
+    if rate_dE > 1:
+        beta_min *= rate_dE
+        beta_max *= rate_dE
+    return [beta_max, beta_min]
