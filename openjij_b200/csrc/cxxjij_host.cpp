@@ -6,6 +6,8 @@
 // Reference bindings mirrored here (names, arguments, errors):
 //   openjij/declare.hpp:43-129   Graph, Dense          openjij/main.cpp:43-47
 //   openjij/declare.hpp:195-217  CSRSparse
+//   openjij/declare.hpp:131-193  Sparse               openjij/main.cpp:44
+//   openjij/declare.hpp:273-405  Dir, Square, ChimeraDir, Chimera (main.cpp:40-48)
 //   openjij/declare.hpp:409-438  ClassicalIsing        openjij/main.cpp:68-73
 //   openjij/declare.hpp:585-641  TransverseIsing       openjij/main.cpp:80-85
 //   openjij/declare.hpp:687-793  Algorithm_SingleSpinFlip_run (4 overloads),
@@ -19,6 +21,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -28,7 +31,9 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <type_traits>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -310,6 +315,212 @@ struct CSRSparse : Graph {
   }
   AugCSR a_;
   mutable std::shared_ptr<DeviceGraph> dev_;
+};
+
+// graph::Sparse (include/openjij/graph/sparse.hpp:32-250): couplings in a hash
+// map keyed by (min(i,j), max(i,j)), the field of i under (i, i), and for every
+// site the list of its neighbours (itself when it has a field).  A list holds
+// at most num_edges sites; a site whose list is full gains no new neighbour
+// (the coupling is stored but not seen by the dynamics), as in the reference's
+// release build.  The dynamics read the augmented matrix built from the lists
+// (utility/eigen.hpp:163-193): M[i][j] = J(i,j) for every listed neighbour
+// j != i, M[i][n] = M[n][i] = h(i) when i lists itself, M[n][n] = 1.
+struct Sparse : Graph {
+  Sparse(size_t n, size_t num_edges) : Graph(n), num_edges_(std::min(n, num_edges)), adj_(n) {}
+  explicit Sparse(size_t n) : Sparse(n, n) {}
+  struct KeyHash {
+    size_t operator()(const std::pair<size_t, size_t>& k) const {
+      return std::hash<uint64_t>()(((uint64_t)k.first << 32) ^ (uint64_t)k.second);
+    }
+  };
+  void check_index(size_t i) const {
+    if (i >= n_) throw std::out_of_range("index " + std::to_string(i) + " out of range");
+  }
+  void link(size_t a, size_t b) {
+    auto& l = adj_[a];
+    if (std::find(l.begin(), l.end(), b) != l.end() || l.size() >= num_edges_) return;
+    l.push_back(b);
+    link(b, a);
+  }
+  double& J(size_t i, size_t j) {
+    check_index(i);
+    check_index(j);
+    link(i, j);
+    dev_.reset();
+    return J_[{std::min(i, j), std::max(i, j)}];
+  }
+  double J(size_t i, size_t j) const {
+    check_index(i);
+    check_index(j);
+    auto it = J_.find({std::min(i, j), std::max(i, j)});
+    if (it == J_.end()) throw std::out_of_range("no interaction between " + std::to_string(i) + " and " + std::to_string(j));
+    return it->second;
+  }
+  double& h(size_t i) { return J(i, i); }
+  double h(size_t i) const { return J(i, i); }
+  const std::vector<size_t>& adj_nodes(size_t i) const {
+    check_index(i);
+    return adj_[i];
+  }
+  size_t get_num_edges() const { return num_edges_; }
+  AugCSR aug() const {
+    std::vector<std::vector<std::pair<int32_t, double>>> rows(n_ + 1);
+    for (size_t i = 0; i < n_; ++i)
+      for (size_t j : adj_[i]) {
+        if (j != i) {
+          rows[i].emplace_back((int32_t)j, J(i, j));
+        } else {
+          rows[i].emplace_back((int32_t)n_, h(i));
+          rows[n_].emplace_back((int32_t)i, h(i));
+        }
+      }
+    rows[n_].emplace_back((int32_t)n_, 1.0);
+    AugCSR a;
+    a.n = n_;
+    a.indptr.push_back(0);
+    for (auto& r : rows) {
+      std::sort(r.begin(), r.end());
+      for (size_t q = 0; q < r.size(); ++q) {
+        if (q + 1 < r.size() && r[q + 1].first == r[q].first) {  // setFromTriplets sums duplicates
+          r[q + 1].second += r[q].second;
+          continue;
+        }
+        a.indices.push_back(r[q].first);
+        a.data.push_back(r[q].second);
+      }
+      a.indptr.push_back((int64_t)a.indices.size());
+    }
+    return a;
+  }
+  py::object get_interactions() const {
+    const AugCSR a = aug();
+    py::module_ sp = py::module_::import("scipy.sparse");
+    py::array_t<double> d(a.data.size());
+    py::array_t<int32_t> ix(a.indices.size());
+    py::array_t<int64_t> ip(a.indptr.size());
+    std::copy(a.data.begin(), a.data.end(), d.mutable_data());
+    std::copy(a.indices.begin(), a.indices.end(), ix.mutable_data());
+    std::copy(a.indptr.begin(), a.indptr.end(), ip.mutable_data());
+    return sp.attr("csr_matrix")(py::make_tuple(d, ix, ip), "shape"_a = py::make_tuple(n_ + 1, n_ + 1));
+  }
+  double energy(const std::vector<int>& s) const { return aug_energy(aug(), s); }
+  oj_graph* device() const {
+    if (!dev_) {
+      const AugCSR a = aug();
+      auto d = std::make_shared<DeviceGraph>();
+      check(oj_graph_create_csr(ctx(), (int32_t)n_, a.indptr.data(), a.indices.data(), a.data.data(), &d->h),
+            "oj_graph_create_csr");
+      dev_ = d;
+    }
+    return dev_->h;
+  }
+  size_t num_edges_;
+  std::vector<std::vector<size_t>> adj_;
+  std::unordered_map<std::pair<size_t, size_t>, double, KeyHash> J_;
+  mutable std::shared_ptr<DeviceGraph> dev_;
+};
+
+// graph::Square (include/openjij/graph/square.hpp:33-387): a rows x cols grid,
+// site (r, c) = cols * r + c; built with the open-boundary bonds and a field
+// per site, all set to init_val; a bond given by direction wraps around the
+// edges (row -1 is row rows-1 and so on).
+enum class Dir { PLUS_R, MINUS_R, PLUS_C, MINUS_C };
+
+struct Square : Sparse {
+  Square(size_t rows, size_t cols, double init_val)
+      : Sparse(checked(rows, cols) * cols, 4 + 1), rows_(rows), cols_(cols) {
+    for (size_t r = 0; r < rows; ++r)
+      for (size_t c = 0; c < cols; ++c) {
+        const size_t i = to_ind((int64_t)r, (int64_t)c);
+        if (r > 0) Sparse::J(i, to_ind((int64_t)r - 1, (int64_t)c)) = init_val;
+        if (c > 0) Sparse::J(i, to_ind((int64_t)r, (int64_t)c - 1)) = init_val;
+        if (r + 1 < rows) Sparse::J(i, to_ind((int64_t)r + 1, (int64_t)c)) = init_val;
+        if (c + 1 < cols) Sparse::J(i, to_ind((int64_t)r, (int64_t)c + 1)) = init_val;
+        Sparse::J(i, i) = init_val;
+      }
+  }
+  static size_t checked(size_t rows, size_t cols) {
+    if (rows < 1 || cols < 1) throw std::invalid_argument("num_row and num_column must be at least 1");
+    return rows;
+  }
+  size_t to_ind(int64_t r, int64_t c) const {
+    if (!(-1 <= r && r <= (int64_t)rows_)) throw std::runtime_error("invalid value r=" + std::to_string(r) + " inserted in Square");
+    if (!(-1 <= c && c <= (int64_t)cols_)) throw std::runtime_error("invalid value c=" + std::to_string(c) + " inserted in Square");
+    return cols_ * (size_t)((r + (int64_t)rows_) % (int64_t)rows_) + (size_t)((c + (int64_t)cols_) % (int64_t)cols_);
+  }
+  std::pair<size_t, size_t> to_rc(size_t ind) const {
+    if (ind >= n_) throw std::runtime_error("invalid value index=" + std::to_string(ind) + " inserted in Square");
+    return {ind / cols_, ind % cols_};
+  }
+  size_t neighbour(size_t r, size_t c, Dir d) const {
+    if (r >= rows_ || c >= cols_) throw std::out_of_range("(r, c) out of range");
+    const int64_t R = (int64_t)r, C = (int64_t)c;
+    switch (d) {
+      case Dir::MINUS_R: return to_ind(R - 1, C);
+      case Dir::MINUS_C: return to_ind(R, C - 1);
+      case Dir::PLUS_R: return to_ind(R + 1, C);
+      default: return to_ind(R, C + 1);
+    }
+  }
+  size_t rows_, cols_;
+};
+
+// graph::Chimera (include/openjij/graph/chimera.hpp:36-513): rows x cols unit
+// cells of 8 sites, site (r, c, i) = 8 cols r + 8 c + i.  Sites 0-3 of a cell
+// couple to 4-7 of the same cell (IN_*) and to the same i in the cells above
+// and below (R directions); sites 4-7 to the same i left and right (C
+// directions).  Built with every bond and field set to init_val, open edges;
+// a bond given by direction wraps around.
+enum class ChimeraDir { PLUS_R, MINUS_R, PLUS_C, MINUS_C, IN_0or4, IN_1or5, IN_2or6, IN_3or7 };
+
+struct Chimera : Sparse {
+  static constexpr size_t kCell = 8;
+  Chimera(size_t rows, size_t cols, double init_val)
+      : Sparse(Square::checked(rows, cols) * cols * kCell, 6 + 1), rows_(rows), cols_(cols) {
+    for (size_t r = 0; r < rows; ++r)
+      for (size_t c = 0; c < cols; ++c)
+        for (size_t i = 0; i < kCell; ++i) {
+          const int64_t R = (int64_t)r, C = (int64_t)c, I = (int64_t)i;
+          const size_t x = to_ind(R, C, I);
+          if (r > 0 && i < 4) Sparse::J(x, to_ind(R - 1, C, I)) = init_val;
+          if (c > 0 && i >= 4) Sparse::J(x, to_ind(R, C - 1, I)) = init_val;
+          if (r + 1 < rows && i < 4) Sparse::J(x, to_ind(R + 1, C, I)) = init_val;
+          if (c + 1 < cols && i >= 4) Sparse::J(x, to_ind(R, C + 1, I)) = init_val;
+          for (int64_t k = 0; k < 4; ++k) Sparse::J(x, to_ind(R, C, (i < 4 ? 4 : 0) + k)) = init_val;
+          Sparse::J(x, x) = init_val;
+        }
+  }
+  size_t to_ind(int64_t r, int64_t c, int64_t i) const {
+    if (!(-1 <= r && r <= (int64_t)rows_)) throw std::runtime_error("invalid value r=" + std::to_string(r) + " inserted in Chimera");
+    if (!(-1 <= c && c <= (int64_t)cols_)) throw std::runtime_error("invalid value c=" + std::to_string(c) + " inserted in Chimera");
+    if (!(0 <= i && i < (int64_t)kCell)) throw std::runtime_error("invalid value i=" + std::to_string(i) + " inserted in Chimera");
+    return cols_ * kCell * (size_t)((r + (int64_t)rows_) % (int64_t)rows_) +
+           kCell * (size_t)((c + (int64_t)cols_) % (int64_t)cols_) + (size_t)i;
+  }
+  std::tuple<size_t, size_t, size_t> to_rci(size_t ind) const {
+    if (ind >= n_) throw std::runtime_error("invalid value index=" + std::to_string(ind) + " inserted in Chimera");
+    return std::make_tuple(ind / (cols_ * kCell), (ind % (cols_ * kCell)) / kCell, ind % kCell);
+  }
+  size_t neighbour(size_t r, size_t c, size_t i, ChimeraDir d) const {
+    if (r >= rows_ || c >= cols_ || i >= kCell) throw std::out_of_range("(r, c, i) out of range");
+    const int64_t R = (int64_t)r, C = (int64_t)c, I = (int64_t)i;
+    const int64_t other = i < 4 ? 4 : 0;
+    switch (d) {
+      case ChimeraDir::MINUS_R:
+      case ChimeraDir::PLUS_R:
+        if (i >= 4) throw std::invalid_argument("R directions couple sites 0-3 of a cell");
+        return to_ind(d == ChimeraDir::PLUS_R ? R + 1 : R - 1, C, I);
+      case ChimeraDir::MINUS_C:
+      case ChimeraDir::PLUS_C:
+        if (i < 4) throw std::invalid_argument("C directions couple sites 4-7 of a cell");
+        return to_ind(R, d == ChimeraDir::PLUS_C ? C + 1 : C - 1, I);
+      case ChimeraDir::IN_0or4: return to_ind(R, C, other + 0);
+      case ChimeraDir::IN_1or5: return to_ind(R, C, other + 1);
+      case ChimeraDir::IN_2or6: return to_ind(R, C, other + 2);
+      default: return to_ind(R, C, other + 3);
+    }
+  }
+  size_t rows_, cols_;
 };
 
 // Single-flip energy changes of the configurations spins[n][K] and the smallest
@@ -841,7 +1052,7 @@ void bind_graph_systems(py::module_& msys, py::module_& malg, py::module_& mres,
   mres.def("get_solution", [](const CI& s) { return solution(s); }, "system"_a);
   mres.def("get_solution", [](const TI& s) { return solution(s); }, "system"_a);
   // Swendsen-Wang: sparse systems only, as the reference (openjij/main.cpp:144-154)
-  if (std::is_same<G, CSRSparse>::value) {
+  if (std::is_same<G, CSRSparse>::value || std::is_same<G, Sparse>::value) {
     const char* sw = "Algorithm_SwendsenWang_run";
     malg.def(
         sw, [](CI& s, uint64_t seed, const py::list& sched, const CCb& cb) { run_swendsen_wang(s, seed, classical_from_list(sched), cb); },
@@ -891,6 +1102,91 @@ PYBIND11_MODULE(_cxxjij, m) {
       .def("_flip_stats", &flip_stats<CSRSparse>, "spins"_a, "threshold"_a)
       .def("calc_energy", [](const CSRSparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
       .def("energy", [](const CSRSparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a);
+
+  py::class_<Sparse, Graph, std::shared_ptr<Sparse>>(mg, "Sparse", py::module_local())
+      .def(py::init<size_t, size_t>(), "num_spins"_a, "num_edges"_a)
+      .def(py::init<size_t>(), "num_spins"_a)
+      .def(py::init<const Sparse&>(), "other"_a)
+      .def("adj_nodes", &Sparse::adj_nodes, "ind"_a)
+      .def("get_num_edges", &Sparse::get_num_edges)
+      .def("get_interactions", &Sparse::get_interactions)
+      .def("_flip_stats", &flip_stats<Sparse>, "spins"_a, "threshold"_a)
+      .def("calc_energy", [](const Sparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
+      .def("energy", [](const Sparse& g, const std::vector<int>& s) { return g.energy(s); }, "spins"_a)
+      .def("__setitem__", [](Sparse& g, std::pair<size_t, size_t> k, double v) { g.J(k.first, k.second) = v; }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Sparse& g, std::pair<size_t, size_t> k) { return g.J(k.first, k.second); }, "key"_a)
+      .def("__setitem__", [](Sparse& g, size_t k, double v) { g.h(k) = v; }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Sparse& g, size_t k) { return g.h(k); }, "key"_a);
+
+  py::enum_<Dir>(mg, "Dir", py::module_local())
+      .value("PLUS_R", Dir::PLUS_R)
+      .value("MINUS_R", Dir::MINUS_R)
+      .value("PLUS_C", Dir::PLUS_C)
+      .value("MINUS_C", Dir::MINUS_C);
+  using SqKey = std::tuple<size_t, size_t, Dir>;
+  py::class_<Square, Sparse, std::shared_ptr<Square>>(mg, "Square", py::module_local())
+      .def(py::init<size_t, size_t, double>(), "num_row"_a, "num_column"_a, "init_val"_a = 0.0)
+      .def(py::init<const Square&>(), "other"_a)
+      .def("to_ind", &Square::to_ind, "r"_a, "c"_a)
+      .def("to_rc", &Square::to_rc, "ind"_a)
+      .def("get_num_row", [](const Square& g) { return g.rows_; })
+      .def("get_num_column", [](const Square& g) { return g.cols_; })
+      .def("__setitem__", [](Square& g, const SqKey& k, double v) {
+             const size_t r = std::get<0>(k), c = std::get<1>(k);
+             const size_t j = g.neighbour(r, c, std::get<2>(k));
+             g.J(g.to_ind((int64_t)r, (int64_t)c), j) = v;
+           }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Square& g, const SqKey& k) {
+             const size_t r = std::get<0>(k), c = std::get<1>(k);
+             const size_t j = g.neighbour(r, c, std::get<2>(k));
+             return g.J(g.to_ind((int64_t)r, (int64_t)c), j);
+           }, "key"_a)
+      .def("__setitem__", [](Square& g, std::pair<size_t, size_t> k, double v) {
+             g.neighbour(k.first, k.second, Dir::PLUS_R);  // range check
+             g.h(g.to_ind((int64_t)k.first, (int64_t)k.second)) = v;
+           }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Square& g, std::pair<size_t, size_t> k) {
+             g.neighbour(k.first, k.second, Dir::PLUS_R);
+             return g.h(g.to_ind((int64_t)k.first, (int64_t)k.second));
+           }, "key"_a);
+
+  py::enum_<ChimeraDir>(mg, "ChimeraDir", py::module_local())
+      .value("PLUS_R", ChimeraDir::PLUS_R)
+      .value("MINUS_R", ChimeraDir::MINUS_R)
+      .value("PLUS_C", ChimeraDir::PLUS_C)
+      .value("MINUS_C", ChimeraDir::MINUS_C)
+      .value("IN_0or4", ChimeraDir::IN_0or4)
+      .value("IN_1or5", ChimeraDir::IN_1or5)
+      .value("IN_2or6", ChimeraDir::IN_2or6)
+      .value("IN_3or7", ChimeraDir::IN_3or7);
+  using ChKey = std::tuple<size_t, size_t, size_t, ChimeraDir>;
+  using ChSite = std::tuple<size_t, size_t, size_t>;
+  py::class_<Chimera, Sparse, std::shared_ptr<Chimera>>(mg, "Chimera", py::module_local())
+      .def(py::init<size_t, size_t, double>(), "num_row"_a, "num_column"_a, "init_val"_a = 0.0)
+      .def(py::init<const Chimera&>(), "other"_a)
+      .def("to_ind", &Chimera::to_ind, "r"_a, "c"_a, "i"_a)
+      .def("to_rci", &Chimera::to_rci, "ind"_a)
+      .def("get_num_row", [](const Chimera& g) { return g.rows_; })
+      .def("get_num_column", [](const Chimera& g) { return g.cols_; })
+      .def("get_num_in_chimera", [](const Chimera&) { return Chimera::kCell; })
+      .def("__setitem__", [](Chimera& g, const ChKey& k, double v) {
+             const size_t r = std::get<0>(k), c = std::get<1>(k), i = std::get<2>(k);
+             const size_t j = g.neighbour(r, c, i, std::get<3>(k));
+             g.J(g.to_ind((int64_t)r, (int64_t)c, (int64_t)i), j) = v;
+           }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Chimera& g, const ChKey& k) {
+             const size_t r = std::get<0>(k), c = std::get<1>(k), i = std::get<2>(k);
+             const size_t j = g.neighbour(r, c, i, std::get<3>(k));
+             return g.J(g.to_ind((int64_t)r, (int64_t)c, (int64_t)i), j);
+           }, "key"_a)
+      .def("__setitem__", [](Chimera& g, const ChSite& k, double v) {
+             g.neighbour(std::get<0>(k), std::get<1>(k), std::get<2>(k), ChimeraDir::IN_0or4);  // range check
+             g.h(g.to_ind((int64_t)std::get<0>(k), (int64_t)std::get<1>(k), (int64_t)std::get<2>(k))) = v;
+           }, "key"_a, "val"_a)
+      .def("__getitem__", [](const Chimera& g, const ChSite& k) {
+             g.neighbour(std::get<0>(k), std::get<1>(k), std::get<2>(k), ChimeraDir::IN_0or4);
+             return g.h(g.to_ind((int64_t)std::get<0>(k), (int64_t)std::get<1>(k), (int64_t)std::get<2>(k)));
+           }, "key"_a);
 
   // ---- utility
   py::class_<ClassicalParam>(mu, "ClassicalUpdaterParameter", py::module_local())
@@ -948,6 +1244,7 @@ PYBIND11_MODULE(_cxxjij, m) {
   // ---- systems, algorithm, result
   bind_graph_systems<Dense>(ms, ma, mr, "_Dense");
   bind_graph_systems<CSRSparse>(ms, ma, mr, "_CSRSparse");
+  bind_graph_systems<Sparse>(ms, ma, mr, "_Sparse");  // Square and Chimera are Sparse graphs
 
   // ---- runtime controls (no reference counterpart)
   m.def(

@@ -85,11 +85,11 @@ class BinaryQuadraticModel:
 
     # ---- constructors ------------------------------------------------------
     @classmethod
-    def from_ising(cls, h: dict, J: dict, offset: float = 0.0, sparse: bool = False):
-        return cls(h, J, offset, SPIN, sparse=sparse)
+    def from_ising(cls, h: dict, J: dict, offset: float = 0.0, **kwargs):
+        return cls(h, J, offset, vartype=SPIN, **kwargs)
 
     @classmethod
-    def from_qubo(cls, Q: dict, offset: float = 0.0, sparse: bool = False):
+    def from_qubo(cls, Q: dict, offset: float = 0.0, **kwargs):
         linear, quad = {}, {}
         for (u, v), b in Q.items():
             if u == v:
@@ -98,7 +98,7 @@ class BinaryQuadraticModel:
                 quad[(u, v)] = quad.get((u, v), 0.0) + b
                 linear.setdefault(u, 0.0)
                 linear.setdefault(v, 0.0)
-        return cls(linear, quad, offset, BINARY, sparse=sparse)
+        return cls(linear, quad, offset, vartype=BINARY, **kwargs)
 
     @classmethod
     def from_numpy_matrix(cls, mat, variables=None, offset: float = 0.0, vartype="BINARY",

@@ -19,7 +19,7 @@ import numpy as np
 import openjij_b200.cxxjij as cxxjij
 from openjij_b200.model.model import BinaryQuadraticModel
 from openjij_b200.sampler.response import Response
-from openjij_b200.sampler.sampler import BaseSampler, _as_bqm, spins_from_initial_state
+from openjij_b200.sampler.sampler import BaseSampler, _as_bqm, _ising_graph, _place, spins_from_initial_state
 from openjij_b200.variable_type import BINARY
 
 
@@ -90,7 +90,7 @@ class SASampler(BaseSampler):
         if name == "swendsenwang":  # runs on sparse graphs only (sa_sampler.py:195-197)
             sparse = True
         model = _as_bqm(bqm, bool(sparse))
-        ising_graph, offset = model.get_cxxjij_ising_graph()
+        ising_graph, offset, sites = _ising_graph(model)
         self._set_params(beta_min=beta_min, beta_max=beta_max, num_sweeps=num_sweeps,
                          num_reads=num_reads, schedule=schedule)
         if self._params["schedule"] is None:
@@ -111,7 +111,7 @@ class SASampler(BaseSampler):
                 rng = np.random.default_rng()
                 return rng.choice(np.array([-1, 1], np.int8), size=(R, n))
         else:
-            s0 = spins_from_initial_state(initial_state, model, n)
+            s0 = _place(spins_from_initial_state(initial_state, model, len(model.variables)), sites, n)
 
             def init_generator(R):
                 return np.tile(s0, (R, 1))
@@ -119,7 +119,7 @@ class SASampler(BaseSampler):
         algorithm = self._algorithm[name]
         system = self._make_system[name](init_generator(1), ising_graph) if n > 0 else None
         response = self._cxxjij_sampling(model, init_generator, algorithm, system, reinitialize_state,
-                                         seed, offset)
+                                         seed, offset, sites)
         response.info["schedule"] = self.schedule_info
         return response
 

@@ -42,6 +42,31 @@ def _as_bqm(bqm, sparse):
                                 str(getattr(bqm.vartype, "name", bqm.vartype)), sparse=sparse)
 
 
+def _ising_graph(model):
+    """(cxxjij graph, Ising offset, sites) of a model.  A lattice model
+    (ChimeraModel) returns its full lattice graph alone; ``sites`` then gives
+    the lattice index of each of its variables, in variable order (None when
+    graph and variables coincide)."""
+    out = model.get_cxxjij_ising_graph()
+    if isinstance(out, tuple):
+        graph, offset = out
+    else:
+        graph, offset = out, model.to_ising()[2]
+    sites = None
+    if hasattr(model, "graph_sites") and graph.size() != len(model.variables):
+        sites = np.asarray(model.graph_sites(), np.int64)
+    return graph, offset, sites
+
+
+def _place(s0, sites, n):
+    """A state over the model's variables placed on the n lattice sites (+1 elsewhere)."""
+    if sites is None:
+        return s0
+    full = np.ones(n, np.int8)
+    full[sites] = s0
+    return full
+
+
 class BaseSampler:
     """Parameter handling and the batched read loop shared by SA and SQA."""
 
@@ -55,7 +80,7 @@ class BaseSampler:
             self._params[key] = self._default_params[key] if value is None else value
 
     def _cxxjij_sampling(self, model, init_generator, algorithm, system, reinitialize_state=True,
-                         seed=None, offset=0.0):
+                         seed=None, offset=0.0, sites=None):
         """Anneals ``num_reads`` replicas of ``system`` and builds the Response.
 
         ``init_generator(R)`` returns an [R][n] (SA) or [R][T][n] (SQA) array.
@@ -80,13 +105,13 @@ class BaseSampler:
             system.reset_spins(init_generator(num_reads))
             dt = measure_time(run)(system)
             exec_times = [dt / num_reads] * num_reads
-            states, energies, sys_info = self._get_result(system, model)
+            states, energies, sys_info = self._get_result(system, model, sites)
             energies = energies + offset
         else:
             rows, ens, infos = [], [], []
             for _ in range(num_reads):
                 exec_times.append(measure_time(run)(system))
-                st, en, inf = self._get_result(system, model)
+                st, en, inf = self._get_result(system, model, sites)
                 rows.append(st[0])
                 ens.append(en[0])
                 infos.append(inf)
@@ -106,11 +131,12 @@ class BaseSampler:
         response.info["run"] = cxxjij.last_run_info()
         return response
 
-    def _get_result(self, system, model):
+    def _get_result(self, system, model, sites=None):
         """(spins [R][n] in +-1, Ising energies [R], extra info)."""
         sol = np.asarray(cxxjij.result.get_solution(system), dtype=np.int8)
         energies = np.asarray(system.energies(), dtype=np.float64).reshape(-1)
-        return sol.reshape(-1, len(model.variables)), energies, {}
+        sol = sol.reshape(len(energies), -1)
+        return (sol if sites is None else sol[:, sites]), energies, {}
 
     # ---- dimod-style entry points (sampler.py:166-248) ---------------------
     def sample(self, bqm, **parameters):  # overridden by the samplers

@@ -13,7 +13,7 @@ from typing import Optional, Union
 import numpy as np
 
 import openjij_b200.cxxjij as cxxjij
-from openjij_b200.sampler.sampler import BaseSampler, _as_bqm, spins_from_initial_state
+from openjij_b200.sampler.sampler import BaseSampler, _as_bqm, _ising_graph, _place, spins_from_initial_state
 
 
 class SQASampler(BaseSampler):
@@ -67,13 +67,15 @@ class SQASampler(BaseSampler):
                          "step_length : int) or (annealing parameter s : float, beta: float, "
                          "step_length : int)")
 
-    def _get_result(self, system, model):
+    def _get_result(self, system, model, sites=None):
         e = np.asarray(system.energies(), dtype=np.float64)  # [R][T] classical energies
         R, T = e.shape
         best = np.argmin(e, axis=1)  # first slice of minimum energy
         tr = np.asarray(system.trotter_spins)
         tr = tr.reshape(R, tr.shape[-2], tr.shape[-1])[:, :-1, :]  # [R][n][T], dummy row dropped
         q_state = np.transpose(tr, (0, 2, 1)).astype(np.int8)  # [R][T][n]
+        if sites is not None:
+            q_state = np.ascontiguousarray(q_state[:, :, sites])
         states = q_state[np.arange(R), best]
         info = {"trotter_state": q_state, "trotter_energies": e}
         return states, e[np.arange(R), best], info
@@ -103,7 +105,7 @@ class SQASampler(BaseSampler):
         if name not in self._algorithm:
             raise ValueError('updater is one of "single spin flip"')
         model = _as_bqm(bqm, bool(sparse))
-        ising_graph, offset = model.get_cxxjij_ising_graph()
+        ising_graph, offset, sites = _ising_graph(model)
         self._set_params(beta=beta, gamma=gamma, num_sweeps=num_sweeps, num_reads=num_reads,
                          trotter=trotter, schedule=schedule)
         p = self._params
@@ -123,7 +125,7 @@ class SQASampler(BaseSampler):
                 rng = np.random.default_rng()
                 return rng.choice(np.array([-1, 1], np.int8), size=(R, T, n))
         else:
-            s0 = spins_from_initial_state(initial_state, model, n)
+            s0 = _place(spins_from_initial_state(initial_state, model, len(model.variables)), sites, n)
 
             def init_generator(R):
                 return np.ascontiguousarray(np.broadcast_to(s0, (R, T, n)))
@@ -131,7 +133,7 @@ class SQASampler(BaseSampler):
         system = (self._make_system[name](init_generator(1), ising_graph, float(p["gamma"]))
                   if n > 0 else None)
         response = self._cxxjij_sampling(model, init_generator, self._algorithm[name], system,
-                                         reinitialize_state, seed, offset)
+                                         reinitialize_state, seed, offset, sites)
         response.info["schedule"] = self.schedule_info
         return response
 
