@@ -997,6 +997,14 @@ py::object solution(const TransverseIsing<G>& sys) {
   return out;
 }
 
+// The replicas' spins as an int8 array of the given shape (a copy), for the
+// sampler layer: no per-spin Python objects.
+py::array_t<int8_t> int8_view(const std::vector<int8_t>& v, std::vector<ssize_t> shape) {
+  py::array_t<int8_t> out(shape);
+  std::copy(v.begin(), v.end(), out.mutable_data());
+  return out;
+}
+
 template <class G>
 void bind_graph_systems(py::module_& msys, py::module_& malg, py::module_& mres, const std::string& suffix) {
   using CI = ClassicalIsing<G>;
@@ -1008,7 +1016,8 @@ void bind_graph_systems(py::module_& msys, py::module_& malg, py::module_& mres,
       .def_property_readonly("interaction", [](const CI& s) { return s.graph->get_interactions(); })
       .def_readonly("num_spins", &CI::num_spins)
       .def_readonly("num_replicas", &CI::R)
-      .def("energies", &CI::energies);
+      .def("energies", &CI::energies)
+      .def("_spins_int8", [](const CI& s) { return int8_view(s.spins, {s.R, (ssize_t)s.num_spins}); });
   msys.def(
       "make_classical_ising", [](const py::object& init, const G& g) { return CI(init, g); }, "init_spin"_a,
       "init_interaction"_a);
@@ -1024,7 +1033,10 @@ void bind_graph_systems(py::module_& msys, py::module_& malg, py::module_& mres,
       .def_readonly("num_replicas", &TI::R)
       .def_readonly("num_trotter_slices", &TI::T)
       .def_readwrite("gamma", &TI::gamma)
-      .def("energies", &TI::energies);
+      .def("energies", &TI::energies)
+      .def("_spins_int8", [](const TI& s) {
+        return int8_view(s.spins, {s.R, s.T, (ssize_t)s.num_classical_spins});
+      });
   msys.def(
       "make_transverse_ising", [](const py::object& tr, const G& g, double gamma) { return TI(tr, g, gamma); },
       "init_trotter_spins"_a, "init_interaction"_a, "gamma"_a);

@@ -133,9 +133,8 @@ class BaseSampler:
 
     def _get_result(self, system, model, sites=None):
         """(spins [R][n] in +-1, Ising energies [R], extra info)."""
-        sol = np.asarray(cxxjij.result.get_solution(system), dtype=np.int8)
+        sol = system._spins_int8()  # get_solution of a classical system: the spins (dummy spin +1)
         energies = np.asarray(system.energies(), dtype=np.float64).reshape(-1)
-        sol = sol.reshape(len(energies), -1)
         return (sol if sites is None else sol[:, sites]), energies, {}
 
     # ---- dimod-style entry points (sampler.py:166-248) ---------------------

@@ -71,9 +71,7 @@ class SQASampler(BaseSampler):
         e = np.asarray(system.energies(), dtype=np.float64)  # [R][T] classical energies
         R, T = e.shape
         best = np.argmin(e, axis=1)  # first slice of minimum energy
-        tr = np.asarray(system.trotter_spins)
-        tr = tr.reshape(R, tr.shape[-2], tr.shape[-1])[:, :-1, :]  # [R][n][T], dummy row dropped
-        q_state = np.transpose(tr, (0, 2, 1)).astype(np.int8)  # [R][T][n]
+        q_state = system._spins_int8()  # [R][T][n]
         if sites is not None:
             q_state = np.ascontiguousarray(q_state[:, :, sites])
         states = q_state[np.arange(R), best]
