@@ -140,7 +140,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t
  * 1 - exp(-2 beta |J|) and every cluster not holding the dummy flips with
  * probability 1/2.  Arguments, schedule, counters and energies as oj_sa_run;
  * flags: OJ_DEVICE_POINTERS only.  One CTA per replica holds the union-find
- * forest in shared memory: n <= 45000. */
+ * forest in shared memory (n <= 45000) or, for larger graphs, in global
+ * scratch of at most 1 GiB (replicas in chunks). */
 oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
                     const double* betas, const int32_t* mcs, int32_t num_sched, uint64_t seed,
                     int64_t first_sweep, int64_t replica_offset, uint32_t flags, double* energies,

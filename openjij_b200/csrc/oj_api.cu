@@ -1239,10 +1239,6 @@ oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     ctx->last_error = "Swendsen-Wang has a single kernel; pass OJ_KERNEL_AUTO";
     return OJ_ERR_UNSUPPORTED;
   }
-  if (n > sw_max_sites()) {
-    ctx->last_error = "Swendsen-Wang kernel supports n <= " + std::to_string(sw_max_sites());
-    return OJ_ERR_UNSUPPORTED;
-  }
   for (int32_t k = 0; k < num_sched; ++k)
     if (!(betas[k] >= 0.0) || std::isinf(betas[k])) return arg_fail(ctx, "beta must be finite and >= 0");
   RngBase rb;
@@ -1270,7 +1266,17 @@ oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   float* d_beta = ctx->params.as<float>();
   if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-  if (S > 0) OJ_CK(launch_sw(g, R, d_spins, d_beta, S, rb, st, &launches), "swendsen-wang kernel");
+  // graphs above the shared-memory size keep the parent links of a chunk of
+  // replicas in global scratch (at most 1 GiB)
+  uint32_t* scratch = nullptr;
+  int chunk = 0;
+  if (n > sw_max_sites()) {
+    const size_t per = ((size_t)n + 1) * 4;
+    chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)R, ((size_t)1 << 30) / per));
+    OJ_CK(ctx->aux.ensure(per * (size_t)chunk), "alloc union-find scratch");
+    scratch = ctx->aux.as<uint32_t>();
+  }
+  if (S > 0) OJ_CK(launch_sw(g, R, d_spins, d_beta, S, rb, scratch, chunk, st, &launches), "swendsen-wang kernel");
   OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   if (energies) {
     double* d_e = energies;

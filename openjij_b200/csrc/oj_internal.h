@@ -179,7 +179,7 @@ size_t sw_smem_bytes(int n);
 int sw_max_sites();
 cudaError_t sw_prepare(oj_graph* g);
 cudaError_t launch_sw(const oj_graph* g, int R, int8_t* spins, const float* betas, int64_t nsweeps, RngBase rb,
-                      cudaStream_t st, int* launches);
+                      uint32_t* scratch, int chunk, cudaStream_t st, int* launches);
 int batch_max_sites();
 int batch_warps();
 int batch_variant_warps(int variant);

@@ -1,4 +1,5 @@
-// Swendsen-Wang cluster updates for sparse Ising graphs, one CTA per replica.
+// Swendsen-Wang cluster updates for sparse Ising graphs, one CTA per replica
+// (state in shared memory up to sw_max_sites() spins, in global memory above).
 //
 // The reference's SwendsenWang updater (include/openjij/updater/swendsen_wang.hpp:43-182)
 // works on the n spins plus the dummy spin n that carries the fields (bond
@@ -49,10 +50,23 @@ struct SwArgs {
   uint32_t sweep0, rep0;
 };
 
+// Parent links live in shared memory (SMEM) or, for graphs too large for it,
+// in a global scratch array; there they are read past L1 (__ldcg), which does
+// not see the L2 atomics of the other threads.
+template <bool SMEM>
+__device__ __forceinline__ uint32_t ld_parent(const uint32_t* p) {
+  if constexpr (SMEM) {
+    return *p;
+  } else {
+    return __ldcg(p);
+  }
+}
+
+template <bool SMEM>
 __device__ __forceinline__ uint32_t find_root(uint32_t* parent, uint32_t x) {
-  uint32_t p = parent[x];
+  uint32_t p = ld_parent<SMEM>(parent + x);
   while (p != x) {
-    const uint32_t gp = parent[p];
+    const uint32_t gp = ld_parent<SMEM>(parent + p);
     if (gp != p) parent[x] = gp;  // path halving (only ever points a node at an ancestor)
     x = p;
     p = gp;
@@ -60,10 +74,11 @@ __device__ __forceinline__ uint32_t find_root(uint32_t* parent, uint32_t x) {
   return x;
 }
 
+template <bool SMEM>
 __device__ __forceinline__ void unite(uint32_t* parent, uint32_t a, uint32_t b) {
   for (int guard = 0; guard < (1 << 20); ++guard) {
-    a = find_root(parent, a);
-    b = find_root(parent, b);
+    a = find_root<SMEM>(parent, a);
+    b = find_root<SMEM>(parent, b);
     if (a == b) return;
     if (a < b) {
       const uint32_t t = a;
@@ -75,14 +90,19 @@ __device__ __forceinline__ void unite(uint32_t* parent, uint32_t a, uint32_t b) 
   }
 }
 
-// Shared memory: parent[n + 1] (u32) | spins[n] (int8)
-__global__ void __launch_bounds__(kSwThreads) sw_kernel(SwArgs a) {
-  extern __shared__ __align__(16) uint32_t parent[];
+// SMEM: shared memory holds parent[n + 1] (u32) | spins[n] (int8).  Otherwise
+// parent is replica r's slice of gparent ([gridDim.x][n + 1]) and the spins
+// are updated in place in global memory.
+template <bool SMEM>
+__global__ void __launch_bounds__(kSwThreads) sw_kernel(SwArgs a, uint32_t* gparent) {
+  extern __shared__ __align__(16) uint32_t smem[];
   const int n = a.n;
-  int8_t* s = reinterpret_cast<int8_t*>(parent + n + 1);
   const int r = blockIdx.x;
   int8_t* gs = a.spins + (size_t)r * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = gs[i];
+  uint32_t* parent = SMEM ? smem : gparent + (size_t)r * (n + 1);
+  int8_t* s = SMEM ? reinterpret_cast<int8_t*>(smem + n + 1) : gs;
+  if (SMEM)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = gs[i];
   const uint32_t rg = a.rep0 + (uint32_t)r;
   for (int64_t k = 0; k < a.nsweeps; ++k) {
     const float beta2 = __fmul_rn(2.0f, __ldg(a.betas + k));
@@ -100,21 +120,22 @@ __global__ void __launch_bounds__(kSwThreads) sw_kernel(SwArgs a) {
         const int i = a.ei[e], j = a.ej[e];
         const int si = s[i], sj = j < n ? s[j] : 1;
         const bool satisfied = (si * sj > 0) != (a.pos[e] != 0);  // J s_i s_j < 0
-        if (satisfied && ojd::neglog(xs[q]) < __fmul_rn(beta2, a.w[e])) unite(parent, (uint32_t)i, (uint32_t)j);
+        if (satisfied && ojd::neglog(xs[q]) < __fmul_rn(beta2, a.w[e])) unite<SMEM>(parent, (uint32_t)i, (uint32_t)j);
       }
     }
     __syncthreads();
     // 2./3. roots and flips; the dummy spin's cluster stays
-    const uint32_t rn = find_root(parent, (uint32_t)n);
+    const uint32_t rn = find_root<SMEM>(parent, (uint32_t)n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t root = find_root(parent, (uint32_t)i);
+      const uint32_t root = find_root<SMEM>(parent, (uint32_t)i);
       if (root == rn) continue;
       const ojd::u4 c = ojd::philox(root >> 2, kk, rg, ojd::TAG_SW_FLIP, a.keys);
       if (ojd::pick(c, (int)(root & 3u)) & 1u) s[i] = (int8_t)-s[i];
     }
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) gs[i] = s[i];
+  if (SMEM)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) gs[i] = s[i];
 }
 
 }  // namespace
@@ -161,10 +182,11 @@ cudaError_t sw_prepare(oj_graph* g) {
 }
 
 cudaError_t launch_sw(const oj_graph* g, int R, int8_t* spins, const float* betas, int64_t nsweeps, RngBase rb,
-                      cudaStream_t st, int* launches) {
+                      uint32_t* scratch, int chunk, cudaStream_t st, int* launches) {
   const int n = g->n;
-  const size_t smem = sw_smem_bytes(n);
-  if (smem > 220 * 1024 || g->sw_ne > (int64_t)0x7FFFFFFF) return cudaErrorInvalidValue;
+  const bool in_smem = n <= sw_max_sites();
+  const size_t smem = in_smem ? sw_smem_bytes(n) : 0;
+  if (g->sw_ne > (int64_t)0x7FFFFFFF || (!in_smem && (!scratch || chunk < 1))) return cudaErrorInvalidValue;
   const int64_t ne = g->sw_ne;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t b_i = al((size_t)ne * 4 + 4), b_w = al((size_t)ne * 4 + 4);
@@ -182,11 +204,24 @@ cudaError_t launch_sw(const oj_graph* g, int R, int8_t* spins, const float* beta
   a.keys = ojd::make_keys(rb.k0, rb.k1);
   a.sweep0 = rb.sweep0;
   a.rep0 = rb.rep0;
-  cudaError_t e = cudaFuncSetAttribute(sw_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  sw_kernel<<<R, kSwThreads, smem, st>>>(a);
-  if (launches) ++*launches;
-  return cudaGetLastError();
+  if (in_smem) {
+    cudaError_t e = cudaFuncSetAttribute(sw_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    sw_kernel<true><<<R, kSwThreads, smem, st>>>(a, nullptr);
+    if (launches) ++*launches;
+    return cudaGetLastError();
+  }
+  // replicas in chunks whose parent arrays fit the scratch ([chunk][n + 1])
+  for (int r0 = 0; r0 < R; r0 += chunk) {
+    SwArgs c = a;
+    c.spins = spins + (size_t)r0 * n;
+    c.rep0 = rb.rep0 + (uint32_t)r0;
+    sw_kernel<false><<<std::min(chunk, R - r0), kSwThreads, 0, st>>>(c, scratch);
+    if (launches) ++*launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 int sw_max_sites() { return (220 * 1024 - 20) / 5; }

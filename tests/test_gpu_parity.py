@@ -381,3 +381,16 @@ def test_swendsen_wang_split_run(ctx):
     N.sw_run(dg, part, betas[:4], mcs[:4], seed=4, replica_offset=32)
     N.sw_run(dg, part, betas[4:], mcs[4:], seed=4, replica_offset=32, first_sweep=int(np.sum(mcs[:4])))
     np.testing.assert_array_equal(part, whole[32:])
+
+
+def test_swendsen_wang_large_graph_global_forest(ctx):
+    """Above the shared-memory size (n > 45,000) the forest lives in global
+    scratch; same bonds, clusters and coins as the replay."""
+    m = I.lattice_pm_j(224, seed=6)[0]
+    g, dg = _graph(ctx, m)
+    assert g.n > 45000
+    betas, mcs = I.geometric_betas(0.2, 1.5, 3)
+    s0 = _init(3, g.n, 8)
+    s = s0.copy()
+    N.sw_run(dg, s, betas, mcs, seed=21)
+    np.testing.assert_array_equal(s, O.replay_sw(g, s0, _per_sweep(betas, mcs), 21))
