@@ -8,8 +8,8 @@
 // until the queue is empty.  One warp runs one replica: its FP32 local fields
 // live in the warp's slice of shared memory, laid out in 128-site chunks with
 // lane l owning sites 4l..4l+3 of every chunk (one float4 per lane), and its
-// spins are bits in shared memory, one word per (chunk c, lane l) with bit e set
-// when site 128c+4l+e is -1.
+// spins are bits in shared memory: lane l's word g holds chunks 8g..8g+7, bit
+// 4(c mod 8)+e set when site 128c+4l+e is -1.
 //
 // Update order and acceptance are the reference's sequential single-spin flip
 // (include/openjij/updater/single_spin_flip.hpp:66-95): sites 0..n-1 in order,
@@ -40,7 +40,7 @@ namespace {
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
 constexpr int kMaxChunks = kBatchMaxN / 128;
-constexpr int kInitRows = 16;                          // J rows per staged initialisation tile
+constexpr int kInitRows = 8;                           // J rows per staged initialisation tile
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -62,7 +62,12 @@ struct BatchArgs {
   uint32_t inst0;          // global index of instance 0
   uint32_t rep0;           // global index of each instance's replica 0
   int fstride;             // fields per warp in shared memory (multiple of 128)
+  int swstride;            // spin words per warp: 32 per eight chunks
 };
+
+// Spin bits of chunk c of lane l: four bits of word 32*(c/8) + l.
+__device__ __forceinline__ int sw_word(int c, int l) { return 32 * (c >> 3) + l; }
+__device__ __forceinline__ int sw_shift(int c) { return 4 * (c & 7); }
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
@@ -76,7 +81,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
-                 (size_t)warp * (a.fstride / 4);  // spin words [chunk][lane]
+                 (size_t)warp * a.swstride;  // spin words [chunk / 8][lane]
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
@@ -95,14 +100,15 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     int8_t* gs = a.spins + a.soff[m] + (size_t)(active ? r : 0) * n;
     // spins -> bits
     if (active)
-      for (int c = 0; c < nch; ++c) {
+      for (int c8 = 0; c8 < nch; c8 += 8) {
         uint32_t w = 0u;
+        for (int c = c8; c < nch && c < c8 + 8; ++c)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int i = 128 * c + 4 * lane + e;
-          if (i < n && gs[i] < 0) w |= 1u << e;
-        }
-        sw[32 * c + lane] = w;
+          for (int e = 0; e < 4; ++e) {
+            const int i = 128 * c + 4 * lane + e;
+            if (i < n && gs[i] < 0) w |= 1u << (sw_shift(c) + e);
+          }
+        sw[sw_word(c8, lane)] = w;
       }
     __syncwarp();
     // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j).
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             const int i = i0 + q;
             if (i >= n) break;
             const float4 v = buf[q * 32 + lane];
-            const bool neg = (sw[32 * (i >> 7) + ((i & 127) >> 2)] >> (i & 3)) & 1u;
+            const bool neg = (sw[sw_word(i >> 7, (i & 127) >> 2)] >> (sw_shift(i >> 7) + (i & 3))) & 1u;
             acc.x = __fadd_rn(acc.x, neg ? -v.x : v.x);
             acc.y = __fadd_rn(acc.y, neg ? -v.y : v.y);
             acc.z = __fadd_rn(acc.z, neg ? -v.z : v.z);
@@ -170,7 +176,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         for (;;) {
           const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
           const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
-          const uint32_t myw = sw[32 * c + lane];
+          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
           uint32_t mask = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -185,8 +191,8 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const int ls = __ffs(lanes) - 1;
           const uint32_t ms = __shfl_sync(0xffffffffu, mask, ls);
           const int es = __ffs(ms) - 1;
-          const uint32_t ws = sw[32 * c + ls];
-          const bool neg = (ws >> es) & 1u;
+          const uint32_t ws = sw[sw_word(c, ls)];
+          const bool neg = (ws >> (sw_shift(c) + es)) & 1u;
           const float coef = neg ? 2.0f : -2.0f;
           const int i = 128 * c + 4 * ls + es;
           const float* Ji = J + (size_t)i * npad + 4 * lane;
@@ -210,14 +216,14 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
               }
           }
           __syncwarp();
-          if (lane == ls) sw[32 * c + ls] = ws ^ (1u << es);
+          if (lane == ls) sw[sw_word(c, ls)] = ws ^ (1u << (sw_shift(c) + es));
           pos = 4 * ls + es + 1;
           __syncwarp();
         }
       }
     }
     for (int c = 0; c < nch; ++c) {
-      const uint32_t w = sw[32 * c + lane];
+      const uint32_t w = sw[sw_word(c, lane)] >> sw_shift(c);
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int i = 128 * c + 4 * lane + e;
@@ -330,9 +336,9 @@ int batch_default_variant() {
 }
 
 template <int W, int MINB, int GROUP>
-cudaError_t launch_variant(const BatchArgs& a, int nitems, int fstride, int sm_count, cudaStream_t st) {
+cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStream_t st) {
   auto kern = sa_batch_kernel<W, MINB, GROUP>;
-  const size_t smem = (size_t)W * fstride * 5;  // FP32 fields + spin words
+  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4);  // FP32 fields + spin words
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -371,15 +377,16 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.inst0 = inst0;
   a.rep0 = rb.rep0;
   a.fstride = fstride;
+  a.swstride = 32 * ((fstride / 128 + 7) / 8);
   cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   switch (variant) {
-    case 45: e = launch_variant<4, 5, 8>(a, nitems, fstride, sm_count, st); break;
-    case 82: e = launch_variant<8, 2, 16>(a, nitems, fstride, sm_count, st); break;
-    case 83: e = launch_variant<8, 3, 4>(a, nitems, fstride, sm_count, st); break;
-    case 84: e = launch_variant<8, 4, 4>(a, nitems, fstride, sm_count, st); break;
-    case 162: e = launch_variant<16, 2, 4>(a, nitems, fstride, sm_count, st); break;
-    default: e = launch_variant<32, 1, 4>(a, nitems, fstride, sm_count, st); break;
+    case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st); break;
+    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st); break;
+    case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st); break;
+    case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st); break;
+    case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st); break;
+    default: e = launch_variant<32, 1, 4>(a, nitems, sm_count, st); break;
   }
   if (e == cudaSuccess && launches) ++*launches;
   return e;
