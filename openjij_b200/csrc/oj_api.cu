@@ -301,6 +301,7 @@ oj_status oj_ctx_destroy(oj_ctx* ctx) {
     ctx->best.release();
     ctx->aux.release();
     ctx->batch.release();
+    ctx->fields.release();
     for (auto& e : ctx->ev)
       if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -560,12 +561,13 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     int variant = tit != g->tuned.end() ? tit->second.variant : batch_default_variant();
     std::vector<int32_t> items = make_items(batch_variant_warps(variant));
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t b_hdr = al(4 + 8), b_items = al(make_items(batch_min_warps()).size() * 4 + 4), b_cnt = al(4),
+    const size_t b_hdr = al(8 + 8 + 8), b_items = al(make_items(batch_min_warps()).size() * 4 + 4), b_cnt = al(4),
                  b_beta = al(bf.size() * 4 + 4);
     OJ_CK(ctx->batch.ensure(b_hdr + b_items + b_cnt + b_beta), "alloc tables");
     char* base = ctx->batch.as<char>();
     int32_t* d_reads = reinterpret_cast<int32_t*>(base);
     int64_t* d_soff = reinterpret_cast<int64_t*>(base + 8);
+    int64_t* d_foff = reinterpret_cast<int64_t*>(base + 16);
     int32_t* d_items = reinterpret_cast<int32_t*>(base + b_hdr);
     int* d_counter = reinterpret_cast<int*>(base + b_hdr + b_items);
     float* d_beta = reinterpret_cast<float*>(base + b_hdr + b_items + b_cnt);
@@ -573,6 +575,10 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     const int64_t hsoff = 0;
     OJ_CK(cudaMemcpyAsync(d_reads, &hreads, 4, cudaMemcpyHostToDevice, st), "H2D reads");
     OJ_CK(cudaMemcpyAsync(d_soff, &hsoff, 8, cudaMemcpyHostToDevice, st), "H2D offsets");
+    OJ_CK(cudaMemcpyAsync(d_foff, &hsoff, 8, cudaMemcpyHostToDevice, st), "H2D offsets");
+    // initial fields of every replica, [R][n rounded up to 128] floats
+    OJ_CK(ctx->fields.ensure(std::max<size_t>((size_t)R * (((size_t)n + 127) / 128 * 128) * 4, 16)), "alloc fields");
+    float* d_fields = ctx->fields.as<float>();
     if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
     if (tit == g->tuned.end() && autotune_requested(flags) && S > 0) {
       // candidates run 16 sweeps with betas spread over the schedule on a copy of the spins
@@ -599,7 +605,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
               loaded = i;
             }
             return launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter,
-                                   scratch, d_tb, Ssub, rb, 0, ctx->sm_count, st, nullptr, cand[i]);
+                                   scratch, d_tb, Ssub, rb, 0, ctx->sm_count, st, nullptr, cand[i], d_fields, d_foff,
+                                   R);
           },
           &terr, (int)(std::find(std::begin(cand), std::end(cand), batch_default_variant()) - std::begin(cand)));
       if (bi == -2) return cuda_fail(ctx, terr, "autotune");
@@ -612,7 +619,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
       OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(items.size() / 2), d_counter, d_spins,
-                            d_beta, S, rb, 0, ctx->sm_count, st, &launches, variant),
+                            d_beta, S, rb, 0, ctx->sm_count, st, &launches, variant, d_fields, d_foff, R),
             "sa dense jump kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     threads_used = batch_variant_warps(variant) * 32;
@@ -1076,15 +1083,17 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     if (!(betas[k] >= 0.0) || std::isinf(betas[k])) return arg_fail(ctx, "beta must be finite and >= 0");
   if (stats) std::memset(stats, 0, sizeof(*stats));
   const int count = b->count;
-  std::vector<int64_t> soff(count), eoff(count);
-  int64_t sbytes = 0, nrep = 0;
+  std::vector<int64_t> soff(count), eoff(count), foff(count);
+  int64_t sbytes = 0, nrep = 0, nfield = 0;
   int max_reads = 0;
   double attempts_per_sweep = 0.0;
   for (int k = 0; k < count; ++k) {
     if (reads[k] < 0) return arg_fail(ctx, "negative read count");
     soff[k] = sbytes;
     eoff[k] = nrep;
+    foff[k] = nfield;
     sbytes += (int64_t)reads[k] * b->n[k];
+    nfield += (int64_t)reads[k] * (((int64_t)b->n[k] + 127) / 128 * 128);
     nrep += reads[k];
     max_reads = std::max(max_reads, (int)reads[k]);
     attempts_per_sweep += (double)reads[k] * b->n[k];
@@ -1128,12 +1137,16 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   } else if (sbytes > 0 && !is_device_ptr(spins)) {
     return arg_fail(ctx, "OJ_DEVICE_POINTERS set but spins is not device memory");
   }
-  // one staging buffer: reads | soff | eoff | items | counter | betas | order
+  // one staging buffer: reads | soff | eoff | items | counter | betas | order | foff
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t b_reads = al((size_t)count * 4), b_soff = al((size_t)count * 8), b_eoff = al((size_t)count * 8),
                b_items = al(items_cap * 4 + 4), b_cnt = al(4), b_beta = al(bf.size() * 4 + 4),
-               b_order = al((size_t)count * 4);
-  OJ_CK(ctx->batch.ensure(b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta + b_order), "alloc batch tables");
+               b_order = al((size_t)count * 4), b_foff = al((size_t)count * 8);
+  OJ_CK(ctx->batch.ensure(b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta + b_order + b_foff),
+        "alloc batch tables");
+  // initial fields of every replica of every instance, [reads][n rounded up to 128] floats each
+  OJ_CK(ctx->fields.ensure(std::max<size_t>((size_t)nfield * 4, 16)), "alloc fields");
+  float* d_fields = ctx->fields.as<float>();
   char* base = ctx->batch.as<char>();
   int32_t* d_reads = reinterpret_cast<int32_t*>(base);
   int64_t* d_soff = reinterpret_cast<int64_t*>(base + b_reads);
@@ -1142,6 +1155,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   int* d_counter = reinterpret_cast<int*>(base + b_reads + b_soff + b_eoff + b_items);
   float* d_beta = reinterpret_cast<float*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt);
   int32_t* d_order = reinterpret_cast<int32_t*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta);
+  int64_t* d_foff = reinterpret_cast<int64_t*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta + b_order);
   int launches = 0;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(d_spins, spins, sbytes, cudaMemcpyHostToDevice, st), "H2D spins");
@@ -1151,6 +1165,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (nitems) OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
   if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
   if (count) OJ_CK(cudaMemcpyAsync(d_order, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st), "H2D order");
+  if (count) OJ_CK(cudaMemcpyAsync(d_foff, foff.data(), (size_t)count * 8, cudaMemcpyHostToDevice, st), "H2D offsets");
   bool tuned_now = false;
   if (bm->tuned_variant == 0 && autotune_requested(flags) && S > 0 && nitems > 0) {
     // the work per sweep follows the acceptance rate, so the candidates run 16
@@ -1178,7 +1193,8 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
             loaded = i;
           }
           return launch_sa_batch(b, d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter, scratch, d_tb, Ssub,
-                                 rb, (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i]);
+                                 rb, (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i], d_fields, d_foff,
+                                 max_reads);
         },
         &terr, (int)(std::find(std::begin(cand), std::end(cand), batch_default_variant()) - std::begin(cand)));
     if (bi == -2) return cuda_fail(ctx, terr, "autotune");
@@ -1192,7 +1208,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (S > 0 && nitems > 0)
     OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
                           (uint32_t)instance_offset, ctx->sm_count, st, &launches,
-                          bm->tuned_variant ? bm->tuned_variant : variant0),
+                          bm->tuned_variant ? bm->tuned_variant : variant0, d_fields, d_foff, max_reads),
           "sa batched kernel");
   OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   if (energies) {

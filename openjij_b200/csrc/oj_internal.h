@@ -130,7 +130,7 @@ struct oj_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string last_error;
-  oj::DevBuf spins, words, params, energies, best, aux, batch;
+  oj::DevBuf spins, words, params, energies, best, aux, batch, fields;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -188,7 +188,7 @@ int batch_default_variant();
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches, int variant = 0);
+                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st);

@@ -25,7 +25,10 @@
 // index (rep0 + index within the instance).
 //
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
-// read through L1 one float4 per lane on every accepted flip; h likewise.
+// read through L1 one float4 per lane on every accepted flip.  The initial
+// fields come from batch_field_kernel, launched just before (it reads J once
+// per 64 replicas), through a global buffer of reads x padded n floats per
+// instance.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,7 +43,6 @@ namespace {
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
 constexpr int kMaxChunks = kBatchMaxN / 128;
-constexpr int kInitRows = 8;                           // J rows per staged initialisation tile
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -63,6 +65,8 @@ struct BatchArgs {
   uint32_t rep0;           // global index of each instance's replica 0
   int fstride;             // fields per warp in shared memory (multiple of 128)
   int swstride;            // spin words per warp: 32 per eight chunks
+  const float* F;          // initial fields, [reads][npad] per instance (batch_field_kernel)
+  const int64_t* foff;     // [count] offset of instance m's fields (floats)
 };
 
 // Spin bits of chunk c of lane l: four bits of word 32*(c/8) + l.
@@ -77,7 +81,6 @@ template <int W, int MINB, int GROUP>
 __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
-  __shared__ float4 jtile[2 * kInitRows * 32];  // J tiles of the field initialisation
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
@@ -92,7 +95,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     if ((unsigned)m >= (unsigned)a.count) continue;  // a corrupt table entry is skipped, never followed
     const int r = a.items[2 * item + 1] * W + warp;
     const int n = a.n[m];
-    const bool active = r < a.reads[m];  // every warp takes part in the field initialisation
+    const bool active = r < a.reads[m];  // warps past the instance's reads wait for the next item
     const int nch = (n + 127) >> 7;
     const int npad = nch << 7;
     const float* J = a.J + a.joff[m];
@@ -110,55 +113,13 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           }
         sw[sw_word(c8, lane)] = w;
       }
-    __syncwarp();
-    // f_j = h_j + sum_i J_ij s_i, i ascending (J symmetric: row i, column j).
-    // The CTA's warps share each tile of kInitRows rows x 128 columns of J,
-    // staged in shared memory (double-buffered, the next tile's loads in flight
-    // while the current one is summed), so J is read once per CTA, not per warp.
-    {
-      const int ntr = (n + kInitRows - 1) / kInitRows;  // row tiles per chunk
-      const int ntiles = nch * ntr;
-      constexpr int NL = (kInitRows * 32 + W * 32 - 1) / (W * 32);  // float4 loads per thread and tile
-      float4 pre[NL];
-      auto load_tile = [&](int t) {
-        const int c = t / ntr, i0 = (t - c * ntr) * kInitRows;
-#pragma unroll
-        for (int q = 0; q < NL; ++q) {
-          const int idx = threadIdx.x + q * W * 32;
-          const int row = idx >> 5, col = idx & 31;
-          pre[q] = (row < kInitRows && i0 + row < n) ? ldg4(J + (size_t)(i0 + row) * npad + 128 * c + 4 * col)
-                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      };
-      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (ntiles > 0) load_tile(0);
-      for (int t = 0; t < ntiles; ++t) {
-        const int c = t / ntr, i0 = (t - c * ntr) * kInitRows;
-        float4* buf = jtile + (t & 1) * (kInitRows * 32);
-#pragma unroll
-        for (int q = 0; q < NL; ++q) {
-          const int idx = threadIdx.x + q * W * 32;
-          if (idx < kInitRows * 32) buf[idx] = pre[q];
-        }
-        __syncthreads();
-        if (t + 1 < ntiles) load_tile(t + 1);
-        if (active) {
-          if (i0 == 0) acc = ldg4(h + 128 * c + 4 * lane);
-          for (int q = 0; q < kInitRows; ++q) {
-            const int i = i0 + q;
-            if (i >= n) break;
-            const float4 v = buf[q * 32 + lane];
-            const bool neg = (sw[sw_word(i >> 7, (i & 127) >> 2)] >> (sw_shift(i >> 7) + (i & 3))) & 1u;
-            acc.x = __fadd_rn(acc.x, neg ? -v.x : v.x);
-            acc.y = __fadd_rn(acc.y, neg ? -v.y : v.y);
-            acc.z = __fadd_rn(acc.z, neg ? -v.z : v.z);
-            acc.w = __fadd_rn(acc.w, neg ? -v.w : v.w);
-          }
-          if (i0 + kInitRows >= n) reinterpret_cast<float4*>(f)[32 * c + lane] = acc;
-        }
-      }
-    }
     if (!active) continue;  // no block-wide barrier until the next item
+    __syncwarp();
+    // the fields f_j = h_j + sum_i J_ij s_i come from batch_field_kernel
+    {
+      const float* Fr = a.F + a.foff[m] + (size_t)r * npad;
+      for (int c = 0; c < nch; ++c) reinterpret_cast<float4*>(f)[32 * c + lane] = ldg4(Fr + 128 * c + 4 * lane);
+    }
     __syncwarp();
     const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
     const uint32_t rg = a.rep0 + (uint32_t)r;
@@ -231,6 +192,70 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
       }
     }
     __syncwarp();
+  }
+}
+
+// Initial fields of every replica of every instance,
+//     F[m][r][j] = h_j + sum_{i = 0..n-1} J_ij s_ri,
+// summed in ascending i with one FP32 rounding per term, the order of the
+// reference's reset_dE row sums (classical_ising.hpp:87-90) restated in FP32.
+// One CTA per (instance, 128 columns, 64 replicas): it stages 32 rows x 128
+// columns of J and the sign bits of those rows for its 64 replicas in shared
+// memory; thread (site quad q, replica group g) accumulates 4 columns of 8
+// replicas, so J is read once per 64 replicas instead of once per replica.
+constexpr int kFieldReplicas = 64;
+constexpr int kFieldRows = 32;
+
+__global__ void __launch_bounds__(256) batch_field_kernel(BatchArgs a, int zbase) {
+  __shared__ float4 jt[kFieldRows * 32];
+  __shared__ uint32_t sgn[kFieldReplicas];
+  const int m = blockIdx.x, jb = blockIdx.y, r0 = (zbase + (int)blockIdx.z) * kFieldReplicas;
+  const int n = a.n[m], R = a.reads[m];
+  const int nch = (n + 127) >> 7;
+  if (jb >= nch || r0 >= R) return;  // the whole CTA leaves together
+  const int npad = nch << 7;
+  const int t = threadIdx.x, sq = t & 31, rg = t >> 5;
+  const float* J = a.J + a.joff[m] + 128 * jb;
+  const int8_t* S = a.spins + a.soff[m];
+  const float4 h4 = ldg4(a.h + a.hoff[m] + 128 * jb + 4 * sq);
+  float4 acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc[q] = h4;
+  for (int i0 = 0; i0 < n; i0 += kFieldRows) {
+    __syncthreads();  // the previous tile is consumed
+    for (int k = t; k < kFieldRows * 32; k += 256) {
+      const int row = k >> 5;
+      jt[k] = i0 + row < n ? ldg4(J + (size_t)(i0 + row) * npad + 4 * (k & 31)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {  // warp rg: sign bits of rows i0..i0+31 of its 8 replicas
+      const int rr = 8 * rg + q, r = r0 + rr, i = i0 + sq;
+      const bool neg = r < R && i < n && S[(size_t)r * n + i] < 0;
+      const uint32_t bits = __ballot_sync(0xffffffffu, neg);
+      if (sq == 0) sgn[rr] = bits;
+    }
+    __syncthreads();
+    uint32_t mk[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) mk[q] = sgn[8 * rg + q];
+    const int rows = min(kFieldRows, n - i0);
+    for (int ii = 0; ii < rows; ++ii) {
+      const float4 v = jt[ii * 32 + sq];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const bool neg = (mk[q] >> ii) & 1u;
+        acc[q].x = __fadd_rn(acc[q].x, neg ? -v.x : v.x);
+        acc[q].y = __fadd_rn(acc[q].y, neg ? -v.y : v.y);
+        acc[q].z = __fadd_rn(acc[q].z, neg ? -v.z : v.z);
+        acc[q].w = __fadd_rn(acc[q].w, neg ? -v.w : v.w);
+      }
+    }
+  }
+  float* Fm = const_cast<float*>(a.F) + a.foff[m] + 128 * jb + 4 * sq;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int r = r0 + 8 * rg + q;
+    if (r < R) *reinterpret_cast<float4*>(Fm + (size_t)r * npad) = acc[q];
   }
 }
 
@@ -353,7 +378,7 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches, int variant) {
+                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads) {
   if (variant == 0) variant = batch_default_variant();
   if (!batch_variant_valid(variant)) return cudaErrorInvalidValue;
   const int fstride = std::max(128, (b->max_n + 127) / 128 * 128);
@@ -378,7 +403,18 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.rep0 = rb.rep0;
   a.fstride = fstride;
   a.swstride = 32 * ((fstride / 128 + 7) / 8);
-  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  a.F = d_fields;
+  a.foff = d_foff;
+  if (b->count == 0 || max_reads <= 0 || nitems <= 0) return cudaSuccess;
+  const int zt = (max_reads + kFieldReplicas - 1) / kFieldReplicas;
+  cudaError_t e = cudaSuccess;
+  for (int z0 = 0; z0 < zt; z0 += 65535) {  // grid z is at most 65535 replica tiles
+    const dim3 fgrid((unsigned)b->count, (unsigned)(fstride / 128), (unsigned)std::min(65535, zt - z0));
+    batch_field_kernel<<<fgrid, 256, 0, st>>>(a, z0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (launches) ++*launches;
+  }
+  e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   switch (variant) {
     case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st); break;
