@@ -174,7 +174,7 @@ oj_status ensure_single(oj_ctx* ctx, oj_graph* g) {
 
 // FP64 energies of R replicas of a dense graph with the batched energy kernel
 // (the coupling matrix is read once per 32 replicas).
-cudaError_t single_energy(oj_graph* g, int R, const int8_t* spins, double* out, cudaStream_t st) {
+cudaError_t single_energy(oj_ctx* ctx, oj_graph* g, int R, const int8_t* spins, double* out, cudaStream_t st) {
   struct Tab {
     int32_t reads, order;
     int64_t soff, eoff;
@@ -183,7 +183,10 @@ cudaError_t single_energy(oj_graph* g, int R, const int8_t* spins, double* out, 
   if (e != cudaSuccess) return e;
   Tab* d = g->single_tab.as<Tab>();
   if ((e = cudaMemcpyAsync(d, &h, sizeof(Tab), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
-  return launch_batch_energy(g->single.get(), &d->reads, &d->soff, &d->eoff, &d->order, R, spins, out, st);
+  const int ns = batch_energy_splits(g->single.get(), R, ctx->sm_count);
+  if (ns > 1 && (e = ctx->eparts.ensure((size_t)ns * R * 8)) != cudaSuccess) return e;
+  return launch_batch_energy(g->single.get(), &d->reads, &d->soff, &d->eoff, &d->order, R, spins, out, st, ns,
+                             ctx->eparts.as<double>(), R);
 }
 
 bool autotune_requested(uint32_t flags) {
@@ -302,6 +305,7 @@ oj_status oj_ctx_destroy(oj_ctx* ctx) {
     ctx->aux.release();
     ctx->batch.release();
     ctx->fields.release();
+    ctx->eparts.release();
     for (auto& e : ctx->ev)
       if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -648,10 +652,12 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       d_e = ctx->energies.as<double>();
     }
     const bool dense = kernel == OJ_KERNEL_DENSE_PLAIN || kernel == OJ_KERNEL_DENSE_TC || kernel == OJ_KERNEL_DENSE_JUMP;
-    if (dense && n <= batch_max_sites() && ensure_single(ctx, g) == OJ_OK)
-      OJ_CK(single_energy(g, R, d_spins, d_e, st), "energy kernel");
-    else
+    if (dense && n <= batch_max_sites() && ensure_single(ctx, g) == OJ_OK) {
+      OJ_CK(single_energy(ctx, g, R, d_spins, d_e, st), "energy kernel");
+      if (batch_energy_splits(g->single.get(), R, ctx->sm_count) > 1) ++launches;  // the parts' sum
+    } else {
       OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+    }
     ++launches;
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
   }
@@ -1217,9 +1223,12 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
       OJ_CK(ctx->energies.ensure((size_t)nrep * 8), "alloc energies");
       d_e = ctx->energies.as<double>();
     }
-    OJ_CK(launch_batch_energy(b, d_reads, d_soff, d_eoff, d_order, max_reads, d_spins, d_e, st),
+    const int ns = batch_energy_splits(b, max_reads, ctx->sm_count);
+    if (ns > 1) OJ_CK(ctx->eparts.ensure((size_t)ns * nrep * 8), "alloc energy parts");
+    OJ_CK(launch_batch_energy(b, d_reads, d_soff, d_eoff, d_order, max_reads, d_spins, d_e, st, ns,
+                              ctx->eparts.as<double>(), nrep),
           "batch energy kernel");
-    ++launches;
+    launches += ns > 1 ? 2 : 1;
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)nrep * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
   }
   if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(spins, d_spins, sbytes, cudaMemcpyDeviceToHost, st), "D2H spins");

@@ -130,7 +130,7 @@ struct oj_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string last_error;
-  oj::DevBuf spins, words, params, energies, best, aux, batch, fields;
+  oj::DevBuf spins, words, params, energies, best, aux, batch, fields, eparts;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -191,7 +191,8 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
                             int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
-                                double* out, cudaStream_t st);
+                                double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep);
+int batch_energy_splits(const oj_batch* b, int max_reads, int sm_count);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
 int flip_stats_max_k();

@@ -241,13 +241,15 @@ __global__ void __launch_bounds__(256) batch_field_kernel(BatchArgs a, int zbase
     const int rows = min(kFieldRows, n - i0);
     for (int ii = 0; ii < rows; ++ii) {
       const float4 v = jt[ii * 32 + sq];
+      const uint32_t bit = 1u << ii;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        const bool neg = (mk[q] >> ii) & 1u;
-        acc[q].x = __fadd_rn(acc[q].x, neg ? -v.x : v.x);
-        acc[q].y = __fadd_rn(acc[q].y, neg ? -v.y : v.y);
-        acc[q].z = __fadd_rn(acc[q].z, neg ? -v.z : v.z);
-        acc[q].w = __fadd_rn(acc[q].w, neg ? -v.w : v.w);
+        // fma(+-1, v, acc) rounds acc +- v once: the same sum as an add
+        const float sg = (mk[q] & bit) ? -1.0f : 1.0f;
+        acc[q].x = __fmaf_rn(sg, v.x, acc[q].x);
+        acc[q].y = __fmaf_rn(sg, v.y, acc[q].y);
+        acc[q].z = __fmaf_rn(sg, v.z, acc[q].z);
+        acc[q].w = __fmaf_rn(sg, v.w, acc[q].w);
       }
     }
   }
@@ -274,7 +276,8 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
                                                            const int64_t* __restrict__ soff,
                                                            const int64_t* __restrict__ eoff,
                                                            const int32_t* __restrict__ order,
-                                                           const int8_t* __restrict__ spins, double* __restrict__ out) {
+                                                           const int8_t* __restrict__ spins, double* __restrict__ out,
+                                                           int64_t nrep) {
   __shared__ uint32_t wsh[kBatchMaxN + 32];
   __shared__ double rowbuf[8][32];
   __shared__ double part[8][32];
@@ -294,8 +297,9 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
   }
   __syncthreads();
   const double* A = J64 + j64off[m];  // augmented (n+1)^2, row-major
+  const int split = blockIdx.z, nsplit = gridDim.z;  // rows i with (i / 8) % nsplit == split
   double acc = 0.0;
-  for (int i = warp; i < n; i += 8) {
+  for (int i = 8 * split + warp; i < n; i += 8 * nsplit) {
     const double* Ai = A + (size_t)i * (n + 1);
     const uint32_t wi = wsh[i];
     double p[4] = {0.0, 0.0, 0.0, 0.0};
@@ -322,8 +326,18 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
   if (warp == 0 && r0 + lane < R) {
     double e = 0.0;
     for (int w = 0; w < 8; ++w) e += part[w][lane];
-    out[eoff[m] + r0 + lane] = e;
+    out[(size_t)split * nrep + eoff[m] + r0 + lane] = e;  // this row split's part
   }
+}
+
+// Sums the row splits' parts of every replica's energy, split 0 first.
+__global__ void batch_energy_sum_kernel(const double* __restrict__ parts, int nsplit, int64_t nrep,
+                                        double* __restrict__ out) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrep) return;
+  double e = 0.0;
+  for (int k = 0; k < nsplit; ++k) e += parts[(size_t)k * nrep + r];
+  out[r] = e;
 }
 
 }  // namespace
@@ -428,13 +442,26 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   return e;
 }
 
+int batch_energy_splits(const oj_batch* b, int max_reads, int sm_count) {
+  // rows split over CTAs until the grid covers the SMs several times (8 rows per
+  // warp pass, so a split keeps at least 64 rows)
+  const int64_t base = (int64_t)b->count * ((max_reads + 31) / 32);
+  int k = 1;
+  while (k < 16 && base * k < 6LL * sm_count && 64 * 2 * k <= b->max_n) k *= 2;
+  return k;
+}
+
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
-                                double* out, cudaStream_t st) {
+                                double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep) {
   if (b->count == 0 || max_reads == 0) return cudaSuccess;
-  dim3 grid(b->count, (max_reads + 31) / 32);
+  if (nsplit < 1 || (nsplit > 1 && !parts)) return cudaErrorInvalidValue;
+  dim3 grid(b->count, (max_reads + 31) / 32, nsplit);
   batch_energy_kernel<<<grid, 256, 0, st>>>(b->d_J64.as<double>(), b->d_j64off.as<int64_t>(), b->d_n.as<int32_t>(),
-                                            d_reads, d_soff, d_eoff, d_order, spins, out);
+                                            d_reads, d_soff, d_eoff, d_order, spins, nsplit > 1 ? parts : out, nrep);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || nsplit == 1) return e;
+  batch_energy_sum_kernel<<<(unsigned)((nrep + 255) / 256), 256, 0, st>>>(parts, nsplit, nrep, out);
   return cudaGetLastError();
 }
 
