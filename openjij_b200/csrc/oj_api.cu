@@ -1,6 +1,7 @@
 // C ABI entry points (include/openjij_b200.h): context, graph upload, the SA
 // and SQA runs with their planner, FP64 energies.  No exception crosses the
 // ABI; every CUDA error becomes a status with a message in the context.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1054,6 +1055,21 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
     return bytes ? cudaMemcpy(d.ptr, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
   };
   OJ_CK(up(b->d_J, J32.data(), J32.size() * 4), "upload J");
+  // flip rows in half the bytes when FP16 holds every FP32 coupling exactly
+  // (integer and quarter-integer couplings of moderate size): the kernel
+  // widens them back to the same FP32 values
+  {
+    std::vector<__half> J16(J32.size());
+    bool exact = true;
+    for (size_t q = 0; q < J32.size() && exact; ++q) {
+      J16[q] = __float2half_rn(J32[q]);
+      exact = __half2float(J16[q]) == J32[q];
+    }
+    if (exact) {
+      OJ_CK(up(b->d_J16, J16.data(), J16.size() * 2), "upload J16");
+      b->j16 = true;
+    }
+  }
   OJ_CK(up(b->d_h, h32.data(), h32.size() * 4), "upload h");
   OJ_CK(up(b->d_J64, J64.data(), J64.size() * 8), "upload J64");
   OJ_CK(up(b->d_joff, joff.data(), joff.size() * 8), "upload offsets");

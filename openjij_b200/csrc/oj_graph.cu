@@ -21,6 +21,7 @@ oj_batch::~oj_batch() {
   cudaGetDevice(&cur);
   if (cur != device) cudaSetDevice(device);
   d_J.release();
+  d_J16.release();
   d_h.release();
   d_J64.release();
   d_joff.release();

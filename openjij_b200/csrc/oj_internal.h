@@ -120,6 +120,8 @@ struct oj_batch {
   int max_n = 0;
   std::vector<int32_t> n;
   oj::DevBuf d_J, d_h, d_J64, d_joff, d_hoff, d_j64off, d_n;
+  oj::DevBuf d_J16;   // J as FP16 when every coupling's FP32 value is exactly an FP16 value (flip rows)
+  bool j16 = false;
   int tuned_variant = 0;  // autotuned register-budget variant, 0 = not tuned
   ~oj_batch();
 };

@@ -29,6 +29,7 @@
 // fields come from batch_field_kernel, launched just before (it reads J once
 // per 64 replicas), through a global buffer of reads x padded n floats per
 // instance.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -65,6 +66,7 @@ struct BatchArgs {
   uint32_t rep0;           // global index of each instance's replica 0
   int fstride;             // fields per warp in shared memory (multiple of 128)
   int swstride;            // spin words per warp: 32 per eight chunks
+  const __half* J16;       // J as FP16 (same offsets), when every value is exact in FP16
   const float* F;          // initial fields, [reads][npad] per instance (batch_field_kernel)
   const int64_t* foff;     // [count] offset of instance m's fields (floats)
 };
@@ -74,10 +76,18 @@ __device__ __forceinline__ int sw_word(int c, int l) { return 32 * (c >> 3) + l;
 __device__ __forceinline__ int sw_shift(int c) { return 4 * (c & 7); }
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// four FP16 couplings widened to FP32 (exact)
+__device__ __forceinline__ float4 ldg4h(const __half* p) {
+  const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
 
 // GROUP: chunks of a flipped site's J row loaded before any is used (the
 // flip's L2 round trips are ceil(chunks / GROUP)); more costs registers.
-template <int W, int MINB, int GROUP>
+// H: the flip rows come from the FP16 copy of J (half the L2 bytes per flip).
+template <int W, int MINB, int GROUP, bool H>
 __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
@@ -157,6 +167,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const float coef = neg ? 2.0f : -2.0f;
           const int i = 128 * c + 4 * ls + es;
           const float* Ji = J + (size_t)i * npad + 4 * lane;
+          const __half* Ji16 = a.J16 + a.joff[m] + (size_t)i * npad + 4 * lane;
           // the row in groups of four chunks whose loads are in flight together
 #pragma unroll
           for (int c0 = 0; c0 < kMaxChunks; c0 += GROUP) {
@@ -164,7 +175,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             float4 v[GROUP];
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
-              if (c0 + q < nch) v[q] = ldg4(Ji + 128 * (c0 + q));
+              if (c0 + q < nch) v[q] = H ? ldg4h(Ji16 + 128 * (c0 + q)) : ldg4(Ji + 128 * (c0 + q));
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
               if (c0 + q < nch) {
@@ -375,8 +386,8 @@ int batch_default_variant() {
 }
 
 template <int W, int MINB, int GROUP>
-cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStream_t st) {
-  auto kern = sa_batch_kernel<W, MINB, GROUP>;
+cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStream_t st, bool h) {
+  auto kern = h ? sa_batch_kernel<W, MINB, GROUP, true> : sa_batch_kernel<W, MINB, GROUP, false>;
   const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4);  // FP32 fields + spin words
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -417,6 +428,7 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.rep0 = rb.rep0;
   a.fstride = fstride;
   a.swstride = 32 * ((fstride / 128 + 7) / 8);
+  a.J16 = b->j16 ? b->d_J16.as<__half>() : nullptr;
   a.F = d_fields;
   a.foff = d_foff;
   if (b->count == 0 || max_reads <= 0 || nitems <= 0) return cudaSuccess;
@@ -431,12 +443,12 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   switch (variant) {
-    case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st); break;
-    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st); break;
-    case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st); break;
-    case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st); break;
-    case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st); break;
-    default: e = launch_variant<32, 1, 4>(a, nitems, sm_count, st); break;
+    case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st, b->j16); break;
+    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st, b->j16); break;
+    case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st, b->j16); break;
+    case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st, b->j16); break;
+    case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st, b->j16); break;
+    default: e = launch_variant<32, 1, 4>(a, nitems, sm_count, st, b->j16); break;
   }
   if (e == cudaSuccess && launches) ++*launches;
   return e;
