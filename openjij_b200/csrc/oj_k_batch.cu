@@ -25,7 +25,8 @@
 // index (rep0 + index within the instance).
 //
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
-// read through L1 one float4 per lane on every accepted flip.  The initial
+// read through L1 one float4 per lane on every accepted flip, or from an FP16
+// copy (8 bytes per lane) when FP16 holds every coupling exactly.  The initial
 // fields come from batch_field_kernel, launched just before (it reads J once
 // per 64 replicas), through a global buffer of reads x padded n floats per
 // instance.
@@ -109,7 +110,6 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     const int nch = (n + 127) >> 7;
     const int npad = nch << 7;
     const float* J = a.J + a.joff[m];
-    const float* h = a.h + a.hoff[m];
     int8_t* gs = a.spins + a.soff[m] + (size_t)(active ? r : 0) * n;
     // spins -> bits
     if (active)
