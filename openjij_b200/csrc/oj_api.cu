@@ -475,6 +475,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   int launches = 0;
   int P_used = 0, threads_used = 0, variant_used = 0;
   bool tuned_now = false;
+  bool energies_in_kernel = false;  // the dense jump kernel wrote them (exact fields)
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED) {
@@ -621,10 +622,21 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       items = make_items(batch_variant_warps(variant));
     }
     OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
+    // exact FP32 fields: the sweep kernel writes the energies (its eoff table is d_soff, zero)
+    double* d_ek = nullptr;
+    if (energies && S > 0 && g->single->exact_fields) {
+      d_ek = energies;
+      if (!devp) {
+        OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
+        d_ek = ctx->energies.as<double>();
+      }
+      energies_in_kernel = true;
+    }
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
       OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(items.size() / 2), d_counter, d_spins,
-                            d_beta, S, rb, 0, ctx->sm_count, st, &launches, variant, d_fields, d_foff, R),
+                            d_beta, S, rb, 0, ctx->sm_count, st, &launches, variant, d_fields, d_foff, R, d_ek,
+                            d_soff),
             "sa dense jump kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     threads_used = batch_variant_warps(variant) * 32;
@@ -646,7 +658,11 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     }
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   }
-  if (energies) {
+  if (energies && energies_in_kernel) {
+    if (!devp)
+      OJ_CK(cudaMemcpyAsync(energies, ctx->energies.as<double>(), (size_t)R * 8, cudaMemcpyDeviceToHost, st),
+            "D2H energies");
+  } else if (energies) {
     double* d_e = energies;
     if (!devp) {
       OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
@@ -1043,7 +1059,41 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
     }
     std::memcpy(J64.data() + j64off[k], A, (size_t)(n1 * n1) * sizeof(double));
   }
+  // The FP32 fields are exact when every coupling and field is a multiple of
+  // 2^-p and no field can reach 2^(24-p): then the sweep kernel's fields give
+  // the FP64 energies exactly, E = 1/2 sum_i s_i (f_i + h_i).
+  bool exact = true;
+  int pmax = 0;
+  double maxrow = 0.0;
+  auto grid_p = [](double v) {  // smallest p <= 24 with v 2^p an integer, -1 if none
+    for (int p = 0; p <= 24; ++p) {
+      const double x = std::ldexp(v, p);
+      if (x == std::floor(x)) return p;
+    }
+    return -1;
+  };
+  for (int32_t k = 0; k < count && exact; ++k) {
+    const int64_t nk = n[k], n1 = nk + 1;
+    const double* A = J_aug + offset[k];
+    for (int64_t i = 0; i < nk && exact; ++i) {
+      double row = 0.0;
+      for (int64_t j = 0; j < n1; ++j) {
+        const double v = A[i * n1 + j];
+        if (v == 0.0) continue;
+        const int p = grid_p(v);
+        if (p < 0) {
+          exact = false;
+          break;
+        }
+        pmax = std::max(pmax, p);
+        row += std::fabs(v);
+      }
+      maxrow = std::max(maxrow, row);
+    }
+  }
+  exact = exact && std::ldexp(maxrow, pmax) < 16777216.0;
   std::unique_ptr<oj_batch> b(new oj_batch());
+  b->exact_fields = exact;
   b->device = ctx->device;
   b->count = count;
   b->max_n = max_n;
@@ -1226,19 +1276,29 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     nitems = (int)(items.size() / 2);
     OJ_CK(cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "H2D items");
   }
-  OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-  if (S > 0 && nitems > 0)
-    OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
-                          (uint32_t)instance_offset, ctx->sm_count, st, &launches,
-                          bm->tuned_variant ? bm->tuned_variant : variant0, d_fields, d_foff, max_reads),
-          "sa batched kernel");
-  OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  // exact FP32 fields: the sweep kernel writes the energies of the replicas it
+  // anneals (every instance with n > 0 has items); instances with n = 0 have E = 0
+  double* d_e = nullptr;
   if (energies) {
-    double* d_e = devp ? energies : nullptr;
+    d_e = devp ? energies : nullptr;
     if (!d_e) {
       OJ_CK(ctx->energies.ensure((size_t)nrep * 8), "alloc energies");
       d_e = ctx->energies.as<double>();
     }
+  }
+  const bool energies_in_kernel = energies && S > 0 && nitems > 0 && b->exact_fields;
+  if (energies_in_kernel) OJ_CK(cudaMemsetAsync(d_e, 0, (size_t)nrep * 8, st), "energies of empty instances");
+  OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+  if (S > 0 && nitems > 0)
+    OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
+                          (uint32_t)instance_offset, ctx->sm_count, st, &launches,
+                          bm->tuned_variant ? bm->tuned_variant : variant0, d_fields, d_foff, max_reads,
+                          energies_in_kernel ? d_e : nullptr, d_eoff),
+          "sa batched kernel");
+  OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+  if (energies_in_kernel) {
+    if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)nrep * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+  } else if (energies) {
     const int ns = batch_energy_splits(b, max_reads, ctx->sm_count);
     if (ns > 1) OJ_CK(ctx->eparts.ensure((size_t)ns * nrep * 8), "alloc energy parts");
     OJ_CK(launch_batch_energy(b, d_reads, d_soff, d_eoff, d_order, max_reads, d_spins, d_e, st, ns,

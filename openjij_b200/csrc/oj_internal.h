@@ -122,6 +122,7 @@ struct oj_batch {
   oj::DevBuf d_J, d_h, d_J64, d_joff, d_hoff, d_j64off, d_n;
   oj::DevBuf d_J16;   // J as FP16 when every coupling's FP32 value is exactly an FP16 value (flip rows)
   bool j16 = false;
+  bool exact_fields = false;  // FP32 fields exact: energies from the fields (sweep kernel epilogue)
   int tuned_variant = 0;  // autotuned register-budget variant, 0 = not tuned
   ~oj_batch();
 };
@@ -190,7 +191,8 @@ int batch_default_variant();
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads);
+                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads,
+                            double* d_energies = nullptr, const int64_t* d_eoff = nullptr);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep);

@@ -70,6 +70,8 @@ struct BatchArgs {
   const __half* J16;       // J as FP16 (same offsets), when every value is exact in FP16
   const float* F;          // initial fields, [reads][npad] per instance (batch_field_kernel)
   const int64_t* foff;     // [count] offset of instance m's fields (floats)
+  double* E;               // FP64 energies from the final fields, or null (exact-field batches)
+  const int64_t* eoff;     // [count] offset of instance m's energies
 };
 
 // Spin bits of chunk c of lane l: four bits of word 32*(c/8) + l.
@@ -193,6 +195,25 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           __syncwarp();
         }
       }
+    }
+    if (a.E) {
+      // exact fields: E = 1/2 sum_i s_i (f_i + h_i), every term and partial sum
+      // exact in FP64, so the result is the FP64 energy in any order
+      const float* h = a.h + a.hoff[m];
+      double e = 0.0;
+      for (int c = 0; c < nch; ++c) {
+        const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
+        const float4 h4 = ldg4(h + 128 * c + 4 * lane);
+        const float fv[4] = {f4.x, f4.y, f4.z, f4.w}, hv[4] = {h4.x, h4.y, h4.z, h4.w};
+        const uint32_t w = sw[sw_word(c, lane)] >> sw_shift(c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double t = (double)fv[q] + (double)hv[q];
+          if (128 * c + 4 * lane + q < n) e += ((w >> q) & 1u) ? -t : t;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+      if (lane == 0) a.E[a.eoff[m] + r] = 0.5 * e;
     }
     for (int c = 0; c < nch; ++c) {
       const uint32_t w = sw[sw_word(c, lane)] >> sw_shift(c);
@@ -403,7 +424,8 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads) {
+                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads,
+                            double* d_energies, const int64_t* d_eoff) {
   if (variant == 0) variant = batch_default_variant();
   if (!batch_variant_valid(variant)) return cudaErrorInvalidValue;
   const int fstride = std::max(128, (b->max_n + 127) / 128 * 128);
@@ -431,6 +453,8 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.J16 = b->j16 ? b->d_J16.as<__half>() : nullptr;
   a.F = d_fields;
   a.foff = d_foff;
+  a.E = b->exact_fields ? d_energies : nullptr;
+  a.eoff = d_eoff;
   if (b->count == 0 || max_reads <= 0 || nitems <= 0) return cudaSuccess;
   const int zt = (max_reads + kFieldReplicas - 1) / kFieldReplicas;
   cudaError_t e = cudaSuccess;
