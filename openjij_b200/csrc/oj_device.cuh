@@ -97,10 +97,11 @@ __device__ __forceinline__ uint32_t pick(const u4& v, int j) {
 }
 
 // -ln(u), u = (2*(x>>9)+1) * 2^-24 in (0,1).  u = m*2^e with m reduced to
-// [sqrt(1/2), sqrt(2)]; ln m = 2 atanh(z), z = (m-1)/(m+1), series through
-// z^9 (truncation error < 1e-9).  Each step is a single IEEE round-to-nearest
-// operation (explicit _rn intrinsics, no contraction), so host code doing the
-// same operations reproduces the bits.
+// [sqrt(1/2), sqrt(2)]; ln m = t + t^2 Q(t), t = m - 1, Q a degree-6
+// polynomial fitted by least squares at Chebyshev nodes to (ln(1+t) - t)/t^2
+// (error below 6e-8, no division).  Each step is a single IEEE
+// round-to-nearest operation (explicit _rn intrinsics, no contraction), so
+// host code doing the same operations reproduces the bits.
 __device__ __forceinline__ float neglog(uint32_t x) {
   const uint32_t k = x >> 9;
   const float u = __fmul_rn(__uint2float_rn(2u * k + 1u), 0x1p-24f);
@@ -111,16 +112,16 @@ __device__ __forceinline__ float neglog(uint32_t x) {
     m = __fmul_rn(m, 0.5f);
     e += 1;
   }
-  const float num = __fsub_rn(m, 1.0f);
-  const float den = __fadd_rn(m, 1.0f);
-  const float z = __fdiv_rn(num, den);
-  const float z2 = __fmul_rn(z, z);
-  float p = __fmaf_rn(z2, 0x1.c71c72p-4f, 0x1.24924ap-3f);
-  p = __fmaf_rn(p, z2, 0x1.99999ap-3f);
-  p = __fmaf_rn(p, z2, 0x1.555556p-2f);
-  const float tz = __fmul_rn(z2, p);
-  const float z2x = __fadd_rn(z, z);
-  const float lnm = __fmaf_rn(z2x, tz, z2x);
+  const float t = __fsub_rn(m, 1.0f);
+  const float t2 = __fmul_rn(t, t);
+  float q = -0x1.8e99cep-4f;
+  q = __fmaf_rn(q, t, 0x1.4c9576p-3f);
+  q = __fmaf_rn(q, t, -0x1.6420eep-3f);
+  q = __fmaf_rn(q, t, 0x1.979cccp-3f);
+  q = __fmaf_rn(q, t, -0x1.ff1d5ep-3f);
+  q = __fmaf_rn(q, t, 0x1.5558fcp-2f);
+  q = __fmaf_rn(q, t, -0x1.0000ecp-1f);
+  const float lnm = __fmaf_rn(t2, q, t);
   const float lnu = __fmaf_rn(__int2float_rn(e), 0x1.62e430p-1f, lnm);
   return -lnu;
 }

@@ -220,9 +220,10 @@ inline uint32_t b_of(float f) {
 }
 
 // -ln(u) for u = (2*(x>>9)+1) * 2^-24, by m*2^e reduction to [sqrt(1/2),
-// sqrt(2)] and the series ln m = 2 atanh(z), z = (m-1)/(m+1), through z^9.
-// Every step is one IEEE round-to-nearest operation, so this and the device
-// copy give the same bits.
+// sqrt(2)] and ln m = t + t^2 Q(t), t = m - 1, Q a degree-6 polynomial fitted
+// by least squares at Chebyshev nodes to (ln(1+t) - t) / t^2 (no division;
+// error below 6e-8).  Every step is one IEEE round-to-nearest operation, so
+// this and the device copy give the same bits.
 float neglog(uint32_t x) {
   const uint32_t k = x >> 9;
   const float u = (float)(2u * k + 1u) * 0x1p-24f;
@@ -233,16 +234,16 @@ float neglog(uint32_t x) {
     m = m * 0.5f;
     e += 1;
   }
-  const float num = m - 1.0f;
-  const float den = m + 1.0f;
-  const float z = num / den;
-  const float z2 = z * z;
-  float p = ORC_FMAF(z2, 0x1.c71c72p-4f, 0x1.24924ap-3f);
-  p = ORC_FMAF(p, z2, 0x1.99999ap-3f);
-  p = ORC_FMAF(p, z2, 0x1.555556p-2f);
-  const float tz = z2 * p;
-  const float z2x = z + z;
-  const float lnm = ORC_FMAF(z2x, tz, z2x);
+  const float t = m - 1.0f;
+  const float t2 = t * t;
+  float q = -0x1.8e99cep-4f;
+  q = ORC_FMAF(q, t, 0x1.4c9576p-3f);
+  q = ORC_FMAF(q, t, -0x1.6420eep-3f);
+  q = ORC_FMAF(q, t, 0x1.979cccp-3f);
+  q = ORC_FMAF(q, t, -0x1.ff1d5ep-3f);
+  q = ORC_FMAF(q, t, 0x1.5558fcp-2f);
+  q = ORC_FMAF(q, t, -0x1.0000ecp-1f);
+  const float lnm = ORC_FMAF(t2, q, t);
   const float lnu = ORC_FMAF((float)e, 0x1.62e430p-1f, lnm);
   return -lnu;
 }
