@@ -665,7 +665,10 @@ std::vector<int8_t> parse_spins(const py::handle& obj, size_t n, int* R_out) {
 template <class G>
 struct ClassicalIsing {
   ClassicalIsing(const py::object& init, const G& g) : graph(snapshot(g)), num_spins(g.size()) { reset(init); }
-  void reset(const py::object& init) { spins = parse_spins(init, num_spins, &R); }
+  void reset(const py::object& init) {
+    spins = parse_spins(init, num_spins, &R);
+    ecache_valid = false;
+  }
   py::array_t<double> get_spin() const {
     std::vector<ssize_t> shape = R == 1 ? std::vector<ssize_t>{(ssize_t)num_spins + 1}
                                         : std::vector<ssize_t>{R, (ssize_t)num_spins + 1};
@@ -684,6 +687,10 @@ struct ClassicalIsing {
       std::fill(out.mutable_data(), out.mutable_data() + R, 0.0);
       return out;
     }
+    if (ecache_valid && ecache.size() == (size_t)R) {  // from the last run's own call
+      std::copy(ecache.begin(), ecache.end(), out.mutable_data());
+      return out;
+    }
     oj_graph* dg = graph->device();
     const int8_t* sp = spins.data();
     double* e = out.mutable_data();
@@ -693,6 +700,9 @@ struct ClassicalIsing {
   std::shared_ptr<G> graph;
   size_t num_spins;
   int R = 1;
+  // energies of the current spins, written by the run call that produced them
+  std::vector<double> ecache;
+  bool ecache_valid = false;
   std::vector<int8_t> spins;
 };
 
@@ -814,6 +824,7 @@ template <class G>
 void run_classical(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<ClassicalSchedule>& sched,
                    const std::function<void(const ClassicalIsing<G>&, double)>& cb) {
   g_last_run = RunInfo();
+  sys.ecache_valid = false;
   if (sys.num_spins == 0 || sched.empty()) {
     if (cb)
       for (auto& s : sched)
@@ -834,10 +845,12 @@ void run_classical(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<Clas
     oj_status rc;
     {
       py::gil_scoped_release release;
+      sys.ecache.resize((size_t)sys.R);
       rc = oj_sa_run(ctx(), dg, sys.R, sys.spins.data(), betas.data(), mcs.data(), (int32_t)betas.size(), seed, 0, 0,
-                     flags, nullptr, &st);
+                     flags, sys.ecache.data(), &st);
     }
     check(rc, "Algorithm_SingleSpinFlip_run");
+    sys.ecache_valid = true;
     record(st);
     return;
   }
@@ -868,6 +881,7 @@ template <class G>
 void run_swendsen_wang(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<ClassicalSchedule>& sched,
                        const std::function<void(const ClassicalIsing<G>&, double)>& cb) {
   g_last_run = RunInfo();
+  sys.ecache_valid = false;
   if (sys.num_spins == 0 || sched.empty()) {
     if (cb)
       for (auto& s : sched)
@@ -887,10 +901,12 @@ void run_swendsen_wang(ClassicalIsing<G>& sys, uint64_t seed, const std::vector<
     oj_status rc;
     {
       py::gil_scoped_release release;
+      sys.ecache.resize((size_t)sys.R);
       rc = oj_sw_run(ctx(), dg, sys.R, sys.spins.data(), betas.data(), mcs.data(), (int32_t)betas.size(), seed, 0, 0,
-                     0, nullptr, &st);
+                     0, sys.ecache.data(), &st);
     }
     check(rc, "Algorithm_SwendsenWang_run");
+    sys.ecache_valid = true;
     record(st);
     return;
   }

@@ -1,7 +1,6 @@
 // C ABI entry points (include/openjij_b200.h): context, graph upload, the SA
 // and SQA runs with their planner, FP64 energies.  No exception crosses the
 // ABI; every CUDA error becomes a status with a message in the context.
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -148,7 +147,7 @@ void sqa_msc_thresholds(const std::vector<float2>& coef, double c, int D, std::v
 }
 
 oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset, const double* J_aug,
-                      oj_batch** out);
+                      oj_batch** out, bool checked = false);
 
 // The graph's augmented matrix as a one-instance batch: FP32 padded rows for
 // the dense jump kernel and the FP64 matrix for the replica-parallel energies.
@@ -168,7 +167,7 @@ oj_status ensure_single(oj_ctx* ctx, oj_graph* g) {
   const int32_t nn = n;
   const int64_t off = 0;
   oj_batch* b1 = nullptr;
-  if (oj_status bs = build_batch(ctx, 1, &nn, &off, A.data(), &b1)) return bs;
+  if (oj_status bs = build_batch(ctx, 1, &nn, &off, A.data(), &b1, true)) return bs;  // the graph is validated
   g->single.reset(b1);
   return OJ_OK;
 }
@@ -1014,7 +1013,7 @@ oj_status oj_batch_create_dense(oj_ctx* ctx, int32_t count, const int32_t* n, co
 
 namespace {
 oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_t* offset, const double* J_aug,
-                      oj_batch** out) {
+                      oj_batch** out, bool checked) {
   if (!ctx || !out || count < 0 || (count > 0 && (!n || !offset || !J_aug)))
     return arg_fail(ctx, "null argument or negative size");
   *out = nullptr;
@@ -1048,7 +1047,7 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
     const double* A = J_aug + offset[k];
     // graph::Dense::set_interaction_matrix checks (dense.hpp:117-140)
     if (A[nk * n1 + nk] != 1.0) return arg_fail(ctx, "the corner of an augmented matrix must be 1");
-    for (int64_t i = 0; i < n1; ++i) {
+    for (int64_t i = 0; i < n1 && !checked; ++i) {
       if (i < nk && A[i * n1 + i] != 0.0) return arg_fail(ctx, "the diagonal of J must be zero (h goes in column n)");
       for (int64_t j = i + 1; j < n1; ++j)
         if (A[i * n1 + j] != A[j * n1 + i]) return arg_fail(ctx, "an augmented matrix is not symmetric");
@@ -1065,12 +1064,14 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
   bool exact = true;
   int pmax = 0;
   double maxrow = 0.0;
-  auto grid_p = [](double v) {  // smallest p <= 24 with v 2^p an integer, -1 if none
-    for (int p = 0; p <= 24; ++p) {
-      const double x = std::ldexp(v, p);
-      if (x == std::floor(x)) return p;
-    }
-    return -1;
+  auto grid_p = [](double v) {  // smallest p >= 0 with v 2^p an integer (v != 0), from its bits
+    uint64_t bits;
+    std::memcpy(&bits, &v, 8);
+    const int ex = (int)((bits >> 52) & 0x7FF);
+    if (ex == 0 || ex == 0x7FF) return 1000;  // subnormal, inf, nan
+    const uint64_t mant = (bits & ((1ull << 52) - 1)) | (1ull << 52);
+    const int low = ex - 1075 + __builtin_ctzll(mant);  // v = odd * 2^low
+    return low >= 0 ? 0 : -low;
   };
   for (int32_t k = 0; k < count && exact; ++k) {
     const int64_t nk = n[k], n1 = nk + 1;
@@ -1081,7 +1082,7 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
         const double v = A[i * n1 + j];
         if (v == 0.0) continue;
         const int p = grid_p(v);
-        if (p < 0) {
+        if (p > 24) {
           exact = false;
           break;
         }
@@ -1109,13 +1110,26 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
   // (integer and quarter-integer couplings of moderate size): the kernel
   // widens them back to the same FP32 values
   {
-    std::vector<__half> J16(J32.size());
-    bool exact = true;
-    for (size_t q = 0; q < J32.size() && exact; ++q) {
-      J16[q] = __float2half_rn(J32[q]);
-      exact = __half2float(J16[q]) == J32[q];
+    // an FP32 value is an FP16 normal (or zero) when its exponent is within
+    // [-14, 15] and its low 13 mantissa bits are zero; the FP16 bits are then
+    // the sign, the rebiased exponent and the top 10 mantissa bits
+    std::vector<uint16_t> J16(J32.size());
+    bool exact16 = true;
+    for (size_t q = 0; q < J32.size() && exact16; ++q) {
+      uint32_t u;
+      std::memcpy(&u, &J32[q], 4);
+      if ((u & 0x7FFFFFFFu) == 0) {
+        J16[q] = (uint16_t)(u >> 16);
+        continue;
+      }
+      const int ex = (int)((u >> 23) & 0xFF) - 127;
+      if (ex < -14 || ex > 15 || (u & 0x1FFFu) != 0) {
+        exact16 = false;
+        break;
+      }
+      J16[q] = (uint16_t)(((u >> 16) & 0x8000u) | ((uint32_t)(ex + 15) << 10) | ((u >> 13) & 0x3FFu));
     }
-    if (exact) {
+    if (exact16) {
       OJ_CK(up(b->d_J16, J16.data(), J16.size() * 2), "upload J16");
       b->j16 = true;
     }

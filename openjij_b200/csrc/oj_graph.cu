@@ -160,7 +160,7 @@ oj_status finish_graph(oj_ctx* ctx, oj_graph* g) {
         row.emplace_back(j, dv[q]);
       }
     }
-    std::sort(row.begin(), row.end());
+    if (!std::is_sorted(row.begin(), row.end())) std::sort(row.begin(), row.end());
     for (size_t a = 0; a < row.size(); ++a) {
       if (a + 1 < row.size() && row[a + 1].first == row[a].first) {
         row[a + 1].second += row[a].second;  // duplicate entries are summed (scipy semantics)
@@ -171,18 +171,26 @@ oj_status finish_graph(oj_ctx* ctx, oj_graph* g) {
     }
     g->rp[i + 1] = (int32_t)g->ci.size();
   }
-  // symmetry check: J_ij == J_ji
+  // symmetry check: J_ij == J_ji.  The transpose, built by counting sort,
+  // has its rows in ascending column order like the rows themselves, so the
+  // matrix is symmetric exactly when both CSR arrays coincide.
   {
+    const size_t nnz = g->ci.size();
+    std::vector<int32_t> tp(n + 1, 0), tci(nnz);
+    std::vector<double> tv(nnz);
+    for (size_t q = 0; q < nnz; ++q) ++tp[g->ci[q] + 1];
+    for (int i = 0; i < n; ++i) tp[i + 1] += tp[i];
+    std::vector<int32_t> fill(tp.begin(), tp.end() - 1);
     for (int i = 0; i < n; ++i)
       for (int q = g->rp[i]; q < g->rp[i + 1]; ++q) {
-        const int j = g->ci[q];
-        const auto b = g->ci.begin() + g->rp[j], e = g->ci.begin() + g->rp[j + 1];
-        const auto it = std::lower_bound(b, e, i);
-        if (it == e || *it != i || g->val64[it - g->ci.begin()] != g->val64[q]) {
-          ctx->last_error = "interaction matrix must be symmetric (as returned by get_interactions())";
-          return OJ_ERR_ARG;
-        }
+        const int32_t at = fill[g->ci[q]]++;
+        tci[at] = i;
+        tv[at] = g->val64[q];
       }
+    if (tp != g->rp || tci != g->ci || tv != g->val64) {
+      ctx->last_error = "interaction matrix must be symmetric (as returned by get_interactions())";
+      return OJ_ERR_ARG;
+    }
   }
   g->val.resize(g->val64.size());
   for (size_t q = 0; q < g->val64.size(); ++q) g->val[q] = (float)g->val64[q];
