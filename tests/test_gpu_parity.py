@@ -394,3 +394,26 @@ def test_swendsen_wang_large_graph_global_forest(ctx):
     s = s0.copy()
     N.sw_run(dg, s, betas, mcs, seed=21)
     np.testing.assert_array_equal(s, O.replay_sw(g, s0, _per_sweep(betas, mcs), 21))
+
+
+def test_graph_validation(ctx):
+    """Graph upload: an asymmetric matrix, a non-zero diagonal and a corner
+    other than 1 are refused; unsorted rows and repeated entries (summed, as
+    scipy does) are taken."""
+    def csr(rows, n):
+        indptr, indices, data = [0], [], []
+        for r in rows:
+            for j, v in r:
+                indices.append(j)
+                data.append(v)
+            indptr.append(len(indices))
+        return (n, np.array(indptr, np.int64), np.array(indices, np.int32), np.array(data, np.float64))
+    good = [[(2, 0.5), (1, -1.0)], [(0, -1.0), (2, 0.5), (2, 0.5)], [(1, 1.0), (0, 0.5)], [(3, 1.0)]]
+    g = N.Graph(ctx, *csr(good, 3))
+    assert g.info()["nnz"] == 6
+    for bad in ([[(1, -1.0)], [(0, -2.0)], [], [(3, 1.0)]],  # J_01 != J_10
+                [[(0, 1.0)], [], [], [(3, 1.0)]],             # diagonal
+                [[], [], [], [(3, 2.0)]]):                    # corner
+        with pytest.raises(N.OJError) as ei:
+            N.Graph(ctx, *csr(bad, 3))
+        assert ei.value.status == N.OJ_ERR_ARG
