@@ -196,6 +196,26 @@ def cpu_reference(m, betas, mcs, reads, threads):
     return attempts / dt, dt
 
 
+def cpu_reference_sw(m, betas, mcs, reads, threads, max_sweeps=200):
+    """OpenJij's Swendsen-Wang updater on the CPU (oracle restatement of
+    updater/swendsen_wang.hpp): ``reads`` reads, one per host thread, over at
+    most ``max_sweeps`` sweeps of the schedule; returns spin updates/s."""
+    from oracle import oracle as O
+    g = O.AugCSR(m)
+    k, acc = 0, 0
+    while k < len(mcs) and acc + int(mcs[k]) <= max_sweeps:
+        acc += int(mcs[k])
+        k += 1
+    k = max(k, 1)
+    rng = np.random.default_rng(0)
+    init = rng.choice(np.array([-1, 1], np.int8), size=(reads, g.n))
+    seeds = np.arange(1, reads + 1, dtype=np.uint64)
+    t0 = time.perf_counter()
+    O.ref_sw_many(g, init, betas[:k], mcs[:k], seeds, threads=threads)
+    dt = time.perf_counter() - t0
+    return reads * g.n * float(np.sum(mcs[:k])) / dt, dt
+
+
 def cpu_reference_sqa(w, threads):
     """OpenJij's CPU SQA path (oracle restatement): one read per thread on a
     bounded number of sweeps (at most 100) of the workload's schedule."""
@@ -243,6 +263,8 @@ def run_reference(args):
     batch_count = [0]
 
     def one():
+        if w["kind"] == "sa" and args.kernel == "swendsen_wang":
+            return cpu_reference_sw(w["matrix"], w["betas"], w["mcs"], reads, threads)
         if w["kind"] == "sa":
             return cpu_reference(w["matrix"], w["betas"], w["mcs"], reads, threads)
         if w["kind"] == "batch":
@@ -260,6 +282,9 @@ def run_reference(args):
     value = float(np.mean(vals))
     sweeps = min(int(np.sum(w["mcs"])), 100) if w["kind"] == "sqa" else int(np.sum(w["mcs"]))
     sample = f"{reads} reads x {sweeps} sweeps of {w['name']} per step, one read per host thread"
+    if w["kind"] == "sa" and args.kernel == "swendsen_wang":
+        sample = (f"{reads} reads of the Swendsen-Wang updater over at most 200 sweeps of {w['name']}'s schedule "
+                  f"per step, one read per host thread")
     if w["kind"] == "batch":
         sample = (f"the first {batch_count[0]} instances of {w['name']}, {reads} reads x {sweeps} sweeps each "
                   f"per step, one read per host thread")
@@ -281,6 +306,10 @@ def _algo_per_attempt(w, n, kernel, degree, R=1):
     """Algorithmic bytes (state-bound kernels) or flops (dense kernels) per
     attempt, and the bytes the kernel's own layout moves per attempt (None for
     the dense kernels)."""
+    if kernel == "swendsen_wang":
+        # per spin update: its d/2 bonds of the shared bond list (two endpoints,
+        # |J| and a sign: 13 B each) and the spin read and write
+        return 13.0 * degree / 2.0 + 2.0, "GB/s", None
     if w["config"] == 2:
         return ALGO_BYTES_PER_ATTEMPT + 0.5 / R, "GB/s", PACKED_BYTES_PER_ATTEMPT
     if w["kind"] == "sqa":
@@ -438,6 +467,8 @@ def run_ours(args):
     rep0 = 0  # every rank runs its own full workload (weak scaling)
 
     def run(spins, seed, device, en):
+        if kernel == "swendsen_wang":  # the cluster updater (oj_sw_run), on the same workload
+            return N.sw_run(graph, spins, betas, mcs, seed=seed, energies=en, device=device, replica_offset=rep0)
         if w["kind"] == "sa":
             return N.sa_run(graph, spins, betas, mcs, seed=seed, energies=en, device=device, kernel=kernel,
                             replica_offset=rep0, tune=True)
@@ -505,7 +536,13 @@ def run_ours(args):
         achieved = attempts_per_step * per / (kms / 1000.0) / 1e12
         peak, peak_kind = _tensor_peak()
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu and w["kind"] == "sa":
+    if rank == 0 and ws == 1 and not args.no_cpu and used_kernel == "swendsen_wang":
+        threads = os.cpu_count() or 1
+        v, dt = cpu_reference_sw(w["matrix"], betas, mcs, threads, threads)
+        cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
+               "sample": f"{threads} reads of the Swendsen-Wang updater, at most 200 sweeps of the schedule, "
+                         f"one read per host thread, {dt:.1f} s"}
+    elif rank == 0 and ws == 1 and not args.no_cpu and w["kind"] == "sa":
         threads = os.cpu_count() or 1
         v, dt = cpu_reference(w["matrix"], betas, mcs, threads, threads)
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
@@ -535,12 +572,16 @@ def run_ours(args):
                                   "a fraction of the int8 count, so frac can pass 1) and is integer-issue "
                                   "bound (profiles/)")
                          if unit == "GB/s" and packed is not None else
+                         ("bond-list bytes per spin update (d/2 bonds of 13 B, spin read and write) against the "
+                          "HBM copy peak; union-find in shared memory, latency bound")
+                         if used_kernel == "swendsen_wang" else
                          "algorithmic int8 state bytes per attempt against the HBM copy peak"
                          if unit == "GB/s" else
                          ("algorithmic 2n flop per attempt against the BF16 tensor peak; the dense "
                           "kernels update a field row only on accepted flips (profiles/)"),
                          "frac": achieved / peak,
-                         "traffic": _traffic_from_profiles() if args.config == 2 else None,
+                         "traffic": _traffic_from_profiles() if args.config == 2 and used_kernel == "bitpacked"
+                         else None,
                          "peak_kind": peak_kind, "kernel_ms": kms,
                          "algorithmic_per_attempt": per, "layout_bytes_per_attempt": packed},
             "cpu_baseline": cpu,
@@ -688,7 +729,8 @@ def main():
     ap.add_argument("--config", type=int, default=2,
                     help="benchmark configuration 1-5 (default 2: the L=128 +-J lattice)")
     ap.add_argument("--kernel", default=None,
-                    help="force a kernel: colour, dense_plain, bitpacked, dense_tc (default: planner)")
+                    help="force a kernel: colour, dense_plain, bitpacked, dense_tc, dense_jump, or "
+                         "swendsen_wang for the cluster updater (default: planner)")
     ap.add_argument("--tts", action="store_true",
                     help="time-to-1%%-energy of the batched/mixed kernel vs the plain kernel (configs 3-5)")
     args = ap.parse_args()
