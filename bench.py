@@ -167,6 +167,10 @@ def _workload(config, sweeps=None, replicas=None):
                  bound="tensor", mats=mats, reads=np.full(len(mats), reads, np.int32), betas=betas, mcs=mcs,
                  replicas=reads, sweeps=S)
         return w
+    elif config == 6:  # the lattice adapters: a Chimera lattice with fields, on the colour-class kernel
+        m, _ = I.chimera_pm_j(16, seed=6, field=0.5)
+        S, R, bmin, bmax = 1000, 1024, 0.1, 5.0
+        w.update(name="chimera_L16_pm_j_fields_R1024_S1000", kernel="auto", bound="hbm")
     else:
         raise SystemExit(f"unknown config {config}")
     S = sweeps or S
@@ -312,6 +316,10 @@ def _algo_per_attempt(w, n, kernel, degree, R=1):
         return 13.0 * degree / 2.0 + 2.0, "GB/s", None
     if w["config"] == 2:
         return ALGO_BYTES_PER_ATTEMPT + 0.5 / R, "GB/s", PACKED_BYTES_PER_ATTEMPT
+    if kernel == "colour" and w["kind"] == "sa":
+        # per attempt: the site's CSR row (column index and FP32 coupling, 8 B per
+        # neighbour) and the spin read and write
+        return 8.0 * degree + 2.0, "GB/s", None
     if w["kind"] == "sqa":
         # int8: d spatial + 2 Trotter neighbours + own read + write
         packed = (2 + degree) * 4.0 / (w["T"] / 2.0) if kernel == "bitpacked" else None
@@ -726,8 +734,8 @@ def main():
     ap.add_argument("--sweeps", type=int, default=None,
                     help="smaller case for profiling (default: the full 2000-sweep workload)")
     ap.add_argument("--replicas", type=int, default=None, help="smaller case for profiling")
-    ap.add_argument("--config", type=int, default=2,
-                    help="benchmark configuration 1-5 (default 2: the L=128 +-J lattice)")
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5, 6],
+                    help="benchmark configuration 1-6 (default 2: the L=128 +-J lattice; 6: a Chimera lattice)")
     ap.add_argument("--kernel", default=None,
                     help="force a kernel: colour, dense_plain, bitpacked, dense_tc, dense_jump, or "
                          "swendsen_wang for the cluster updater (default: planner)")

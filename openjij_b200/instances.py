@@ -76,6 +76,35 @@ def lattice_pm_j(L: int, seed: int = 2):
     return augmented_from_ising(np.zeros(n), (lo, hi, v), n), 0.0
 
 
+def chimera_pm_j(L: int, seed: int = 6, field: float = 0.0):
+    """L x L Chimera lattice (unit cells of 8, site 8 L r + 8 c + z, open
+    edges as cxxjij.graph.Chimera builds it): sites 0-3 of a cell couple to
+    4-7 of the same cell and to the same site of the cells above and below,
+    sites 4-7 to the same site of the cells left and right; J in {-1,+1}
+    (p = 1/2), fields uniform in [-field, field]."""
+    rng = np.random.default_rng(seed)
+    ind = lambda r, c, z: 8 * L * r + 8 * c + z  # noqa: E731
+    a, b = [], []
+    for r in range(L):
+        for c in range(L):
+            for z in range(4):
+                for w in range(4, 8):
+                    a.append(ind(r, c, z))
+                    b.append(ind(r, c, w))
+                if r + 1 < L:
+                    a.append(ind(r, c, z))
+                    b.append(ind(r + 1, c, z))
+            for z in range(4, 8):
+                if c + 1 < L:
+                    a.append(ind(r, c, z))
+                    b.append(ind(r, c + 1, z))
+    a, b = np.array(a), np.array(b)
+    n = 8 * L * L
+    v = rng.choice([-1.0, 1.0], size=a.size)
+    h = rng.uniform(-field, field, n) if field else np.zeros(n)
+    return augmented_from_ising(h, (np.minimum(a, b), np.maximum(a, b), v), n), 0.0
+
+
 def random_regular_pm_j(n: int, d: int = 3, seed: int = 4, max_tries: int = 1000):
     """Random d-regular graph (configuration model, multi-edges and loops
     rejected), J in {-1,+1} (p = 1/2), h = 0."""
