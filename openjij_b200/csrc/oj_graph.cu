@@ -85,6 +85,35 @@ std::vector<int32_t> greedy_colouring(int n, const std::vector<int32_t>& rp, con
   return col;
 }
 
+// Two colours for a bipartite graph: the smallest site of every component gets
+// colour 0 and the others alternate along a breadth-first search (on a graph
+// the greedy colouring already 2-colours, this is that colouring); false when
+// an odd cycle shows up.
+bool two_colouring(int n, const std::vector<int32_t>& rp, const std::vector<int32_t>& ci,
+                   std::vector<int32_t>& col) {
+  col.assign(n, -1);
+  std::vector<int32_t> queue;
+  queue.reserve(n);
+  for (int s = 0; s < n; ++s) {
+    if (col[s] >= 0) continue;
+    col[s] = 0;
+    queue.assign(1, s);
+    for (size_t h = 0; h < queue.size(); ++h) {
+      const int u = queue[h];
+      for (int q = rp[u]; q < rp[u + 1]; ++q) {
+        const int v = ci[q];
+        if (col[v] < 0) {
+          col[v] = 1 - col[u];
+          queue.push_back(v);
+        } else if (col[v] == col[u]) {
+          return false;
+        }
+      }
+    }
+  }
+  return true;
+}
+
 // Evens out the classes of a proper colouring (the colour-class kernels run
 // one class per phase with a barrier between phases, so the largest class
 // sets the phase time).  target = ceil(n / ncol); a pass visits the sites in
@@ -201,7 +230,12 @@ oj_status finish_graph(oj_ctx* ctx, oj_graph* g) {
   inf.n = n;
   inf.nnz = (int64_t)g->ci.size();
   int ncol = 0;
-  g->colour = greedy_colouring(n, g->rp, g->ci, &ncol);
+  if (two_colouring(n, g->rp, g->ci, g->colour)) {
+    ncol = 0;
+    for (int i = 0; i < n; ++i) ncol = std::max(ncol, g->colour[i] + 1);
+  } else {
+    g->colour = greedy_colouring(n, g->rp, g->ci, &ncol);
+  }
   balance_colouring(n, g->rp, g->ci, ncol, g->colour);
   inf.num_colours = ncol;
   int dmax = 0, dmin = n > 0 ? 1 << 30 : 0;

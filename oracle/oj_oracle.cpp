@@ -269,13 +269,41 @@ std::vector<int> greedy_colour(int n, const int64_t* rp, const int32_t* ci) {
   return col;
 }
 
-// The colouring the colour-class kernels use: the greedy colouring above with
-// its classes evened out.  With target t = ceil(n / ncol), each pass goes over
+// The colouring the colour-class kernels use: two colours for a bipartite
+// graph (two_colour), else the greedy colouring above, with its classes evened
+// out.  With target t = ceil(n / ncol), each pass goes over
 // the sites 0..n-1 and puts a site whose class holds more than t sites into
 // the smallest-index colour whose class holds fewer than t sites and none of
 // the site's neighbours; passes stop after one without a move, or after 8.
+// A bipartite graph takes two colours: site 0 of every component (the
+// smallest index) gets colour 0 and the rest alternate along a breadth-first
+// search; false if an odd cycle shows up.
+bool two_colour(int n, const int64_t* rp, const int32_t* ci, std::vector<int>& col) {
+  col.assign(n, -1);
+  std::vector<int> queue;
+  for (int s = 0; s < n; ++s) {
+    if (col[s] >= 0) continue;
+    col[s] = 0;
+    queue.assign(1, s);
+    for (size_t h = 0; h < queue.size(); ++h) {
+      const int u = queue[h];
+      for (int64_t p = rp[u]; p < rp[u + 1]; ++p) {
+        const int v = ci[p];
+        if (col[v] < 0) {
+          col[v] = 1 - col[u];
+          queue.push_back(v);
+        } else if (col[v] == col[u]) {
+          return false;
+        }
+      }
+    }
+  }
+  return true;
+}
+
 std::vector<int> kernel_colour(int n, const int64_t* rp, const int32_t* ci) {
-  std::vector<int> col = greedy_colour(n, rp, ci);
+  std::vector<int> col;
+  if (!two_colour(n, rp, ci, col)) col = greedy_colour(n, rp, ci);
   int ncol = 0;
   for (int c : col) ncol = std::max(ncol, c + 1);
   if (ncol < 2) return col;
