@@ -156,7 +156,9 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             const int t = 4 * lane + e;
             const bool neg = (myw >> e) & 1u;
             const float dE = neg ? 2.0f * fv[e] : -2.0f * fv[e];
-            const bool acc = dE <= 0.0f || __fmul_rn(beta, dE) < L[e];
+            // dE <= 0 accepts without a draw; as -ln u > 0 for every u and beta
+            // is finite and >= 0, beta*dE < -ln u covers that case too
+            const bool acc = __fmul_rn(beta, dE) < L[e];
             if (acc && t >= pos && 128 * c + t < n) mask |= 1u << e;
           }
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
