@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
     const uint32_t rg = a.rep0 + (uint32_t)r;
     for (int64_t k = 0; k < a.nsweeps; ++k) {
-      const float beta = __ldg(a.betas + k);
+      const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
       for (int c = 0; c < nch; ++c) {
         const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
@@ -155,10 +155,12 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           for (int e = 0; e < 4; ++e) {
             const int t = 4 * lane + e;
             const bool neg = (myw >> e) & 1u;
-            const float dE = neg ? 2.0f * fv[e] : -2.0f * fv[e];
-            // dE <= 0 accepts without a draw; as -ln u > 0 for every u and beta
-            // is finite and >= 0, beta*dE < -ln u covers that case too
-            const bool acc = __fmul_rn(beta, dE) < L[e];
+            // beta*dE with dE = -+2 f: (2 beta) f is the same number (scaling by
+            // 2 is exact).  dE <= 0 accepts without a draw; as -ln u > 0 for
+            // every u and beta is finite and >= 0, beta*dE < -ln u covers that
+            // case too
+            const float bf = __fmul_rn(beta2, fv[e]);
+            const bool acc = (neg ? bf : -bf) < L[e];
             if (acc && t >= pos && 128 * c + t < n) mask |= 1u << e;
           }
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
