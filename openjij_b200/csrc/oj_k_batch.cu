@@ -146,23 +146,26 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         L[2] = ojd::neglog(x.z);
         L[3] = ojd::neglog(x.w);
         int pos = 0;  // chunk-local index of the first site not yet decided
+        // this lane's sites that exist (site index below n), as a 4-bit mask
+        const uint32_t inside = 0xFu >> (4 - min(max(n - 128 * c - 4 * lane, 0), 4));
         for (;;) {
           const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
           const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
           const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
+          // ... and not yet decided in this chunk (chunk-local index >= pos)
+          const uint32_t open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
           uint32_t mask = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
-            const int t = 4 * lane + e;
             const bool neg = (myw >> e) & 1u;
             // beta*dE with dE = -+2 f: (2 beta) f is the same number (scaling by
             // 2 is exact).  dE <= 0 accepts without a draw; as -ln u > 0 for
             // every u and beta is finite and >= 0, beta*dE < -ln u covers that
             // case too
             const float bf = __fmul_rn(beta2, fv[e]);
-            const bool acc = (neg ? bf : -bf) < L[e];
-            if (acc && t >= pos && 128 * c + t < n) mask |= 1u << e;
+            if ((neg ? bf : -bf) < L[e]) mask |= 1u << e;
           }
+          mask &= open;
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
           if (!lanes) break;
           const int ls = __ffs(lanes) - 1;
