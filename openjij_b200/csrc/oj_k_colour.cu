@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kColourThreads)
     __syncthreads();
   }
   for (int64_t k = 0; k < nsweeps; ++k) {
-    const float beta = betas[k];
+    const float beta2 = 2.0f * betas[k];
     for (int c = 0; c < ncol; ++c) {
       const int lo = coff[c], hi = coff[c + 1];
       for (int idx = lo + threadIdx.x; idx < hi; idx += blockDim.x) {
@@ -72,9 +72,11 @@ __global__ void __launch_bounds__(kColourThreads)
         for (int rl = 0; rl < 4; ++rl) {
           if (rl < nr) {
             const int8_t si = S[rl * n + i];
-            const float dE = si > 0 ? -2.0f * fs[rl] : 2.0f * fs[rl];
-            const float L = ojd::neglog(ojd::pick(rnd, rl));
-            if (dE <= 0.0f || __fmul_rn(beta, dE) < L) S[rl * n + i] = (int8_t)(-si);
+            // beta*dE, dE = -+2 f, is (2 beta) f with the sign of -s_i (scaling
+            // by 2 is exact); dE <= 0 accepts without a draw, and so does the
+            // comparison, since -ln u > 0 and beta is finite and >= 0
+            const float bf = __fmul_rn(beta2, fs[rl]);
+            if ((si > 0 ? -bf : bf) < ojd::neglog(ojd::pick(rnd, rl))) S[rl * n + i] = (int8_t)(-si);
           }
         }
       }
