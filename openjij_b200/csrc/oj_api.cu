@@ -564,6 +564,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     const uint64_t key = ((uint64_t)OJ_KERNEL_DENSE_JUMP << 40) | (uint64_t)R;
     auto tit = g->tuned.find(key);
     int variant = tit != g->tuned.end() ? tit->second.variant : batch_default_variant();
+    if (n > batch_variant_max_n(variant)) variant = 83;
     std::vector<int32_t> items = make_items(batch_variant_warps(variant));
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t b_hdr = al(8 + 8 + 8), b_items = al(make_items(batch_min_warps()).size() * 4 + 4), b_cnt = al(4),
@@ -587,7 +588,9 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
     if (tit == g->tuned.end() && autotune_requested(flags) && S > 0) {
       // candidates run 16 sweeps with betas spread over the schedule on a copy of the spins
-      const int cand[6] = {45, 82, 83, 84, 162, 321};
+      std::vector<int> cand;
+      for (int v : {45, 82, 83, 84, 162, 321})
+        if (n <= batch_variant_max_n(v)) cand.push_back(v);
       const int64_t Ssub = std::min<int64_t>(S, 32);
       std::vector<float> tb(Ssub);
       for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
@@ -600,7 +603,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       std::vector<int32_t> it;
       int loaded = -1;
       const int bi = time_candidates(
-          st, 6, [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
+          st, (int)cand.size(),
+          [&] { return cudaMemcpyAsync(scratch, d_spins, spin_bytes, cudaMemcpyDeviceToDevice, st); },
           [&](int i) {
             if (loaded != i) {
               it = make_items(batch_variant_warps(cand[i]));
@@ -613,7 +617,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
                                    scratch, d_tb, Ssub, rb, 0, ctx->sm_count, st, nullptr, cand[i], d_fields, d_foff,
                                    R);
           },
-          &terr, (int)(std::find(std::begin(cand), std::end(cand), batch_default_variant()) - std::begin(cand)));
+          &terr, (int)(std::find(cand.begin(), cand.end(), variant) - cand.begin()));
       if (bi == -2) return cuda_fail(ctx, terr, "autotune");
       variant = bi >= 0 ? cand[bi] : 83;
       g->tuned[key] = Shape{0, 0, variant};
@@ -1203,7 +1207,8 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     return it;
   };
   oj_batch* bm = const_cast<oj_batch*>(b);
-  const int variant0 = bm->tuned_variant ? bm->tuned_variant : batch_default_variant();
+  int variant0 = bm->tuned_variant ? bm->tuned_variant : batch_default_variant();
+  if (b->max_n > batch_variant_max_n(variant0)) variant0 = 83;
   std::vector<int32_t> items = make_items(batch_variant_warps(variant0));
   const size_t items_cap = make_items(batch_min_warps()).size();  // the most items of any variant
   int nitems = (int)(items.size() / 2);
@@ -1256,7 +1261,9 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (bm->tuned_variant == 0 && autotune_requested(flags) && S > 0 && nitems > 0) {
     // the work per sweep follows the acceptance rate, so the candidates run 16
     // sweeps whose betas are spread over the whole schedule
-    const int cand[6] = {45, 82, 83, 84, 162, 321};
+    std::vector<int> cand;
+    for (int v : {45, 82, 83, 84, 162, 321})
+      if (b->max_n <= batch_variant_max_n(v)) cand.push_back(v);
     const int64_t Ssub = std::min<int64_t>(S, 32);
     std::vector<float> tb(Ssub);
     for (int64_t q = 0; q < Ssub; ++q) tb[q] = bf[(size_t)((q * S) / Ssub)];
@@ -1269,7 +1276,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     int loaded = -1;  // variant whose items are in d_items
     std::vector<int32_t> it;
     const int bi = time_candidates(
-        st, 6, [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
+        st, (int)cand.size(), [&] { return cudaMemcpyAsync(scratch, d_spins, sbytes, cudaMemcpyDeviceToDevice, st); },
         [&](int i) {
           if (loaded != i) {
             it = make_items(batch_variant_warps(cand[i]));
@@ -1282,7 +1289,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
                                  rb, (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i], d_fields, d_foff,
                                  max_reads);
         },
-        &terr, (int)(std::find(std::begin(cand), std::end(cand), batch_default_variant()) - std::begin(cand)));
+        &terr, (int)(std::find(cand.begin(), cand.end(), variant0) - cand.begin()));
     if (bi == -2) return cuda_fail(ctx, terr, "autotune");
     bm->tuned_variant = bi >= 0 ? cand[bi] : 83;
     tuned_now = true;

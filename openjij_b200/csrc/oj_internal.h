@@ -188,6 +188,7 @@ int batch_warps();
 int batch_variant_warps(int variant);
 int batch_min_warps();  // fewest warps per CTA of any variant (most work items)
 int batch_default_variant();
+int batch_variant_max_n(int variant);  // largest instance a launch variant takes
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,

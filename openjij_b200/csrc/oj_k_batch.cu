@@ -405,6 +405,16 @@ bool batch_variant_valid(int variant) {
   return variant == 45 || variant == 82 || variant == 83 || variant == 84 || variant == 162 || variant == 321;
 }
 
+// largest n whose fields fit the variant: W warps x (FP32 fields + spin
+// words) within the 227 KB of shared memory per CTA
+int batch_variant_max_n(int variant) {
+  switch (variant) {
+    case 321: return 1664;
+    case 162: return 3456;
+    default: return kBatchMaxN;
+  }
+}
+
 int batch_default_variant() {
   if (const char* env = std::getenv("OJ_BATCH_VARIANT")) {
     const int v = std::atoi(env);
@@ -434,7 +444,7 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
                             int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads,
                             double* d_energies, const int64_t* d_eoff) {
   if (variant == 0) variant = batch_default_variant();
-  if (!batch_variant_valid(variant)) return cudaErrorInvalidValue;
+  if (!batch_variant_valid(variant) || b->max_n > batch_variant_max_n(variant)) return cudaErrorInvalidValue;
   const int fstride = std::max(128, (b->max_n + 127) / 128 * 128);
   BatchArgs a;
   a.J = b->d_J.as<float>();

@@ -138,3 +138,29 @@ def test_dense_jump_replica_shards(ctx):
     part = s0[32:].copy()
     N.sa_run(g, part, betas, mcs, seed=3, kernel="dense_jump", replica_offset=32)
     np.testing.assert_array_equal(part, whole[32:])
+
+
+_VARIANT_MAX_N = {45: 4096, 82: 4096, 83: 4096, 84: 4096, 162: 3456, 321: 1664}
+
+
+@pytest.mark.parametrize("variant", sorted(_VARIANT_MAX_N))
+@pytest.mark.parametrize("kind", ["integer", "normal"])
+def test_batched_launch_variants_same_bits(ctx, monkeypatch, variant, kind):
+    """Every launch variant, with FP16 rows (integer couplings) or FP32 rows,
+    gives the replay's spins and energies; the batch's largest instance is the
+    variant's shared-memory limit (up to 2048 sites)."""
+    monkeypatch.setenv("OJ_BATCH_VARIANT", str(variant))
+    top = min(_VARIANT_MAX_N[variant], 2048)
+    sizes = [top, 1, 7, 130, 300, 255, 129]
+    reads = [3, 1, 8, 9, 2, 0, 33]
+    mats = _int_batch(sizes, 60) if kind == "integer" else _normal_batch(sizes, 70)
+    b = N.Batch(ctx, mats)
+    betas, mcs = I.geometric_betas(0.05, 5.0, 6)
+    s0 = _spins(mats, reads, 5)
+    s = s0.copy()
+    e = np.zeros(sum(reads))
+    st = N.sa_run_batched(b, reads, s, betas, mcs, seed=91, energies=e)
+    assert st["variant"] == variant
+    ref = O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), 91)
+    np.testing.assert_array_equal(s, ref)
+    np.testing.assert_allclose(e, _energies(mats, reads, ref), rtol=1e-12, atol=1e-9)
