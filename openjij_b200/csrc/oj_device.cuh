@@ -102,16 +102,21 @@ __device__ __forceinline__ uint32_t pick(const u4& v, int j) {
 // (error below 6e-8, no division).  Each step is a single IEEE
 // round-to-nearest operation (explicit _rn intrinsics, no contraction), so
 // host code doing the same operations reproduces the bits.
+//
+// The range reduction uses integer steps that give exactly the values of the
+// arithmetic definition (u = float(2k+1) * 2^-24; m = the mantissa in [1,2),
+// halved with e + 1 when above 0x1.6a09e6p+0; float(e)) in fewer instructions:
+//   * 0x3F800000 | k is the float 1 + k 2^-23 (one funnel shift of x), and
+//     adding -(1 - 2^-24) gives (2k+1) 2^-24 exactly (the sum is representable);
+//   * with b' = bits(u) - 0x3F3504F4 (0x3504F4: the first mantissa above
+//     0x1.6a09e6p+0), b' >> 23 (arithmetic) is e and (b' & 0x7FFFFF) +
+//     0x3F3504F4 the bits of m, the halving included;
+//   * float(e) = float(0x4B400000 + e) - 1.5 * 2^23 (exact for |e| < 2^22).
 __device__ __forceinline__ float neglog(uint32_t x) {
-  const uint32_t k = x >> 9;
-  const float u = __fmul_rn(__uint2float_rn(2u * k + 1u), 0x1p-24f);
-  const uint32_t b = __float_as_uint(u);
-  int e = (int)(b >> 23) - 127;
-  float m = __uint_as_float((b & 0x007FFFFFu) | 0x3F800000u);
-  if (m > 0x1.6a09e6p+0f) {
-    m = __fmul_rn(m, 0.5f);
-    e += 1;
-  }
+  const float u = __fadd_rn(__uint_as_float(__funnelshift_r(x, 0x7Fu, 9)), -0x1.fffffep-1f);
+  const uint32_t b = __float_as_uint(u) - 0x3F3504F4u;
+  const float m = __uint_as_float((b & 0x007FFFFFu) + 0x3F3504F4u);
+  const float ef = __fsub_rn(__int_as_float(0x4B400000 + ((int)b >> 23)), 0x1.8p23f);
   const float t = __fsub_rn(m, 1.0f);
   const float t2 = __fmul_rn(t, t);
   float q = -0x1.8e99cep-4f;
@@ -122,7 +127,7 @@ __device__ __forceinline__ float neglog(uint32_t x) {
   q = __fmaf_rn(q, t, 0x1.5558fcp-2f);
   q = __fmaf_rn(q, t, -0x1.0000ecp-1f);
   const float lnm = __fmaf_rn(t2, q, t);
-  const float lnu = __fmaf_rn(__int2float_rn(e), 0x1.62e430p-1f, lnm);
+  const float lnu = __fmaf_rn(ef, 0x1.62e430p-1f, lnm);
   return -lnu;
 }
 

@@ -135,6 +135,9 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     __syncwarp();
     const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
     const uint32_t rg = a.rep0 + (uint32_t)r;
+    // this lane's sites of the last chunk that exist (site index below n), as
+    // a 4-bit mask; every site of the other chunks exists
+    const uint32_t inside_last = 0xFu >> (4 - min(max(n - 128 * (nch - 1) - 4 * lane, 0), 4));
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
@@ -145,15 +148,14 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         L[1] = ojd::neglog(x.y);
         L[2] = ojd::neglog(x.z);
         L[3] = ojd::neglog(x.w);
-        int pos = 0;  // chunk-local index of the first site not yet decided
-        // this lane's sites that exist (site index below n), as a 4-bit mask
-        const uint32_t inside = 0xFu >> (4 - min(max(n - 128 * c - 4 * lane, 0), 4));
+        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
+        // this lane's sites that exist and are not yet decided in this chunk
+        // (chunk-local index at or past the last flip's + 1)
+        uint32_t open = inside;
         for (;;) {
           const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
           const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
           const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
-          // ... and not yet decided in this chunk (chunk-local index >= pos)
-          const uint32_t open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
           uint32_t mask = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -198,7 +200,8 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           }
           __syncwarp();
           if (lane == ls) sw[sw_word(c, ls)] = ws ^ (1u << (sw_shift(c) + es));
-          pos = 4 * ls + es + 1;
+          const int pos = 4 * ls + es + 1;  // chunk-local index of the first site not yet decided
+          open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
           __syncwarp();
         }
       }

@@ -42,6 +42,33 @@ def test_neglog_accuracy():
         assert abs(got - want) <= 4e-7 * max(1.0, want), (x, got, want)
 
 
+def test_neglog_integer_range_reduction():
+    """The sweep kernels reduce u by integer steps (1 + k 2^-23 from the bits
+    0x3F800000 | k, minus 1 - 2^-24; an offset split of the bits for m and e;
+    float(e) through 0x4B400000 + e): for every k = x >> 9 these give the u, m
+    and float(e) of the arithmetic definition the oracle follows, so both
+    compute the same -ln u."""
+    f32 = np.float32
+    for lo in range(0, 1 << 23, 1 << 21):
+        k = np.arange(lo, lo + (1 << 21), dtype=np.uint32)
+        u = (2 * k + 1).astype(f32) * f32(2.0**-24)
+        u_int = (np.uint32(0x3F800000) | k).view(f32) + f32(float.fromhex("-0x1.fffffep-1"))
+        np.testing.assert_array_equal(u.view(np.uint32), u_int.view(np.uint32))
+        b = u.view(np.uint32)
+        e = (b >> 23).astype(np.int32) - 127
+        m = ((b & np.uint32(0x7FFFFF)) | np.uint32(0x3F800000)).view(f32)
+        big = m > f32(float.fromhex("0x1.6a09e6p+0"))
+        m = np.where(big, m * f32(0.5), m)
+        e = e + big.astype(np.int32)
+        bb = b - np.uint32(0x3F3504F4)
+        e_int = bb.view(np.int32) >> 23
+        m_int = ((bb & np.uint32(0x7FFFFF)) + np.uint32(0x3F3504F4)).view(f32)
+        ef = (np.int32(0x4B400000) + e_int).view(f32) - f32(12582912.0)
+        np.testing.assert_array_equal(m.view(np.uint32), m_int.view(np.uint32))
+        np.testing.assert_array_equal(e, e_int)
+        np.testing.assert_array_equal(e.astype(f32), ef)
+
+
 def test_schedules_match_reference_formula():
     b = O.classical_schedule(0.1, 100.0, 100)
     assert b[0] == 0.1 and abs(b[-1] - 100.0) < 1e-9
