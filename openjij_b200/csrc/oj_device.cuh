@@ -112,6 +112,10 @@ __device__ __forceinline__ uint32_t pick(const u4& v, int j) {
 //     0x1.6a09e6p+0), b' >> 23 (arithmetic) is e and (b' & 0x7FFFFF) +
 //     0x3F3504F4 the bits of m, the halving included;
 //   * float(e) = float(0x4B400000 + e) - 1.5 * 2^23 (exact for |e| < 2^22).
+// The largest value neglog takes (at u = 2^-24): a site whose beta*dE is at
+// least this is rejected whatever its uniform.
+constexpr float kNegLogMax = 0x1.0a2b24p+4f;
+
 __device__ __forceinline__ float neglog(uint32_t x) {
   const float u = __fadd_rn(__uint_as_float(__funnelshift_r(x, 0x7Fu, 9)), -0x1.fffffep-1f);
   const uint32_t b = __float_as_uint(u) - 0x3F3504F4u;

@@ -142,13 +142,28 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
       for (int c = 0; c < nch; ++c) {
+        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
+        {
+          // a chunk none of whose sites has beta*dE below the largest -ln u
+          // keeps its state: its uniforms are not drawn (the stream is
+          // counter-based, so nothing after it moves)
+          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
+          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
+          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
+          uint32_t can = 0u;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float bf = __fmul_rn(beta2, fv[e]);
+            if ((((myw >> e) & 1u) ? bf : -bf) < ojd::kNegLogMax) can |= 1u << e;
+          }
+          if (!__any_sync(0xffffffffu, (can & inside) != 0u)) continue;
+        }
         const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
         float L[4];
         L[0] = ojd::neglog(x.x);
         L[1] = ojd::neglog(x.y);
         L[2] = ojd::neglog(x.z);
         L[3] = ojd::neglog(x.w);
-        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
         // this lane's sites that exist and are not yet decided in this chunk
         // (chunk-local index at or past the last flip's + 1)
         uint32_t open = inside;

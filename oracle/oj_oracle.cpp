@@ -386,6 +386,12 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 }
 
 float orc_neglog(uint32_t x) { return neglog(x); }
+// the largest -ln u over every input (k = x >> 9 takes 2^23 values)
+float orc_neglog_max() {
+  float m = 0.0f;
+  for (uint32_t k = 0; k < (1u << 23); ++k) m = std::max(m, neglog(k << 9));
+  return m;
+}
 
 void orc_greedy_colour(int n, const int64_t* rp, const int32_t* ci, int32_t* out) {
   auto c = greedy_colour(n, rp, ci);

@@ -49,6 +49,8 @@ def lib():
         L.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
         L.orc_neglog.argtypes = [C.c_uint32]
         L.orc_neglog.restype = C.c_float
+        L.orc_neglog_max.argtypes = []
+        L.orc_neglog_max.restype = C.c_float
         L.orc_greedy_colour.argtypes = [C.c_int, _i64p, _i32p, _i32p]
         L.orc_kernel_colour.argtypes = [C.c_int, _i64p, _i32p, _i32p]
         L.orc_gen_spin.argtypes = [C.c_uint64, C.c_int, C.c_int, _i8p]
@@ -150,6 +152,11 @@ def philox4x32_10(ctr, key):
 
 def neglog(x: int) -> float:
     return float(lib().orc_neglog(int(x) & 0xFFFFFFFF))
+
+
+def neglog_max() -> float:
+    """The largest value neglog takes over all 2^32 inputs."""
+    return float(lib().orc_neglog_max())
 
 
 def greedy_colour(g: AugCSR):

@@ -42,6 +42,13 @@ def test_neglog_accuracy():
         assert abs(got - want) <= 4e-7 * max(1.0, want), (x, got, want)
 
 
+def test_neglog_largest_value():
+    """The sweep kernels skip the uniforms of a 128-site chunk when every
+    site's beta*dE is at least 0x1.0a2b24p+4: no -ln u reaches past it (the
+    largest, at u = 2^-24, is exactly that)."""
+    assert O.neglog_max() == float.fromhex("0x1.0a2b24p+4") == O.neglog(0)
+
+
 def test_neglog_integer_range_reduction():
     """The sweep kernels reduce u by integer steps (1 + k 2^-23 from the bits
     0x3F800000 | k, minus 1 - 2^-24; an offset split of the bits for m and e;
