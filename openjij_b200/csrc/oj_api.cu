@@ -1067,7 +1067,7 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
   // the FP64 energies exactly, E = 1/2 sum_i s_i (f_i + h_i).
   bool exact = true;
   int pmax = 0;
-  double maxrow = 0.0;
+  double maxrow = 0.0, maxj = 0.0;  // largest row sum of |values| (h included), largest |J|
   auto grid_p = [](double v) {  // smallest p >= 0 with v 2^p an integer (v != 0), from its bits
     uint64_t bits;
     std::memcpy(&bits, &v, 8);
@@ -1092,6 +1092,7 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
         }
         pmax = std::max(pmax, p);
         row += std::fabs(v);
+        if (j < nk) maxj = std::max(maxj, std::fabs(v));
       }
       maxrow = std::max(maxrow, row);
     }
@@ -1137,6 +1138,14 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
       OJ_CK(up(b->d_J16, J16.data(), J16.size() * 2), "upload J16");
       b->j16 = true;
     }
+  }
+  // exact fields with every J 2^p an integer of at most 127: J 2^p as int8
+  if (exact && std::ldexp(maxj, pmax) <= 127.0) {
+    std::vector<int8_t> J8(J32.size());
+    for (size_t q = 0; q < J32.size(); ++q) J8[q] = (int8_t)std::ldexp((double)J32[q], pmax);
+    OJ_CK(up(b->d_J8, J8.data(), J8.size()), "upload J8");
+    b->j8 = true;
+    b->j8_scale = (float)std::ldexp(1.0, -pmax);
   }
   OJ_CK(up(b->d_h, h32.data(), h32.size() * 4), "upload h");
   OJ_CK(up(b->d_J64, J64.data(), J64.size() * 8), "upload J64");

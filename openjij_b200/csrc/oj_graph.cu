@@ -22,6 +22,7 @@ oj_batch::~oj_batch() {
   if (cur != device) cudaSetDevice(device);
   d_J.release();
   d_J16.release();
+  d_J8.release();
   d_h.release();
   d_J64.release();
   d_joff.release();

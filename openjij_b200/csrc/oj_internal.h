@@ -123,6 +123,11 @@ struct oj_batch {
   oj::DevBuf d_J16;   // J as FP16 when every coupling's FP32 value is exactly an FP16 value (flip rows)
   bool j16 = false;
   bool exact_fields = false;  // FP32 fields exact: energies from the fields (sweep kernel epilogue)
+  // J * 2^p as int8 (exact fields and every scaled coupling in [-127, 127]):
+  // the initial fields are then exact integer dot products
+  oj::DevBuf d_J8;
+  bool j8 = false;
+  float j8_scale = 1.0f;  // 2^-p
   int tuned_variant = 0;  // autotuned register-budget variant, 0 = not tuned
   ~oj_batch();
 };

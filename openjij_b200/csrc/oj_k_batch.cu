@@ -318,6 +318,96 @@ __global__ void __launch_bounds__(256) batch_field_kernel(BatchArgs a, int zbase
   }
 }
 
+// Initial fields of a batch with exact fields and int8 couplings (J8 = J 2^p,
+// every value in [-127, 127]): f_j = h_j + 2^-p sum_i J8[j][i] s_i, four sites
+// per __dp4a into an int32 (J is symmetric: row j holds column j).  The batch's
+// exactness bound (|h_j| + sum_i |J_ij| below 2^(24-p), all multiples of 2^-p)
+// makes the sum, its conversion, the scaling and the addition of h exact, so
+// these are the values of batch_field_kernel's FP32 row sums (exact too).  One
+// CTA per (instance, 128 columns, 64 replicas): 64-site slices of its 128 rows
+// and of the 64 replicas' spins are staged in shared memory as packed words;
+// thread (tr, tj) accumulates replicas tr + 16q (q < 4) x sites tj + 16x (x < 8).
+constexpr int kI8Slice = 64;
+
+__global__ void __launch_bounds__(256)
+    batch_field_i8_kernel(BatchArgs a, const int8_t* __restrict__ J8, float scale, int zbase) {
+  __shared__ int32_t jt[kI8Slice / 4][128];
+  __shared__ int32_t sp[kI8Slice / 4][kFieldReplicas + 1];  // + 1: the transposing stores hit distinct banks
+  const int m = blockIdx.x, jb = blockIdx.y, r0 = (zbase + (int)blockIdx.z) * kFieldReplicas;
+  const int n = a.n[m], R = a.reads[m];
+  const int nch = (n + 127) >> 7;
+  if (jb >= nch || r0 >= R) return;  // the whole CTA leaves together
+  const int npad = nch << 7;
+  const int t = threadIdx.x, tr = t >> 4, tj = t & 15;
+  const int8_t* Jm = J8 + a.joff[m];
+  const int8_t* S = a.spins + a.soff[m];
+  int acc[4][8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int x = 0; x < 8; ++x) acc[q][x] = 0;
+  for (int k0 = 0; k0 < npad; k0 += kI8Slice) {
+    __syncthreads();  // the previous slice is consumed
+    // rows 128 jb + j at sites k0..k0+63, 16 bytes per (row, quarter); rows
+    // past n are zero, columns past n are the zero padding of J
+    for (int idx = t; idx < 128 * 4; idx += 256) {
+      const int j = idx & 127, qq = idx >> 7;
+      const int row = 128 * jb + j;
+      int4 v = make_int4(0, 0, 0, 0);
+      if (row < n) v = __ldg(reinterpret_cast<const int4*>(Jm + (size_t)row * npad + k0 + 16 * qq));
+      jt[4 * qq + 0][j] = v.x;
+      jt[4 * qq + 1][j] = v.y;
+      jt[4 * qq + 2][j] = v.z;
+      jt[4 * qq + 3][j] = v.w;
+    }
+    // spins of replicas r0..r0+63 at sites k0..k0+63, four sites per word;
+    // consecutive threads read consecutive words of a replica's row (one
+    // 32-bit load where the row segment is 4-byte aligned and inside n)
+    for (int idx = t; idx < kFieldReplicas * (kI8Slice / 4); idx += 256) {
+      const int w = idx & (kI8Slice / 4 - 1), rr = idx / (kI8Slice / 4);
+      const int r = r0 + rr;
+      const int i0 = k0 + 4 * w;
+      uint32_t word = 0u;
+      if (r < R && i0 < n) {
+        const int8_t* sp8 = S + (size_t)r * n + i0;
+        if (i0 + 3 < n && ((reinterpret_cast<uintptr_t>(sp8) & 3u) == 0u)) {
+          word = __ldg(reinterpret_cast<const uint32_t*>(sp8));
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (i0 + e < n) word |= (uint32_t)(uint8_t)sp8[e] << (8 * e);
+        }
+      }
+      sp[w][rr] = (int32_t)word;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int w = 0; w < kI8Slice / 4; ++w) {
+      int sv[4], jv[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) sv[q] = sp[w][tr + 16 * q];
+#pragma unroll
+      for (int x = 0; x < 8; ++x) jv[x] = jt[w][tj + 16 * x];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int x = 0; x < 8; ++x) acc[q][x] = __dp4a(sv[q], jv[x], acc[q][x]);
+    }
+  }
+  const float* h = a.h + a.hoff[m] + 128 * jb;
+  float* Fm = const_cast<float*>(a.F) + a.foff[m] + 128 * jb;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = r0 + tr + 16 * q;
+    if (r >= R) continue;
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      const int j = tj + 16 * x;
+      Fm[(size_t)r * npad + j] = __fadd_rn(__ldg(h + j), __fmul_rn(__int2float_rn(acc[q][x]), scale));
+    }
+  }
+}
+
 // FP64 energy of every replica: E = sum_{i<j} J_ij s_i s_j + sum_i h_i s_i
 // (dense.hpp:176-192) from the FP64 augmented matrix.  One CTA per (instance,
 // 32 replicas), instances largest first: the spins are staged as one word per
@@ -495,7 +585,10 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   cudaError_t e = cudaSuccess;
   for (int z0 = 0; z0 < zt; z0 += 65535) {  // grid z is at most 65535 replica tiles
     const dim3 fgrid((unsigned)b->count, (unsigned)(fstride / 128), (unsigned)std::min(65535, zt - z0));
-    batch_field_kernel<<<fgrid, 256, 0, st>>>(a, z0);
+    if (b->j8)
+      batch_field_i8_kernel<<<fgrid, 256, 0, st>>>(a, b->d_J8.as<int8_t>(), b->j8_scale, z0);
+    else
+      batch_field_kernel<<<fgrid, 256, 0, st>>>(a, z0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (launches) ++*launches;
   }
