@@ -326,26 +326,29 @@ __global__ void __launch_bounds__(256) batch_field_kernel(BatchArgs a, int zbase
 // these are the values of batch_field_kernel's FP32 row sums (exact too).  One
 // CTA per (instance, 128 columns, 64 replicas): 64-site slices of its 128 rows
 // and of the 64 replicas' spins are staged in shared memory as packed words;
-// thread (tr, tj) accumulates replicas tr + 16q (q < 4) x sites tj + 16x (x < 8).
+// warp tr accumulates replicas 8tr..8tr+7 and its lane tj sites 4tj..4tj+3, so
+// a step of four sites is two broadcast 16-byte loads of spin words and one
+// conflict-free 16-byte load of J words for 32 __dp4a.
 constexpr int kI8Slice = 64;
+constexpr int kI8Stride = kFieldReplicas + 4;  // spin words per slice word (16-byte rows)
 
 __global__ void __launch_bounds__(256)
     batch_field_i8_kernel(BatchArgs a, const int8_t* __restrict__ J8, float scale, int zbase) {
-  __shared__ int32_t jt[kI8Slice / 4][128];
-  __shared__ int32_t sp[kI8Slice / 4][kFieldReplicas + 1];  // + 1: the transposing stores hit distinct banks
+  __shared__ __align__(16) int32_t jt[kI8Slice / 4][128];
+  __shared__ __align__(16) int32_t sp[kI8Slice / 4][kI8Stride];
   const int m = blockIdx.x, jb = blockIdx.y, r0 = (zbase + (int)blockIdx.z) * kFieldReplicas;
   const int n = a.n[m], R = a.reads[m];
   const int nch = (n + 127) >> 7;
   if (jb >= nch || r0 >= R) return;  // the whole CTA leaves together
   const int npad = nch << 7;
-  const int t = threadIdx.x, tr = t >> 4, tj = t & 15;
+  const int t = threadIdx.x, tr = t >> 5, tj = t & 31;
   const int8_t* Jm = J8 + a.joff[m];
   const int8_t* S = a.spins + a.soff[m];
-  int acc[4][8];
+  int acc[8][4];
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < 8; ++q)
 #pragma unroll
-    for (int x = 0; x < 8; ++x) acc[q][x] = 0;
+    for (int x = 0; x < 4; ++x) acc[q][x] = 0;
   for (int k0 = 0; k0 < npad; k0 += kI8Slice) {
     __syncthreads();  // the previous slice is consumed
     // rows 128 jb + j at sites k0..k0+63, 16 bytes per (row, quarter); rows
@@ -369,13 +372,13 @@ __global__ void __launch_bounds__(256)
       const int i0 = k0 + 4 * w;
       uint32_t word = 0u;
       if (r < R && i0 < n) {
-        const int8_t* sp8 = S + (size_t)r * n + i0;
-        if (i0 + 3 < n && ((reinterpret_cast<uintptr_t>(sp8) & 3u) == 0u)) {
-          word = __ldg(reinterpret_cast<const uint32_t*>(sp8));
+        const int8_t* s8 = S + (size_t)r * n + i0;
+        if (i0 + 3 < n && ((reinterpret_cast<uintptr_t>(s8) & 3u) == 0u)) {
+          word = __ldg(reinterpret_cast<const uint32_t*>(s8));
         } else {
 #pragma unroll
           for (int e = 0; e < 4; ++e)
-            if (i0 + e < n) word |= (uint32_t)(uint8_t)sp8[e] << (8 * e);
+            if (i0 + e < n) word |= (uint32_t)(uint8_t)s8[e] << (8 * e);
         }
       }
       sp[w][rr] = (int32_t)word;
@@ -383,28 +386,29 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
 #pragma unroll 4
     for (int w = 0; w < kI8Slice / 4; ++w) {
-      int sv[4], jv[8];
+      const int4 s0 = *reinterpret_cast<const int4*>(&sp[w][8 * tr]);
+      const int4 s1 = *reinterpret_cast<const int4*>(&sp[w][8 * tr + 4]);
+      const int4 jv = *reinterpret_cast<const int4*>(&jt[w][4 * tj]);
+      const int sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+      const int jj[4] = {jv.x, jv.y, jv.z, jv.w};
 #pragma unroll
-      for (int q = 0; q < 4; ++q) sv[q] = sp[w][tr + 16 * q];
+      for (int q = 0; q < 8; ++q)
 #pragma unroll
-      for (int x = 0; x < 8; ++x) jv[x] = jt[w][tj + 16 * x];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int x = 0; x < 8; ++x) acc[q][x] = __dp4a(sv[q], jv[x], acc[q][x]);
+        for (int x = 0; x < 4; ++x) acc[q][x] = __dp4a(sv[q], jj[x], acc[q][x]);
     }
   }
-  const float* h = a.h + a.hoff[m] + 128 * jb;
-  float* Fm = const_cast<float*>(a.F) + a.foff[m] + 128 * jb;
+  const float4 h4 = __ldg(reinterpret_cast<const float4*>(a.h + a.hoff[m] + 128 * jb + 4 * tj));
+  float* Fm = const_cast<float*>(a.F) + a.foff[m] + 128 * jb + 4 * tj;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int r = r0 + tr + 16 * q;
+  for (int q = 0; q < 8; ++q) {
+    const int r = r0 + 8 * tr + q;
     if (r >= R) continue;
-#pragma unroll
-    for (int x = 0; x < 8; ++x) {
-      const int j = tj + 16 * x;
-      Fm[(size_t)r * npad + j] = __fadd_rn(__ldg(h + j), __fmul_rn(__int2float_rn(acc[q][x]), scale));
-    }
+    float4 o;
+    o.x = __fadd_rn(h4.x, __fmul_rn(__int2float_rn(acc[q][0]), scale));
+    o.y = __fadd_rn(h4.y, __fmul_rn(__int2float_rn(acc[q][1]), scale));
+    o.z = __fadd_rn(h4.z, __fmul_rn(__int2float_rn(acc[q][2]), scale));
+    o.w = __fadd_rn(h4.w, __fmul_rn(__int2float_rn(acc[q][3]), scale));
+    *reinterpret_cast<float4*>(Fm + (size_t)r * npad) = o;
   }
 }
 
