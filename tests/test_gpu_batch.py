@@ -38,11 +38,21 @@ def _energies(mats, reads, spins):
     return np.array(out)
 
 
-@pytest.mark.parametrize("kind", ["integer", "normal"])
+def _wide_int_batch(sizes, seed):
+    """Integer couplings up to 225 in magnitude: exact FP32 fields and FP16 flip
+    rows, but past the int8 range of the dp4a initial fields."""
+    return [I.dense_qubo_int(int(n), lo=-900, hi=900, seed=seed + k)[0].toarray() for k, n in enumerate(sizes)]
+
+
+@pytest.mark.parametrize("kind", ["integer", "normal", "wide"])
 def test_batched_bit_exact(ctx, kind):
+    """Spins and energies against the replay: integer couplings (int8 initial
+    fields, FP16 rows), wide integers (FP32 initial fields, FP16 rows) and
+    N(0, 1) couplings (FP32 throughout)."""
     sizes = [1, 7, 64, 130, 300, 1024, 255, 129]
     reads = [1, 3, 8, 9, 17, 2, 0, 33]
-    mats = _int_batch(sizes, 40) if kind == "integer" else _normal_batch(sizes, 50)
+    make = {"integer": (_int_batch, 40), "normal": (_normal_batch, 50), "wide": (_wide_int_batch, 45)}[kind]
+    mats = make[0](sizes, make[1])
     b = N.Batch(ctx, mats)
     betas, mcs = I.geometric_betas(0.1, 10.0, 30)
     s0 = _spins(mats, reads, 1)
