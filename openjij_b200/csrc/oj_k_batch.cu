@@ -87,10 +87,37 @@ __device__ __forceinline__ float4 ldg4h(const __half* p) {
   return make_float4(a.x, a.y, b.x, b.y);
 }
 
+// A flip row's four couplings of one lane, from global memory (through L1)
+// or from the copy of the instance's couplings in shared memory (SJ).
+template <bool SJ>
+__device__ __forceinline__ float4 row4(const float* p) {
+  if constexpr (SJ) return *reinterpret_cast<const float4*>(p);
+  else return ldg4(p);
+}
+template <bool SJ>
+__device__ __forceinline__ float4 row4h(const __half* p) {
+  if constexpr (SJ) {
+    const uint2 u = *reinterpret_cast<const uint2*>(p);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+  } else {
+    return ldg4h(p);
+  }
+}
+
+// The couplings of an instance are staged in shared memory (SJ) when the
+// batch's largest block of n rows x npad columns takes at most this many bytes.
+constexpr size_t kBatchSmemJBytes = 96 * 1024;
+
 // GROUP: chunks of a flipped site's J row loaded before any is used (the
 // flip's L2 round trips are ceil(chunks / GROUP)); more costs registers.
 // H: the flip rows come from the FP16 copy of J (half the L2 bytes per flip).
-template <int W, int MINB, int GROUP, bool H>
+// SJ: every work item first copies its instance's couplings (FP32 or FP16
+// rows, as H says) into shared memory after the warps' fields and spin words,
+// and the flips read their rows there (small instances: no L2 round trip per
+// flip).
+template <int W, int MINB, int GROUP, bool H, bool SJ>
 __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
   __shared__ int item_sh;
@@ -98,6 +125,8 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
                  (size_t)warp * a.swstride;  // spin words [chunk / 8][lane]
+  // the staged couplings (SJ): after every warp's fields and spin words
+  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride);
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
@@ -113,6 +142,18 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     const int npad = nch << 7;
     const float* J = a.J + a.joff[m];
     int8_t* gs = a.spins + a.soff[m] + (size_t)(active ? r : 0) * n;
+    if (SJ) {
+      // n rows of npad couplings, 16 bytes per thread and step; every warp of
+      // the CTA takes part before any leaves for an inactive replica
+      const int4* src = reinterpret_cast<const int4*>(H ? static_cast<const void*>(a.J16 + a.joff[m])
+                                                          : static_cast<const void*>(J));
+      int4* dst = reinterpret_cast<int4*>(jsh);
+      const int total = n * npad * (H ? 2 : 4) / 16;
+      for (int q = threadIdx.x; q < total; q += blockDim.x) dst[q] = __ldg(src + q);
+      __syncthreads();
+    }
+    const float* Jr = SJ ? reinterpret_cast<const float*>(jsh) : J;
+    const __half* Jr16 = SJ ? reinterpret_cast<const __half*>(jsh) : (H ? a.J16 + a.joff[m] : nullptr);
     // spins -> bits
     if (active)
       for (int c8 = 0; c8 < nch; c8 += 8) {
@@ -192,8 +233,8 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const bool neg = (ws >> (sw_shift(c) + es)) & 1u;
           const float coef = neg ? 2.0f : -2.0f;
           const int i = 128 * c + 4 * ls + es;
-          const float* Ji = J + (size_t)i * npad + 4 * lane;
-          const __half* Ji16 = a.J16 + a.joff[m] + (size_t)i * npad + 4 * lane;
+          const float* Ji = Jr + (size_t)i * npad + 4 * lane;
+          const __half* Ji16 = Jr16 + (size_t)i * npad + 4 * lane;
           // the row in groups of four chunks whose loads are in flight together
 #pragma unroll
           for (int c0 = 0; c0 < kMaxChunks; c0 += GROUP) {
@@ -201,7 +242,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             float4 v[GROUP];
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
-              if (c0 + q < nch) v[q] = H ? ldg4h(Ji16 + 128 * (c0 + q)) : ldg4(Ji + 128 * (c0 + q));
+              if (c0 + q < nch) v[q] = H ? row4h<SJ>(Ji16 + 128 * (c0 + q)) : row4<SJ>(Ji + 128 * (c0 + q));
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
               if (c0 + q < nch) {
@@ -536,9 +577,12 @@ int batch_default_variant() {
 }
 
 template <int W, int MINB, int GROUP>
-cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStream_t st, bool h) {
-  auto kern = h ? sa_batch_kernel<W, MINB, GROUP, true> : sa_batch_kernel<W, MINB, GROUP, false>;
-  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4);  // FP32 fields + spin words
+cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStream_t st, bool h, size_t jbytes) {
+  const bool sj = jbytes > 0;
+  auto kern = h ? (sj ? sa_batch_kernel<W, MINB, GROUP, true, true> : sa_batch_kernel<W, MINB, GROUP, true, false>)
+                : (sj ? sa_batch_kernel<W, MINB, GROUP, false, true> : sa_batch_kernel<W, MINB, GROUP, false, false>);
+  // FP32 fields + spin words per warp, then the staged couplings
+  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4) + jbytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -598,13 +642,16 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   }
   e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
+  // the largest instance's couplings in shared memory when they are small
+  size_t jbytes = (size_t)b->max_n * (size_t)fstride * (b->j16 ? 2 : 4);
+  if (jbytes > kBatchSmemJBytes) jbytes = 0;
   switch (variant) {
-    case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st, b->j16); break;
-    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st, b->j16); break;
-    case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st, b->j16); break;
-    case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st, b->j16); break;
-    case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st, b->j16); break;
-    default: e = launch_variant<32, 1, 4>(a, nitems, sm_count, st, b->j16); break;
+    case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    default: e = launch_variant<32, 1, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
   }
   if (e == cudaSuccess && launches) ++*launches;
   return e;

@@ -174,3 +174,42 @@ def test_batched_launch_variants_same_bits(ctx, monkeypatch, variant, kind):
     ref = O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), 91)
     np.testing.assert_array_equal(s, ref)
     np.testing.assert_allclose(e, _energies(mats, reads, ref), rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("variant", [82, 83, 321])
+@pytest.mark.parametrize("kind,sizes", [("normal", [1, 7, 64, 100, 128]), ("integer", [1, 7, 64, 100, 128]),
+                                        ("integer", [150, 192, 5])])
+def test_batched_small_instances_staged_couplings(ctx, monkeypatch, variant, kind, sizes):
+    """Batches whose largest block of couplings fits the shared-memory budget
+    (FP32 rows up to n = 128, FP16 rows up to n = 192): every work item copies
+    its instance's couplings to shared memory and the flips read them there."""
+    monkeypatch.setenv("OJ_BATCH_VARIANT", str(variant))
+    reads = [5, 3, 9, 2, 33][:len(sizes)]
+    mats = _int_batch(sizes, 80) if kind == "integer" else _normal_batch(sizes, 90)
+    b = N.Batch(ctx, mats)
+    betas, mcs = I.geometric_betas(0.1, 10.0, 40)
+    s0 = _spins(mats, reads, 9)
+    s = s0.copy()
+    e = np.zeros(sum(reads))
+    st = N.sa_run_batched(b, reads, s, betas, mcs, seed=23, energies=e)
+    assert st["variant"] == variant
+    ref = O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), 23)
+    np.testing.assert_array_equal(s, ref)
+    np.testing.assert_allclose(e, _energies(mats, reads, ref), rtol=1e-12, atol=1e-9)
+
+
+def test_dense_jump_small_dense_ising(ctx):
+    """The dense jump path on a 100-spin dense Ising instance (staged FP32
+    couplings), as the 100-spin benchmark case runs it."""
+    A = I.dense_ising_uniform(100, seed=1)[0].toarray()
+    g = N.Graph(ctx, *I.augmented_csr(A))
+    betas, mcs = I.geometric_betas(0.1, 10.0, 50)
+    R = 20
+    s0 = np.random.default_rng(4).choice(np.array([-1, 1], np.int8), size=(R, 100))
+    s = s0.copy()
+    e = np.zeros(R)
+    st = N.sa_run(g, s, betas, mcs, seed=5, kernel="dense_jump", energies=e)
+    assert st["kernel"] == "dense_jump"
+    ref = O.replay_sa_batch([A], [R], s0.ravel(), _per_sweep(betas, mcs), 5).reshape(R, 100)
+    np.testing.assert_array_equal(s, ref)
+    np.testing.assert_allclose(e, _energies([A], [R], ref.ravel()), rtol=1e-12, atol=1e-9)
