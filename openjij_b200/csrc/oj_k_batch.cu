@@ -293,6 +293,119 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   }
 }
 
+// Batches whose instances have at most 128 sites (one chunk): the sweep of
+// sa_batch_kernel with each lane's four fields and spin bits in registers for
+// the whole run and the instance's coupling rows (FP32, or FP16 when H) staged
+// in shared memory by every work item, so that a flip is a ballot, a shuffle,
+// one shared-memory row load and four FMAs.  Same random stream, acceptance
+// test, skipping of chunks that cannot flip and FMA order, so the same bits.
+template <int W, bool H>
+__global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) float shb[];  // [n][128] couplings of the item's instance
+  __shared__ int item_sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int item = item_sh;
+    if (item >= a.nitems) break;
+    const int m = a.items[2 * item];
+    if ((unsigned)m >= (unsigned)a.count) continue;  // a corrupt table entry is skipped, never followed
+    const int n = a.n[m];
+    if (n > 128) continue;  // the host launches this kernel only for n <= 128
+    const int r = a.items[2 * item + 1] * W + warp;
+    {
+      // n rows of 128 couplings, 16 bytes per thread and step, by every warp
+      // of the CTA before any leaves for an inactive replica
+      const int4* src = reinterpret_cast<const int4*>(H ? static_cast<const void*>(a.J16 + a.joff[m])
+                                                          : static_cast<const void*>(a.J + a.joff[m]));
+      int4* dst = reinterpret_cast<int4*>(shb);
+      const int total = n * 128 * (H ? 2 : 4) / 16;
+      for (int q = threadIdx.x; q < total; q += blockDim.x) dst[q] = __ldg(src + q);
+      __syncthreads();
+    }
+    if (r >= a.reads[m]) continue;  // warps past the instance's reads wait for the next item
+    int8_t* gs = a.spins + a.soff[m] + (size_t)r * n;
+    uint32_t wd = 0u;  // bit e: site 4*lane + e is -1
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = 4 * lane + e;
+      if (i < n && gs[i] < 0) wd |= 1u << e;
+    }
+    float4 fc = ldg4(a.F + a.foff[m] + (size_t)r * 128 + 4 * lane);
+    const uint32_t inside = 0xFu >> (4 - min(max(n - 4 * lane, 0), 4));
+    const float* Js = shb + 4 * lane;
+    const __half* Js16 = reinterpret_cast<const __half*>(shb) + 4 * lane;
+    const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
+    const uint32_t rg = a.rep0 + (uint32_t)r;
+    for (int64_t k = 0; k < a.nsweeps; ++k) {
+      const float beta2 = 2.0f * __ldg(a.betas + k);
+      {
+        // no site below the largest -ln u: the chunk keeps its state
+        const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
+        uint32_t can = 0u;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float bf = __fmul_rn(beta2, fv[e]);
+          if ((((wd >> e) & 1u) ? bf : -bf) < ojd::kNegLogMax) can |= 1u << e;
+        }
+        if (!__any_sync(0xffffffffu, (can & inside) != 0u)) continue;
+      }
+      const ojd::u4 x = ojd::philox((uint32_t)lane, a.sweep0 + (uint32_t)k, rg, tag, a.keys);
+      float L[4];
+      L[0] = ojd::neglog(x.x);
+      L[1] = ojd::neglog(x.y);
+      L[2] = ojd::neglog(x.z);
+      L[3] = ojd::neglog(x.w);
+      uint32_t open = inside;  // sites that exist and are not yet decided in this sweep
+      for (;;) {
+        const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
+        uint32_t mask = 0u;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float bf = __fmul_rn(beta2, fv[e]);
+          if ((((wd >> e) & 1u) ? bf : -bf) < L[e]) mask |= 1u << e;
+        }
+        mask &= open;
+        const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
+        if (!lanes) break;
+        const int ls = __ffs(lanes) - 1;
+        // the first accepting lane's mask and spin bits
+        const uint32_t pk = __shfl_sync(0xffffffffu, mask | (wd << 4), ls);
+        const int es = __ffs(pk & 0xFu) - 1;
+        const float coef = ((pk >> (4 + es)) & 1u) ? 2.0f : -2.0f;
+        const int i = 4 * ls + es;
+        const float4 v = H ? row4h<true>(Js16 + 128 * i) : row4<true>(Js + 128 * i);
+        fc.x = __fmaf_rn(coef, v.x, fc.x);
+        fc.y = __fmaf_rn(coef, v.y, fc.y);
+        fc.z = __fmaf_rn(coef, v.z, fc.z);
+        fc.w = __fmaf_rn(coef, v.w, fc.w);
+        if (lane == ls) wd ^= 1u << es;
+        open = inside & (0xFu << min(max(i + 1 - 4 * lane, 0), 4));
+      }
+    }
+    if (a.E) {
+      // exact fields: E = 1/2 sum_i s_i (f_i + h_i), as in sa_batch_kernel
+      const float4 h4 = ldg4(a.h + a.hoff[m] + 4 * lane);
+      const float fv[4] = {fc.x, fc.y, fc.z, fc.w}, hv[4] = {h4.x, h4.y, h4.z, h4.w};
+      double e = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double t = (double)fv[q] + (double)hv[q];
+        if (4 * lane + q < n) e += ((wd >> q) & 1u) ? -t : t;
+      }
+      for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+      if (lane == 0) a.E[a.eoff[m] + r] = 0.5 * e;
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = 4 * lane + e;
+      if (i < n) gs[i] = ((wd >> e) & 1u) ? (int8_t)-1 : (int8_t)1;
+    }
+  }
+}
+
 // Initial fields of every replica of every instance,
 //     F[m][r][j] = h_j + sum_{i = 0..n-1} J_ij s_ri,
 // summed in ascending i with one FP32 rounding per term, the order of the
@@ -594,6 +707,21 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
   return cudaGetLastError();
 }
 
+template <int W>
+cudaError_t launch_one_chunk(const BatchArgs& a, int max_n, int nitems, int sm_count, cudaStream_t st, bool h) {
+  auto kern = h ? sa_batch1_kernel<W, true> : sa_batch1_kernel<W, false>;
+  const size_t smem = (size_t)max_n * 128 * (h ? 2 : 4);  // the staged couplings
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = std::max(1, std::min(nitems, per_sm * sm_count));
+  kern<<<grid, W * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
@@ -642,6 +770,18 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   }
   e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
+  if (b->max_n <= 128) {
+    // one chunk per instance: fields and spin bits in registers (same warps
+    // per CTA as the variant, so the same work items)
+    switch (batch_variant_warps(variant)) {
+      case 4: e = launch_one_chunk<4>(a, b->max_n, nitems, sm_count, st, b->j16); break;
+      case 16: e = launch_one_chunk<16>(a, b->max_n, nitems, sm_count, st, b->j16); break;
+      case 32: e = launch_one_chunk<32>(a, b->max_n, nitems, sm_count, st, b->j16); break;
+      default: e = launch_one_chunk<8>(a, b->max_n, nitems, sm_count, st, b->j16); break;
+    }
+    if (e == cudaSuccess && launches) ++*launches;
+    return e;
+  }
   // the largest instance's couplings in shared memory when they are small
   size_t jbytes = (size_t)b->max_n * (size_t)fstride * (b->j16 ? 2 : 4);
   if (jbytes > kBatchSmemJBytes) jbytes = 0;

@@ -176,13 +176,14 @@ def test_batched_launch_variants_same_bits(ctx, monkeypatch, variant, kind):
     np.testing.assert_allclose(e, _energies(mats, reads, ref), rtol=1e-12, atol=1e-9)
 
 
-@pytest.mark.parametrize("variant", [82, 83, 321])
+@pytest.mark.parametrize("variant", [45, 82, 83, 162, 321])
 @pytest.mark.parametrize("kind,sizes", [("normal", [1, 7, 64, 100, 128]), ("integer", [1, 7, 64, 100, 128]),
                                         ("integer", [150, 192, 5])])
 def test_batched_small_instances_staged_couplings(ctx, monkeypatch, variant, kind, sizes):
     """Batches whose largest block of couplings fits the shared-memory budget
     (FP32 rows up to n = 128, FP16 rows up to n = 192): every work item copies
-    its instance's couplings to shared memory and the flips read them there."""
+    its instance's couplings to shared memory and the flips read them there;
+    up to 128 sites the one-chunk kernel keeps fields and spins in registers."""
     monkeypatch.setenv("OJ_BATCH_VARIANT", str(variant))
     reads = [5, 3, 9, 2, 33][:len(sizes)]
     mats = _int_batch(sizes, 80) if kind == "integer" else _normal_batch(sizes, 90)
