@@ -1,8 +1,8 @@
 // Batched dense SA over many instances of uneven size in one persistent launch.
 //
 // Work item = (instance m, group of up to W replicas of m, W = warps per CTA
-// of the launch variant: 8, 16 or 32; with 32 all reads of a 32-read instance
-// share one SM and its L1 for the J rows).  Items
+// of the launch variant: 4, 8, 16 or 32; with 32 all reads of a 32-read
+// instance share one SM and its L1 for the J rows).  Items
 // are ordered by decreasing n (longest first) and handed out through an atomic
 // counter, so the CTAs resident on the SMs keep pulling the next largest item
 // until the queue is empty.  One warp runs one replica: its FP32 local fields
@@ -26,10 +26,12 @@
 //
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
 // read through L1 one float4 per lane on every accepted flip, or from an FP16
-// copy (8 bytes per lane) when FP16 holds every coupling exactly.  The initial
-// fields come from batch_field_kernel, launched just before (it reads J once
-// per 64 replicas), through a global buffer of reads x padded n floats per
-// instance.
+// copy (8 bytes per lane) when FP16 holds every coupling exactly; small
+// instances' rows are staged in shared memory, and batches of instances of at
+// most 128 sites run sa_batch1_kernel (fields and spin bits in registers).
+// The initial fields come from batch_field_kernel (or batch_field_i8_kernel for
+// exact int8 couplings), launched just before, through a global buffer of
+// reads x padded n floats per instance.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
