@@ -200,6 +200,22 @@ def cpu_reference(m, betas, mcs, reads, threads):
     return attempts / dt, dt
 
 
+CPU_BASELINE_SECONDS = 10.0  # the cpu_baseline leg repeats its sample until about this much CPU work
+
+
+def _repeat_for(fn, min_seconds=CPU_BASELINE_SECONDS, max_reps=100000):
+    """Runs the bounded CPU sample ``fn`` (returning attempts/s and seconds)
+    until about ``min_seconds`` of work; returns attempts/s over all of it, the
+    seconds and the repetitions."""
+    attempts, seconds, reps = 0.0, 0.0, 0
+    while reps < max_reps and (reps == 0 or seconds < min_seconds):
+        v, dt = fn()
+        attempts += v * dt
+        seconds += dt
+        reps += 1
+    return attempts / seconds, seconds, reps
+
+
 def cpu_reference_sw(m, betas, mcs, reads, threads, max_sweeps=200):
     """OpenJij's Swendsen-Wang updater on the CPU (oracle restatement of
     updater/swendsen_wang.hpp): ``reads`` reads, one per host thread, over at
@@ -238,11 +254,13 @@ def cpu_reference_sqa(w, threads):
 def cpu_reference_batch(w, threads, budget_s=8.0):
     """OpenJij's CPU path on the batch: instances in order, one read per host
     thread each, until about ``budget_s`` seconds of work; returns attempts/s,
-    seconds and the number of instances run."""
+    seconds and the number of instance runs."""
     from oracle import oracle as O
     attempts, spent, count = 0.0, 0.0, 0
     sweeps = float(np.sum(w["mcs"]))
-    for A in w["mats"]:
+    mats = w["mats"]
+    while count < 20 * len(mats):  # the instances in order, again from the first once all have run
+        A = mats[count % len(mats)]
         g = O.AugCSR(A)
         rng = np.random.default_rng(count)
         init = rng.choice(np.array([-1, 1], np.int8), size=(threads, g.n))
@@ -290,7 +308,8 @@ def run_reference(args):
         sample = (f"{reads} reads of the Swendsen-Wang updater over at most 200 sweeps of {w['name']}'s schedule "
                   f"per step, one read per host thread")
     if w["kind"] == "batch":
-        sample = (f"the first {batch_count[0]} instances of {w['name']}, {reads} reads x {sweeps} sweeps each "
+        sample = (f"{batch_count[0]} instance runs of {w['name']} (its instances in order, from the first "
+                  f"again once all have run), {reads} reads x {sweeps} sweeps each "
                   f"per step, one read per host thread")
     line = {
         "impl": "reference", "metric": "spin-flip attempts/s", "value": value,
@@ -411,9 +430,10 @@ def run_ours_batch(args, w):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt, cnt = cpu_reference_batch(w, threads)
+        v, dt, cnt = cpu_reference_batch(w, threads, budget_s=CPU_BASELINE_SECONDS)
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
-               "sample": f"the first {cnt} instances, {threads} reads x {S} sweeps each, one read per host "
+               "sample": f"{cnt} instance runs (the batch's instances in order, from the first again once all "
+                         f"have run), {threads} reads x {S} sweeps each, one read per host "
                          f"thread, {dt:.1f} s"}
     if rank == 0:
         line = {
@@ -546,22 +566,22 @@ def run_ours(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu and used_kernel == "swendsen_wang":
         threads = os.cpu_count() or 1
-        v, dt = cpu_reference_sw(w["matrix"], betas, mcs, threads, threads)
+        v, dt, reps = _repeat_for(lambda: cpu_reference_sw(w["matrix"], betas, mcs, threads, threads))
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
-               "sample": f"{threads} reads of the Swendsen-Wang updater, at most 200 sweeps of the schedule, "
-                         f"one read per host thread, {dt:.1f} s"}
+               "sample": f"{reps} x {threads} reads of the Swendsen-Wang updater, at most 200 sweeps of the "
+                         f"schedule, one read per host thread, {dt:.1f} s"}
     elif rank == 0 and ws == 1 and not args.no_cpu and w["kind"] == "sa":
         threads = os.cpu_count() or 1
-        v, dt = cpu_reference(w["matrix"], betas, mcs, threads, threads)
+        v, dt, reps = _repeat_for(lambda: cpu_reference(w["matrix"], betas, mcs, threads, threads))
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
-               "sample": f"{threads} reads x {int(np.sum(mcs))} sweeps of the same instance, one read "
+               "sample": f"{reps} x {threads} reads x {int(np.sum(mcs))} sweeps of the same instance, one read "
                          f"per host thread, {dt:.1f} s"}
     elif rank == 0 and ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt = cpu_reference_sqa(w, threads)
+        v, dt, reps = _repeat_for(lambda: cpu_reference_sqa(w, threads))
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
-               "sample": f"{threads} reads x {T} slices x {min(int(np.sum(mcs)), 100)} sweeps, one read per "
-                         f"host thread, {dt:.1f} s"}
+               "sample": f"{reps} x {threads} reads x {T} slices x {min(int(np.sum(mcs)), 100)} sweeps, one read "
+                         f"per host thread, {dt:.1f} s"}
     if rank == 0:
         line = {
             "metric": "spin-flip attempts/s", "value": value, "unit": "attempts/s", "n_gpus": ws,
