@@ -1,0 +1,49 @@
+"""Host-side parts of bench.py on the CPU: the reference arm's JSON line (the
+fields a driver reads), the time-to-solution formula and the repetition of
+the CPU baseline's sample."""
+import json
+import math
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def test_t99_is_the_reference_formula():
+    # openjij/utils/benchmark.py:205-224: tau * ln(1 - 0.99) / ln(1 - p_s)
+    assert bench._t99(10.0, 0.5) == pytest.approx(10.0 * math.log(0.01) / math.log(0.5))
+    assert bench._t99(3.0, 1.0) == 3.0
+    assert bench._t99(3.0, 0.0) == float("inf")
+
+
+def test_repeat_for_accumulates_until_the_budget():
+    calls = []
+
+    def sample():
+        calls.append(1)
+        return 1000.0, 0.25  # 1000 attempts/s for 0.25 s
+
+    v, seconds, reps = bench._repeat_for(sample, min_seconds=1.0)
+    assert reps == 4 and len(calls) == 4
+    assert seconds == pytest.approx(1.0) and v == pytest.approx(1000.0)
+    # one sample at least, even with no budget
+    v, seconds, reps = bench._repeat_for(sample, min_seconds=0.0)
+    assert reps == 1 and seconds == pytest.approx(0.25)
+
+
+def test_reference_arm_prints_the_contract_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--config", "1",
+                          "--steps", "1", "--warmup", "0"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == "spin-flip attempts/s"
+    assert line["value"] > 0 and line["higher_is_better"] is True and line["steps"] == 1
+    assert line["e2e"] == {"value": line["value"], "unit": "attempts/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["config"]["workload"] == "dense_ising_N100_R100_S1000"
