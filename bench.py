@@ -136,10 +136,46 @@ def _dist():
     return ws, rank, local
 
 
+_INSTANCES = None
+
+
+def _instances():
+    """openjij_b200/instances.py loaded from its path (numpy and scipy only).
+    Importing it through the package would run openjij_b200/__init__.py, which
+    loads the library's native extension; the reference arm must map none of
+    the product's shared objects."""
+    global _INSTANCES
+    if _INSTANCES is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("_ojb200_instances",
+                                                      os.path.join(ROOT, "openjij_b200", "instances.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _INSTANCES = mod
+    return _INSTANCES
+
+
+L2_NOTE = "GPU arm: L2 flushed between timed steps (256 MB write)"
+
+
+def _config_of(w):
+    """The workload keys of the JSON line's ``config``, identical in both arms."""
+    if w["kind"] == "batch":
+        sizes = [m.shape[0] - 1 for m in w["mats"]]
+        S = int(np.sum(w["mcs"]))
+        return {"workload": w["name"], "instances": len(sizes), "spins_total": int(np.sum(sizes)),
+                "replicas_per_instance": int(w["replicas"]), "num_sweeps": S,
+                "attempts_per_step": float(np.sum(np.asarray(sizes, np.float64) * w["reads"])) * S, "l2": L2_NOTE}
+    n = w["matrix"].shape[0] - 1
+    S = int(np.sum(w["mcs"]))
+    return {"workload": w["name"], "spins": n, "replicas": int(w["replicas"]), "trotter": int(w["T"]),
+            "num_sweeps": S, "attempts_per_step": float(w["replicas"]) * w["T"] * n * S, "l2": L2_NOTE}
+
+
 def _workload(config, sweeps=None, replicas=None):
     """The seeded workloads of the five benchmark configurations.  Config 2 is
     the default bench line; the others are measured with --config."""
-    from openjij_b200 import instances as I
+    I = _instances()
     w = {"config": config, "kind": "sa", "T": 1}
     if config == 1:
         m, _ = I.dense_ising_uniform(100, seed=1)
@@ -316,7 +352,8 @@ def run_reference(args):
         "unit": "attempts/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded instance)",
-        "config": {"workload": w["name"], "sample_reads_per_step": reads, "host_threads": threads},
+        "config": _config_of(w),
+        "sample": {"reads_per_step": reads, "host_threads": threads, "what": sample},
         "cpu_baseline": {"value": value, "unit": "attempts/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -440,11 +477,9 @@ def run_ours_batch(args, w):
             "metric": "spin-flip attempts/s", "value": value, "unit": "attempts/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded instances)",
-            "config": {"workload": w["name"], "instances": len(mats), "spins_total": int(np.sum(sizes)),
-                       "replicas_per_instance": int(w["replicas"]), "num_sweeps": S, "kernel": "batched",
-                       "launch_shape": {"threads": st["threads"], "variant": st["variant"],
-                                        "autotuned": True},
-                       "l2": "flushed between steps (256 MB write)", "attempts_per_step": attempts_per_step},
+            "config": _config_of(w),
+            "kernel": {"name": "batched", "launch_shape": {"threads": st["threads"], "variant": st["variant"],
+                                                           "autotuned": True}},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "kernel_ms": kms,
                          "algorithmic_per_attempt": "2n flop"},
@@ -473,7 +508,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from openjij_b200 import _native as N
-    from openjij_b200 import instances as I
+    I = _instances()
     w = _workload(args.config, args.sweeps, args.replicas)
     kernel = args.kernel or w["kernel"]
     n, indptr, indices, data = I.augmented_csr(w["matrix"])
@@ -588,12 +623,9 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32" if used_kernel == "bitpacked" else "f32",
             "data": "synthetic (seeded instance)",
-            "config": {"workload": w["name"], "spins": n, "replicas": R, "trotter": T,
-                       "num_sweeps": int(np.sum(mcs)), "kernel": used_kernel,
-                       "launch_shape": {"cluster": st["cluster"], "threads": st["threads"],
-                                        "variant": st["variant"], "autotuned": True},
-                       "l2": "flushed between steps (256 MB write)",
-                       "attempts_per_step": attempts_per_step},
+            "config": _config_of(w),
+            "kernel": {"name": used_kernel, "launch_shape": {"cluster": st["cluster"], "threads": st["threads"],
+                                                             "variant": st["variant"], "autotuned": True}},
             "roofline": {"bound": w["bound"], "achieved": achieved, "peak": peak, "unit": unit,
                          "note": ("algorithmic int8 state bytes per attempt against the HBM copy peak; the "
                                   "kernel keeps the state bit-packed in shared memory (layout_bytes_per_attempt, "
@@ -628,7 +660,12 @@ def run_ours(args):
 
 
 def _t99(tau_ms, p):
-    """OpenJij's TTS formula (openjij/utils/benchmark.py:205-224): tau*ln(1-0.99)/ln(1-p_s)."""
+    """OpenJij's TTS formula (openjij/utils/benchmark.py:205-224): tau*ln(1-0.99)/ln(1-p_s).
+
+    One deviation: at p_s = 1 the reference returns 0 (benchmark.py:216-217);
+    here it returns tau, the time of the one call that already reached the
+    target.  A T99 of 0 would make every ladder step that reaches p_s = 1 tie
+    at 0 and the minimum over the ladder meaningless."""
     if p <= 0.0:
         return float("inf")
     if p >= 1.0:
@@ -651,7 +688,7 @@ def run_tts(args):
     R99(p) = ln(0.01)/ln(1-p) repetitions."""
     import torch
     from openjij_b200 import _native as N
-    from openjij_b200 import instances as I
+    I = _instances()
     torch.cuda.set_device(0)
     ctx = N.Context(0)
     w = _workload(args.config, None, None)

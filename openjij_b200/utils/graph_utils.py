@@ -1,21 +1,24 @@
-"""Graph helpers (reference: openjij/utils/graph_utils.py)."""
+"""Graph helpers with the behaviour of the reference's openjij/utils/graph_utils.py."""
 from __future__ import annotations
 
 import numpy as np
 
 
 def qubo_to_ising(mat: np.ndarray):
-    """In place: a QUBO matrix to its Ising form (divide by 4, then add each
-    row's sum to its diagonal), as openjij/utils/graph_utils.py:5-13."""
+    """Turns a QUBO matrix into its Ising form in place: every entry divided by
+    4, then every diagonal entry increased by the sum of its (divided) row.
+    The row sums do not involve other rows' diagonals, so all of them are taken
+    before the diagonal changes."""
     mat /= 4
-    for i in range(mat.shape[0]):
-        mat[i, i] += np.sum(mat[i, :])
+    mat[np.diag_indices_from(mat)] += mat.sum(axis=1)
 
 
 def chimera_to_ind(r: int, c: int, z: int, L: int):
-    """1-D index r*8L + c*8 + z of Chimera site (r, c, z) on an L x L grid of
-    unit cells; ValueError outside the grid (graph_utils.py:16-36)."""
-    if not (0 <= r < L and 0 <= c < L and 0 <= z < 8):
-        raise ValueError("0 <= r < L or 0 <= c < L or 0 <= z < 8. "
-                         "your input r={}, c={}, z={}, L={}".format(r, c, z, L))
-    return r * L * 8 + c * 8 + z
+    """Linear index of site z (0..7) of the Chimera unit cell in row r,
+    column c of an L x L grid: cells in row-major order, 8 sites each.
+    Raises ValueError for a site outside the grid."""
+    try:
+        return int(np.ravel_multi_index((r, c, z), (L, L, 8)))
+    except ValueError:
+        raise ValueError(f"Chimera site (r={r}, c={c}, z={z}) is outside an L={L} grid "
+                         f"(0 <= r < L, 0 <= c < L, 0 <= z < 8)") from None

@@ -17,6 +17,8 @@ import bench  # noqa: E402
 def test_t99_is_the_reference_formula():
     # openjij/utils/benchmark.py:205-224: tau * ln(1 - 0.99) / ln(1 - p_s)
     assert bench._t99(10.0, 0.5) == pytest.approx(10.0 * math.log(0.01) / math.log(0.5))
+    # deviation (stated in bench._t99): the reference gives 0 at p_s = 1
+    # (benchmark.py:216-217), here the time of the one call, tau
     assert bench._t99(3.0, 1.0) == 3.0
     assert bench._t99(3.0, 0.0) == float("inf")
 
@@ -47,3 +49,27 @@ def test_reference_arm_prints_the_contract_line():
                            "d2h_bytes_per_step": 0}
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["config"]["workload"] == "dense_ising_N100_R100_S1000"
+    # the same workload keys as the GPU arm's line
+    assert line["config"] == json.loads(json.dumps(bench._config_of(bench._workload(1))))
+
+
+_MAPS_PROBE = """
+import runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--config", "1", "--steps", "1", "--warmup", "0"]
+try:
+    runpy.run_path("bench.py", run_name="__main__")
+except SystemExit:
+    pass
+maps = open("/proc/self/maps").read()
+print("MAPS", int("libojb200" in maps), int("_cxxjij" in maps), int("liboj_oracle" in maps))
+"""
+
+
+def test_reference_arm_maps_no_product_library():
+    """The reference arm runs the oracle's restatement of the reference's CPU
+    path only: after a whole run the process has mapped the oracle's library
+    and neither of the product's shared objects."""
+    out = subprocess.run([sys.executable, "-c", _MAPS_PROBE], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    tag = [ln for ln in out.stdout.splitlines() if ln.startswith("MAPS")][-1].split()
+    assert tag[1:] == ["0", "0", "1"], tag
