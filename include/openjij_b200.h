@@ -175,12 +175,14 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32
  * in one fixed 16 MiB device array inside the library (held by every GPU that
  * loads it until exit): words (ceil(R/32) * n * 4 B) plus thresholds
  * (sweeps * (degree+1) * 4 B) plus sweeps * 4 B must fit, else OJ_ERR_ARG.
- * spins: DEVICE pointer [R][n], in/out.  The graph must be regular with
- * couplings +-c, h = 0, and must have run oj_sa_run once (which builds its
- * site partition), else OJ_ERR_UNSUPPORTED.  The call is asynchronous on the
- * context's stream.  The first call on a device looks up the array's device
- * address, so make it before any stream capture; calls overlapping on one GPU
- * share the array and race. */
+ * spins: DEVICE pointer [R][n] on the context's device, in/out (a host
+ * pointer or another device's memory -> OJ_ERR_ARG).  The graph must be
+ * regular with couplings +-c, h = 0, and must have run oj_sa_run once (which
+ * builds its site partition), else OJ_ERR_UNSUPPORTED.  The call is
+ * asynchronous on the context's stream.  oj_ctx_create places the array on
+ * the context's device and loads the kernels this entry point launches, so the
+ * call itself allocates no device memory; calls overlapping on one GPU share
+ * the array and race. */
 oj_status oj_sa_run_bitpacked_noalloc(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int8_t* spins,
                                       const double* betas, const int32_t* mcs, int32_t num_sched,
                                       uint64_t seed, int64_t first_sweep, int64_t replica_offset);

@@ -288,6 +288,13 @@ oj_status oj_ctx_create(int32_t device, oj_ctx** out) {
   }
   ctx->own_stream = true;
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  // set-up of oj_sa_run_bitpacked_noalloc on this device, so that its calls
+  // allocate nothing; a failure only disables that entry point
+  const cudaError_t pe = noalloc_prepare(device);
+  if (pe != cudaSuccess) {
+    cudaGetLastError();
+    ctx->noalloc_error = std::string("set-up of the allocation-free entry point failed: ") + cudaGetErrorString(pe);
+  }
   *out = ctx;
   return OJ_OK;
 }

@@ -138,6 +138,7 @@ struct oj_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string last_error;
+  std::string noalloc_error;  // why the allocation-free entry point could not be set up ("" = ready)
   oj::DevBuf spins, words, params, energies, best, aux, batch, fields, eparts;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -205,6 +206,13 @@ cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const
 int batch_energy_splits(const oj_batch* b, int max_reads, int sm_count);
 cudaError_t launch_pack(const int8_t* spins, int R, int n, uint32_t* words, cudaStream_t st);
 cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cudaStream_t st);
+// Load the named kernels' code on the current device (CUDA loads modules
+// lazily, which allocates device memory at a kernel's first use).
+cudaError_t pack_preload();
+cudaError_t msc_preload();
+// Set-up of the allocation-free entry point on the current device: looks up
+// its fixed scratch array's device address and loads the kernels it launches.
+cudaError_t noalloc_prepare(int device);
 int flip_stats_max_k();
 cudaError_t launch_flip_stats(const oj_graph* g, int K, const int8_t* s, double thr, double* quad, double* lin,
                               unsigned long long* amin, cudaStream_t st);

@@ -336,4 +336,10 @@ cudaError_t launch_unpack(const uint32_t* words, int R, int n, int8_t* spins, cu
   return cudaGetLastError();
 }
 
+cudaError_t pack_preload() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, pack_kernel);
+  return e != cudaSuccess ? e : cudaFuncGetAttributes(&fa, unpack_kernel);
+}
+
 }  // namespace oj

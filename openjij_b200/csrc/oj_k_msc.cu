@@ -273,6 +273,19 @@ cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st
 }  // namespace
 
 int msc_max_degree() { return kMscMaxDegree; }
+
+cudaError_t msc_preload() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaSuccess;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<1>)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<2>)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<3>)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<4>)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<5>)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<6>)) != cudaSuccess) return e;
+  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<7>)) != cudaSuccess) return e;
+  return cudaFuncGetAttributes(&fa, sa_msc_kernel<8>);
+}
 int msc_default_threads() { return msc_threads(); }
 
 // Cluster size: the number of CTAs per replica group.  One CTA per SM, as

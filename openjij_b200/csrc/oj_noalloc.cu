@@ -9,11 +9,15 @@
 // the per-sweep acceptance thresholds) in one fixed, file-scope device array
 // instead of context workspace allocated on demand.
 //
-// The array is kNoAllocScratchBytes (16 MiB) and every GPU that loads this
-// library holds it until the process exits.  All calls share it, and each
-// call overwrites what it uses (the words are rebuilt from the caller's spins,
-// the thresholds rewritten for the call's schedule), so nothing has to start
-// at zero; two calls that overlap on the GPU (different streams or contexts on
+// The array is kNoAllocScratchBytes (16 MiB).  CUDA loads a library's device
+// code and its __device__ arrays lazily, so oj_ctx_create does the set-up with
+// the context's device current: it looks up the array's device address (which
+// places the array on the device) and loads the kernels this entry point
+// launches.  From then on the device holds the array until the process exits,
+// and a call allocates nothing.  All calls share the array, and each call
+// overwrites what it uses (the words are rebuilt from the caller's spins, the
+// thresholds rewritten for the call's schedule), so nothing has to start at
+// zero; two calls that overlap on the GPU (different streams or contexts on
 // one device) race on the array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
@@ -38,17 +42,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 std::mutex g_scratch_mu;
 void* g_scratch_ptr[kNoAllocMaxDevices] = {};
 
-cudaError_t scratch_address(int device, void** out) {
-  if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+// The device address recorded by noalloc_prepare, or null.
+void* scratch_address(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return nullptr;
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_ptr[device] = p;
-  }
-  *out = g_scratch_ptr[device];
-  return cudaSuccess;
+  return g_scratch_ptr[device];
 }
 
 // thr = floor(exp(-beta*2c*m) * 2^32), m = 1..D; always bit m when the
@@ -71,6 +69,23 @@ void threshold_row(float beta, double c, int D, uint32_t* thr, uint32_t* always)
 }
 
 }  // namespace
+
+// Once per device, with `device` current (oj_ctx_create).
+cudaError_t noalloc_prepare(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_ptr[device]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return e;
+      g_scratch_ptr[device] = p;
+    }
+  }
+  const cudaError_t e = pack_preload();
+  return e != cudaSuccess ? e : msc_preload();
+}
+
 }  // namespace oj
 
 using namespace oj;
@@ -142,9 +157,19 @@ extern "C" oj_status oj_sa_run_bitpacked_noalloc(oj_ctx* ctx, const oj_graph* g,
     if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return OJ_ERR_ARG;
   }
-  void* base = nullptr;
-  cudaError_t e = scratch_address(ctx->device, &base);
-  if (e != cudaSuccess) return fail(e, "cudaGetSymbolAddress");
+  if (pa.device != ctx->device) {
+    ctx->last_error = "spins are on another device than the context's";
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return OJ_ERR_ARG;
+  }
+  void* base = scratch_address(ctx->device);
+  if (!base) {
+    ctx->last_error = ctx->noalloc_error.empty() ? "the allocation-free entry point was not set up on this device"
+                                                 : ctx->noalloc_error;
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return OJ_ERR_CUDA;
+  }
+  cudaError_t e = cudaSuccess;
   uint32_t* d_words = static_cast<uint32_t*>(base);
   uint32_t* d_thr = reinterpret_cast<uint32_t*>(static_cast<char*>(base) + al(words_bytes));
   uint32_t* d_alw = reinterpret_cast<uint32_t*>(static_cast<char*>(base) + al(words_bytes) + al(thr_bytes));

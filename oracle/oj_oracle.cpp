@@ -967,7 +967,8 @@ void orc_replay_sqa_split(int n, const int64_t* indptr, const int32_t* indices, 
 // blocks concatenated.
 void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset, const double* J_aug,
                          const int32_t* reads, int8_t* spins, const float* betas_f, int64_t nsweeps,
-                         uint64_t seed, uint32_t inst0, int threads, float* fields_out) {
+                         uint64_t seed, uint32_t inst0, int threads, float* fields_out, uint32_t rep0,
+                         uint32_t sweep0) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   std::vector<int64_t> soff(count + 1, 0);
   std::vector<int> rm, rr;  // flattened (instance, replica)
@@ -1001,7 +1002,7 @@ void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset,
       const float beta = betas_f[k];
       for (int i = 0; i < n; ++i) {
         const float dE = s[i] > 0 ? -2.0f * f[i] : 2.0f * f[i];
-        const P4 u = philox((uint32_t)(i >> 2), (uint32_t)k, (uint32_t)r, tag, k0, k1);
+        const P4 u = philox((uint32_t)(i >> 2), sweep0 + (uint32_t)k, rep0 + (uint32_t)r, tag, k0, k1);
         const float L = neglog(u.v[i & 3]);
         if (dE <= 0.0f || beta * dE < L) {
           const float c = s[i] > 0 ? -2.0f : 2.0f;

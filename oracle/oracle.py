@@ -80,7 +80,7 @@ def lib():
         L.orc_replay_sqa_split.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _u32p,
                                            _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
         L.orc_replay_sa_batch.argtypes = [C.c_int, _i32p, _i64p, _f64p, _i32p, _i8p, _f32p, C.c_int64,
-                                          C.c_uint64, C.c_uint32, C.c_int, C.c_void_p]
+                                          C.c_uint64, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, C.c_uint32]
         L.orc_ref_sw.argtypes = [C.c_int, _i64p, _i32p, _f64p, _i8p, _f64p, _i64p, C.c_int64, C.c_uint64]
         L.orc_ref_sw_many.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f64p, _i64p, C.c_int64,
                                       _u64p, C.c_int]
@@ -383,10 +383,13 @@ def replay_sqa_split(g: AugCSR, init3d, thr, mode, seed, threads=None):
     return S
 
 
-def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, threads=None, fields=False):
+def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, threads=None, fields=False,
+                    rep0=0, sweep0=0):
     """Batched dense SA replay; mats: augmented (n+1)x(n+1) FP64 matrices,
     spins_flat: the instances' [reads[m]][n[m]] int8 blocks concatenated.
-    fields=True also returns the final incrementally updated FP32 fields."""
+    fields=True also returns the final incrementally updated FP32 fields.
+    inst0 / rep0 / sweep0: global index of instance 0, of every instance's
+    replica 0 and of the first sweep (a slice of a larger run)."""
     n = np.array([m.shape[0] - 1 for m in mats], np.int32)
     sizes = np.array([(k + 1) * (k + 1) for k in n], np.int64)
     offset = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
@@ -396,7 +399,7 @@ def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, thr
     fo = np.zeros(s.shape, np.float32) if fields else None
     lib().orc_replay_sa_batch(len(mats), n, offset, flat, np.ascontiguousarray(reads, np.int32), s, b, len(b),
                               int(seed), int(inst0), _threads(threads),
-                              None if fo is None else fo.ctypes.data)
+                              None if fo is None else fo.ctypes.data, int(rep0), int(sweep0))
     return (s, fo) if fields else s
 
 

@@ -5,7 +5,9 @@ application whose device memory is already held by another framework's
 allocator, or code that cannot take cudaMalloc's implicit device
 synchronisation — by keeping its scratch in a fixed device array inside the
 library.  It must give exactly the spins of the regular oj_sa_run bit-packed
-path, on consecutive calls that reuse (and overwrite) that array.
+path, on consecutive calls that reuse (and overwrite) that array, without the
+device's free memory moving across a call, and it must refuse what it cannot
+run before touching the spins.
 """
 import numpy as np
 import pytest
@@ -35,8 +37,12 @@ def test_noalloc_matches_regular_entry_point_twice():
         want = init.clone()
         N.sa_run(graph, want, betas, mcs, seed=seed, kernel="bitpacked", device=True)
         got = init.clone()
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         N.sa_run_bitpacked_noalloc(graph, got, betas, mcs, seed=seed)
         torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        assert free_after == free_before, f"call {call}: device free memory moved by {free_before - free_after} B"
         assert torch.equal(got, want), f"call {call}: allocation-free run differs from oj_sa_run"
         assert not torch.equal(got, init)
 
@@ -47,5 +53,32 @@ def test_noalloc_matches_regular_entry_point_twice():
     assert ei.value.status == N.OJ_ERR_ARG
     torch.cuda.synchronize()
     assert torch.equal(spins, init)
-    graph.close()
+
+    # host memory is refused
+    host = init.cpu().numpy().copy()
+    with pytest.raises(N.OJError) as ei:
+        N.sa_run_bitpacked_noalloc(graph, host, betas, mcs, seed=1)
+    assert ei.value.status == N.OJ_ERR_ARG
+    np.testing.assert_array_equal(host, init.cpu().numpy())
+
+    # a graph that has not run oj_sa_run yet has no site partition
+    fresh = N.Graph(ctx, g.n, g.indptr, g.indices, g.data)
+    with pytest.raises(N.OJError) as ei:
+        N.sa_run_bitpacked_noalloc(fresh, spins, betas, mcs, seed=1)
+    assert ei.value.status == N.OJ_ERR_UNSUPPORTED
+
+    # couplings of two magnitudes are not the bit-packed kernel's +-c
+    A = m.toarray()
+    i, j = 0, int(np.flatnonzero(A[0, :g.n])[0])
+    A[i, j] *= 2.0
+    A[j, i] *= 2.0
+    mixed = O.AugCSR(A)
+    gm = N.Graph(ctx, mixed.n, mixed.indptr, mixed.indices, mixed.data)
+    with pytest.raises(N.OJError) as ei:
+        N.sa_run_bitpacked_noalloc(gm, spins, betas, mcs, seed=1)
+    assert ei.value.status == N.OJ_ERR_UNSUPPORTED
+    torch.cuda.synchronize()
+    assert torch.equal(spins, init)
+    for x in (gm, fresh, graph):
+        x.close()
     ctx.close()
