@@ -683,15 +683,23 @@ def run_tts(args):
     num_sweeps {S/16, S/8, S/4, S/2, S}.  E* is the best energy found by any
     run of any method (per instance for config 5); a read succeeds when
     E <= E* + 0.01|E*|; tau is the call's device time with host buffers in and
-    out.  Config 5: plain = one call per instance, T99 = sum over instances of
-    tau_m * R99(p_m); batched = one call for all, T99 = tau * max_m R99(p_m),
-    R99(p) = ln(0.01)/ln(1-p) repetitions."""
+    out (pinned host memory, as a caller keeping its buffers pinned sees it;
+    the same for both methods).  Config 5: plain = one call per instance, T99 =
+    sum over instances of tau_m * R99(p_m); batched = one call for all, T99 =
+    tau * max_m R99(p_m), R99(p) = ln(0.01)/ln(1-p) repetitions."""
     import torch
     from openjij_b200 import _native as N
     I = _instances()
     torch.cuda.set_device(0)
     ctx = N.Context(0)
     w = _workload(args.config, None, None)
+
+    def pinned(a):
+        """A pinned host copy of the numpy array a (its numpy view)."""
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype))).pin_memory()
+        v = t.numpy()
+        v[...] = a
+        return v
     S = int(w["sweeps"]) if w["kind"] == "batch" else int(np.sum(w["mcs"]))
     ladder = sorted({max(1, S // d) for d in (16, 8, 4, 2, 1)})
     runs = []  # (method, S_l, tau_ms, energies, per-instance taus)
@@ -704,19 +712,25 @@ def run_tts(args):
         rng = np.random.default_rng(7)
         init = [rng.choice(np.array([-1, 1], np.int8), size=(int(r), n)) for r, n in zip(reads, sizes)]
         off = np.concatenate([[0], np.cumsum(reads)])
+        flat0 = np.concatenate([x.ravel() for x in init])
+        flat = pinned(flat0)
+        e = pinned(np.zeros(int(np.sum(reads))))
+        init_p = [pinned(x) for x in init]
+        em_p = [pinned(np.zeros(int(r))) for r in reads]
         for Sl in ladder:
             betas, mcs = I.geometric_betas(0.1, 10.0, Sl)
-            flat = np.concatenate([x.ravel() for x in init])
-            e = np.zeros(int(np.sum(reads)))
-            N.sa_run_batched(batch, reads, flat.copy(), betas, mcs, seed=3, energies=e)  # warm-up
+            flat[...] = flat0
+            N.sa_run_batched(batch, reads, flat, betas, mcs, seed=3, energies=e)  # warm-up
+            flat[...] = flat0
             st = N.sa_run_batched(batch, reads, flat, betas, mcs, seed=3, energies=e)
-            runs.append(("batched", Sl, st["total_ms"], [e[off[m]:off[m + 1]] for m in range(len(mats))], None))
+            runs.append(("batched", Sl, st["total_ms"], [e[off[m]:off[m + 1]].copy() for m in range(len(mats))],
+                         None))
             taus, es = [], []
             for m, g in enumerate(graphs):
-                em = np.zeros(int(reads[m]))
-                st = N.sa_run(g, init[m].copy(), betas, mcs, seed=3, kernel="dense_plain", energies=em)
+                init_p[m][...] = init[m]
+                st = N.sa_run(g, init_p[m], betas, mcs, seed=3, kernel="dense_plain", energies=em_p[m])
                 taus.append(st["total_ms"])
-                es.append(em)
+                es.append(em_p[m].copy())
             runs.append(("plain", Sl, float(np.sum(taus)), es, taus))
         emin = [min(float(np.min(r[3][m])) for r in runs) for m in range(len(mats))]
         out = {}
@@ -744,22 +758,27 @@ def run_tts(args):
                    "plain": "dense_plain" if args.config == 3 else "colour"}
         if args.kernel:
             methods["batched"] = args.kernel
+        sp = pinned(init)
+        e_sa = pinned(np.zeros(R))
+        e_sqa = pinned(np.zeros((R, T)))
         for Sl in ladder:
             for meth, kern in methods.items():
-                sp = init.copy()
                 if w["kind"] == "sa":
                     betas, mcs = I.geometric_betas(0.05, 5.0, Sl)
-                    e = np.zeros(R)
-                    N.sa_run(graph, sp.copy(), betas, mcs, seed=3, kernel=kern)  # warm-up
-                    st = N.sa_run(graph, sp, betas, mcs, seed=3, kernel=kern, energies=e)
+                    sp[...] = init
+                    N.sa_run(graph, sp, betas, mcs, seed=3, kernel=kern)  # warm-up
+                    sp[...] = init
+                    st = N.sa_run(graph, sp, betas, mcs, seed=3, kernel=kern, energies=e_sa)
+                    e = e_sa.copy()
                 else:
                     ss = np.linspace(0.0, 1.0, Sl)
                     betas = np.full(Sl, w["beta"])
                     mcs = np.ones(Sl, np.int32)
-                    et = np.zeros((R, T))
-                    N.sqa_run(graph, sp.copy(), w["gamma"], betas, ss, mcs, seed=3, kernel=kern)
-                    st = N.sqa_run(graph, sp, w["gamma"], betas, ss, mcs, seed=3, kernel=kern, energies=et)
-                    e = et.min(axis=1)  # get_solution: the best slice of each replica
+                    sp[...] = init
+                    N.sqa_run(graph, sp, w["gamma"], betas, ss, mcs, seed=3, kernel=kern)
+                    sp[...] = init
+                    st = N.sqa_run(graph, sp, w["gamma"], betas, ss, mcs, seed=3, kernel=kern, energies=e_sqa)
+                    e = e_sqa.min(axis=1)  # get_solution: the best slice of each replica
                 runs.append((meth, Sl, st["total_ms"], e, None))
         best = min(float(np.min(r[3])) for r in runs)
         out = {}

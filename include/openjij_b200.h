@@ -88,6 +88,9 @@ typedef struct oj_run_stats {
   int32_t threads;       /* threads per CTA of the annealing launch (tunable kernels, else 0) */
   int32_t variant;       /* register-budget variant (batched kernel, else 0) */
   int32_t tuned;         /* 1 when this call ran the autotuner */
+  double accepted;       /* accepted single-spin flips over all replicas and sweeps (the bit-packed
+                            kernels count every bit of their 32-replica words, padding replicas
+                            included); -1 for Swendsen-Wang, whose cluster moves are not counted */
 } oj_run_stats;
 
 const char* oj_version(void);

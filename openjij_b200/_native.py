@@ -49,7 +49,8 @@ class GraphInfo(C.Structure):
 class RunStats(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("launches", C.c_int32), ("sweeps", C.c_int64),
                 ("attempts", C.c_double), ("anneal_ms", C.c_float), ("total_ms", C.c_float),
-                ("cluster", C.c_int32), ("threads", C.c_int32), ("variant", C.c_int32), ("tuned", C.c_int32)]
+                ("cluster", C.c_int32), ("threads", C.c_int32), ("variant", C.c_int32), ("tuned", C.c_int32),
+                ("accepted", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

@@ -89,6 +89,7 @@ struct RunInfo {
   long long sweeps = 0;
   double attempts = 0;
   double anneal_ms = 0, total_ms = 0;
+  double accepted = 0;
 };
 RunInfo g_last_run;
 
@@ -101,6 +102,7 @@ void record(const oj_run_stats& st) {
   g_last_run.attempts += st.attempts;
   g_last_run.anneal_ms += st.anneal_ms;
   g_last_run.total_ms += st.total_ms;
+  g_last_run.accepted = (st.accepted < 0 || g_last_run.accepted < 0) ? -1.0 : g_last_run.accepted + st.accepted;
 }
 
 // ---------------------------------------------------------------------------
@@ -1298,6 +1300,7 @@ PYBIND11_MODULE(_cxxjij, m) {
     d["attempts"] = g_last_run.attempts;
     d["anneal_ms"] = g_last_run.anneal_ms;
     d["total_ms"] = g_last_run.total_ms;
+    d["accepted"] = g_last_run.accepted;
     return d;
   });
   m.def("version", []() { return std::string(oj_version()); });

@@ -189,6 +189,28 @@ cudaError_t single_energy(oj_ctx* ctx, oj_graph* g, int R, const int8_t* spins, 
                              ctx->eparts.as<double>(), R);
 }
 
+// The run's accepted-flip counter, zeroed on the stream, when statistics are
+// asked for: the main annealing launch gets rb with it, tuning launches do not.
+oj_status arm_counter(oj_ctx* ctx, oj_run_stats* stats, RngBase* rb) {
+  if (!stats) return OJ_OK;
+  cudaError_t e = ctx->counters.ensure(16);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters.ptr, 0, 16, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "run counters");
+  rb->flips = ctx->counters.as<unsigned long long>();
+  return OJ_OK;
+}
+
+// Reads the counter after the stream has drained.
+double read_counter(oj_ctx* ctx) {
+  unsigned long long v = 0;
+  if (cudaMemcpyAsync(&v, ctx->counters.ptr, 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return -1.0;
+  }
+  return (double)v;
+}
+
 bool autotune_requested(uint32_t flags) {
   if (flags & OJ_AUTOTUNE) return true;
   const char* e = std::getenv("OJ_AUTOTUNE");
@@ -313,6 +335,7 @@ oj_status oj_ctx_destroy(oj_ctx* ctx) {
     ctx->batch.release();
     ctx->fields.release();
     ctx->eparts.release();
+    ctx->counters.release();
     for (auto& e : ctx->ev)
       if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -482,6 +505,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   int P_used = 0, threads_used = 0, variant_used = 0;
   bool tuned_now = false;
   bool energies_in_kernel = false;  // the dense jump kernel wrote them (exact fields)
+  RngBase rbm = rb;                 // rb of the main annealing launch (counts accepted flips)
+  if (oj_status cs = arm_counter(ctx, stats, &rbm)) return cs;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED) {
@@ -554,7 +579,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     }
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
-      OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, rb, st, &launches, threads_used), "sa bit-packed kernel");
+      OJ_CK(launch_sa_msc(g, G, d_words, d_thr, d_alw, S, rbm, st, &launches, threads_used), "sa bit-packed kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_unpack(d_words, R, n, d_spins, st), "unpack");
     ++launches;
@@ -645,7 +670,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
       OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(items.size() / 2), d_counter, d_spins,
-                            d_beta, S, rb, 0, ctx->sm_count, st, &launches, variant, d_fields, d_foff, R, d_ek,
+                            d_beta, S, rbm, 0, ctx->sm_count, st, &launches, variant, d_fields, d_foff, R, d_ek,
                             d_soff),
             "sa dense jump kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
@@ -660,11 +685,11 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     if (S > 0) {
       if (kernel == OJ_KERNEL_DENSE_TC) {
         OJ_CK(cudaMemsetAsync(g->tc->status.ptr, 0, sizeof(int), st), "status reset");
-        OJ_CK(launch_sa_dense_tc(g, R, d_spins, d_beta, S, rb, 16, st, &launches), "sa dense tensor-core kernel");
+        OJ_CK(launch_sa_dense_tc(g, R, d_spins, d_beta, S, rbm, 16, st, &launches), "sa dense tensor-core kernel");
       } else if (kernel == OJ_KERNEL_DENSE_PLAIN)
-        OJ_CK(launch_sa_dense_plain(g, R, d_spins, d_beta, S, rb, st, &launches), "sa dense kernel");
+        OJ_CK(launch_sa_dense_plain(g, R, d_spins, d_beta, S, rbm, st, &launches), "sa dense kernel");
       else
-        OJ_CK(launch_sa_colour(g, R, d_spins, d_beta, S, rb, st, &launches), "sa colour kernel");
+        OJ_CK(launch_sa_colour(g, R, d_spins, d_beta, S, rbm, st, &launches), "sa colour kernel");
     }
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   }
@@ -710,6 +735,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+    stats->accepted = read_counter(ctx);
   }
   return OJ_OK;
 }
@@ -768,6 +794,8 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   int launches = 0;
   int P_used = 0, threads_used = 0;
   bool tuned_now = false;
+  RngBase rbm = rb;  // rb of the main annealing launch (counts accepted flips)
+  if (oj_status cs = arm_counter(ctx, stats, &rbm)) return cs;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED && split_ok) {
@@ -838,7 +866,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     threads_used = shp.threads ? shp.threads : split_default_threads();
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
-      OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rb, st, &launches, threads_used),
+      OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rbm, st, &launches, threads_used),
             "sqa slice-split kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_sqa_split_unpack(d_words, R, T, n, G, d_spins, st), "unpack");
@@ -859,7 +887,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     OJ_CK(launch_sqa_pack(d_spins, R, T, n, d_words, st), "pack");
     ++launches;
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-    if (S > 0) OJ_CK(launch_sqa_msc(g, R, T, d_words, d_thr, d_mode, S, rb, st, &launches), "sqa bit-packed kernel");
+    if (S > 0) OJ_CK(launch_sqa_msc(g, R, T, d_words, d_thr, d_mode, S, rbm, st, &launches), "sqa bit-packed kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     OJ_CK(launch_sqa_unpack(d_words, R, T, n, d_spins, st), "unpack");
     ++launches;
@@ -870,7 +898,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
       OJ_CK(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(float2), cudaMemcpyHostToDevice, st),
             "H2D coef");
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-    if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, rb, st, &launches), "sqa kernel");
+    if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, rbm, st, &launches), "sqa kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   }
   if (energies || best_slice) {
@@ -907,6 +935,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+    stats->accepted = read_counter(ctx);
   }
   return OJ_OK;
 }
@@ -1325,6 +1354,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   }
   const bool energies_in_kernel = energies && S > 0 && nitems > 0 && b->exact_fields;
   if (energies_in_kernel) OJ_CK(cudaMemsetAsync(d_e, 0, (size_t)nrep * 8, st), "energies of empty instances");
+  if (oj_status cs = arm_counter(ctx, stats, &rb)) return cs;  // after the tuning launches
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
   if (S > 0 && nitems > 0)
     OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
@@ -1358,6 +1388,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     stats->attempts = attempts_per_sweep * (double)S;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+    stats->accepted = read_counter(ctx);
   }
   return OJ_OK;
 }
@@ -1435,6 +1466,7 @@ oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     stats->sweeps = S;
     stats->attempts = (double)R * n * (double)S;
     stats->threads = 512;
+    stats->accepted = -1.0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
   }

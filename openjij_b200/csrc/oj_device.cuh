@@ -38,6 +38,15 @@ struct u4 {
   uint32_t x, y, z, w;
 };
 
+// Adds the warp's accepted flips (the sum of v over its lanes) to *ctr with
+// one atomic; every lane of the warp calls it, ctr may be null.
+__device__ __forceinline__ void add_flips(unsigned long long* ctr, unsigned long long v) {
+  if (!ctr) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
+}
+
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): per round
 // (c0,c1,c2,c3) <- (hi(M1*c2)^c1^k0, lo(M1*c2), hi(M0*c0)^c3^k1, lo(M0*c0)),
 // key bumped by the Weyl constants between rounds.

@@ -140,6 +140,7 @@ struct oj_ctx {
   std::string last_error;
   std::string noalloc_error;  // why the allocation-free entry point could not be set up ("" = ready)
   oj::DevBuf spins, words, params, energies, best, aux, batch, fields, eparts;
+  oj::DevBuf counters;  // device counters of a run (accepted flips)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -147,11 +148,14 @@ namespace oj {
 
 // Counter base of a run: Philox key and the global indices of the first sweep
 // and the first replica, so that a run split over calls (first_sweep) or over
-// GPUs (replica_offset) draws exactly the numbers of the unsplit run.
+// GPUs (replica_offset) draws exactly the numbers of the unsplit run; and the
+// device counter the annealing kernels add their accepted flips to (null: not
+// counted).
 struct RngBase {
   uint32_t k0, k1;
   uint32_t sweep0;
   uint32_t rep0;
+  unsigned long long* flips = nullptr;
 };
 
 // ---- launchers (each returns cudaGetLastError() after the launch) ---------

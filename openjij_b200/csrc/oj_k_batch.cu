@@ -20,9 +20,16 @@
 // the current fields, jumps to the first accepted site, applies that flip and
 // re-evaluates the sites after it: sites that do not flip leave the state
 // unchanged, so this is the sequential sweep, with one step per flip instead
-// of one per site.  The uniform of site i, sweep k, replica r of instance m is
-// Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3], r the replica's global
-// index (rep0 + index within the instance).
+// of one per site.  A flip updates at once only the fields of its own chunk
+// (held in registers, the sites still to be decided read them); it is noted in
+// the warp's flip list, and when the chunk is done every other chunk's fields
+// take the list in site order.  The next read of a field comes after that, and
+// each field takes the same FMAs in the same order as with the whole row
+// applied at every flip, so the state is that of the plain sequential sweep,
+// bit for bit; the field traffic in shared memory is one pass per chunk
+// instead of one per flip.  The uniform of site i, sweep k, replica r of
+// instance m is Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3], r the
+// replica's global index (rep0 + index within the instance).
 //
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
 // read through L1 one float4 per lane on every accepted flip, or from an FP16
@@ -46,7 +53,6 @@ namespace {
 
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
-constexpr int kMaxChunks = kBatchMaxN / 128;
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -74,6 +80,7 @@ struct BatchArgs {
   const int64_t* foff;     // [count] offset of instance m's fields (floats)
   double* E;               // FP64 energies from the final fields, or null (exact-field batches)
   const int64_t* eoff;     // [count] offset of instance m's energies
+  unsigned long long* flips;  // accepted-flip counter, or null
 };
 
 // Spin bits of chunk c of lane l: four bits of word 32*(c/8) + l.
@@ -111,9 +118,11 @@ __device__ __forceinline__ float4 row4h(const __half* p) {
 // The couplings of an instance are staged in shared memory (SJ) when the
 // batch's largest block of n rows x npad columns takes at most this many bytes.
 constexpr size_t kBatchSmemJBytes = 96 * 1024;
+// Bytes of each warp's flip list (one entry per site of a chunk).
+constexpr int kFlipList = 128;
 
-// GROUP: chunks of a flipped site's J row loaded before any is used (the
-// flip's L2 round trips are ceil(chunks / GROUP)); more costs registers.
+// GROUP: chunks whose fields take a chunk's delayed flips together (their row
+// loads are in flight at once); more costs registers.
 // H: the flip rows come from the FP16 copy of J (half the L2 bytes per flip).
 // SJ: every work item first copies its instance's couplings (FP32 or FP16
 // rows, as H says) into shared memory after the warps' fields and spin words,
@@ -127,8 +136,13 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
                  (size_t)warp * a.swstride;  // spin words [chunk / 8][lane]
-  // the staged couplings (SJ): after every warp's fields and spin words
-  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride);
+  // the warp's flips in the current chunk: chunk-local site | 0x80 when the
+  // spin was -1 before the flip
+  uint8_t* fl = reinterpret_cast<uint8_t*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride) +
+                (size_t)warp * kFlipList;
+  // the staged couplings (SJ): after every warp's fields, spin words and flip list
+  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride) + (size_t)W * kFlipList;
+  unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
@@ -186,13 +200,15 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
       const uint32_t kk = a.sweep0 + (uint32_t)k;
       for (int c = 0; c < nch; ++c) {
         const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
+        // the chunk's fields and this lane's spin bits stay in registers while
+        // the chunk is decided
+        float4 fc = reinterpret_cast<const float4*>(f)[32 * c + lane];
+        uint32_t myw = (sw[sw_word(c, lane)] >> sw_shift(c)) & 0xFu;
         {
           // a chunk none of whose sites has beta*dE below the largest -ln u
           // keeps its state: its uniforms are not drawn (the stream is
           // counter-based, so nothing after it moves)
-          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
-          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
-          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
+          const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
           uint32_t can = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -210,10 +226,9 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         // this lane's sites that exist and are not yet decided in this chunk
         // (chunk-local index at or past the last flip's + 1)
         uint32_t open = inside;
+        int nfl = 0;  // flips in this chunk (the same in every lane)
         for (;;) {
-          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
-          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
-          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
+          const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
           uint32_t mask = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -229,39 +244,65 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
           if (!lanes) break;
           const int ls = __ffs(lanes) - 1;
-          const uint32_t ms = __shfl_sync(0xffffffffu, mask, ls);
-          const int es = __ffs(ms) - 1;
-          const uint32_t ws = sw[sw_word(c, ls)];
-          const bool neg = (ws >> (sw_shift(c) + es)) & 1u;
+          // the first accepting lane's mask and spin bits
+          const uint32_t pk = __shfl_sync(0xffffffffu, mask | (myw << 4), ls);
+          const int es = __ffs(pk & 0xFu) - 1;
+          const uint32_t neg = (pk >> (4 + es)) & 1u;
           const float coef = neg ? 2.0f : -2.0f;
-          const int i = 128 * c + 4 * ls + es;
-          const float* Ji = Jr + (size_t)i * npad + 4 * lane;
-          const __half* Ji16 = Jr16 + (size_t)i * npad + 4 * lane;
-          // the row in groups of four chunks whose loads are in flight together
+          const int il = 4 * ls + es;  // chunk-local site
+          // the flip reaches this chunk's fields now (the sites still to be
+          // decided read them); the other chunks get it at the end of the chunk
+          const size_t roff = (size_t)(128 * c + il) * npad + 128 * c + 4 * lane;
+          const float4 v = H ? row4h<SJ>(Jr16 + roff) : row4<SJ>(Jr + roff);
+          fc.x = __fmaf_rn(coef, v.x, fc.x);
+          fc.y = __fmaf_rn(coef, v.y, fc.y);
+          fc.z = __fmaf_rn(coef, v.z, fc.z);
+          fc.w = __fmaf_rn(coef, v.w, fc.w);
+          if (lane == ls) myw ^= 1u << es;
+          if (lane == 0) {
+            fl[nfl] = (uint8_t)(il | (neg << 7));
+            ++nflip;
+          }
+          ++nfl;
+          open = inside & (0xFu << min(max(il + 1 - 4 * lane, 0), 4));
+        }
+        if (nfl == 0) continue;
+        reinterpret_cast<float4*>(f)[32 * c + lane] = fc;
+        {
+          uint32_t& wd = sw[sw_word(c, lane)];
+          wd = (wd & ~(0xFu << sw_shift(c))) | (myw << sw_shift(c));
+        }
+        __syncwarp();  // the flip list is complete
+        // Delayed update: every other chunk's fields take the chunk's flips in
+        // site order, one FMA each (c * J_ij exact), GROUP chunks at a time so
+        // their row loads are in flight together.  Each field sees the same
+        // sequence of roundings as with the whole row applied at every flip.
+#pragma unroll 1
+        for (int c0 = 0; c0 < nch; c0 += GROUP) {
+          float4 g[GROUP];
 #pragma unroll
-          for (int c0 = 0; c0 < kMaxChunks; c0 += GROUP) {
-            if (c0 >= nch) break;
-            float4 v[GROUP];
+          for (int q = 0; q < GROUP; ++q)
+            if (c0 + q < nch && c0 + q != c) g[q] = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
+#pragma unroll 2
+          for (int t = 0; t < nfl; ++t) {
+            const uint32_t e = fl[t];
+            const float cf = (e & 0x80u) ? 2.0f : -2.0f;
+            const size_t ro = (size_t)(128 * c + (int)(e & 0x7Fu)) * npad + 4 * lane;
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
-              if (c0 + q < nch) v[q] = H ? row4h<SJ>(Ji16 + 128 * (c0 + q)) : row4<SJ>(Ji + 128 * (c0 + q));
-#pragma unroll
-            for (int q = 0; q < GROUP; ++q)
-              if (c0 + q < nch) {
-                float4 g = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
-                g.x = __fmaf_rn(coef, v[q].x, g.x);
-                g.y = __fmaf_rn(coef, v[q].y, g.y);
-                g.z = __fmaf_rn(coef, v[q].z, g.z);
-                g.w = __fmaf_rn(coef, v[q].w, g.w);
-                reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g;
+              if (c0 + q < nch && c0 + q != c) {
+                const float4 v = H ? row4h<SJ>(Jr16 + ro + 128 * (c0 + q)) : row4<SJ>(Jr + ro + 128 * (c0 + q));
+                g[q].x = __fmaf_rn(cf, v.x, g[q].x);
+                g[q].y = __fmaf_rn(cf, v.y, g[q].y);
+                g[q].z = __fmaf_rn(cf, v.z, g[q].z);
+                g[q].w = __fmaf_rn(cf, v.w, g[q].w);
               }
           }
-          __syncwarp();
-          if (lane == ls) sw[sw_word(c, ls)] = ws ^ (1u << (sw_shift(c) + es));
-          const int pos = 4 * ls + es + 1;  // chunk-local index of the first site not yet decided
-          open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
-          __syncwarp();
+#pragma unroll
+          for (int q = 0; q < GROUP; ++q)
+            if (c0 + q < nch && c0 + q != c) reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g[q];
         }
+        __syncwarp();  // the list is read before the next chunk rewrites it
       }
     }
     if (a.E) {
@@ -293,6 +334,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     }
     __syncwarp();
   }
+  ojd::add_flips(a.flips, nflip);
 }
 
 // Batches whose instances have at most 128 sites (one chunk): the sweep of
@@ -306,6 +348,7 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];  // [n][128] couplings of the item's instance
   __shared__ int item_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) item_sh = atomicAdd(a.counter, 1);
@@ -384,6 +427,7 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
         fc.z = __fmaf_rn(coef, v.z, fc.z);
         fc.w = __fmaf_rn(coef, v.w, fc.w);
         if (lane == ls) wd ^= 1u << es;
+        if (lane == 0) ++nflip;
         open = inside & (0xFu << min(max(i + 1 - 4 * lane, 0), 4));
       }
     }
@@ -406,6 +450,7 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
       if (i < n) gs[i] = ((wd >> e) & 1u) ? (int8_t)-1 : (int8_t)1;
     }
   }
+  ojd::add_flips(a.flips, nflip);
 }
 
 // Initial fields of every replica of every instance,
@@ -652,10 +697,11 @@ __global__ void batch_energy_sum_kernel(const double* __restrict__ parts, int ns
 int batch_max_sites() { return kBatchMaxN; }
 int batch_warps() { return kBatchWarps; }
 
-// Launch variants: warps per CTA x minimum CTAs per SM (register budget).
+// Launch variants: warps per CTA x minimum CTAs per SM (register budget), and
+// the chunks that take a chunk's delayed flips together.
 // 45 = 4 warps, 102 registers, 8 chunks at a time (more CTAs per SM when the
 //      fields' shared memory limits residency);
-// 82 = 8 warps, 128 registers, a flip row's loads 16 chunks at a time;
+// 82 = 8 warps, 128 registers, 8 chunks at a time;
 // 83 = 8 warps, 80 registers; 84 = 8 warps, 64; 162 = 16 warps, 64; 321 = 32 warps, 64
 // (4 chunks at a time).
 int batch_min_warps() { return 4; }
@@ -674,11 +720,11 @@ bool batch_variant_valid(int variant) {
 }
 
 // largest n whose fields fit the variant: W warps x (FP32 fields + spin
-// words) within the 227 KB of shared memory per CTA
+// words + flip list) within the 227 KB of shared memory per CTA
 int batch_variant_max_n(int variant) {
   switch (variant) {
-    case 321: return 1664;
-    case 162: return 3456;
+    case 321: return 1536;
+    case 162: return 3328;
     default: return kBatchMaxN;
   }
 }
@@ -696,8 +742,8 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
   const bool sj = jbytes > 0;
   auto kern = h ? (sj ? sa_batch_kernel<W, MINB, GROUP, true, true> : sa_batch_kernel<W, MINB, GROUP, true, false>)
                 : (sj ? sa_batch_kernel<W, MINB, GROUP, false, true> : sa_batch_kernel<W, MINB, GROUP, false, false>);
-  // FP32 fields + spin words per warp, then the staged couplings
-  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4) + jbytes;
+  // FP32 fields + spin words + flip list per warp, then the staged couplings
+  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4 + kFlipList) + jbytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -758,6 +804,7 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.foff = d_foff;
   a.E = b->exact_fields ? d_energies : nullptr;
   a.eoff = d_eoff;
+  a.flips = rb.flips;
   if (b->count == 0 || max_reads <= 0 || nitems <= 0) return cudaSuccess;
   const int zt = (max_reads + kFieldReplicas - 1) / kFieldReplicas;
   cudaError_t e = cudaSuccess;
@@ -789,7 +836,7 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   if (jbytes > kBatchSmemJBytes) jbytes = 0;
   switch (variant) {
     case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st, b->j16, jbytes); break;
-    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    case 82: e = launch_variant<8, 2, 8>(a, nitems, sm_count, st, b->j16, jbytes); break;
     case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
     case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
     case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;

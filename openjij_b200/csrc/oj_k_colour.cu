@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(kColourThreads)
   const int r0 = 4 * q;
   const int nr = min(4, R - r0);
   int8_t* S = SMEM ? sh : spins + (size_t)r0 * n;
+  unsigned long long nflip = 0;
   if (SMEM) {
     for (int idx = threadIdx.x; idx < 4 * n; idx += blockDim.x) {
       const int rl = idx / n;
@@ -76,7 +77,10 @@ __global__ void __launch_bounds__(kColourThreads)
             // by 2 is exact); dE <= 0 accepts without a draw, and so does the
             // comparison, since -ln u > 0 and beta is finite and >= 0
             const float bf = __fmul_rn(beta2, fs[rl]);
-            if ((si > 0 ? -bf : bf) < ojd::neglog(ojd::pick(rnd, rl))) S[rl * n + i] = (int8_t)(-si);
+            if ((si > 0 ? -bf : bf) < ojd::neglog(ojd::pick(rnd, rl))) {
+              S[rl * n + i] = (int8_t)(-si);
+              ++nflip;
+            }
           }
         }
       }
@@ -86,6 +90,7 @@ __global__ void __launch_bounds__(kColourThreads)
   if (SMEM) {
     for (int idx = threadIdx.x; idx < nr * n; idx += blockDim.x) spins[(size_t)r0 * n + idx] = S[idx];
   }
+  ojd::add_flips(rb.flips, nflip);
 }
 
 constexpr int kSqaThreads = 512;
@@ -102,6 +107,7 @@ __global__ void __launch_bounds__(kSqaThreads)
   const int r = blockIdx.x;
   const size_t tn = (size_t)T * n;
   int8_t* S = SMEM ? sh : spins + (size_t)r * tn;
+  unsigned long long nflip = 0;
   if (SMEM) {
     for (size_t idx = threadIdx.x; idx < tn; idx += blockDim.x) S[idx] = spins[(size_t)r * tn + idx];
     __syncthreads();
@@ -146,7 +152,10 @@ __global__ void __launch_bounds__(kSqaThreads)
             const float dEtrot = (float)(-2 * (int)si * ssum);
             const float dE = __fadd_rn(__fmul_rn(ab.x, dEsp), __fmul_rn(ab.y, dEtrot));
             const float L = ojd::neglog(ojd::pick(rnd, j));
-            if (dE < L) St[i] = (int8_t)(-si);
+            if (dE < L) {
+              St[i] = (int8_t)(-si);
+              ++nflip;
+            }
           }
         }
         __syncthreads();
@@ -156,6 +165,7 @@ __global__ void __launch_bounds__(kSqaThreads)
   if (SMEM) {
     for (size_t idx = threadIdx.x; idx < tn; idx += blockDim.x) spins[(size_t)r * tn + idx] = S[idx];
   }
+  ojd::add_flips(rb.flips, nflip);
 }
 
 // FP64 energies of 32 spin vectors per CTA:

@@ -36,6 +36,7 @@ __global__ void __launch_bounds__(128)
   }
   __syncwarp();
   const uint32_t rg = rb.rep0 + (uint32_t)r;  // global replica index
+  unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   const uint32_t c2 = rg >> 2;
   const int lane_r = (int)(rg & 3u);
   for (int64_t k = 0; k < nsweeps; ++k) {
@@ -57,7 +58,10 @@ __global__ void __launch_bounds__(128)
           const float* Ji = J + (size_t)i * n;
           for (int j = lane; j < n; j += 32) f[j] = __fadd_rn(f[j], __fmul_rn(c, Ji[j]));
           __syncwarp();
-          if (lane == 0) s[i] = (int8_t)(-si);
+          if (lane == 0) {
+            s[i] = (int8_t)(-si);
+            ++nflip;
+          }
           __syncwarp();
         }
       }
@@ -65,6 +69,7 @@ __global__ void __launch_bounds__(128)
   }
   __syncwarp();
   for (int j = lane; j < n; j += 32) gs[j] = s[j];
+  ojd::add_flips(rb.flips, nflip);
 }
 
 }  // namespace

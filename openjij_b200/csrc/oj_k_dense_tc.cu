@@ -61,6 +61,7 @@ struct TcArgs {
   ojd::Keys keys;
   uint32_t sweep0, rep0;
   int* status;
+  unsigned long long* flips;  // accepted-flip counter, or null
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -217,6 +218,7 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
   const uint32_t tbase = *tslot;
   uint32_t ph_mma = 0, ph_full[2] = {0, 0};  // phase parities (meaningful in thread 0)
   bool ok = true;
+  unsigned long long nflip = 0;
 
   // B tile of block kb (hi and lo) into buffer `buf` (thread 0 only)
   auto load_b = [&](int kb, int buf) {
@@ -385,6 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
             }
           }
           const uint32_t nw = w ^ flips;
+          if (r_base + tid < a.R) nflip += __popc(flips);
           // dS row (BF16: +-2 where flipped = new s - old s) into every CTA's A buffer
           uint32_t pk[16];
 #pragma unroll
@@ -446,6 +449,7 @@ __global__ void __launch_bounds__(kThreads, 1) sa_dense_tc_kernel(TcArgs a) {
     }
   }
   if (!ok && tid == 0) atomicExch(a.status, 1);
+  ojd::add_flips(a.flips, nflip);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(tmem_cols));
@@ -557,6 +561,7 @@ cudaError_t launch_sa_dense_tc(const oj_graph* g, int R, int8_t* spins, const fl
   a.sweep0 = rb.sweep0;
   a.rep0 = rb.rep0;
   a.status = pl.status.as<int>();
+  a.flips = rb.flips;
   const size_t smem = dense_tc_smem(pl);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   auto kern = sa_dense_tc_kernel;

@@ -65,6 +65,7 @@ struct MscArgs {
   ojd::Keys keys;
   uint32_t sweep0;  // global index of the first sweep
   uint32_t group0;  // global index of the first replica group
+  unsigned long long* flips;  // accepted-flip counter (every bit of the group's words), or null
 };
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -158,23 +159,29 @@ __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restr
   return w ^ (flip | lt);
 }
 
-// Updates own slots [lo, hi), two independent sites per thread and iteration.
+// Updates own slots [lo, hi), two independent sites per thread and iteration;
+// returns the number of spins this thread flipped.
 template <int D>
-__device__ __forceinline__ void msc_range(int lo, int hi, uint32_t* __restrict__ Wsh,
-                                          const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
-                                          const uint16_t* __restrict__ nbr, const MscSweep<D>& sw,
-                                          uint32_t k, uint32_t g, const ojd::Keys& K) {
+__device__ __forceinline__ uint32_t msc_range(int lo, int hi, uint32_t* __restrict__ Wsh,
+                                              const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
+                                              const uint16_t* __restrict__ nbr, const MscSweep<D>& sw,
+                                              uint32_t k, uint32_t g, const ojd::Keys& K) {
   const int T = blockDim.x;
+  uint32_t nf = 0u;
   for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
     const int s2 = s + T;
-    const uint32_t a = msc_site<D>(Wsh[s], Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, K);
+    const uint32_t w0 = Wsh[s];
+    const uint32_t a = msc_site<D>(w0, Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, K);
     if (s2 < hi) {
-      const uint32_t b =
-          msc_site<D>(Wsh[s2], Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, K);
+      const uint32_t w2 = Wsh[s2];
+      const uint32_t b = msc_site<D>(w2, Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, K);
       Wsh[s2] = b;
+      nf += __popc(b ^ w2);
     }
     Wsh[s] = a;
+    nf += __popc(a ^ w0);
   }
+  return nf;
 }
 
 // Shared memory: words[slots] | gid[nlocmax] | jm[nlocmax] | nbr[nlocmax][D]
@@ -206,12 +213,13 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
   for (int s = threadIdx.x; s < nloc * D; s += blockDim.x) nbr[s] = nbr_g[s];
   __syncthreads();
   cluster_arrive();
+  unsigned long long nflip = 0;
   int prev = -1;  // colour class updated by the previous phase
   for (int64_t k = 0; k < a.nsweeps; ++k) {
     const MscSweep<D> sw = msc_sweep<D>(a.thr + (size_t)k * (D + 1), a.always[k]);
     const uint32_t kk = a.sweep0 + (uint32_t)k, gg = a.group0 + (uint32_t)g;
     for (int c = 0; c < a.ncol; ++c) {
-      msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
+      nflip += msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_wait();
       if (prev >= 0) {
         const int hlo = ho[prev], hhi = ho[prev + 1];
@@ -222,7 +230,7 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
         }
       }
       __syncthreads();
-      msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
+      nflip += msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_arrive();
       __syncthreads();
       prev = c;
@@ -230,6 +238,7 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
   }
   cluster_wait();
   for (int s = threadIdx.x; s < nloc; s += blockDim.x) gw[gid[s]] = Wsh[s];
+  ojd::add_flips(a.flips, nflip);
 }
 
 size_t msc_smem_bytes(const MscPlan& pl) {
@@ -469,6 +478,7 @@ cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint3
   a.keys = ojd::make_keys(rb.k0, rb.k1);
   a.sweep0 = rb.sweep0;
   a.group0 = rb.rep0 >> 5;
+  a.flips = rb.flips;
   if (launches) ++*launches;
   switch (pl.D) {
     case 1: return launch_d<1>(pl, a, G, st, threads);

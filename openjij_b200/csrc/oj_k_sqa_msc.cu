@@ -44,6 +44,7 @@ struct SqaMscArgs {
   int64_t nsweeps;
   ojd::Keys keys;
   uint32_t sweep0, rep0;
+  unsigned long long* flips;  // accepted-flip counter, or null
 };
 
 template <int D>
@@ -132,6 +133,7 @@ __global__ void __launch_bounds__(kSqaMscThreads) sqa_msc_kernel(SqaMscArgs a) {
   for (int t = 1; t < T; t += 2) gm1 |= 1u << t;
   const uint32_t gm2 = (T & 1) ? (1u << (T - 1)) : 0u;
   const uint32_t rep = a.rep0 + (uint32_t)r;
+  unsigned long long nflip = 0;
   __syncthreads();
   for (int64_t k = 0; k < a.nsweeps; ++k) {
     uint32_t th[NC];
@@ -146,14 +148,18 @@ __global__ void __launch_bounds__(kSqaMscThreads) sqa_msc_kernel(SqaMscArgs a) {
         const int lo = a.coff[c], hi = a.coff[c + 1];
         for (int idx = lo + threadIdx.x; idx < hi; idx += blockDim.x) {
           const int i = a.order[idx];
-          W[i] = sqa_site<D>(W[i], W, nbr + (size_t)i * D, jm[i], gmask, tmask, T, th, always, live,
-                             (uint32_t)i, kk, rep, (uint32_t)grp, a.keys);
+          const uint32_t w0 = W[i];
+          const uint32_t w1 = sqa_site<D>(w0, W, nbr + (size_t)i * D, jm[i], gmask, tmask, T, th, always, live,
+                                          (uint32_t)i, kk, rep, (uint32_t)grp, a.keys);
+          W[i] = w1;
+          nflip += __popc(w1 ^ w0);
         }
         __syncthreads();
       }
     }
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) gw[i] = W[i];
+  ojd::add_flips(a.flips, nflip);
 }
 
 // [R][T][n] int8 <-> [R][n] words (bit t = slice t, set iff s = -1)
@@ -230,6 +236,7 @@ cudaError_t launch_sqa_msc(const oj_graph* g, int R, int T, uint32_t* words, con
   a.keys = ojd::make_keys(rb.k0, rb.k1);
   a.sweep0 = rb.sweep0;
   a.rep0 = rb.rep0;
+  a.flips = rb.flips;
   if (launches) ++*launches;
   switch (g->info.max_degree) {
     case 1: return launch_d<1>(a, R, st);

@@ -62,6 +62,7 @@ struct SplitArgs {
   int64_t nsweeps;
   ojd::Keys keys;
   uint32_t sweep0, group0;
+  unsigned long long* flips;   // accepted-flip counter (every used bit of the words), or null
 };
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -142,28 +143,39 @@ __device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __res
   return x ^ flip ^ lt;
 }
 
+// Updates slots [lo, hi) of half X; returns the spins this thread flipped.
 template <int D>
-__device__ __forceinline__ void split_range(int lo, int hi, uint32_t* __restrict__ X, const uint32_t* __restrict__ Y,
-                                            const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
-                                            const uint16_t* __restrict__ nbr, int q, const SplitArgs& a,
-                                            const SplitSweep<D>& sw, uint32_t k, uint32_t g) {
+__device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __restrict__ X,
+                                                const uint32_t* __restrict__ Y, const int32_t* __restrict__ gid,
+                                                const uint16_t* __restrict__ jm, const uint16_t* __restrict__ nbr,
+                                                int q, const SplitArgs& a, const SplitSweep<D>& sw, uint32_t k,
+                                                uint32_t g) {
   const int T = blockDim.x;
+  uint32_t nf = 0u;
   if constexpr (D <= 4) {  // two independent sites per iteration
     for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
       const int s2 = s + T;
-      const uint32_t v =
-          split_site<D>(X[s], X, nbr + (size_t)s * D, jm[s], Y[s], q, a, sw, (uint32_t)gid[s], k, g);
+      const uint32_t x0 = X[s];
+      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, sw, (uint32_t)gid[s], k, g);
       if (s2 < hi) {
+        const uint32_t x2 = X[s2];
         const uint32_t w2 =
-            split_site<D>(X[s2], X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, sw, (uint32_t)gid[s2], k, g);
+            split_site<D>(x2, X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, sw, (uint32_t)gid[s2], k, g);
         X[s2] = w2;
+        nf += __popc(w2 ^ x2);
       }
       X[s] = v;
+      nf += __popc(v ^ x0);
     }
   } else {
-    for (int s = lo + threadIdx.x; s < hi; s += T)
-      X[s] = split_site<D>(X[s], X, nbr + (size_t)s * D, jm[s], Y[s], q, a, sw, (uint32_t)gid[s], k, g);
+    for (int s = lo + threadIdx.x; s < hi; s += T) {
+      const uint32_t x0 = X[s];
+      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, sw, (uint32_t)gid[s], k, g);
+      X[s] = v;
+      nf += __popc(v ^ x0);
+    }
   }
+  return nf;
 }
 
 // Shared memory: E[slots] | O[slots] | gid[nlocmax] | jm[nlocmax] | nbr[nlocmax][D]
@@ -204,6 +216,7 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
   for (int s = threadIdx.x; s < nloc * D; s += blockDim.x) nbr[s] = nbr_g[s];
   __syncthreads();
   if constexpr (CL) cluster_arrive();
+  unsigned long long nflip = 0;
   int prev_c = -1, prev_q = 0;  // colour class and half updated by the previous phase
   const uint32_t gg = a.group0 + (uint32_t)g;
   for (int64_t k = 0; k < a.nsweeps; ++k) {
@@ -219,7 +232,7 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
       for (int c = 0; c < a.ncol; ++c) {
         if constexpr (CL) {
           cg::cluster_group cl = cg::this_cluster();
-          split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          nflip += split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
           cluster_wait();
           if (prev_c >= 0) {
             uint32_t* P = prev_q ? WO : WE;
@@ -231,13 +244,13 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
             }
           }
           __syncthreads();
-          split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          nflip += split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
           cluster_arrive();
           __syncthreads();
           prev_c = c;
           prev_q = q;
         } else {
-          split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          nflip += split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
           __syncthreads();
         }
       }
@@ -249,6 +262,7 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
     gE[i] = WE[s];
     gO[i] = WO[s];
   }
+  ojd::add_flips(a.flips, nflip);
 }
 
 // [R][T][n] int8 <-> [G][2][n] words
@@ -409,6 +423,7 @@ cudaError_t launch_sqa_split(const oj_graph* g, int G, int T, uint32_t* words, c
   a.keys = ojd::make_keys(rb.k0, rb.k1);
   a.sweep0 = rb.sweep0;
   a.group0 = rb.rep0 / (uint32_t)P;
+  a.flips = rb.flips;
   if (launches) ++*launches;
   switch (pl.D) {
     case 1: return launch_d<1>(pl, a, G, st, threads);
