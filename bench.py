@@ -383,6 +383,60 @@ def _algo_per_attempt(w, n, kernel, degree, R=1):
     return 2.0 * n, "TFLOP/s", None  # one field-row update of 2n flop per attempt
 
 
+def _issue_profile(kernel_key):
+    """Warp instructions per attempt of a bit-packed kernel, from the committed
+    ncu summary profiles/issue_counts.json (smsp__inst_executed.sum of one
+    launch over its attempts), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "issue_counts.json")) as f:
+            d = json.load(f)
+        return d[kernel_key]
+    except Exception:
+        return None
+
+
+def _sm_clock_hz(clk):
+    """The sampled median SM clock of the timed region (else the measured maximum)."""
+    if clk.get("sm_mhz"):
+        return float(clk["sm_mhz"]) * 1e6
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["sm_max_mhz"]) * 1e6
+    except Exception:
+        return 1965e6
+
+
+def _roofline_issue(kernel_key, attempts, kms, clk, sm_count, hbm_side):
+    """Integer-issue roofline of a bit-packed kernel: warp instructions per
+    attempt (ncu, committed) x attempts / kernel time against one instruction
+    per cycle on each of the 4 schedulers of every SM at the sampled clock."""
+    prof = _issue_profile(kernel_key)
+    f = _sm_clock_hz(clk)
+    peak = sm_count * 4 * f / 1e9
+    out = {"bound": "issue", "unit": "Gwarp-inst/s", "peak": peak,
+           "peak_kind": f"{sm_count} SMs x 4 schedulers x the sampled SM clock ({f / 1e6:.0f} MHz)",
+           "kernel_ms": kms, "hbm_side": hbm_side}
+    if prof is None:
+        out.update(achieved=None, frac=None, note="no committed instruction count for this kernel")
+        return out
+    ipa = float(prof["inst_per_attempt"])
+    achieved = ipa * attempts / (kms / 1000.0) / 1e9
+    out.update(achieved=achieved, frac=achieved / peak, inst_per_attempt=ipa,
+               inst_source=f"profiles/issue_counts.json [{kernel_key}]: {prof['workload']}")
+    return out
+
+
+def _roofline_fp32(flops, kms, clk, sm_count, note):
+    """FP32 roofline of a CUDA-core dense kernel: the field-row FMAs it
+    executes (2n flop per accepted flip) against 128 FP32 FMA lanes per SM."""
+    f = _sm_clock_hz(clk)
+    peak = sm_count * 128 * 2 * f / 1e12
+    achieved = flops / (kms / 1000.0) / 1e12
+    return {"bound": "fp32", "unit": "TFLOP/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "peak_kind": f"{sm_count} SMs x 128 FP32 lanes x 2 flop x the sampled SM clock ({f / 1e6:.0f} MHz)",
+            "kernel_ms": kms, "note": note}
+
+
 def run_ours_batch(args, w):
     """Config 5: every instance of the batch in one oj_sa_run_batched call."""
     import torch
@@ -428,7 +482,7 @@ def run_ours_batch(args, w):
     torch.cuda.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kern_ms, launches = [], 0
+    kern_ms, launches, acc_steps, drift_steps = [], 0, [], []
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.zero_()
@@ -437,6 +491,9 @@ def run_ours_batch(args, w):
             st = step(args.warmup + k, work, energies, True)
             ends[k].record(stream)
             kern_ms.append(st["anneal_ms"])
+            acc_steps.append(st["accepted"])
+            if st["field_drift"] >= 0:
+                drift_steps.append(st["field_drift"])
             launches += st["launches"] + 1
         torch.cuda.synchronize()
     ms = float(np.mean([a.elapsed_time(b) for a, b in zip(starts, ends)]))
@@ -461,9 +518,14 @@ def run_ours_batch(args, w):
         t = torch.tensor([e2], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2 = float(t[0])
-    peak, peak_kind = _tensor_peak()
-    flops = float(np.sum(reads * 2.0 * sizes * sizes)) * S  # algorithmic 2n flop per attempt
-    achieved = flops / (kms / 1000.0) / 1e12
+    acc_per_step = float(np.mean(acc_steps))
+    n_eff = float(np.sum(reads * sizes.astype(np.float64) ** 2) / np.sum(reads * sizes))
+    clk_sum = clk.summary()
+    roof = _roofline_fp32(acc_per_step * 2.0 * n_eff, kms, clk_sum, torch.cuda.get_device_properties(local).multi_processor_count,
+                          f"executed field-row updates: accepted flips per step ({acc_per_step:.4g}) x 2 n_eff flop, "
+                          f"n_eff = {n_eff:.1f} the attempt-weighted instance size")
+    roof["traffic"] = None
+    roof["field_drift"] = float(np.max(drift_steps)) if drift_steps else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -480,14 +542,12 @@ def run_ours_batch(args, w):
             "config": _config_of(w),
             "kernel": {"name": "batched", "launch_shape": {"threads": st["threads"], "variant": st["variant"],
                                                            "autotuned": True}},
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "kernel_ms": kms,
-                         "algorithmic_per_attempt": "2n flop"},
+            "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": attempts_per_step * ws / (e2 / 1000.0), "unit": "attempts/s",
                     "h2d_bytes_per_step": total, "d2h_bytes_per_step": total + 8 * nrep, "ms_per_step": e2},
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clk_sum,
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -552,7 +612,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kern_ms, launches = [], 0
+    kern_ms, launches, acc_steps, drift_steps = [], 0, [], []
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.zero_()  # L2 flush between timed steps (the state fits in L2)
@@ -560,6 +620,9 @@ def run_ours(args):
             st = step(args.warmup + k)
             ends[k].record(stream)
             kern_ms.append(st["anneal_ms"])
+            acc_steps.append(st["accepted"])
+            if st.get("field_drift", -1.0) >= 0:
+                drift_steps.append(st["field_drift"])
             used_kernel = st["kernel"]
             launches += st["launches"] + 1  # + the device-to-device copy of the initial spins
         torch.cuda.synchronize()
@@ -592,12 +655,32 @@ def run_ours(args):
 
     hbm_peak, peak_kind = _peaks()
     per, unit, packed = _algo_per_attempt(w, n, used_kernel, graph.info()["max_degree"], R)
-    if unit == "GB/s":
-        achieved = attempts_per_step * per / (kms / 1000.0) / 1e9
-        peak = hbm_peak
+    clk_sum = clk.summary()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    if used_kernel == "bitpacked":
+        # integer-issue bound (profiles/): the int8-state HBM figure is a side number
+        hbm = attempts_per_step * per / (kms / 1000.0) / 1e9
+        side = {"achieved_gbs": hbm, "peak_gbs": hbm_peak, "frac": hbm / hbm_peak, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_attempt": per, "layout_bytes_per_attempt": packed,
+                "note": "int8 state bytes per attempt against the HBM copy peak; the kernel keeps the state "
+                        "bit-packed in shared memory and DRAM is idle"}
+        key = "sa_msc_kernel" if w["kind"] == "sa" else "sqa_split_kernel"
+        roof = _roofline_issue(key, attempts_per_step, kms, clk_sum, sm_count, side)
+        roof["traffic"] = _traffic_from_profiles() if args.config == 2 else None
+    elif used_kernel in ("dense_jump", "dense_plain", "dense_tc"):
+        acc = float(np.mean(acc_steps))
+        roof = _roofline_fp32(acc * 2.0 * n, kms, clk_sum, sm_count,
+                              f"executed field-row updates: accepted flips per step ({acc:.4g}) x 2n flop")
+        roof["traffic"] = None
+        roof["field_drift"] = float(np.max(drift_steps)) if drift_steps else None
     else:
-        achieved = attempts_per_step * per / (kms / 1000.0) / 1e12
-        peak, peak_kind = _tensor_peak()
+        achieved = attempts_per_step * per / (kms / 1000.0) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": None, "peak_kind": peak_kind, "kernel_ms": kms, "algorithmic_per_attempt": per,
+                "note": ("bond-list bytes per spin update (d/2 bonds of 13 B, spin read and write) against the "
+                         "HBM copy peak; union-find in shared memory, latency bound")
+                if used_kernel == "swendsen_wang" else
+                "algorithmic int8 state bytes per attempt against the HBM copy peak"}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu and used_kernel == "swendsen_wang":
         threads = os.cpu_count() or 1
@@ -626,30 +709,17 @@ def run_ours(args):
             "config": _config_of(w),
             "kernel": {"name": used_kernel, "launch_shape": {"cluster": st["cluster"], "threads": st["threads"],
                                                              "variant": st["variant"], "autotuned": True}},
-            "roofline": {"bound": w["bound"], "achieved": achieved, "peak": peak, "unit": unit,
-                         "note": ("algorithmic int8 state bytes per attempt against the HBM copy peak; the "
-                                  "kernel keeps the state bit-packed in shared memory (layout_bytes_per_attempt, "
-                                  "a fraction of the int8 count, so frac can pass 1) and is integer-issue "
-                                  "bound (profiles/)")
-                         if unit == "GB/s" and packed is not None else
-                         ("bond-list bytes per spin update (d/2 bonds of 13 B, spin read and write) against the "
-                          "HBM copy peak; union-find in shared memory, latency bound")
-                         if used_kernel == "swendsen_wang" else
-                         "algorithmic int8 state bytes per attempt against the HBM copy peak"
-                         if unit == "GB/s" else
-                         ("algorithmic 2n flop per attempt against the BF16 tensor peak; the dense "
-                          "kernels update a field row only on accepted flips (profiles/)"),
-                         "frac": achieved / peak,
-                         "traffic": _traffic_from_profiles() if args.config == 2 and used_kernel == "bitpacked"
-                         else None,
-                         "peak_kind": peak_kind, "kernel_ms": kms,
-                         "algorithmic_per_attempt": per, "layout_bytes_per_attempt": packed},
+            "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(R * T * n),
                     "d2h_bytes_per_step": int(R * T * n + 8 * R * T), "ms_per_step": e2},
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clk_sum,
         }
+        if ws == 1 and not args.no_tts and args.config == 2 and kernel == w["kernel"]:
+            # time to 1 % of the best energy, batched / mixed against the plain
+            # single-instance FP32 kernel (configs 3-5), outside the timed region
+            line["time_to_1pct"] = tts_summary()
         print(json.dumps(line), flush=True)
     graph.close()
     ctx.close()
@@ -678,6 +748,27 @@ def _best_of(cands):
 
 
 def run_tts(args):
+    """Prints the time-to-1%-energy line of --config (see tts_line)."""
+    print(json.dumps(tts_line(args.config, args.kernel)), flush=True)
+    return 0
+
+
+def tts_summary():
+    """The configs 3-5 time-to-1%-energy comparison, carried by the default
+    bench line: per config the two T99 (ms) and plain / batched."""
+    out = {}
+    for c in (3, 4, 5):
+        d = tts_line(c, None)
+        out[f"config{c}"] = {"workload": d["config"]["workload"], "batched_t99_ms": d["batched"]["t99_ms"],
+                             "batched_kernel": d["batched"].get("kernel", "batched"),
+                             "batched_num_sweeps": d["batched"]["num_sweeps"],
+                             "plain_t99_ms": d["plain"]["t99_ms"], "plain_kernel": d["plain"].get("kernel", "dense_plain"),
+                             "plain_num_sweeps": d["plain"]["num_sweeps"],
+                             "plain_over_batched": d["plain_over_batched"]}
+    return out
+
+
+def tts_line(config, kernel=None):
     """Time-to-1%-energy on configs 3-5: the batched / mixed-precision kernel
     against the plain single-instance FP32 kernel, each over a ladder of
     num_sweeps {S/16, S/8, S/4, S/2, S}.  E* is the best energy found by any
@@ -692,7 +783,7 @@ def run_tts(args):
     I = _instances()
     torch.cuda.set_device(0)
     ctx = N.Context(0)
-    w = _workload(args.config, None, None)
+    w = _workload(config, None, None)
 
     def pinned(a):
         """A pinned host copy of the numpy array a (its numpy view)."""
@@ -754,10 +845,10 @@ def run_tts(args):
         rng = np.random.default_rng(7)
         shape = (R, n) if w["kind"] == "sa" else (R, T, n)
         init = rng.choice(np.array([-1, 1], np.int8), size=shape)
-        methods = {"batched": "dense_jump" if args.config == 3 else "bitpacked",
-                   "plain": "dense_plain" if args.config == 3 else "colour"}
-        if args.kernel:
-            methods["batched"] = args.kernel
+        methods = {"batched": "dense_jump" if config == 3 else "bitpacked",
+                   "plain": "dense_plain" if config == 3 else "colour"}
+        if kernel:
+            methods["batched"] = kernel
         sp = pinned(init)
         e_sa = pinned(np.zeros(R))
         e_sqa = pinned(np.zeros((R, T)))
@@ -796,8 +887,8 @@ def run_tts(args):
             "config": {"workload": w["name"], "ladder": ladder}, "best_energy": best,
             "batched": out["batched"], "plain": out["plain"],
             "plain_over_batched": out["plain"]["t99_ms"] / out["batched"]["t99_ms"]}
-    print(json.dumps(line), flush=True)
-    return 0
+    ctx.close()
+    return line
 
 
 def main():
@@ -815,6 +906,8 @@ def main():
     ap.add_argument("--kernel", default=None,
                     help="force a kernel: colour, dense_plain, bitpacked, dense_tc, dense_jump, or "
                          "swendsen_wang for the cluster updater (default: planner)")
+    ap.add_argument("--no-tts", action="store_true",
+                    help="leave the configs 3-5 time-to-1%% comparison out of the default line")
     ap.add_argument("--tts", action="store_true",
                     help="time-to-1%%-energy of the batched/mixed kernel vs the plain kernel (configs 3-5)")
     args = ap.parse_args()

@@ -91,6 +91,12 @@ typedef struct oj_run_stats {
   double accepted;       /* accepted single-spin flips over all replicas and sweeps (the bit-packed
                             kernels count every bit of their 32-replica words, padding replicas
                             included); -1 for Swendsen-Wang, whose cluster moves are not counted */
+  double field_drift;    /* batched / dense-jump runs: the largest |f - f_exact| of the FP32
+                            incremental fields over sites, replicas and the points where they are
+                            recomputed (every oj_ctx_set_field_recompute sweeps) or checked (after
+                            the last sweep), f_exact the tensor-core fields of the same spins
+                            (within n 2^(E-27) of the FP64 field, E the exponent of max|J|);
+                            0 when the couplings make the FP32 sums exact; -1 for other kernels */
 } oj_run_stats;
 
 const char* oj_version(void);
@@ -103,6 +109,21 @@ oj_status oj_ctx_destroy(oj_ctx* ctx);
 oj_status oj_ctx_set_stream(oj_ctx* ctx, void* cuda_stream);
 oj_status oj_ctx_synchronize(oj_ctx* ctx);
 const char* oj_ctx_last_error(const oj_ctx* ctx);
+
+/* Full field recompute interval of the batched and dense-jump runs (the
+ * reference's reset_dE, include/openjij/system/classical_ising.hpp:87-90, on
+ * the tensor cores): for couplings whose FP32 field sums are not exact, the
+ * fields are computed anew from the spins before every global sweep that is a
+ * multiple of `sweeps` (default 16; 0 = only at the start of a call).  A run
+ * split over calls at multiples of `sweeps` reproduces the unsplit run. */
+oj_status oj_ctx_set_field_recompute(oj_ctx* ctx, int32_t sweeps);
+
+/* Iterations after which the field kernel's pipeline waits give up (< 0: the
+ * default, about a second).  A wait that gives up makes the kernel stop
+ * issuing work, wait for its copies and MMAs in flight with the default limit,
+ * free its tensor memory and return; the call reports OJ_ERR_TIMEOUT and the
+ * context stays usable.  For tests of that path (0 gives up at once). */
+oj_status oj_ctx_set_wait_limit(oj_ctx* ctx, int64_t iterations);
 
 /* Graph upload.  Replaces cxxjij.graph.Dense(num_spins).set_interaction_matrix
  * (openjij/declare.hpp:75-129; include/openjij/graph/dense.hpp:117-140) and

@@ -36,7 +36,8 @@ EXPORTS = [
     "oj_ctx_synchronize", "oj_ctx_last_error", "oj_graph_create_dense", "oj_graph_create_csr",
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
     "oj_sa_run_bitpacked_noalloc", "oj_batch_create_dense", "oj_batch_destroy", "oj_sa_run_batched",
-    "oj_sw_run", "oj_graph_flip_stats", "oj_batch_flip_stats",
+    "oj_sw_run", "oj_graph_flip_stats", "oj_batch_flip_stats", "oj_ctx_set_field_recompute",
+    "oj_ctx_set_wait_limit",
 ]
 
 
@@ -50,7 +51,7 @@ class RunStats(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("launches", C.c_int32), ("sweeps", C.c_int64),
                 ("attempts", C.c_double), ("anneal_ms", C.c_float), ("total_ms", C.c_float),
                 ("cluster", C.c_int32), ("threads", C.c_int32), ("variant", C.c_int32), ("tuned", C.c_int32),
-                ("accepted", C.c_double)]
+                ("accepted", C.c_double), ("field_drift", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -82,6 +83,8 @@ def lib():
         L.oj_ctx_destroy.argtypes = [vp]
         L.oj_ctx_set_stream.argtypes = [vp, vp]
         L.oj_ctx_synchronize.argtypes = [vp]
+        L.oj_ctx_set_field_recompute.argtypes = [vp, i32]
+        L.oj_ctx_set_wait_limit.argtypes = [vp, i64]
         L.oj_ctx_last_error.argtypes = [vp]
         L.oj_ctx_last_error.restype = C.c_char_p
         L.oj_graph_create_dense.argtypes = [vp, i32, vp, C.POINTER(vp)]
@@ -138,6 +141,14 @@ class Context:
 
     def synchronize(self):
         self.check(lib().oj_ctx_synchronize(self._h), "synchronize")
+
+    def set_field_recompute(self, sweeps: int):
+        """Full field recompute every `sweeps` sweeps of batched / dense-jump runs (0 = never)."""
+        self.check(lib().oj_ctx_set_field_recompute(self._h, int(sweeps)), "set_field_recompute")
+
+    def set_wait_limit(self, iterations: int):
+        """Iterations of the field kernel's bounded pipeline waits (< 0: the default)."""
+        self.check(lib().oj_ctx_set_wait_limit(self._h, int(iterations)), "set_wait_limit")
 
     def close(self):
         if self._h:

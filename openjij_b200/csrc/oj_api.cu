@@ -189,26 +189,116 @@ cudaError_t single_energy(oj_ctx* ctx, oj_graph* g, int R, const int8_t* spins, 
                              ctx->eparts.as<double>(), R);
 }
 
-// The run's accepted-flip counter, zeroed on the stream, when statistics are
-// asked for: the main annealing launch gets rb with it, tuning launches do not.
-oj_status arm_counter(oj_ctx* ctx, oj_run_stats* stats, RngBase* rb) {
-  if (!stats) return OJ_OK;
-  cudaError_t e = ctx->counters.ensure(16);
-  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters.ptr, 0, 16, ctx->stream);
+// Device counters of a run, zeroed on the stream before its launches:
+// [0] accepted flips (u64), [8] largest field drift (float bits), [12] status
+// of the bounded device waits.  The main annealing launch gets rb with the
+// flip counter when statistics are asked for (tuning launches never do).
+oj_status arm_counters(oj_ctx* ctx, oj_run_stats* stats, RngBase* rb) {
+  cudaError_t e = ctx->counters.ensure(32);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters.ptr, 0, 32, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "run counters");
-  rb->flips = ctx->counters.as<unsigned long long>();
+  if (stats) rb->flips = ctx->counters.as<unsigned long long>();
   return OJ_OK;
 }
 
-// Reads the counter after the stream has drained.
-double read_counter(oj_ctx* ctx) {
-  unsigned long long v = 0;
-  if (cudaMemcpyAsync(&v, ctx->counters.ptr, 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+struct RunCounters {
+  double flips = -1.0;
+  float drift = -1.0f;
+  int status = 0;
+};
+
+// The counters after the stream has drained.
+RunCounters read_counters(oj_ctx* ctx) {
+  RunCounters rc;
+  unsigned char buf[16];
+  if (cudaMemcpyAsync(buf, ctx->counters.ptr, 16, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
       cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
     cudaGetLastError();
-    return -1.0;
+    return rc;
   }
-  return (double)v;
+  unsigned long long f;
+  std::memcpy(&f, buf, 8);
+  std::memcpy(&rc.drift, buf + 8, 4);
+  std::memcpy(&rc.status, buf + 12, 4);
+  rc.flips = (double)f;
+  return rc;
+}
+
+// Work items of the tensor-core field kernel for a batch call, uploaded to the
+// context; drift and status go to the run counters (armed before).
+oj_status field_call(oj_ctx* ctx, const oj_batch* b, const int32_t* reads, const std::vector<int>& order,
+                     int max_reads, FieldCall* fc) {
+  fc->NT = field_tc_tile_replicas(b, max_reads);
+  std::vector<int32_t> it;
+  field_tc_items(b, reads, order, fc->NT, it);
+  fc->nitems = (int)(it.size() / 3);
+  cudaError_t e = ctx->fitems.ensure(std::max<size_t>(it.size() * 4, 16));
+  if (e == cudaSuccess && !it.empty())
+    e = cudaMemcpyAsync(ctx->fitems.ptr, it.data(), it.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "field items");
+  fc->items = ctx->fitems.as<int32_t>();
+  char* cb = ctx->counters.as<char>();
+  fc->drift = reinterpret_cast<unsigned int*>(cb + 8);
+  fc->status = reinterpret_cast<int*>(cb + 12);
+  fc->wait_limit = ctx->wait_limit;
+  return OJ_OK;
+}
+
+// Sweep-kernel arguments of a batched run besides the sweep range.
+struct SweepPlan {
+  const oj_batch* b;
+  const int32_t* d_reads;
+  const int64_t* d_soff;
+  const int32_t* d_items;
+  int nitems;
+  int* d_counter;
+  int8_t* spins;
+  const float* d_betas;  // one per sweep
+  uint32_t inst0;
+  int variant;
+  float* d_fields;
+  const int64_t* d_foff;
+  double* d_energies;
+  const int64_t* d_eoff;
+};
+
+// A batched (or dense-jump) run of S sweeps: the fields of the initial spins on
+// the tensor cores, then the sweeps.  When the batch's FP32 field sums are not
+// exact, the run is cut at every multiple of ctx->recompute global sweeps and
+// the fields are computed anew there from the spins (the same cut points for a
+// run split over calls at such multiples); with `measure`, the sweep kernel
+// stores its incremental fields before each recompute and after the last
+// sweep, and the field kernel records their largest deviation (the drift).
+cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, const FieldCall& fc, bool measure,
+                      int* launches) {
+  cudaStream_t st = ctx->stream;
+  const bool exact = p.b->exact_fields;
+  const bool wf = measure && !exact;
+  cudaError_t e = launch_field_tc(p.b, p.d_reads, p.d_soff, p.spins, p.d_fields, p.d_foff, fc.items, fc.nitems, fc.NT,
+                                  false, fc.drift, fc.status, fc.wait_limit, st);
+  if (e != cudaSuccess) return e;
+  ++*launches;
+  const int64_t K = exact ? 0 : ctx->recompute;
+  int64_t k = 0;
+  while (k < S) {
+    const uint64_t g = (uint64_t)rb.sweep0 + (uint64_t)k;
+    int64_t len = S - k;
+    if (K > 0) len = std::min<int64_t>(len, K - (int64_t)(g % (uint64_t)K));
+    RngBase rs = rb;
+    rs.sweep0 = (uint32_t)g;
+    e = launch_batch_sweeps(p.b, p.d_reads, p.d_soff, p.d_items, p.nitems, p.d_counter, p.spins, p.d_betas + k, len,
+                            rs, p.inst0, ctx->sm_count, st, launches, p.variant, p.d_fields, p.d_foff, p.d_energies,
+                            p.d_eoff, wf);
+    if (e != cudaSuccess) return e;
+    k += len;
+    if (k < S || wf) {
+      e = launch_field_tc(p.b, p.d_reads, p.d_soff, p.spins, p.d_fields, p.d_foff, fc.items, fc.nitems, fc.NT, wf,
+                          fc.drift, fc.status, fc.wait_limit, st);
+      if (e != cudaSuccess) return e;
+      ++*launches;
+    }
+  }
+  return cudaSuccess;
 }
 
 bool autotune_requested(uint32_t flags) {
@@ -365,6 +455,18 @@ oj_status oj_ctx_synchronize(oj_ctx* ctx) {
 
 const char* oj_ctx_last_error(const oj_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+oj_status oj_ctx_set_field_recompute(oj_ctx* ctx, int32_t sweeps) {
+  if (!ctx || sweeps < 0) return arg_fail(ctx, "the recompute interval must be >= 0");
+  ctx->recompute = sweeps;
+  return OJ_OK;
+}
+
+oj_status oj_ctx_set_wait_limit(oj_ctx* ctx, int64_t iterations) {
+  if (!ctx) return OJ_ERR_ARG;
+  ctx->wait_limit = iterations < 0 ? -1 : (long long)iterations;
+  return OJ_OK;
+}
+
 oj_status oj_graph_create_csr(oj_ctx* ctx, int32_t n, const int64_t* indptr, const int32_t* indices,
                               const double* data, oj_graph** out) {
   if (!ctx || !out || n < 0 || !indptr) return arg_fail(ctx, "null argument or negative size");
@@ -506,7 +608,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   bool tuned_now = false;
   bool energies_in_kernel = false;  // the dense jump kernel wrote them (exact fields)
   RngBase rbm = rb;                 // rb of the main annealing launch (counts accepted flips)
-  if (oj_status cs = arm_counter(ctx, stats, &rbm)) return cs;
+  if (oj_status cs = arm_counters(ctx, stats, &rbm)) return cs;
+  bool field_run = false;           // the tensor-core field kernel ran (drift and status to read)
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED) {
@@ -618,6 +721,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     OJ_CK(ctx->fields.ensure(std::max<size_t>((size_t)R * (((size_t)n + 127) / 128 * 128) * 4, 16)), "alloc fields");
     float* d_fields = ctx->fields.as<float>();
     if (S > 0) OJ_CK(cudaMemcpyAsync(d_beta, bf.data(), bf.size() * 4, cudaMemcpyHostToDevice, st), "H2D betas");
+    FieldCall fc;
+    if (oj_status fs = field_call(ctx, g->single.get(), &hreads, std::vector<int>{0}, R, &fc)) return fs;
     if (tit == g->tuned.end() && autotune_requested(flags) && S > 0) {
       // candidates run 16 sweeps with betas spread over the schedule on a copy of the spins
       std::vector<int> cand;
@@ -647,7 +752,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
             }
             return launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter,
                                    scratch, d_tb, Ssub, rb, 0, ctx->sm_count, st, nullptr, cand[i], d_fields, d_foff,
-                                   R);
+                                   fc);
           },
           &terr, (int)(std::find(cand.begin(), cand.end(), variant) - cand.begin()));
       if (bi == -2) return cuda_fail(ctx, terr, "autotune");
@@ -668,11 +773,12 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       energies_in_kernel = true;
     }
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-    if (S > 0)
-      OJ_CK(launch_sa_batch(g->single.get(), d_reads, d_soff, d_items, (int)(items.size() / 2), d_counter, d_spins,
-                            d_beta, S, rbm, 0, ctx->sm_count, st, &launches, variant, d_fields, d_foff, R, d_ek,
-                            d_soff),
-            "sa dense jump kernel");
+    if (S > 0) {
+      const SweepPlan sp{g->single.get(), d_reads, d_soff, d_items, (int)(items.size() / 2), d_counter, d_spins,
+                         d_beta, 0, variant, d_fields, d_foff, d_ek, d_soff};
+      OJ_CK(run_batch(ctx, sp, S, rbm, fc, stats != nullptr, &launches), "sa dense jump kernel");
+      field_run = true;
+    }
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
     threads_used = batch_variant_warps(variant) * 32;
     variant_used = variant;
@@ -715,7 +821,13 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   }
   if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
   OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
-  if (!devp || stats || kernel == OJ_KERNEL_DENSE_TC) OJ_CK(cudaStreamSynchronize(st), "run");
+  if (!devp || stats || kernel == OJ_KERNEL_DENSE_TC || field_run) OJ_CK(cudaStreamSynchronize(st), "run");
+  RunCounters rc;
+  if (stats || field_run) rc = read_counters(ctx);
+  if (field_run && rc.status) {
+    ctx->last_error = "tensor-core field kernel: a bounded device wait ran out";
+    return OJ_ERR_TIMEOUT;
+  }
   if (kernel == OJ_KERNEL_DENSE_TC && S > 0) {
     int flag = 0;
     OJ_CK(cudaMemcpy(&flag, g->tc->status.ptr, sizeof(int), cudaMemcpyDeviceToHost), "status read");
@@ -735,7 +847,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
-    stats->accepted = read_counter(ctx);
+    stats->accepted = rc.flips;
+    stats->field_drift = !field_run ? -1.0 : (g->single->exact_fields ? 0.0 : (double)rc.drift);
   }
   return OJ_OK;
 }
@@ -795,7 +908,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   int P_used = 0, threads_used = 0;
   bool tuned_now = false;
   RngBase rbm = rb;  // rb of the main annealing launch (counts accepted flips)
-  if (oj_status cs = arm_counter(ctx, stats, &rbm)) return cs;
+  if (oj_status cs = arm_counters(ctx, stats, &rbm)) return cs;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED && split_ok) {
@@ -935,7 +1048,8 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
-    stats->accepted = read_counter(ctx);
+    stats->accepted = read_counters(ctx).flips;
+    stats->field_drift = -1.0;
   }
   return OJ_OK;
 }
@@ -1175,14 +1289,16 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
       b->j16 = true;
     }
   }
-  // exact fields with every J 2^p an integer of at most 127: J 2^p as int8
+  // exact fields with every J 2^p an integer of at most 127: J 2^p as int8,
+  // one digit of the tensor-core field kernel; other couplings get four digits
+  std::vector<int8_t> J8;
   if (exact && std::ldexp(maxj, pmax) <= 127.0) {
-    std::vector<int8_t> J8(J32.size());
+    J8.resize(J32.size());
     for (size_t q = 0; q < J32.size(); ++q) J8[q] = (int8_t)std::ldexp((double)J32[q], pmax);
-    OJ_CK(up(b->d_J8, J8.data(), J8.size()), "upload J8");
     b->j8 = true;
     b->j8_scale = (float)std::ldexp(1.0, -pmax);
   }
+  OJ_CK(field_tc_prepare(b.get(), J32, joff, b->j8 ? &J8 : nullptr, pmax), "field digits");
   OJ_CK(up(b->d_h, h32.data(), h32.size() * 4), "upload h");
   OJ_CK(up(b->d_J64, J64.data(), J64.size() * 8), "upload J64");
   OJ_CK(up(b->d_joff, joff.data(), joff.size() * 8), "upload offsets");
@@ -1293,6 +1409,10 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   int32_t* d_order = reinterpret_cast<int32_t*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta);
   int64_t* d_foff = reinterpret_cast<int64_t*>(base + b_reads + b_soff + b_eoff + b_items + b_cnt + b_beta + b_order);
   int launches = 0;
+  RngBase rbm = rb;  // rb of the main annealing launch (counts accepted flips)
+  if (oj_status cs = arm_counters(ctx, stats, &rbm)) return cs;
+  FieldCall fc;
+  if (oj_status fs = field_call(ctx, b, reads, order, max_reads, &fc)) return fs;
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
   if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(d_spins, spins, sbytes, cudaMemcpyHostToDevice, st), "H2D spins");
   OJ_CK(cudaMemcpyAsync(d_reads, reads, (size_t)count * 4, cudaMemcpyHostToDevice, st), "H2D reads");
@@ -1332,7 +1452,7 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
           }
           return launch_sa_batch(b, d_reads, d_soff, d_items, (int)(it.size() / 2), d_counter, scratch, d_tb, Ssub,
                                  rb, (uint32_t)instance_offset, ctx->sm_count, st, nullptr, cand[i], d_fields, d_foff,
-                                 max_reads);
+                                 fc);
         },
         &terr, (int)(std::find(cand.begin(), cand.end(), variant0) - cand.begin()));
     if (bi == -2) return cuda_fail(ctx, terr, "autotune");
@@ -1354,14 +1474,14 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   }
   const bool energies_in_kernel = energies && S > 0 && nitems > 0 && b->exact_fields;
   if (energies_in_kernel) OJ_CK(cudaMemsetAsync(d_e, 0, (size_t)nrep * 8, st), "energies of empty instances");
-  if (oj_status cs = arm_counter(ctx, stats, &rb)) return cs;  // after the tuning launches
   OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-  if (S > 0 && nitems > 0)
-    OJ_CK(launch_sa_batch(b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, S, rb,
-                          (uint32_t)instance_offset, ctx->sm_count, st, &launches,
-                          bm->tuned_variant ? bm->tuned_variant : variant0, d_fields, d_foff, max_reads,
-                          energies_in_kernel ? d_e : nullptr, d_eoff),
-          "sa batched kernel");
+  const bool field_run = S > 0 && nitems > 0;
+  if (field_run) {
+    const SweepPlan sp{b, d_reads, d_soff, d_items, nitems, d_counter, d_spins, d_beta, (uint32_t)instance_offset,
+                       bm->tuned_variant ? bm->tuned_variant : variant0, d_fields, d_foff,
+                       energies_in_kernel ? d_e : nullptr, d_eoff};
+    OJ_CK(run_batch(ctx, sp, S, rbm, fc, stats != nullptr, &launches), "sa batched kernel");
+  }
   OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   if (energies_in_kernel) {
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)nrep * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
@@ -1377,6 +1497,11 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
   if (!devp && sbytes > 0) OJ_CK(cudaMemcpyAsync(spins, d_spins, sbytes, cudaMemcpyDeviceToHost, st), "D2H spins");
   OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
   OJ_CK(cudaStreamSynchronize(st), "run");
+  const RunCounters rc = read_counters(ctx);
+  if (field_run && rc.status) {
+    ctx->last_error = "tensor-core field kernel: a bounded device wait ran out";
+    return OJ_ERR_TIMEOUT;
+  }
   if (stats) {
     stats->kernel = 0;
     stats->launches = launches;
@@ -1388,7 +1513,8 @@ oj_status oj_sa_run_batched(oj_ctx* ctx, const oj_batch* b, const int32_t* reads
     stats->attempts = attempts_per_sweep * (double)S;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
-    stats->accepted = read_counter(ctx);
+    stats->accepted = rc.flips;
+    stats->field_drift = !field_run ? -1.0 : (b->exact_fields ? 0.0 : (double)rc.drift);
   }
   return OJ_OK;
 }
@@ -1467,6 +1593,7 @@ oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     stats->attempts = (double)R * n * (double)S;
     stats->threads = 512;
     stats->accepted = -1.0;
+    stats->field_drift = -1.0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
   }

@@ -22,13 +22,15 @@ oj_batch::~oj_batch() {
   if (cur != device) cudaSetDevice(device);
   d_J.release();
   d_J16.release();
-  d_J8.release();
   d_h.release();
   d_J64.release();
   d_joff.release();
   d_hoff.release();
   d_j64off.release();
   d_n.release();
+  d_dig.release();
+  d_dtoff.release();
+  d_uexp.release();
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
 }
 

@@ -123,12 +123,15 @@ struct oj_batch {
   oj::DevBuf d_J16;   // J as FP16 when every coupling's FP32 value is exactly an FP16 value (flip rows)
   bool j16 = false;
   bool exact_fields = false;  // FP32 fields exact: energies from the fields (sweep kernel epilogue)
-  // J * 2^p as int8 (exact fields and every scaled coupling in [-127, 127]):
-  // the initial fields are then exact integer dot products
-  oj::DevBuf d_J8;
+  // J * 2^p is int8 (exact fields and every scaled coupling in [-127, 127]):
+  // the fields are then one int8 digit per coupling
   bool j8 = false;
   float j8_scale = 1.0f;  // 2^-p
   int tuned_variant = 0;  // autotuned register-budget variant, 0 = not tuned
+  // the couplings as int8 digits on a per-instance grid 2^uexp, tiled for the
+  // tensor-core field kernel (oj_k_field_tc.cu): ndig digits per coupling
+  oj::DevBuf d_dig, d_dtoff, d_uexp;
+  int ndig = 0;
   ~oj_batch();
 };
 
@@ -140,7 +143,10 @@ struct oj_ctx {
   std::string last_error;
   std::string noalloc_error;  // why the allocation-free entry point could not be set up ("" = ready)
   oj::DevBuf spins, words, params, energies, best, aux, batch, fields, eparts;
-  oj::DevBuf counters;  // device counters of a run (accepted flips)
+  oj::DevBuf counters;  // device counters of a run: accepted flips (u64), field drift (float bits), status
+  oj::DevBuf fitems;    // work items of the tensor-core field kernel
+  int recompute = 16;   // full field recompute every this many sweeps (real couplings; 0 = never)
+  long long wait_limit = -1;  // iterations of the field kernel's pipeline waits (< 0: the default)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -199,11 +205,37 @@ int batch_variant_warps(int variant);
 int batch_min_warps();  // fewest warps per CTA of any variant (most work items)
 int batch_default_variant();
 int batch_variant_max_n(int variant);  // largest instance a launch variant takes
+// Tensor-core local fields of a batch (oj_k_field_tc.cu).
+struct FieldCall {
+  const int32_t* items = nullptr;  // device [nitems][3]: instance, site tile, replica tile
+  int nitems = 0;
+  int NT = 16;                     // replicas per tile
+  unsigned int* drift = nullptr;   // max |F_new - F_old| (float bits) in compare mode
+  int* status = nullptr;           // set when a bounded wait runs out
+  long long wait_limit = 0;
+};
+// Fields on the tensor cores, then the sweeps (one segment, no recompute).
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
                             int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads,
-                            double* d_energies = nullptr, const int64_t* d_eoff = nullptr);
+                            int* launches, int variant, float* d_fields, const int64_t* d_foff,
+                            const FieldCall& fc, double* d_energies = nullptr, const int64_t* d_eoff = nullptr);
+int field_tc_tile_replicas(const oj_batch* b, int max_reads);
+void field_tc_items(const oj_batch* b, const int32_t* reads, const std::vector<int>& order, int NT,
+                    std::vector<int32_t>& items);
+cudaError_t launch_field_tc(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff, const int8_t* spins,
+                            float* F, const int64_t* d_foff, const int32_t* d_items, int nitems, int NT, bool compare,
+                            unsigned int* d_drift, int* d_status, long long wait_limit, cudaStream_t st);
+cudaError_t field_tc_prepare(oj_batch* b, const std::vector<float>& J32, const std::vector<int64_t>& joff,
+                             const std::vector<int8_t>* J8, int pmax);
+// The batched sweep kernel alone (no fields): nsweeps sweeps from the fields in
+// d_fields; with write_fields it stores its final fields back there.
+cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                                const int32_t* d_items, int nitems, int* d_counter, int8_t* spins,
+                                const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count,
+                                cudaStream_t st, int* launches, int variant, float* d_fields,
+                                const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
+                                bool write_fields);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep);

@@ -36,9 +36,12 @@
 // copy (8 bytes per lane) when FP16 holds every coupling exactly; small
 // instances' rows are staged in shared memory, and batches of instances of at
 // most 128 sites run sa_batch1_kernel (fields and spin bits in registers).
-// The initial fields come from batch_field_kernel (or batch_field_i8_kernel for
-// exact int8 couplings), launched just before, through a global buffer of
-// reads x padded n floats per instance.
+// The fields come from the tensor-core field kernel (oj_k_field_tc.cu),
+// launched just before, through a global buffer of reads x padded n floats per
+// instance; for couplings that are not exact in FP32 sums a run is cut into
+// segments at multiples of the recompute interval and the fields are computed
+// anew between segments (the sweep kernel then stores its final fields back,
+// so that the field kernel can measure their drift).
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -76,8 +79,9 @@ struct BatchArgs {
   int fstride;             // fields per warp in shared memory (multiple of 128)
   int swstride;            // spin words per warp: 32 per eight chunks
   const __half* J16;       // J as FP16 (same offsets), when every value is exact in FP16
-  const float* F;          // initial fields, [reads][npad] per instance (batch_field_kernel)
+  const float* F;          // initial fields, [reads][npad] per instance (tensor-core field kernel)
   const int64_t* foff;     // [count] offset of instance m's fields (floats)
+  float* Fw;               // when set, each replica's final fields are stored here (same layout)
   double* E;               // FP64 energies from the final fields, or null (exact-field batches)
   const int64_t* eoff;     // [count] offset of instance m's energies
   unsigned long long* flips;  // accepted-flip counter, or null
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
       }
     if (!active) continue;  // no block-wide barrier until the next item
     __syncwarp();
-    // the fields f_j = h_j + sum_i J_ij s_i come from batch_field_kernel
+    // the fields f_j = h_j + sum_i J_ij s_i come from the tensor-core field kernel
     {
       const float* Fr = a.F + a.foff[m] + (size_t)r * npad;
       for (int c = 0; c < nch; ++c) reinterpret_cast<float4*>(f)[32 * c + lane] = ldg4(Fr + 128 * c + 4 * lane);
@@ -304,6 +308,11 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         }
         __syncwarp();  // the list is read before the next chunk rewrites it
       }
+    }
+    if (a.Fw) {
+      float* Fr = a.Fw + a.foff[m] + (size_t)r * npad;
+      for (int c = 0; c < nch; ++c)
+        *reinterpret_cast<float4*>(Fr + 128 * c + 4 * lane) = reinterpret_cast<const float4*>(f)[32 * c + lane];
     }
     if (a.E) {
       // exact fields: E = 1/2 sum_i s_i (f_i + h_i), every term and partial sum
@@ -431,6 +440,7 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
         open = inside & (0xFu << min(max(i + 1 - 4 * lane, 0), 4));
       }
     }
+    if (a.Fw) *reinterpret_cast<float4*>(a.Fw + a.foff[m] + (size_t)r * 128 + 4 * lane) = fc;
     if (a.E) {
       // exact fields: E = 1/2 sum_i s_i (f_i + h_i), as in sa_batch_kernel
       const float4 h4 = ldg4(a.h + a.hoff[m] + 4 * lane);
@@ -451,166 +461,6 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
     }
   }
   ojd::add_flips(a.flips, nflip);
-}
-
-// Initial fields of every replica of every instance,
-//     F[m][r][j] = h_j + sum_{i = 0..n-1} J_ij s_ri,
-// summed in ascending i with one FP32 rounding per term, the order of the
-// reference's reset_dE row sums (classical_ising.hpp:87-90) restated in FP32.
-// One CTA per (instance, 128 columns, 64 replicas): it stages 32 rows x 128
-// columns of J and the sign bits of those rows for its 64 replicas in shared
-// memory; thread (site quad q, replica group g) accumulates 4 columns of 8
-// replicas, so J is read once per 64 replicas instead of once per replica.
-constexpr int kFieldReplicas = 64;
-constexpr int kFieldRows = 32;
-
-__global__ void __launch_bounds__(256) batch_field_kernel(BatchArgs a, int zbase) {
-  __shared__ float4 jt[kFieldRows * 32];
-  __shared__ uint32_t sgn[kFieldReplicas];
-  const int m = blockIdx.x, jb = blockIdx.y, r0 = (zbase + (int)blockIdx.z) * kFieldReplicas;
-  const int n = a.n[m], R = a.reads[m];
-  const int nch = (n + 127) >> 7;
-  if (jb >= nch || r0 >= R) return;  // the whole CTA leaves together
-  const int npad = nch << 7;
-  const int t = threadIdx.x, sq = t & 31, rg = t >> 5;
-  const float* J = a.J + a.joff[m] + 128 * jb;
-  const int8_t* S = a.spins + a.soff[m];
-  const float4 h4 = ldg4(a.h + a.hoff[m] + 128 * jb + 4 * sq);
-  float4 acc[8];
-#pragma unroll
-  for (int q = 0; q < 8; ++q) acc[q] = h4;
-  for (int i0 = 0; i0 < n; i0 += kFieldRows) {
-    __syncthreads();  // the previous tile is consumed
-    for (int k = t; k < kFieldRows * 32; k += 256) {
-      const int row = k >> 5;
-      jt[k] = i0 + row < n ? ldg4(J + (size_t)(i0 + row) * npad + 4 * (k & 31)) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {  // warp rg: sign bits of rows i0..i0+31 of its 8 replicas
-      const int rr = 8 * rg + q, r = r0 + rr, i = i0 + sq;
-      const bool neg = r < R && i < n && S[(size_t)r * n + i] < 0;
-      const uint32_t bits = __ballot_sync(0xffffffffu, neg);
-      if (sq == 0) sgn[rr] = bits;
-    }
-    __syncthreads();
-    uint32_t mk[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) mk[q] = sgn[8 * rg + q];
-    const int rows = min(kFieldRows, n - i0);
-    for (int ii = 0; ii < rows; ++ii) {
-      const float4 v = jt[ii * 32 + sq];
-      const uint32_t bit = 1u << ii;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        // fma(+-1, v, acc) rounds acc +- v once: the same sum as an add
-        const float sg = (mk[q] & bit) ? -1.0f : 1.0f;
-        acc[q].x = __fmaf_rn(sg, v.x, acc[q].x);
-        acc[q].y = __fmaf_rn(sg, v.y, acc[q].y);
-        acc[q].z = __fmaf_rn(sg, v.z, acc[q].z);
-        acc[q].w = __fmaf_rn(sg, v.w, acc[q].w);
-      }
-    }
-  }
-  float* Fm = const_cast<float*>(a.F) + a.foff[m] + 128 * jb + 4 * sq;
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const int r = r0 + 8 * rg + q;
-    if (r < R) *reinterpret_cast<float4*>(Fm + (size_t)r * npad) = acc[q];
-  }
-}
-
-// Initial fields of a batch with exact fields and int8 couplings (J8 = J 2^p,
-// every value in [-127, 127]): f_j = h_j + 2^-p sum_i J8[j][i] s_i, four sites
-// per __dp4a into an int32 (J is symmetric: row j holds column j).  The batch's
-// exactness bound (|h_j| + sum_i |J_ij| below 2^(24-p), all multiples of 2^-p)
-// makes the sum, its conversion, the scaling and the addition of h exact, so
-// these are the values of batch_field_kernel's FP32 row sums (exact too).  One
-// CTA per (instance, 128 columns, 64 replicas): 64-site slices of its 128 rows
-// and of the 64 replicas' spins are staged in shared memory as packed words;
-// warp tr accumulates replicas 8tr..8tr+7 and its lane tj sites 4tj..4tj+3, so
-// a step of four sites is two broadcast 16-byte loads of spin words and one
-// conflict-free 16-byte load of J words for 32 __dp4a.
-constexpr int kI8Slice = 64;
-constexpr int kI8Stride = kFieldReplicas + 4;  // spin words per slice word (16-byte rows)
-
-__global__ void __launch_bounds__(256)
-    batch_field_i8_kernel(BatchArgs a, const int8_t* __restrict__ J8, float scale, int zbase) {
-  __shared__ __align__(16) int32_t jt[kI8Slice / 4][128];
-  __shared__ __align__(16) int32_t sp[kI8Slice / 4][kI8Stride];
-  const int m = blockIdx.x, jb = blockIdx.y, r0 = (zbase + (int)blockIdx.z) * kFieldReplicas;
-  const int n = a.n[m], R = a.reads[m];
-  const int nch = (n + 127) >> 7;
-  if (jb >= nch || r0 >= R) return;  // the whole CTA leaves together
-  const int npad = nch << 7;
-  const int t = threadIdx.x, tr = t >> 5, tj = t & 31;
-  const int8_t* Jm = J8 + a.joff[m];
-  const int8_t* S = a.spins + a.soff[m];
-  int acc[8][4];
-#pragma unroll
-  for (int q = 0; q < 8; ++q)
-#pragma unroll
-    for (int x = 0; x < 4; ++x) acc[q][x] = 0;
-  for (int k0 = 0; k0 < npad; k0 += kI8Slice) {
-    __syncthreads();  // the previous slice is consumed
-    // rows 128 jb + j at sites k0..k0+63, 16 bytes per (row, quarter); rows
-    // past n are zero, columns past n are the zero padding of J
-    for (int idx = t; idx < 128 * 4; idx += 256) {
-      const int j = idx & 127, qq = idx >> 7;
-      const int row = 128 * jb + j;
-      int4 v = make_int4(0, 0, 0, 0);
-      if (row < n) v = __ldg(reinterpret_cast<const int4*>(Jm + (size_t)row * npad + k0 + 16 * qq));
-      jt[4 * qq + 0][j] = v.x;
-      jt[4 * qq + 1][j] = v.y;
-      jt[4 * qq + 2][j] = v.z;
-      jt[4 * qq + 3][j] = v.w;
-    }
-    // spins of replicas r0..r0+63 at sites k0..k0+63, four sites per word;
-    // consecutive threads read consecutive words of a replica's row (one
-    // 32-bit load where the row segment is 4-byte aligned and inside n)
-    for (int idx = t; idx < kFieldReplicas * (kI8Slice / 4); idx += 256) {
-      const int w = idx & (kI8Slice / 4 - 1), rr = idx / (kI8Slice / 4);
-      const int r = r0 + rr;
-      const int i0 = k0 + 4 * w;
-      uint32_t word = 0u;
-      if (r < R && i0 < n) {
-        const int8_t* s8 = S + (size_t)r * n + i0;
-        if (i0 + 3 < n && ((reinterpret_cast<uintptr_t>(s8) & 3u) == 0u)) {
-          word = __ldg(reinterpret_cast<const uint32_t*>(s8));
-        } else {
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (i0 + e < n) word |= (uint32_t)(uint8_t)s8[e] << (8 * e);
-        }
-      }
-      sp[w][rr] = (int32_t)word;
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int w = 0; w < kI8Slice / 4; ++w) {
-      const int4 s0 = *reinterpret_cast<const int4*>(&sp[w][8 * tr]);
-      const int4 s1 = *reinterpret_cast<const int4*>(&sp[w][8 * tr + 4]);
-      const int4 jv = *reinterpret_cast<const int4*>(&jt[w][4 * tj]);
-      const int sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
-      const int jj[4] = {jv.x, jv.y, jv.z, jv.w};
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-#pragma unroll
-        for (int x = 0; x < 4; ++x) acc[q][x] = __dp4a(sv[q], jj[x], acc[q][x]);
-    }
-  }
-  const float4 h4 = __ldg(reinterpret_cast<const float4*>(a.h + a.hoff[m] + 128 * jb + 4 * tj));
-  float* Fm = const_cast<float*>(a.F) + a.foff[m] + 128 * jb + 4 * tj;
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const int r = r0 + 8 * tr + q;
-    if (r >= R) continue;
-    float4 o;
-    o.x = __fadd_rn(h4.x, __fmul_rn(__int2float_rn(acc[q][0]), scale));
-    o.y = __fadd_rn(h4.y, __fmul_rn(__int2float_rn(acc[q][1]), scale));
-    o.z = __fadd_rn(h4.z, __fmul_rn(__int2float_rn(acc[q][2]), scale));
-    o.w = __fadd_rn(h4.w, __fmul_rn(__int2float_rn(acc[q][3]), scale));
-    *reinterpret_cast<float4*>(Fm + (size_t)r * npad) = o;
-  }
 }
 
 // FP64 energy of every replica: E = sum_{i<j} J_ij s_i s_j + sum_i h_i s_i
@@ -770,13 +620,15 @@ cudaError_t launch_one_chunk(const BatchArgs& a, int max_n, int nitems, int sm_c
   return cudaGetLastError();
 }
 
-cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
-                            const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
-                            int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
-                            int* launches, int variant, float* d_fields, const int64_t* d_foff, int max_reads,
-                            double* d_energies, const int64_t* d_eoff) {
+cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                                const int32_t* d_items, int nitems, int* d_counter, int8_t* spins,
+                                const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count,
+                                cudaStream_t st, int* launches, int variant, float* d_fields,
+                                const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
+                                bool write_fields) {
   if (variant == 0) variant = batch_default_variant();
   if (!batch_variant_valid(variant) || b->max_n > batch_variant_max_n(variant)) return cudaErrorInvalidValue;
+  if (b->count == 0 || nitems <= 0 || nsweeps <= 0) return cudaSuccess;
   const int fstride = std::max(128, (b->max_n + 127) / 128 * 128);
   BatchArgs a;
   a.J = b->d_J.as<float>();
@@ -802,22 +654,11 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   a.J16 = b->j16 ? b->d_J16.as<__half>() : nullptr;
   a.F = d_fields;
   a.foff = d_foff;
+  a.Fw = write_fields ? d_fields : nullptr;
   a.E = b->exact_fields ? d_energies : nullptr;
   a.eoff = d_eoff;
   a.flips = rb.flips;
-  if (b->count == 0 || max_reads <= 0 || nitems <= 0) return cudaSuccess;
-  const int zt = (max_reads + kFieldReplicas - 1) / kFieldReplicas;
-  cudaError_t e = cudaSuccess;
-  for (int z0 = 0; z0 < zt; z0 += 65535) {  // grid z is at most 65535 replica tiles
-    const dim3 fgrid((unsigned)b->count, (unsigned)(fstride / 128), (unsigned)std::min(65535, zt - z0));
-    if (b->j8)
-      batch_field_i8_kernel<<<fgrid, 256, 0, st>>>(a, b->d_J8.as<int8_t>(), b->j8_scale, z0);
-    else
-      batch_field_kernel<<<fgrid, 256, 0, st>>>(a, z0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (launches) ++*launches;
-  }
-  e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   if (b->max_n <= 128) {
     // one chunk per instance: fields and spin bits in registers (same warps
@@ -844,6 +685,20 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   }
   if (e == cudaSuccess && launches) ++*launches;
   return e;
+}
+
+cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
+                            const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
+                            int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count, cudaStream_t st,
+                            int* launches, int variant, float* d_fields, const int64_t* d_foff,
+                            const FieldCall& fc, double* d_energies, const int64_t* d_eoff) {
+  if (b->count == 0 || nitems <= 0) return cudaSuccess;
+  cudaError_t e = launch_field_tc(b, d_reads, d_soff, spins, d_fields, d_foff, fc.items, fc.nitems, fc.NT, false,
+                                  fc.drift, fc.status, fc.wait_limit, st);
+  if (e != cudaSuccess) return e;
+  if (launches) ++*launches;
+  return launch_batch_sweeps(b, d_reads, d_soff, d_items, nitems, d_counter, spins, betas, nsweeps, rb, inst0,
+                             sm_count, st, launches, variant, d_fields, d_foff, d_energies, d_eoff, false);
 }
 
 int batch_energy_splits(const oj_batch* b, int max_reads, int sm_count) {

@@ -1,0 +1,455 @@
+// Local fields of a batch of dense instances on the tensor cores (tcgen05.mma
+// kind::i8, accumulators in tensor memory):
+//
+//     F[m][r][j] = fp32( fp64(h_j) + u_m * sum_i q_ij s_ri ),   q_ij = J_ij / u_m
+//
+// The classical system's dE = -2 s (J s) of the reference
+// (include/openjij/system/classical_ising.hpp:87-90, reset_dE), computed for
+// every replica of every instance at once.  J enters as integers on a per-
+// instance grid u_m = 2^e_m: couplings that are int8 multiples of 2^-p (the
+// exact-field integer QUBOs) use q = J 2^p directly, one int8 "digit"; any
+// other FP32 couplings are rounded (half to even) to the grid
+// u_m = 2^(E - 26), E the binary exponent of max |J| (2^(E-1) <= max|J| < 2^E),
+// and q is split into four balanced base-128 digits d_t in [-64, 63],
+// q = sum_t d_t 128^t.  Each digit is one int8 x int8 -> int32 MMA pass with
+// the +-1 spins; the passes are combined exactly in int64, converted exactly to
+// FP64, scaled by u_m, added to h_j in FP64 and rounded once to FP32.  The
+// result is a deterministic function of (J, h, s) that the CPU replay
+// reproduces exactly, and it is within n u_m / 2 of the exact field (for the
+// exact-field batches it is the exact field).
+//
+// Tiles: a CTA computes 128 sites (TMEM lanes) x NT replicas (TMEM columns per
+// digit).  The digits are stored tiled in global memory in the canonical
+// K-major layout of the MMA operand (8 x 16-byte core matrices, no swizzle), so
+// one 16 KB tile (128 sites x 128 sites) is one bulk copy; the spins of the
+// NT replicas are written into shared memory by the threads in the same
+// layout.  Two stages: the copies of a K chunk overlap the MMAs of the
+// previous one.  Epilogue: tcgen05.ld of the accumulators, the exact
+// combination above, coalesced FP32 stores of F (replica-major, sites
+// contiguous), and in compare mode max |F_new - F_old| before the store (the
+// drift of the sweep kernel's incremental fields).  Every wait is bounded:
+// a wait that runs out sets *status and the kernel finishes without hanging.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "oj_internal.h"
+
+namespace oj {
+namespace {
+
+constexpr int kTileSites = 128;                    // GEMM M: sites per tile (TMEM lanes)
+constexpr int kChunk = 128;                        // GEMM K per stage: sites (bytes)
+constexpr uint32_t kTileBytes = kTileSites * kChunk;  // one int8 digit tile
+constexpr int kFieldThreads = 128;
+constexpr long long kDrainLimit = 1ll << 26;  // iterations of a drain wait (the default wait limit too)
+
+struct FieldArgs {
+  const int8_t* digits;    // tiled digits, instance m at dtoff[m]: [D][mt][kt] tiles
+  const int64_t* dtoff;    // [count] byte offsets
+  const int32_t* uexp;     // [count] grid exponent e_m
+  const float* h;          // padded fields
+  const int64_t* hoff;
+  const int32_t* n;
+  const int32_t* reads;
+  const int64_t* soff;     // spins of instance m: [reads][n] int8
+  const int8_t* spins;
+  float* F;                // [reads][npad] per instance
+  const int64_t* foff;
+  const int32_t* items;    // [nitems][3]: instance, site tile, replica tile
+  int nitems;
+  int compare;             // measure max |F_new - F_old| into *drift
+  unsigned int* drift;     // float bits (non-negative values order as integers)
+  int* status;
+  long long wait_limit;    // iterations of a pipeline wait (0: give up at once)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Matrix descriptor, K-major, no swizzle: LBO = distance of K-adjacent core
+// matrices, SBO = distance of adjacent 8-row groups.
+__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor: s8 x s8 -> s32, K-major A and B, M = 128, N = nn.
+__device__ __forceinline__ uint32_t idesc_i8(int nn) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nn >> 3) << 17) | ((uint32_t)(kTileSites >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t ph, long long limit) {
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(b)), "r"(ph)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+          dtmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = (int32_t)r[j];
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// byte offset of (row, k) in a canonical K-major tile of 128-byte rows
+__host__ __device__ __forceinline__ uint32_t canon(int row, int k) {
+  return (uint32_t)((row >> 3) * 1024 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15));
+}
+
+template <int D, int NT>
+struct FieldShape {
+  static constexpr uint32_t kA = D * kTileBytes;         // digit tiles of one K chunk
+  static constexpr uint32_t kB = NT * kChunk;            // spin tile of one K chunk
+  static constexpr uint32_t kStage = (kA + kB + 1023) / 1024 * 1024;
+  static constexpr uint32_t kCols = D * NT <= 32 ? 32 : (D * NT <= 64 ? 64 : (D * NT <= 128 ? 128 : (D * NT <= 256 ? 256 : 512)));
+  static constexpr size_t kSmem = 2 * (size_t)kStage + 64;  // + 4 mbarriers, TMEM slot, abort flag
+};
+
+template <int D, int NT>
+__global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a) {
+  using S = FieldShape<D, NT>;
+  static_assert(D * NT <= 512, "accumulators exceed tensor memory");
+  static_assert(NT % 16 == 0 && NT >= 16 && NT <= 256, "MMA N with M = 128");
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int item = blockIdx.x;
+  if (item >= a.nitems) return;  // the whole CTA
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m = a.items[3 * item], mt = a.items[3 * item + 1], nt = a.items[3 * item + 2];
+  const int n = a.n[m], R = a.reads[m];
+  const int nch = (n + kChunk - 1) / kChunk;
+  const int npad = nch * kChunk;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * S::kStage);  // full[2], done[2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 4);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(S::kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int q = 0; q < 4; ++q) mbar_init(bar + q, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  // Pipeline waits use a.wait_limit; one that runs out aborts the loop: no new
+  // copies or MMAs are issued, the ones in flight are waited for with the
+  // default limit (kDrainLimit), tensor memory is freed and F is left as it was.
+  // thread 0's bookkeeping, bit s for stage s: phase parities of the full and
+  // done barriers, and copies / MMA commits issued but not yet seen complete
+  uint32_t ph_full = 0u, ph_done = 0u, pend_full = 0u, pend_done = 0u;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+  if (tid == 0) *abort_flag = 0;
+  const int8_t* dig = a.digits + a.dtoff[m];
+  const int8_t* sp = a.spins + a.soff[m];
+  const int r0 = nt * NT;
+  for (int kc = 0; kc < nch; ++kc) {
+    const int s = kc & 1;
+    unsigned char* As = sm + s * S::kStage;
+    unsigned char* Bs = As + S::kA;
+    const uint32_t sb = 1u << s;
+    if (tid == 0 && (pend_done & sb)) {  // the stage's previous MMAs (chunk kc - 2) have read it
+      if (mbar_wait(bar + 2 + s, (ph_done >> s) & 1u, a.wait_limit)) {
+        ph_done ^= sb;
+        pend_done &= ~sb;
+      } else {
+        *abort_flag = 1;
+      }
+    }
+    __syncthreads();
+    if (*abort_flag) break;
+    if (tid == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar + s)), "r"(S::kA)
+                   : "memory");
+#pragma unroll
+      for (int t = 0; t < D; ++t)
+        bulk_copy(As + t * kTileBytes, dig + ((size_t)(t * nch + mt) * nch + kc) * kTileBytes, kTileBytes, bar + s);
+      pend_full |= sb;
+    }
+    // spins of replicas r0..r0+NT-1 at sites 128 kc .. +127, 16 bytes a piece;
+    // zero past the instance's reads and sites
+    for (int idx = tid; idx < NT * 8; idx += kFieldThreads) {
+      const int rr = idx >> 3, pc = idx & 7;
+      const int r = r0 + rr, k = kc * kChunk + 16 * pc;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (r < R && k < n) {
+        const int8_t* p = sp + (size_t)r * n + k;
+        const int valid = min(16, n - k);
+        if (valid == 16 && (reinterpret_cast<uintptr_t>(p) & 15u) == 0u) {
+          v = __ldg(reinterpret_cast<const uint4*>(p));
+        } else if (valid == 16 && (reinterpret_cast<uintptr_t>(p) & 3u) == 0u) {
+          const uint32_t* p4 = reinterpret_cast<const uint32_t*>(p);
+          v = make_uint4(__ldg(p4), __ldg(p4 + 1), __ldg(p4 + 2), __ldg(p4 + 3));
+        } else {
+          unsigned long long lo = 0ull, hi = 0ull;
+          for (int e = 0; e < valid; ++e) {
+            const unsigned long long bv = (unsigned long long)(uint8_t)p[e];
+            if (e < 8) lo |= bv << (8 * e);
+            else hi |= bv << (8 * (e - 8));
+          }
+          v = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+        }
+      }
+      *reinterpret_cast<uint4*>(Bs + canon(rr, 16 * pc)) = v;
+    }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      if (mbar_wait(bar + s, (ph_full >> s) & 1u, a.wait_limit)) {
+        ph_full ^= sb;
+        pend_full &= ~sb;
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+#pragma unroll
+        for (int t = 0; t < D; ++t)
+#pragma unroll
+          for (int kk = 0; kk < kChunk / 32; ++kk)
+            mma_i8(tbase + (uint32_t)(t * NT), desc_kmajor(a0 + t * kTileBytes + kk * 256, 128, 1024),
+                   desc_kmajor(b0 + kk * 256, 128, 1024), idesc_i8(NT), (kc | kk) ? 1u : 0u);
+        mma_commit(bar + 2 + s);
+        pend_done |= sb;
+      } else {
+        *abort_flag = 1;
+      }
+    }
+  }
+  // drain: every copy and MMA this CTA issued has completed before it goes on
+  bool ok = true;
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s) {
+      if ((pend_full >> s) & 1u) ok &= mbar_wait(bar + s, (ph_full >> s) & 1u, kDrainLimit);
+      if ((pend_done >> s) & 1u) ok &= mbar_wait(bar + 2 + s, (ph_done >> s) & 1u, kDrainLimit);
+    }
+    if (*abort_flag || !ok) atomicExch(a.status, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (*abort_flag) {
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(S::kCols));
+    return;
+  }
+  // ---- epilogue: warp w reads TMEM lanes 32w..32w+31 = sites of the tile
+  const int site = mt * kTileSites + 32 * warp + lane;
+  const double hv = (double)a.h[a.hoff[m] + site];  // zero past n (padding)
+  const int e = a.uexp[m];
+  float* Fm = a.F + a.foff[m] + site;
+  float dmax = 0.0f;
+  for (int j0 = 0; j0 < NT; j0 += 16) {
+    if (r0 + j0 >= R) break;  // warp-uniform
+    long long tot[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) tot[j] = 0;
+#pragma unroll
+    for (int t = 0; t < D; ++t) {
+      int32_t acc[16];
+      tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(t * NT + j0), acc);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) tot[j] += (long long)acc[j] * (1ll << (7 * t));
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = r0 + j0 + j;
+      if (r >= R) break;
+      const float f = __double2float_rn(__dadd_rn(hv, ldexp((double)tot[j], e)));
+      float* dst = Fm + (size_t)r * npad;
+      if (a.compare && site < n) dmax = fmaxf(dmax, fabsf(f - *dst));
+      *dst = f;
+    }
+  }
+  if (a.compare) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if (lane == 0 && dmax > 0.0f) atomicMax(a.drift, __float_as_uint(dmax));
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(S::kCols));
+}
+
+template <int D, int NT>
+cudaError_t launch_field_dn(const FieldArgs& a, cudaStream_t st) {
+  using S = FieldShape<D, NT>;
+  auto kern = field_tc_kernel<D, NT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
+  if (e != cudaSuccess) return e;
+  // every CTA resident on an SM must find its tensor-memory columns
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFieldThreads, S::kSmem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1 || (size_t)per_sm * S::kCols > 512) return cudaErrorInvalidConfiguration;
+  kern<<<a.nitems, kFieldThreads, S::kSmem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int D>
+cudaError_t launch_field_d(const FieldArgs& a, int NT, cudaStream_t st) {
+  switch (NT) {
+    case 16: return launch_field_dn<D, 16>(a, st);
+    case 32: return launch_field_dn<D, 32>(a, st);
+    case 64: return launch_field_dn<D, 64>(a, st);
+    case 128: return launch_field_dn<D, 128>(a, st);
+    default:
+      if constexpr (D == 1) return launch_field_dn<1, 256>(a, st);
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+int field_tc_tile_replicas(const oj_batch* b, int max_reads) {
+  const int cap = b->ndig == 1 ? 256 : 128;
+  int nt = 16;
+  while (nt < max_reads && nt < cap) nt *= 2;
+  return nt;
+}
+
+void field_tc_items(const oj_batch* b, const int32_t* reads, const std::vector<int>& order, int NT,
+                    std::vector<int32_t>& items) {
+  items.clear();
+  for (int m : order) {
+    const int n = b->n[m];
+    if (n == 0 || reads[m] == 0) continue;
+    const int nch = (n + kChunk - 1) / kChunk;
+    for (int mt = 0; mt < nch; ++mt)
+      for (int nt = 0; nt * NT < reads[m]; ++nt) {
+        items.push_back(m);
+        items.push_back(mt);
+        items.push_back(nt);
+      }
+  }
+}
+
+cudaError_t launch_field_tc(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff, const int8_t* spins,
+                            float* F, const int64_t* d_foff, const int32_t* d_items, int nitems, int NT, bool compare,
+                            unsigned int* d_drift, int* d_status, long long wait_limit, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  FieldArgs a;
+  a.digits = b->d_dig.as<int8_t>();
+  a.dtoff = b->d_dtoff.as<int64_t>();
+  a.uexp = b->d_uexp.as<int32_t>();
+  a.h = b->d_h.as<float>();
+  a.hoff = b->d_hoff.as<int64_t>();
+  a.n = b->d_n.as<int32_t>();
+  a.reads = d_reads;
+  a.soff = d_soff;
+  a.spins = spins;
+  a.F = F;
+  a.foff = d_foff;
+  a.items = d_items;
+  a.nitems = nitems;
+  a.compare = compare ? 1 : 0;
+  a.drift = d_drift;
+  a.status = d_status;
+  a.wait_limit = wait_limit >= 0 ? wait_limit : kDrainLimit;
+  return b->ndig == 1 ? launch_field_d<1>(a, NT, st) : launch_field_d<4>(a, NT, st);
+}
+
+// Host side: the grid of every instance and its digits, tiled.  Instance m's
+// couplings J32 (n x npad, row-major, FP32, zero padding) become q_ij on the
+// grid 2^uexp[m]; with j8 (int8 couplings J 2^p) one digit q = J8 and
+// uexp = -p, otherwise four balanced base-128 digits on 2^(E - 26).
+cudaError_t field_tc_prepare(oj_batch* b, const std::vector<float>& J32, const std::vector<int64_t>& joff,
+                             const std::vector<int8_t>* J8, int pmax) {
+  const int count = b->count;
+  const int D = (J8 && b->j8) ? 1 : 4;
+  std::vector<int64_t> dtoff(std::max(count, 1), 0);
+  std::vector<int32_t> uexp(std::max(count, 1), 0);
+  int64_t total = 0;
+  for (int m = 0; m < count; ++m) {
+    const int64_t nch = ((int64_t)b->n[m] + kChunk - 1) / kChunk;
+    dtoff[m] = total;
+    total += (int64_t)D * nch * nch * kTileBytes;
+  }
+  std::vector<int8_t> tiles((size_t)std::max<int64_t>(total, 16), 0);
+  for (int m = 0; m < count; ++m) {
+    const int n = b->n[m];
+    if (n == 0) continue;
+    const int nch = (n + kChunk - 1) / kChunk, npad = nch * kChunk;
+    const float* Jm = J32.data() + joff[m];
+    int e = 0;
+    if (D == 1) {
+      e = -pmax;
+    } else {
+      float amax = 0.0f;
+      for (int64_t q = 0; q < (int64_t)n * npad; ++q) amax = std::max(amax, std::fabs(Jm[q]));
+      int E = 0;
+      if (amax > 0.0f) std::frexp((double)amax, &E);  // 2^(E-1) <= amax < 2^E
+      e = amax > 0.0f ? E - 26 : 0;
+    }
+    uexp[m] = e;
+    int8_t* base = tiles.data() + dtoff[m];
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        const int mt = j / kChunk, kt = i / kChunk;
+        const uint32_t off = canon(j % kChunk, i % kChunk);
+        if (D == 1) {
+          base[((size_t)mt * nch + kt) * kTileBytes + off] = (*J8)[(size_t)(joff[m] + (int64_t)j * npad + i)];
+          continue;
+        }
+        int64_t q = (int64_t)std::nearbyint(std::ldexp((double)Jm[(size_t)j * npad + i], -e));
+        for (int t = 0; t < 4; ++t) {
+          const int64_t d = ((q + 64) & 127) - 64;
+          q = (q - d) >> 7;
+          base[((size_t)(t * nch + mt) * nch + kt) * kTileBytes + off] = (int8_t)d;
+        }
+      }
+  }
+  b->ndig = D;
+  cudaError_t err;
+  if ((err = b->d_dig.ensure(tiles.size())) != cudaSuccess) return err;
+  if ((err = cudaMemcpy(b->d_dig.ptr, tiles.data(), tiles.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return err;
+  if ((err = b->d_dtoff.ensure(dtoff.size() * 8)) != cudaSuccess) return err;
+  if ((err = cudaMemcpy(b->d_dtoff.ptr, dtoff.data(), dtoff.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return err;
+  if ((err = b->d_uexp.ensure(uexp.size() * 4)) != cudaSuccess) return err;
+  return cudaMemcpy(b->d_uexp.ptr, uexp.data(), uexp.size() * 4, cudaMemcpyHostToDevice);
+}
+
+}  // namespace oj

@@ -968,41 +968,66 @@ void orc_replay_sqa_split(int n, const int64_t* indptr, const int32_t* indices, 
 void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset, const double* J_aug,
                          const int32_t* reads, int8_t* spins, const float* betas_f, int64_t nsweeps,
                          uint64_t seed, uint32_t inst0, int threads, float* fields_out, uint32_t rep0,
-                         uint32_t sweep0) {
+                         uint32_t sweep0, int recompute, float* drift_out) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int64_t> soff(count + 1, 0);
+  std::vector<int64_t> soff(count + 1, 0), roff(count + 1, 0);
   std::vector<int> rm, rr;  // flattened (instance, replica)
   for (int m = 0; m < count; ++m) {
     soff[m + 1] = soff[m] + (int64_t)reads[m] * n_arr[m];
+    roff[m + 1] = roff[m] + reads[m];
     for (int r = 0; r < reads[m]; ++r) {
       rm.push_back(m);
       rr.push_back(r);
     }
   }
-  parallel_for((int)rm.size(), threads, [&](int q) {
-    const int m = rm[q], r = rr[q], n = n_arr[m];
+  parallel_for((int)rm.size(), threads, [&](int qx) {
+    const int m = rm[qx], r = rr[qx], n = n_arr[m];
     const int64_t n1 = n + 1;
     const double* A = J_aug + offset[m];
-    std::vector<float> J((size_t)n * n), h(n), f(n);
+    std::vector<float> J((size_t)n * n), h(n), f(n), fq(n);
+    float amax = 0.0f;
     for (int i = 0; i < n; ++i) {
-      for (int j = 0; j < n; ++j) J[(size_t)i * n + j] = (float)A[i * n1 + j];
+      for (int j = 0; j < n; ++j) {
+        J[(size_t)i * n + j] = (float)A[i * n1 + j];
+        amax = std::max(amax, std::fabs(J[(size_t)i * n + j]));
+      }
       h[i] = (float)A[i * n1 + n];
     }
+    // The field definition of the tensor-core field kernel: J on the grid
+    // 2^e, e = E - 26 with 2^(E-1) <= max|J| < 2^E, q = J / 2^e rounded half
+    // to even; f_j = fp32(fp64(h_j) + 2^e * sum_i q_ij s_i), the sum exact.
+    int E = 0;
+    if (amax > 0.0f) std::frexp((double)amax, &E);
+    const int e = amax > 0.0f ? E - 26 : 0;
+    std::vector<int64_t> q((size_t)n * n);
+    for (size_t t = 0; t < q.size(); ++t) q[t] = (int64_t)std::nearbyint(std::ldexp((double)J[t], -e));
     int8_t* s = spins + soff[m] + (size_t)r * n;
-    for (int j = 0; j < n; ++j) {
-      float acc = h[j];
-      for (int i = 0; i < n; ++i) {
-        const float v = J[(size_t)i * n + j];
-        acc = acc + (s[i] > 0 ? v : -v);
+    auto qfield = [&](std::vector<float>& out) {
+      for (int j = 0; j < n; ++j) {
+        int64_t acc = 0;
+        const int64_t* qj = &q[(size_t)j * n];  // J symmetric: row j holds column j
+        for (int i = 0; i < n; ++i) acc += s[i] > 0 ? qj[i] : -qj[i];
+        out[j] = (float)((double)h[j] + std::ldexp((double)acc, e));
       }
-      f[j] = acc;
-    }
+    };
+    float drift = 0.0f;
+    auto recompute_now = [&]() {
+      qfield(fq);
+      for (int j = 0; j < n; ++j) {
+        drift = std::max(drift, std::fabs(fq[j] - f[j]));
+        f[j] = fq[j];
+      }
+    };
+    qfield(f);
     const uint32_t tag = ((inst0 + (uint32_t)m) << 8) | TAG_BATCH;
     for (int64_t k = 0; k < nsweeps; ++k) {
+      const uint32_t g = sweep0 + (uint32_t)k;
+      // fields anew before every global sweep that is a multiple of the interval
+      if (recompute > 0 && k > 0 && g % (uint32_t)recompute == 0) recompute_now();
       const float beta = betas_f[k];
       for (int i = 0; i < n; ++i) {
         const float dE = s[i] > 0 ? -2.0f * f[i] : 2.0f * f[i];
-        const P4 u = philox((uint32_t)(i >> 2), sweep0 + (uint32_t)k, rep0 + (uint32_t)r, tag, k0, k1);
+        const P4 u = philox((uint32_t)(i >> 2), g, rep0 + (uint32_t)r, tag, k0, k1);
         const float L = neglog(u.v[i & 3]);
         if (dE <= 0.0f || beta * dE < L) {
           const float c = s[i] > 0 ? -2.0f : 2.0f;
@@ -1015,6 +1040,12 @@ void orc_replay_sa_batch(int count, const int32_t* n_arr, const int64_t* offset,
     // the incrementally updated FP32 fields at the end (same layout as spins)
     if (fields_out)
       for (int j = 0; j < n; ++j) fields_out[soff[m] + (size_t)r * n + j] = f[j];
+    // the drift at the recompute points and against the final spins' fields
+    if (drift_out) {
+      qfield(fq);
+      for (int j = 0; j < n; ++j) drift = std::max(drift, std::fabs(fq[j] - f[j]));
+      drift_out[roff[m] + r] = drift;
+    }
   });
 }
 

@@ -80,7 +80,8 @@ def lib():
         L.orc_replay_sqa_split.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, C.c_int, _i8p, _u32p,
                                            _u32p, C.c_int, C.c_int64, C.c_uint64, C.c_int]
         L.orc_replay_sa_batch.argtypes = [C.c_int, _i32p, _i64p, _f64p, _i32p, _i8p, _f32p, C.c_int64,
-                                          C.c_uint64, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, C.c_uint32]
+                                          C.c_uint64, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32, C.c_uint32,
+                                          C.c_int, C.c_void_p]
         L.orc_ref_sw.argtypes = [C.c_int, _i64p, _i32p, _f64p, _i8p, _f64p, _i64p, C.c_int64, C.c_uint64]
         L.orc_ref_sw_many.argtypes = [C.c_int, _i64p, _i32p, _f64p, C.c_int, _i8p, _f64p, _i64p, C.c_int64,
                                       _u64p, C.c_int]
@@ -384,10 +385,14 @@ def replay_sqa_split(g: AugCSR, init3d, thr, mode, seed, threads=None):
 
 
 def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, threads=None, fields=False,
-                    rep0=0, sweep0=0):
+                    rep0=0, sweep0=0, recompute=16, drift=False):
     """Batched dense SA replay; mats: augmented (n+1)x(n+1) FP64 matrices,
     spins_flat: the instances' [reads[m]][n[m]] int8 blocks concatenated.
-    fields=True also returns the final incrementally updated FP32 fields.
+    The fields start from (and, before every global sweep that is a multiple
+    of ``recompute``, are set anew to) the tensor-core field kernel's
+    definition; 0 = never anew.  fields=True also returns the final
+    incrementally updated FP32 fields, drift=True the largest |f - f_exact| at
+    the recompute points and after the last sweep (per replica).
     inst0 / rep0 / sweep0: global index of instance 0, of every instance's
     replica 0 and of the first sweep (a slice of a larger run)."""
     n = np.array([m.shape[0] - 1 for m in mats], np.int32)
@@ -397,10 +402,17 @@ def replay_sa_batch(mats, reads, spins_flat, betas_per_sweep, seed, inst0=0, thr
     s = np.array(spins_flat, np.int8, copy=True)
     b = np.ascontiguousarray(betas_per_sweep, np.float32)
     fo = np.zeros(s.shape, np.float32) if fields else None
+    dr = np.zeros(int(np.sum(reads)), np.float32) if drift else None
     lib().orc_replay_sa_batch(len(mats), n, offset, flat, np.ascontiguousarray(reads, np.int32), s, b, len(b),
                               int(seed), int(inst0), _threads(threads),
-                              None if fo is None else fo.ctypes.data, int(rep0), int(sweep0))
-    return (s, fo) if fields else s
+                              None if fo is None else fo.ctypes.data, int(rep0), int(sweep0), int(recompute),
+                              None if dr is None else dr.ctypes.data)
+    out = (s,)
+    if fields:
+        out += (fo,)
+    if drift:
+        out += (dr,)
+    return out if len(out) > 1 else s
 
 
 def ref_sw_many(g: AugCSR, init2d, betas, mcs, seeds, threads=None):

@@ -263,24 +263,38 @@ def test_slice_split_sqa_replay_matches_python_restatement(T, R):
     np.testing.assert_array_equal(got, want)
 
 
-def _py_replay_sa_batch(mats, reads, spins, betas, seed, inst0=0):
-    """Python restatement of the batched dense SA replay (tiny sizes)."""
+def _py_replay_sa_batch(mats, reads, spins, betas, seed, inst0=0, recompute=0):
+    """Python restatement of the batched dense SA replay (tiny sizes): fields
+    on the grid 2^e (e = E - 26, 2^(E-1) <= max|J| < 2^E, couplings rounded
+    half to even), f = fp32(fp64(h) + 2^e sum q s); set anew before every
+    sweep k > 0 that is a multiple of `recompute`.  Returns the spins and the
+    largest |f - f_new| per replica (recompute points and the end)."""
+    import math
     out = np.array(spins, np.int64)
     k0, k1 = seed & 0xFFFFFFFF, seed >> 32
     off = 0
+    drifts = []
     for m, A in enumerate(mats):
         n = A.shape[0] - 1
         J = A[:n, :n].astype(np.float32)
         h = A[:n, n].astype(np.float32)
+        amax = float(np.abs(J).max()) if n else 0.0
+        e = math.frexp(amax)[1] - 26 if amax > 0 else 0
+        q = [[int(np.rint(math.ldexp(float(J[j, i]), -e))) for i in range(n)] for j in range(n)]
+
+        def field(s):
+            return np.array([np.float32(float(h[j]) + math.ldexp(sum(q[j][i] * int(s[i]) for i in range(n)), e))
+                             for j in range(n)], np.float32)
+
         for r in range(reads[m]):
             s = out[off + r * n: off + (r + 1) * n]
-            f = np.zeros(n, np.float32)
-            for j in range(n):
-                acc = np.float32(h[j])
-                for i in range(n):
-                    acc = np.float32(acc + (J[i, j] if s[i] > 0 else -J[i, j]))
-                f[j] = acc
+            f = field(s)
+            drift = np.float32(0.0)
             for k, beta in enumerate(np.asarray(betas, np.float32)):
+                if recompute and k > 0 and k % recompute == 0:
+                    fn = field(s)
+                    drift = max(drift, np.abs(fn - f).max())
+                    f = fn
                 for i in range(n):
                     dE = np.float32(-2.0) * f[i] if s[i] > 0 else np.float32(2.0) * f[i]
                     u = O.philox4x32_10([i >> 2, k, r, ((inst0 + m) << 8) | 0x96], [k0, k1])[i & 3]
@@ -288,11 +302,13 @@ def _py_replay_sa_batch(mats, reads, spins, betas, seed, inst0=0):
                         c = np.float32(-2.0 if s[i] > 0 else 2.0)
                         f = (f + c * J[i]).astype(np.float32)
                         s[i] = -s[i]
+            drifts.append(max(drift, np.abs(field(s) - f).max()))
         off += reads[m] * n
-    return out.astype(np.int8)
+    return out.astype(np.int8), np.array(drifts, np.float32)
 
 
-def test_batched_replay_matches_python_restatement():
+@pytest.mark.parametrize("recompute", [0, 2])
+def test_batched_replay_matches_python_restatement(recompute):
     rng = np.random.default_rng(7)
     mats = []
     for n in (5, 3, 6):
@@ -304,10 +320,13 @@ def test_batched_replay_matches_python_restatement():
         mats.append(A)
     reads = [2, 3, 1]
     spins = rng.choice(np.array([-1, 1], np.int8), size=sum(r * (m.shape[0] - 1) for r, m in zip(reads, mats)))
-    betas = np.array([0.3, 1.0, 2.0, 4.0])
-    got = O.replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4)
-    want = _py_replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4)
+    betas = np.array([0.3, 1.0, 2.0, 4.0, 6.0])
+    got, drift = O.replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4, recompute=recompute,
+                                   drift=True)
+    want, want_drift = _py_replay_sa_batch(mats, reads, spins, betas, seed=0x55_0000_0011, inst0=4,
+                                           recompute=recompute)
     np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(drift, want_drift)
 
 
 def test_kernel_colouring_is_proper_and_even():
