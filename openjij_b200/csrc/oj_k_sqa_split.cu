@@ -72,22 +72,64 @@ __device__ __forceinline__ void cluster_wait() {
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
+// Acceptance tables of one sweep, in shared memory.  For row l < 32 (bit
+// 31 - l of the thresholds), Trotter alignment k (0..2 aligned neighbours) and
+// unsatisfied-bond count u, word [l][k][u] is all ones when class c = 3u + k
+// is live (compared against U) and bit 31 - l of its threshold is set; row 32
+// marks the always-accepting classes, row 33 the live ones.  A word's class
+// bits are then sets of its bits: with the count u held as NB bit planes, the
+// table word of every bit is picked by a multiplexer tree over the planes (one
+// three-input logic operation per node) instead of a pass over every class.
 template <int D>
-struct SplitSweep {
-  static constexpr int NC = (D + 1) * 3;
-  uint32_t th[NC];
-  uint32_t always, live;
+struct SplitTab {
+  static constexpr int NB = D <= 1 ? 1 : (D <= 3 ? 2 : (D <= 7 ? 3 : 4));  // bit planes of u
+  static constexpr int E = 1 << NB;                                        // words per (row, k)
+  static constexpr int ROWS = 34;
+  static constexpr int WORDS = ROWS * 3 * E;
 };
 
+// Per bit, the table word of its count u: a multiplexer tree over the planes.
+template <int NB>
+__device__ __forceinline__ uint32_t tab_pick(const uint32_t* __restrict__ t, const uint32_t (&cnt)[NB]) {
+  constexpr int E = 1 << NB;
+  uint32_t v[E];
+  if constexpr (E >= 4) {
+#pragma unroll
+    for (int e = 0; e < E; e += 4) {
+      const uint4 q4 = *reinterpret_cast<const uint4*>(t + e);
+      v[e] = q4.x;
+      v[e + 1] = q4.y;
+      v[e + 2] = q4.z;
+      v[e + 3] = q4.w;
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = t[e];
+  }
+#pragma unroll
+  for (int b = 0; b < NB; ++b)
+#pragma unroll
+    for (int e = 0; e < (E >> (b + 1)); ++e) v[e] = (cnt[b] & v[2 * e + 1]) | (~cnt[b] & v[2 * e]);
+  return v[0];
+}
+
+// The bits of a word whose class has its table word set in `row` ([3][E]).
+template <int D>
+__device__ __forceinline__ uint32_t tab_eval(const uint32_t* __restrict__ row, uint32_t kk0, uint32_t kk1,
+                                             uint32_t kk2, const uint32_t (&cnt)[SplitTab<D>::NB]) {
+  constexpr int NB = SplitTab<D>::NB, E = SplitTab<D>::E;
+  return (kk0 & tab_pick<NB>(row, cnt)) | (kk1 & tab_pick<NB>(row + E, cnt)) |
+         (kk2 & tab_pick<NB>(row + 2 * E, cnt));
+}
+
 // New value of word x (half q) of one site: nb are the neighbour slots in X
-// (the array being updated), y the site's other half.
+// (the array being updated), y the site's other half, tab the sweep's tables.
 template <int D>
 __device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __restrict__ X,
                                                const uint16_t* __restrict__ nb, uint32_t jmk, uint32_t y,
-                                               int q, const SplitArgs& a, const SplitSweep<D>& sw,
+                                               int q, const SplitArgs& a, const uint32_t* __restrict__ tab,
                                                uint32_t site, uint32_t sweep, uint32_t grp) {
-  constexpr int NB = D <= 1 ? 1 : (D <= 3 ? 2 : (D <= 7 ? 3 : 4));
-  constexpr int NC = SplitSweep<D>::NC;
+  constexpr int NB = SplitTab<D>::NB, E = SplitTab<D>::E;
   uint32_t cnt[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) cnt[b] = 0u;
@@ -107,35 +149,18 @@ __device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __res
                             : (((y >> 1) & ~a.high) | ((y << (a.H - 1)) & a.high));
   const uint32_t al_y = ~(x ^ y), al_z = ~(x ^ z);
   const uint32_t kk2 = al_y & al_z, kk1 = al_y ^ al_z, kk0 = ~(al_y | al_z);
-  uint32_t cls[NC];
-  uint32_t flip = 0u, pending = 0u;
-#pragma unroll
-  for (int u = 0; u <= D; ++u) {
-    uint32_t mu = a.valid;
-#pragma unroll
-    for (int b = 0; b < NB; ++b) mu &= ((u >> b) & 1) ? cnt[b] : ~cnt[b];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int c = 3 * u + k;
-      const uint32_t m = mu & (k == 0 ? kk0 : (k == 1 ? kk1 : kk2));
-      if ((sw.always >> c) & 1u) flip |= m;
-      cls[c] = ((sw.live >> c) & 1u) ? m : 0u;
-      pending |= cls[c];
-    }
-  }
+  const uint32_t flip = tab_eval<D>(tab + 32 * 3 * E, kk0, kk1, kk2, cnt) & a.valid;
+  uint32_t pending = tab_eval<D>(tab + 33 * 3 * E, kk0, kk1, kk2, cnt) & a.valid;
   uint32_t lt = 0u;
-#pragma unroll
+#pragma unroll 1
   for (int qq = 0; qq < 8; ++qq) {
     if (!pending) break;
     const ojd::u4 r =
         ojd::philox(site, sweep, grp, ((uint32_t)qq << 16) | ((uint32_t)q << 8) | ojd::TAG_SQA_SPLIT, a.keys);
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
-      const int bitpos = 31 - (4 * qq + l);
       const uint32_t wl = ojd::pick(r, l);
-      uint32_t pm = 0u;
-#pragma unroll
-      for (int c = 0; c < NC; ++c) pm |= cls[c] & (0u - ((sw.th[c] >> bitpos) & 1u));
+      const uint32_t pm = tab_eval<D>(tab + (4 * qq + l) * 3 * E, kk0, kk1, kk2, cnt);
       lt |= pending & pm & ~wl;
       pending &= ~(pm ^ wl);
     }
@@ -148,19 +173,19 @@ template <int D>
 __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __restrict__ X,
                                                 const uint32_t* __restrict__ Y, const int32_t* __restrict__ gid,
                                                 const uint16_t* __restrict__ jm, const uint16_t* __restrict__ nbr,
-                                                int q, const SplitArgs& a, const SplitSweep<D>& sw, uint32_t k,
-                                                uint32_t g) {
+                                                int q, const SplitArgs& a, const uint32_t* __restrict__ tab,
+                                                uint32_t k, uint32_t g) {
   const int T = blockDim.x;
   uint32_t nf = 0u;
   if constexpr (D <= 4) {  // two independent sites per iteration
     for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
       const int s2 = s + T;
       const uint32_t x0 = X[s];
-      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, sw, (uint32_t)gid[s], k, g);
+      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
       if (s2 < hi) {
         const uint32_t x2 = X[s2];
         const uint32_t w2 =
-            split_site<D>(x2, X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, sw, (uint32_t)gid[s2], k, g);
+            split_site<D>(x2, X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, tab, (uint32_t)gid[s2], k, g);
         X[s2] = w2;
         nf += __popc(w2 ^ x2);
       }
@@ -170,7 +195,7 @@ __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __rest
   } else {
     for (int s = lo + threadIdx.x; s < hi; s += T) {
       const uint32_t x0 = X[s];
-      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, sw, (uint32_t)gid[s], k, g);
+      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
       X[s] = v;
       nf += __popc(v ^ x0);
     }
@@ -184,7 +209,9 @@ __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __rest
 template <int D, bool CL>
 __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a) {
   extern __shared__ __align__(16) uint32_t sh[];
-  constexpr int NC = SplitSweep<D>::NC;
+  constexpr int NC = (D + 1) * 3;
+  constexpr int E = SplitTab<D>::E;
+  __shared__ __align__(16) uint32_t tab[SplitTab<D>::WORDS];
   const int p = CL ? (int)cg::this_cluster().block_rank() : 0;
   const int g = blockIdx.y;
   const int32_t* gid_g = a.gidx + (size_t)p * a.slots;
@@ -220,11 +247,26 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
   int prev_c = -1, prev_q = 0;  // colour class and half updated by the previous phase
   const uint32_t gg = a.group0 + (uint32_t)g;
   for (int64_t k = 0; k < a.nsweeps; ++k) {
-    SplitSweep<D> sw;
-#pragma unroll
-    for (int c = 0; c < NC; ++c) sw.th[c] = __ldg(a.thr + (size_t)k * NC + c);
-    sw.always = __ldg(a.mode + 2 * k);
-    sw.live = __ldg(a.mode + 2 * k + 1);
+    {
+      // the sweep's tables (every thread finished the previous sweep's last
+      // phase at its closing barrier)
+      const uint32_t alw = __ldg(a.mode + 2 * k), live = __ldg(a.mode + 2 * k + 1);
+      for (int idx = threadIdx.x; idx < SplitTab<D>::WORDS; idx += blockDim.x) {
+        const int row = idx / (3 * E), kq = (idx / E) % 3, u = idx % E;
+        uint32_t w = 0u;
+        if (u <= D) {
+          const int c = 3 * u + kq;
+          bool on;
+          if (row < 32)
+            on = ((live >> c) & 1u) && ((__ldg(a.thr + (size_t)k * NC + c) >> (31 - row)) & 1u);
+          else
+            on = row == 32 ? ((alw >> c) & 1u) : ((live >> c) & 1u);
+          w = on ? 0xFFFFFFFFu : 0u;
+        }
+        tab[idx] = w;
+      }
+      __syncthreads();
+    }
     const uint32_t kk = a.sweep0 + (uint32_t)k;
     for (int q = 0; q < 2; ++q) {
       uint32_t* X = q ? WO : WE;
@@ -232,7 +274,7 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
       for (int c = 0; c < a.ncol; ++c) {
         if constexpr (CL) {
           cg::cluster_group cl = cg::this_cluster();
-          nflip += split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          nflip += split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
           cluster_wait();
           if (prev_c >= 0) {
             uint32_t* P = prev_q ? WO : WE;
@@ -244,13 +286,13 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
             }
           }
           __syncthreads();
-          nflip += split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          nflip += split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
           cluster_arrive();
           __syncthreads();
           prev_c = c;
           prev_q = q;
         } else {
-          nflip += split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, sw, kk, gg);
+          nflip += split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
           __syncthreads();
         }
       }
