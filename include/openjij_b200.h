@@ -125,6 +125,14 @@ oj_status oj_ctx_set_field_recompute(oj_ctx* ctx, int32_t sweeps);
  * context stays usable.  For tests of that path (0 gives up at once). */
 oj_status oj_ctx_set_wait_limit(oj_ctx* ctx, int64_t iterations);
 
+/* Host-side fault injection for tests of the error paths (no device fault is
+ * made).  OJ_FAULT_ALLOC: the `after`-th device allocation from now (0 = the
+ * next one) of any context of the process fails as if the device were out of
+ * memory, so the call reports OJ_ERR_OOM; OJ_FAULT_NONE clears it. */
+#define OJ_FAULT_NONE 0
+#define OJ_FAULT_ALLOC 1
+oj_status oj_ctx_inject_fault(oj_ctx* ctx, int32_t kind, int64_t after);
+
 /* Graph upload.  Replaces cxxjij.graph.Dense(num_spins).set_interaction_matrix
  * (openjij/declare.hpp:75-129; include/openjij/graph/dense.hpp:117-140) and
  * cxxjij.graph.CSRSparse(csr) (declare.hpp:195-217; csr_sparse.hpp:96-101).

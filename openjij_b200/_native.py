@@ -37,7 +37,7 @@ EXPORTS = [
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
     "oj_sa_run_bitpacked_noalloc", "oj_batch_create_dense", "oj_batch_destroy", "oj_sa_run_batched",
     "oj_sw_run", "oj_graph_flip_stats", "oj_batch_flip_stats", "oj_ctx_set_field_recompute",
-    "oj_ctx_set_wait_limit",
+    "oj_ctx_set_wait_limit", "oj_ctx_inject_fault",
 ]
 
 
@@ -85,6 +85,7 @@ def lib():
         L.oj_ctx_synchronize.argtypes = [vp]
         L.oj_ctx_set_field_recompute.argtypes = [vp, i32]
         L.oj_ctx_set_wait_limit.argtypes = [vp, i64]
+        L.oj_ctx_inject_fault.argtypes = [vp, i32, i64]
         L.oj_ctx_last_error.argtypes = [vp]
         L.oj_ctx_last_error.restype = C.c_char_p
         L.oj_graph_create_dense.argtypes = [vp, i32, vp, C.POINTER(vp)]
@@ -145,6 +146,12 @@ class Context:
     def set_field_recompute(self, sweeps: int):
         """Full field recompute every `sweeps` sweeps of batched / dense-jump runs (0 = never)."""
         self.check(lib().oj_ctx_set_field_recompute(self._h, int(sweeps)), "set_field_recompute")
+
+    def inject_alloc_failure(self, after):
+        """Host-side fault injection: the after-th device allocation from now
+        fails as out of memory (None clears it)."""
+        kind, n = (0, 0) if after is None else (1, int(after))
+        self.check(lib().oj_ctx_inject_fault(self._h, kind, n), "inject_fault")
 
     def set_wait_limit(self, iterations: int):
         """Iterations of the field kernel's bounded pipeline waits (< 0: the default)."""

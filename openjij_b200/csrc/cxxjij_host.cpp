@@ -90,6 +90,7 @@ struct RunInfo {
   double attempts = 0;
   double anneal_ms = 0, total_ms = 0;
   double accepted = 0;
+  double field_drift = -1.0;  // largest over the calls of the run (-1: not measured)
 };
 RunInfo g_last_run;
 
@@ -103,6 +104,7 @@ void record(const oj_run_stats& st) {
   g_last_run.anneal_ms += st.anneal_ms;
   g_last_run.total_ms += st.total_ms;
   g_last_run.accepted = (st.accepted < 0 || g_last_run.accepted < 0) ? -1.0 : g_last_run.accepted + st.accepted;
+  g_last_run.field_drift = std::max(g_last_run.field_drift, st.field_drift);
 }
 
 // ---------------------------------------------------------------------------
@@ -1301,6 +1303,7 @@ PYBIND11_MODULE(_cxxjij, m) {
     d["anneal_ms"] = g_last_run.anneal_ms;
     d["total_ms"] = g_last_run.total_ms;
     d["accepted"] = g_last_run.accepted;
+    d["field_drift"] = g_last_run.field_drift;
     return d;
   });
   m.def("version", []() { return std::string(oj_version()); });

@@ -461,6 +461,17 @@ oj_status oj_ctx_set_field_recompute(oj_ctx* ctx, int32_t sweeps) {
   return OJ_OK;
 }
 
+oj_status oj_ctx_inject_fault(oj_ctx* ctx, int32_t kind, int64_t after) {
+  if (!ctx) return OJ_ERR_ARG;
+  if (kind == OJ_FAULT_NONE) {
+    alloc_fail_countdown().store(-1);
+    return OJ_OK;
+  }
+  if (kind != OJ_FAULT_ALLOC || after < 0) return arg_fail(ctx, "unknown fault kind or negative count");
+  alloc_fail_countdown().store((long long)after);
+  return OJ_OK;
+}
+
 oj_status oj_ctx_set_wait_limit(oj_ctx* ctx, int64_t iterations) {
   if (!ctx) return OJ_ERR_ARG;
   ctx->wait_limit = iterations < 0 ? -1 : (long long)iterations;
@@ -1201,6 +1212,8 @@ oj_status build_batch(oj_ctx* ctx, int32_t count, const int32_t* n, const int64_
     const double* A = J_aug + offset[k];
     // graph::Dense::set_interaction_matrix checks (dense.hpp:117-140)
     if (A[nk * n1 + nk] != 1.0) return arg_fail(ctx, "the corner of an augmented matrix must be 1");
+    for (int64_t q = 0; q < n1 * n1; ++q)
+      if (!std::isfinite(A[q])) return arg_fail(ctx, "couplings and fields must be finite");
     for (int64_t i = 0; i < n1 && !checked; ++i) {
       if (i < nk && A[i * n1 + i] != 0.0) return arg_fail(ctx, "the diagonal of J must be zero (h goes in column n)");
       for (int64_t j = i + 1; j < n1; ++j)

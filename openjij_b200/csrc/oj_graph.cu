@@ -181,6 +181,10 @@ oj_status finish_graph(oj_ctx* ctx, oj_graph* g) {
         ctx->last_error = "column index out of range";
         return OJ_ERR_ARG;
       }
+      if (!std::isfinite(dv[q])) {
+        ctx->last_error = "couplings and fields must be finite";
+        return OJ_ERR_ARG;
+      }
       if (j == n) {
         g->h64[i] += dv[q];
       } else if (j == i) {

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -14,12 +15,22 @@
 
 namespace oj {
 
+// Host-side fault injection for tests (oj_ctx_inject_fault): while it is >= 0,
+// every device allocation counts it down, and the one that finds it at zero
+// fails as if the device were out of memory (no allocation is attempted).
+inline std::atomic<long long>& alloc_fail_countdown() {
+  static std::atomic<long long> c{-1};
+  return c;
+}
+
 // Grow-only device buffer owned by a context or graph.
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
   cudaError_t ensure(size_t want) {
     if (want <= bytes) return cudaSuccess;
+    if (alloc_fail_countdown().load() >= 0 && alloc_fail_countdown().fetch_sub(1) == 0)
+      return cudaErrorMemoryAllocation;  // the buffer keeps its old contents and size
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     bytes = 0;

@@ -194,6 +194,8 @@ class SASampler(BaseSampler):
             resp.info["schedule"] = {"beta_min": bmin, "beta_max": bmax, "num_sweeps": S}
             resp.info["sampling_time"] = elapsed * 1e6
             resp.info["run"] = st
+            resp.info["accepted_flips"] = st["accepted"]  # over the whole batch call
+            resp.info["field_drift"] = st["field_drift"]
             out.append(resp)
         return out
 

@@ -128,7 +128,13 @@ class BaseSampler:
         response.info["sampling_time"] = sampling_time * 1e6
         response.info["execution_time"] = (float(np.mean(exec_times)) * 1e6) if exec_times else 0.0
         response.info["list_exec_times"] = np.asarray(exec_times) * 1e6
-        response.info["run"] = cxxjij.last_run_info()
+        run_info = cxxjij.last_run_info()
+        response.info["run"] = run_info
+        # per call: accepted single-spin flips, and for the dense kernels the
+        # largest deviation of the incremental FP32 fields from the exact fields
+        # of the same spins (-1 where not measured)
+        response.info["accepted_flips"] = run_info.get("accepted", -1.0)
+        response.info["field_drift"] = run_info.get("field_drift", -1.0)
         return response
 
     def _get_result(self, system, model, sites=None):

@@ -176,6 +176,29 @@ def test_sa_energies_match_model():
         assert e == pytest.approx(bqm.energy(st), abs=1e-9)
 
 
+def test_response_info_states_flips_and_field_drift():
+    """Response.info carries the call's accepted flips and, for the dense
+    kernels, the largest deviation of the incremental FP32 fields from the
+    exact fields (recomputed on the tensor cores): positive and small for real
+    couplings, zero for integer ones, -1 for the sparse kernels."""
+    rng = np.random.default_rng(11)
+    n = 300
+    Qr = rng.standard_normal((n, n))
+    Qi = rng.integers(-8, 9, (n, n)).astype(np.float64)
+    for Q, exact in ((np.triu(Qr), False), (np.triu(Qi), True)):
+        res = oj.SASampler().sample_qubo(Q, num_reads=16, num_sweeps=64, seed=3)
+        assert res.info["run"]["kernel"] == "dense_jump"
+        assert res.info["accepted_flips"] > 0
+        if exact:
+            assert res.info["field_drift"] == 0.0
+        else:
+            assert 0.0 < res.info["field_drift"] < 1e-2
+    h = {i: 0.0 for i in range(16)}
+    J = {(i, (i + 1) % 16): -1.0 for i in range(16)}
+    res = oj.SASampler().sample_ising(h, J, num_reads=4, num_sweeps=20, seed=1)
+    assert res.info["accepted_flips"] > 0 and res.info["field_drift"] == -1.0
+
+
 def test_sqa_sampler_reference_cases():
     s = oj.SQASampler()
     run_samplers(s)
