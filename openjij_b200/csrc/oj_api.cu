@@ -49,6 +49,16 @@ oj_status cuda_fail(oj_ctx* ctx, cudaError_t e, const char* where) {
     if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
   } while (0)
 
+// A kernel's host preparation failed: a stated reason means the kernel cannot
+// run this graph; otherwise a CUDA error (out of memory included).
+oj_status prep_fail(oj_ctx* ctx, cudaError_t e, const std::string& why) {
+  if (!why.empty()) {
+    ctx->last_error = why;
+    return OJ_ERR_UNSUPPORTED;
+  }
+  return cuda_fail(ctx, e, "kernel preparation");
+}
+
 oj_status arg_fail(oj_ctx* ctx, const char* msg) {
   if (ctx) ctx->last_error = msg;
   return OJ_ERR_ARG;
@@ -601,8 +611,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     std::string why;
     cudaError_t pe = dense_tc_prepare(g, &why);
     if (pe != cudaSuccess) {
-      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
-      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+      return prep_fail(ctx, pe, why);
     }
   }
   cudaStream_t st = ctx->stream;
@@ -634,8 +643,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
                                                                        : msc_choose_cluster(g, G, ctx->sm_count);
     cudaError_t pe = msc_prepare(g, P, &why);
     if (pe != cudaSuccess) {
-      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
-      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+      return prep_fail(ctx, pe, why);
     }
     std::vector<uint32_t> thr, alw;
     msc_thresholds(bf, inf.coupling_abs, D, thr, alw);
@@ -688,8 +696,7 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
     threads_used = shp.threads ? shp.threads : msc_default_threads();
     pe = msc_prepare(g, P_used, &why);
     if (pe != cudaSuccess) {
-      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
-      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+      return prep_fail(ctx, pe, why);
     }
     OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
     if (S > 0)
@@ -932,8 +939,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     const cudaError_t pe =
         sqa_split_prepare(g, G, ctx->sm_count, &why, cached != g->tuned.end() ? cached->second.cluster : 0);
     if (pe != cudaSuccess) {
-      ctx->last_error = why.empty() ? cudaGetErrorString(pe) : why;
-      return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+      return prep_fail(ctx, pe, why);
     }
     std::vector<uint32_t> thr, mode;
     sqa_msc_thresholds(coef, g->info.coupling_abs, g->info.max_degree, thr, mode);
@@ -982,8 +988,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     {
       const cudaError_t pe2 = sqa_split_prepare(g, G, ctx->sm_count, &why, shp.cluster);
       if (pe2 != cudaSuccess) {
-        ctx->last_error = why.empty() ? cudaGetErrorString(pe2) : why;
-        return why.empty() ? OJ_ERR_CUDA : OJ_ERR_UNSUPPORTED;
+        return prep_fail(ctx, pe2, why);
       }
     }
     P_used = g->msc->P;
