@@ -451,6 +451,8 @@ def run_ours_batch(args, w):
     stream = torch.cuda.current_stream()
     ctx = N.Context(local)
     ctx.set_stream(stream.cuda_stream)
+    if args.field_recompute is not None:
+        ctx.set_field_recompute(args.field_recompute)
     mats, reads = w["mats"], w["reads"]
     batch = N.Batch(ctx, mats)
     sizes = np.array([m.shape[0] - 1 for m in mats], np.int64)
@@ -541,7 +543,8 @@ def run_ours_batch(args, w):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded instances)",
             "config": _config_of(w),
             "kernel": {"name": "batched", "launch_shape": {"threads": st["threads"], "variant": st["variant"],
-                                                           "autotuned": True}},
+                                                           "autotuned": True},
+                       "field_recompute_sweeps": 16 if args.field_recompute is None else args.field_recompute},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": attempts_per_step * ws / (e2 / 1000.0), "unit": "attempts/s",
@@ -577,6 +580,8 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     ctx = N.Context(local)
     ctx.set_stream(stream.cuda_stream)
+    if args.field_recompute is not None:
+        ctx.set_field_recompute(args.field_recompute)
     graph = N.Graph(ctx, n, indptr, indices, data)
     rng = np.random.default_rng(1000 + rank)
     shape = (R, n) if w["kind"] == "sa" else (R, T, n)
@@ -906,6 +911,9 @@ def main():
     ap.add_argument("--kernel", default=None,
                     help="force a kernel: colour, dense_plain, bitpacked, dense_tc, dense_jump, or "
                          "swendsen_wang for the cluster updater (default: planner)")
+    ap.add_argument("--field-recompute", type=int, default=None,
+                    help="dense / batched kernels: full field recompute every this many sweeps for couplings whose "
+                         "FP32 sums are not exact (default: the library's, 16; 0 = only at the start of a call)")
     ap.add_argument("--no-tts", action="store_true",
                     help="leave the configs 3-5 time-to-1%% comparison out of the default line")
     ap.add_argument("--tts", action="store_true",
