@@ -119,14 +119,51 @@ __device__ __forceinline__ float4 row4h(const __half* p) {
   }
 }
 
+// Four couplings of a row segment as loaded (raw FP16 pairs or FP32 values),
+// widened only where they are used: a whole row's loads in flight take half
+// the registers with FP16 rows.
+template <bool H>
+struct Raw4;
+template <>
+struct Raw4<true> {
+  uint2 v;
+};
+template <>
+struct Raw4<false> {
+  float4 v;
+};
+template <bool H, bool SJ>
+__device__ __forceinline__ Raw4<H> raw4(const float* p32, const __half* p16) {
+  Raw4<H> r;
+  if constexpr (H) r.v = SJ ? *reinterpret_cast<const uint2*>(p16) : __ldg(reinterpret_cast<const uint2*>(p16));
+  else r.v = SJ ? *reinterpret_cast<const float4*>(p32) : ldg4(p32);
+  return r;
+}
+template <bool H>
+__device__ __forceinline__ float4 widen4(const Raw4<H>& r) {
+  if constexpr (H) {
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&r.v.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&r.v.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+  } else {
+    return r.v;
+  }
+}
+
 // The couplings of an instance are staged in shared memory (SJ) when the
 // batch's largest block of n rows x npad columns takes at most this many bytes.
 constexpr size_t kBatchSmemJBytes = 96 * 1024;
 // Bytes of each warp's flip list (one entry per site of a chunk).
 constexpr int kFlipList = 128;
+constexpr int kDelayAt = 3;
 
 // GROUP: chunks whose fields take a chunk's delayed flips together (their row
-// loads are in flight at once); more costs registers.
+// loads are in flight at once); more costs registers.  A chunk is decided in
+// one of two modes with the same FMAs in the same order per field: direct (a
+// flip applies its whole row at once, the row's loads in flight together;
+// few flips per chunk) or delayed (a flip updates its own chunk at once and
+// the others at the end of the chunk; many flips).  The warp takes the delayed
+// mode for a chunk when the chunk it decided last had at least kDelayAt flips.
 // H: the flip rows come from the FP16 copy of J (half the L2 bytes per flip).
 // SJ: every work item first copies its instance's couplings (FP32 or FP16
 // rows, as H says) into shared memory after the warps' fields and spin words,
@@ -199,6 +236,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     // this lane's sites of the last chunk that exist (site index below n), as
     // a 4-bit mask; every site of the other chunks exists
     const uint32_t inside_last = 0xFu >> (4 - min(max(n - 128 * (nch - 1) - 4 * lane, 0), 4));
+    bool delayed = true;  // the mode of the next chunk (the first sweeps flip many spins)
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
@@ -254,28 +292,61 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const uint32_t neg = (pk >> (4 + es)) & 1u;
           const float coef = neg ? 2.0f : -2.0f;
           const int il = 4 * ls + es;  // chunk-local site
-          // the flip reaches this chunk's fields now (the sites still to be
-          // decided read them); the other chunks get it at the end of the chunk
-          const size_t roff = (size_t)(128 * c + il) * npad + 128 * c + 4 * lane;
-          const float4 v = H ? row4h<SJ>(Jr16 + roff) : row4<SJ>(Jr + roff);
-          fc.x = __fmaf_rn(coef, v.x, fc.x);
-          fc.y = __fmaf_rn(coef, v.y, fc.y);
-          fc.z = __fmaf_rn(coef, v.z, fc.z);
-          fc.w = __fmaf_rn(coef, v.w, fc.w);
-          if (lane == ls) myw ^= 1u << es;
-          if (lane == 0) {
-            fl[nfl] = (uint8_t)(il | (neg << 7));
-            ++nflip;
+          const size_t rrow = (size_t)(128 * c + il) * npad + 4 * lane;
+          if (delayed) {
+            // the flip reaches this chunk's fields now (the sites still to be
+            // decided read them); the other chunks get it at the end of the chunk
+            const float4 v = widen4<H>(raw4<H, SJ>(Jr + rrow + 128 * c, Jr16 + rrow + 128 * c));
+            fc.x = __fmaf_rn(coef, v.x, fc.x);
+            fc.y = __fmaf_rn(coef, v.y, fc.y);
+            fc.z = __fmaf_rn(coef, v.z, fc.z);
+            fc.w = __fmaf_rn(coef, v.w, fc.w);
+            if (lane == 0) fl[nfl] = (uint8_t)(il | (neg << 7));
+          } else {
+            // the whole row now: this chunk's fields in registers, the others in
+            // shared memory, DG chunks' loads in flight together (the same
+            // registers as GROUP chunks of FP32 values)
+            constexpr int DG = H ? 2 * GROUP : GROUP;
+#pragma unroll 1
+            for (int c0 = 0; c0 < nch; c0 += DG) {
+              Raw4<H> v[DG];
+#pragma unroll
+              for (int q = 0; q < DG; ++q)
+                if (c0 + q < nch) v[q] = raw4<H, SJ>(Jr + rrow + 128 * (c0 + q), Jr16 + rrow + 128 * (c0 + q));
+#pragma unroll
+              for (int q = 0; q < DG; ++q) {
+                if (c0 + q >= nch) break;
+                const float4 w4 = widen4<H>(v[q]);
+                if (c0 + q == c) {
+                  fc.x = __fmaf_rn(coef, w4.x, fc.x);
+                  fc.y = __fmaf_rn(coef, w4.y, fc.y);
+                  fc.z = __fmaf_rn(coef, w4.z, fc.z);
+                  fc.w = __fmaf_rn(coef, w4.w, fc.w);
+                } else {
+                  float4 g = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
+                  g.x = __fmaf_rn(coef, w4.x, g.x);
+                  g.y = __fmaf_rn(coef, w4.y, g.y);
+                  g.z = __fmaf_rn(coef, w4.z, g.z);
+                  g.w = __fmaf_rn(coef, w4.w, g.w);
+                  reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g;
+                }
+              }
+            }
           }
+          if (lane == ls) myw ^= 1u << es;
+          if (lane == 0) ++nflip;
           ++nfl;
           open = inside & (0xFu << min(max(il + 1 - 4 * lane, 0), 4));
         }
+        const bool was_delayed = delayed;
+        delayed = nfl >= kDelayAt;  // the mode of the next chunk
         if (nfl == 0) continue;
         reinterpret_cast<float4*>(f)[32 * c + lane] = fc;
         {
           uint32_t& wd = sw[sw_word(c, lane)];
           wd = (wd & ~(0xFu << sw_shift(c))) | (myw << sw_shift(c));
         }
+        if (!was_delayed) continue;
         __syncwarp();  // the flip list is complete
         // Delayed update: every other chunk's fields take the chunk's flips in
         // site order, one FMA each (c * J_ij exact), GROUP chunks at a time so
@@ -295,7 +366,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
               if (c0 + q < nch && c0 + q != c) {
-                const float4 v = H ? row4h<SJ>(Jr16 + ro + 128 * (c0 + q)) : row4<SJ>(Jr + ro + 128 * (c0 + q));
+                const float4 v = widen4<H>(raw4<H, SJ>(Jr + ro + 128 * (c0 + q), Jr16 + ro + 128 * (c0 + q)));
                 g[q].x = __fmaf_rn(cf, v.x, g[q].x);
                 g[q].y = __fmaf_rn(cf, v.y, g[q].y);
                 g[q].z = __fmaf_rn(cf, v.z, g[q].z);
