@@ -144,8 +144,12 @@ struct FieldShape {
   static constexpr uint32_t kA = D * kTileBytes;         // digit tiles of one K chunk
   static constexpr uint32_t kB = NT * kChunk;            // spin tile of one K chunk
   static constexpr uint32_t kStage = (kA + kB + 1023) / 1024 * 1024;
+  // stages in the ring: four-digit tiles stream from DRAM and want several
+  // chunks in flight (three when 220 KB hold them); one-digit tiles keep two,
+  // so that two CTAs share an SM and one's epilogue overlaps the other's loop
+  static constexpr int kStages = (D > 1 && 3u * kStage <= 220u * 1024u) ? 3 : 2;
   static constexpr uint32_t kCols = D * NT <= 32 ? 32 : (D * NT <= 64 ? 64 : (D * NT <= 128 ? 128 : (D * NT <= 256 ? 256 : 512)));
-  static constexpr size_t kSmem = 2 * (size_t)kStage + 64;  // + 4 mbarriers, TMEM slot, abort flag
+  static constexpr size_t kSmem = kStages * (size_t)kStage + 16 * kStages + 16;  // mbarriers, TMEM slot, abort flag
 };
 
 template <int D, int NT>
@@ -161,24 +165,27 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   const int n = a.n[m], R = a.reads[m];
   const int nch = (n + kChunk - 1) / kChunk;
   const int npad = nch * kChunk;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * S::kStage);  // full[2], done[2]
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 4);
+  constexpr int ST = S::kStages;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + ST * S::kStage);  // full[ST], done[ST]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2 * ST);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(S::kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int q = 0; q < 4; ++q) mbar_init(bar + q, 1);
+    for (int q = 0; q < 2 * ST; ++q) mbar_init(bar + q, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tslot;
-  // Pipeline waits use a.wait_limit; one that runs out aborts the loop: no new
-  // copies or MMAs are issued, the ones in flight are waited for with the
-  // default limit (kDrainLimit), tensor memory is freed and F is left as it was.
+  // Ring of ST stages: the digit tiles of chunk kc + ST - 1 are copied while
+  // chunk kc's spins are written and its MMAs run.  Pipeline waits use
+  // a.wait_limit; one that runs out aborts the loop: no new copies or MMAs are
+  // issued, the ones in flight are waited for with the default limit
+  // (kDrainLimit), tensor memory is freed and F is left as it was.
   // thread 0's bookkeeping, bit s for stage s: phase parities of the full and
   // done barriers, and copies / MMA commits issued but not yet seen complete
   uint32_t ph_full = 0u, ph_done = 0u, pend_full = 0u, pend_done = 0u;
@@ -187,29 +194,38 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   const int8_t* dig = a.digits + a.dtoff[m];
   const int8_t* sp = a.spins + a.soff[m];
   const int r0 = nt * NT;
+  // digit tiles of chunk kc into stage kc % ST (thread 0; the stage is free)
+  auto issue_a = [&](int kc) {
+    const int s = kc % ST;
+    unsigned char* As = sm + s * S::kStage;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar + s)), "r"(S::kA)
+                 : "memory");
+#pragma unroll
+    for (int t = 0; t < D; ++t)
+      bulk_copy(As + t * kTileBytes, dig + ((size_t)(t * nch + mt) * nch + kc) * kTileBytes, kTileBytes, bar + s);
+    pend_full |= 1u << s;
+  };
+  if (tid == 0)
+    for (int kc = 0; kc < ST - 1 && kc < nch; ++kc) issue_a(kc);
   for (int kc = 0; kc < nch; ++kc) {
-    const int s = kc & 1;
+    const int s = kc % ST;
     unsigned char* As = sm + s * S::kStage;
     unsigned char* Bs = As + S::kA;
-    const uint32_t sb = 1u << s;
-    if (tid == 0 && (pend_done & sb)) {  // the stage's previous MMAs (chunk kc - 2) have read it
-      if (mbar_wait(bar + 2 + s, (ph_done >> s) & 1u, a.wait_limit)) {
-        ph_done ^= sb;
-        pend_done &= ~sb;
-      } else {
-        *abort_flag = 1;
+    if (tid == 0 && kc + ST - 1 < nch) {
+      // the stage of chunk kc + ST - 1 last held chunk kc - 1: its MMAs first
+      const int sn = (kc + ST - 1) % ST;
+      if ((pend_done >> sn) & 1u) {
+        if (mbar_wait(bar + ST + sn, (ph_done >> sn) & 1u, a.wait_limit)) {
+          ph_done ^= 1u << sn;
+          pend_done &= ~(1u << sn);
+        } else {
+          *abort_flag = 1;
+        }
       }
+      if (!*abort_flag) issue_a(kc + ST - 1);
     }
-    __syncthreads();
+    __syncthreads();  // stage s's spin tile is free (chunk kc - ST's MMAs were seen complete)
     if (*abort_flag) break;
-    if (tid == 0) {
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar + s)), "r"(S::kA)
-                   : "memory");
-#pragma unroll
-      for (int t = 0; t < D; ++t)
-        bulk_copy(As + t * kTileBytes, dig + ((size_t)(t * nch + mt) * nch + kc) * kTileBytes, kTileBytes, bar + s);
-      pend_full |= sb;
-    }
     // spins of replicas r0..r0+NT-1 at sites 128 kc .. +127, 16 bytes a piece;
     // zero past the instance's reads and sites
     for (int idx = tid; idx < NT * 8; idx += kFieldThreads) {
@@ -241,8 +257,8 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
     __syncthreads();
     if (tid == 0) {
       if (mbar_wait(bar + s, (ph_full >> s) & 1u, a.wait_limit)) {
-        ph_full ^= sb;
-        pend_full &= ~sb;
+        ph_full ^= 1u << s;
+        pend_full &= ~(1u << s);
         tc_fence_after();
         const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
 #pragma unroll
@@ -251,8 +267,8 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
           for (int kk = 0; kk < kChunk / 32; ++kk)
             mma_i8(tbase + (uint32_t)(t * NT), desc_kmajor(a0 + t * kTileBytes + kk * 256, 128, 1024),
                    desc_kmajor(b0 + kk * 256, 128, 1024), idesc_i8(NT), (kc | kk) ? 1u : 0u);
-        mma_commit(bar + 2 + s);
-        pend_done |= sb;
+        mma_commit(bar + ST + s);
+        pend_done |= 1u << s;
       } else {
         *abort_flag = 1;
       }
@@ -261,9 +277,9 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   // drain: every copy and MMA this CTA issued has completed before it goes on
   bool ok = true;
   if (tid == 0) {
-    for (int s = 0; s < 2; ++s) {
-      if ((pend_full >> s) & 1u) ok &= mbar_wait(bar + s, (ph_full >> s) & 1u, kDrainLimit);
-      if ((pend_done >> s) & 1u) ok &= mbar_wait(bar + 2 + s, (ph_done >> s) & 1u, kDrainLimit);
+    for (int q = 0; q < ST; ++q) {
+      if ((pend_full >> q) & 1u) ok &= mbar_wait(bar + q, (ph_full >> q) & 1u, kDrainLimit);
+      if ((pend_done >> q) & 1u) ok &= mbar_wait(bar + ST + q, (ph_done >> q) & 1u, kDrainLimit);
     }
     if (*abort_flag || !ok) atomicExch(a.status, 1);
   }
@@ -277,8 +293,11 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   }
   // ---- epilogue: warp w reads TMEM lanes 32w..32w+31 = sites of the tile
   const int site = mt * kTileSites + 32 * warp + lane;
-  const double hv = (double)a.h[a.hoff[m] + site];  // zero past n (padding)
-  const int e = a.uexp[m];
+  const float hf = a.h[a.hoff[m] + site];  // zero past n (padding)
+  const double hv = (double)hf;
+  // 2^e: multiplying by it is exact (the products stay normal)
+  const double scale = ldexp(1.0, a.uexp[m]);
+  const float scale_f = (float)scale;
   float* Fm = a.F + a.foff[m] + site;
   float dmax = 0.0f;
   for (int j0 = 0; j0 < NT; j0 += 16) {
@@ -297,7 +316,10 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
     for (int j = 0; j < 16; ++j) {
       const int r = r0 + j0 + j;
       if (r >= R) break;
-      const float f = __double2float_rn(__dadd_rn(hv, ldexp((double)tot[j], e)));
+      // one int8 digit: the exact-field integer batches, where h + 2^e acc is
+      // an FP32 value and the FP32 operations are exact (the same value)
+      const float f = D == 1 ? __fadd_rn(hf, __fmul_rn(__ll2float_rn(tot[j]), scale_f))
+                             : __double2float_rn(__dadd_rn(hv, __dmul_rn(__ll2double_rn(tot[j]), scale)));
       float* dst = Fm + (size_t)r * npad;
       if (a.compare && site < n) dmax = fmaxf(dmax, fabsf(f - *dst));
       *dst = f;
