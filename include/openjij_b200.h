@@ -46,7 +46,8 @@ enum {
  * candidate launch shapes (cluster size, threads per CTA, register budget)
  * for a few sweeps on a copy of the call's own state and keep the fastest for
  * later calls.  Every shape gives the same spins; only the time differs.
- * Also enabled by the environment variable OJ_AUTOTUNE=1. */
+ * Also enabled by the environment variable OJ_AUTOTUNE=1; OJ_AUTOTUNE=0 disables it
+ * even when the flag is given (fixed launch shapes, e.g. for profiling). */
 #define OJ_AUTOTUNE 0x2u
 /* kernel selection (bits 4..7) */
 #define OJ_KERNEL_SHIFT 4

@@ -311,10 +311,12 @@ cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, co
   return cudaSuccess;
 }
 
+// OJ_AUTOTUNE=1 in the environment tunes every call's first use of a shape,
+// OJ_AUTOTUNE=0 none (not even on request: fixed shapes for profiling).
 bool autotune_requested(uint32_t flags) {
-  if (flags & OJ_AUTOTUNE) return true;
   const char* e = std::getenv("OJ_AUTOTUNE");
-  return e && e[0] == '1';
+  if (e && e[0] == '0') return false;
+  return (flags & OJ_AUTOTUNE) || (e && e[0] == '1');
 }
 
 // Autotuner core: for each candidate, restore() puts the call's own initial

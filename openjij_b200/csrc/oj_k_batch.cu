@@ -20,16 +20,10 @@
 // the current fields, jumps to the first accepted site, applies that flip and
 // re-evaluates the sites after it: sites that do not flip leave the state
 // unchanged, so this is the sequential sweep, with one step per flip instead
-// of one per site.  A flip updates at once only the fields of its own chunk
-// (held in registers, the sites still to be decided read them); it is noted in
-// the warp's flip list, and when the chunk is done every other chunk's fields
-// take the list in site order.  The next read of a field comes after that, and
-// each field takes the same FMAs in the same order as with the whole row
-// applied at every flip, so the state is that of the plain sequential sweep,
-// bit for bit; the field traffic in shared memory is one pass per chunk
-// instead of one per flip.  The uniform of site i, sweep k, replica r of
-// instance m is Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3], r the
-// replica's global index (rep0 + index within the instance).
+// of one per site; a flip applies its whole coupling row to the warp's fields
+// at once.  The uniform of site i, sweep k, replica r of instance m is
+// Philox((i >> 2, k, r, m << 8 | TAG_BATCH))[i & 3], r the replica's global
+// index (rep0 + index within the instance).
 //
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
 // read through L1 one float4 per lane on every accepted flip, or from an FP16
@@ -56,6 +50,7 @@ namespace {
 
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
+constexpr int kMaxChunks = kBatchMaxN / 128;
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -119,56 +114,16 @@ __device__ __forceinline__ float4 row4h(const __half* p) {
   }
 }
 
-// Four couplings of a row segment as loaded (raw FP16 pairs or FP32 values),
-// widened only where they are used: a whole row's loads in flight take half
-// the registers with FP16 rows.
-template <bool H>
-struct Raw4;
-template <>
-struct Raw4<true> {
-  uint2 v;
-};
-template <>
-struct Raw4<false> {
-  float4 v;
-};
-template <bool H, bool SJ>
-__device__ __forceinline__ Raw4<H> raw4(const float* p32, const __half* p16) {
-  Raw4<H> r;
-  if constexpr (H) r.v = SJ ? *reinterpret_cast<const uint2*>(p16) : __ldg(reinterpret_cast<const uint2*>(p16));
-  else r.v = SJ ? *reinterpret_cast<const float4*>(p32) : ldg4(p32);
-  return r;
-}
-template <bool H>
-__device__ __forceinline__ float4 widen4(const Raw4<H>& r) {
-  if constexpr (H) {
-    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&r.v.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&r.v.y));
-    return make_float4(a.x, a.y, b.x, b.y);
-  } else {
-    return r.v;
-  }
-}
-
 // The couplings of an instance are staged in shared memory (SJ) when the
 // batch's largest block of n rows x npad columns takes at most this many bytes.
 constexpr size_t kBatchSmemJBytes = 96 * 1024;
-// Bytes of each warp's flip list (one entry per site of a chunk).
-constexpr int kFlipList = 128;
-constexpr int kDelayAt = 3;
 
-// GROUP: chunks whose fields take a chunk's delayed flips together (their row
-// loads are in flight at once); more costs registers.  A chunk is decided in
-// one of two modes with the same FMAs in the same order per field: direct (a
-// flip applies its whole row at once, the row's loads in flight together;
-// few flips per chunk) or delayed (a flip updates its own chunk at once and
-// the others at the end of the chunk; many flips).  The warp takes the delayed
-// mode for a chunk when the chunk it decided last had at least kDelayAt flips.
-// H: the flip rows come from the FP16 copy of J (half the L2 bytes per flip).
-// SJ: every work item first copies its instance's couplings (FP32 or FP16
-// rows, as H says) into shared memory after the warps' fields and spin words,
-// and the flips read their rows there (small instances: no L2 round trip per
-// flip).
+// GROUP: chunks of a flip row whose loads are in flight together (more costs
+// registers).  H: the flip rows come from the FP16 copy of J (half the L2
+// bytes per flip).  SJ: every work item first copies its instance's couplings
+// (FP32 or FP16 rows, as H says) into shared memory after the warps' fields and
+// spin words, and the flips read their rows there (small instances: no L2
+// round trip per flip).
 template <int W, int MINB, int GROUP, bool H, bool SJ>
 __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];
@@ -177,12 +132,8 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
                  (size_t)warp * a.swstride;  // spin words [chunk / 8][lane]
-  // the warp's flips in the current chunk: chunk-local site | 0x80 when the
-  // spin was -1 before the flip
-  uint8_t* fl = reinterpret_cast<uint8_t*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride) +
-                (size_t)warp * kFlipList;
-  // the staged couplings (SJ): after every warp's fields, spin words and flip list
-  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride) + (size_t)W * kFlipList;
+  // the staged couplings (SJ): after every warp's fields and spin words
+  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride);
   unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   for (;;) {
     __syncthreads();
@@ -236,21 +187,18 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     // this lane's sites of the last chunk that exist (site index below n), as
     // a 4-bit mask; every site of the other chunks exists
     const uint32_t inside_last = 0xFu >> (4 - min(max(n - 128 * (nch - 1) - 4 * lane, 0), 4));
-    bool delayed = true;  // the mode of the next chunk (the first sweeps flip many spins)
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
       for (int c = 0; c < nch; ++c) {
         const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
-        // the chunk's fields and this lane's spin bits stay in registers while
-        // the chunk is decided
-        float4 fc = reinterpret_cast<const float4*>(f)[32 * c + lane];
-        uint32_t myw = (sw[sw_word(c, lane)] >> sw_shift(c)) & 0xFu;
         {
           // a chunk none of whose sites has beta*dE below the largest -ln u
           // keeps its state: its uniforms are not drawn (the stream is
           // counter-based, so nothing after it moves)
-          const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
+          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
+          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
+          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
           uint32_t can = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -268,9 +216,10 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
         // this lane's sites that exist and are not yet decided in this chunk
         // (chunk-local index at or past the last flip's + 1)
         uint32_t open = inside;
-        int nfl = 0;  // flips in this chunk (the same in every lane)
         for (;;) {
-          const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
+          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
+          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
+          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
           uint32_t mask = 0u;
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -286,98 +235,40 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
           if (!lanes) break;
           const int ls = __ffs(lanes) - 1;
-          // the first accepting lane's mask and spin bits
-          const uint32_t pk = __shfl_sync(0xffffffffu, mask | (myw << 4), ls);
-          const int es = __ffs(pk & 0xFu) - 1;
-          const uint32_t neg = (pk >> (4 + es)) & 1u;
+          const uint32_t ms = __shfl_sync(0xffffffffu, mask, ls);
+          const int es = __ffs(ms) - 1;
+          const uint32_t ws = sw[sw_word(c, ls)];
+          const bool neg = (ws >> (sw_shift(c) + es)) & 1u;
           const float coef = neg ? 2.0f : -2.0f;
-          const int il = 4 * ls + es;  // chunk-local site
-          const size_t rrow = (size_t)(128 * c + il) * npad + 4 * lane;
-          if (delayed) {
-            // the flip reaches this chunk's fields now (the sites still to be
-            // decided read them); the other chunks get it at the end of the chunk
-            const float4 v = widen4<H>(raw4<H, SJ>(Jr + rrow + 128 * c, Jr16 + rrow + 128 * c));
-            fc.x = __fmaf_rn(coef, v.x, fc.x);
-            fc.y = __fmaf_rn(coef, v.y, fc.y);
-            fc.z = __fmaf_rn(coef, v.z, fc.z);
-            fc.w = __fmaf_rn(coef, v.w, fc.w);
-            if (lane == 0) fl[nfl] = (uint8_t)(il | (neg << 7));
-          } else {
-            // the whole row now: this chunk's fields in registers, the others in
-            // shared memory, DG chunks' loads in flight together (the same
-            // registers as GROUP chunks of FP32 values)
-            constexpr int DG = H ? 2 * GROUP : GROUP;
-#pragma unroll 1
-            for (int c0 = 0; c0 < nch; c0 += DG) {
-              Raw4<H> v[DG];
+          const int i = 128 * c + 4 * ls + es;
+          const float* Ji = Jr + (size_t)i * npad + 4 * lane;
+          const __half* Ji16 = Jr16 + (size_t)i * npad + 4 * lane;
+          // the row in groups of GROUP chunks whose loads are in flight together
 #pragma unroll
-              for (int q = 0; q < DG; ++q)
-                if (c0 + q < nch) v[q] = raw4<H, SJ>(Jr + rrow + 128 * (c0 + q), Jr16 + rrow + 128 * (c0 + q));
-#pragma unroll
-              for (int q = 0; q < DG; ++q) {
-                if (c0 + q >= nch) break;
-                const float4 w4 = widen4<H>(v[q]);
-                if (c0 + q == c) {
-                  fc.x = __fmaf_rn(coef, w4.x, fc.x);
-                  fc.y = __fmaf_rn(coef, w4.y, fc.y);
-                  fc.z = __fmaf_rn(coef, w4.z, fc.z);
-                  fc.w = __fmaf_rn(coef, w4.w, fc.w);
-                } else {
-                  float4 g = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
-                  g.x = __fmaf_rn(coef, w4.x, g.x);
-                  g.y = __fmaf_rn(coef, w4.y, g.y);
-                  g.z = __fmaf_rn(coef, w4.z, g.z);
-                  g.w = __fmaf_rn(coef, w4.w, g.w);
-                  reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g;
-                }
-              }
-            }
-          }
-          if (lane == ls) myw ^= 1u << es;
-          if (lane == 0) ++nflip;
-          ++nfl;
-          open = inside & (0xFu << min(max(il + 1 - 4 * lane, 0), 4));
-        }
-        const bool was_delayed = delayed;
-        delayed = nfl >= kDelayAt;  // the mode of the next chunk
-        if (nfl == 0) continue;
-        reinterpret_cast<float4*>(f)[32 * c + lane] = fc;
-        {
-          uint32_t& wd = sw[sw_word(c, lane)];
-          wd = (wd & ~(0xFu << sw_shift(c))) | (myw << sw_shift(c));
-        }
-        if (!was_delayed) continue;
-        __syncwarp();  // the flip list is complete
-        // Delayed update: every other chunk's fields take the chunk's flips in
-        // site order, one FMA each (c * J_ij exact), GROUP chunks at a time so
-        // their row loads are in flight together.  Each field sees the same
-        // sequence of roundings as with the whole row applied at every flip.
-#pragma unroll 1
-        for (int c0 = 0; c0 < nch; c0 += GROUP) {
-          float4 g[GROUP];
-#pragma unroll
-          for (int q = 0; q < GROUP; ++q)
-            if (c0 + q < nch && c0 + q != c) g[q] = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
-#pragma unroll 2
-          for (int t = 0; t < nfl; ++t) {
-            const uint32_t e = fl[t];
-            const float cf = (e & 0x80u) ? 2.0f : -2.0f;
-            const size_t ro = (size_t)(128 * c + (int)(e & 0x7Fu)) * npad + 4 * lane;
+          for (int c0 = 0; c0 < kMaxChunks; c0 += GROUP) {
+            if (c0 >= nch) break;
+            float4 v[GROUP];
 #pragma unroll
             for (int q = 0; q < GROUP; ++q)
-              if (c0 + q < nch && c0 + q != c) {
-                const float4 v = widen4<H>(raw4<H, SJ>(Jr + ro + 128 * (c0 + q), Jr16 + ro + 128 * (c0 + q)));
-                g[q].x = __fmaf_rn(cf, v.x, g[q].x);
-                g[q].y = __fmaf_rn(cf, v.y, g[q].y);
-                g[q].z = __fmaf_rn(cf, v.z, g[q].z);
-                g[q].w = __fmaf_rn(cf, v.w, g[q].w);
+              if (c0 + q < nch) v[q] = H ? row4h<SJ>(Ji16 + 128 * (c0 + q)) : row4<SJ>(Ji + 128 * (c0 + q));
+#pragma unroll
+            for (int q = 0; q < GROUP; ++q)
+              if (c0 + q < nch) {
+                float4 g = reinterpret_cast<const float4*>(f)[32 * (c0 + q) + lane];
+                g.x = __fmaf_rn(coef, v[q].x, g.x);
+                g.y = __fmaf_rn(coef, v[q].y, g.y);
+                g.z = __fmaf_rn(coef, v[q].z, g.z);
+                g.w = __fmaf_rn(coef, v[q].w, g.w);
+                reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g;
               }
           }
-#pragma unroll
-          for (int q = 0; q < GROUP; ++q)
-            if (c0 + q < nch && c0 + q != c) reinterpret_cast<float4*>(f)[32 * (c0 + q) + lane] = g[q];
+          __syncwarp();
+          if (lane == ls) sw[sw_word(c, ls)] = ws ^ (1u << (sw_shift(c) + es));
+          if (lane == 0) ++nflip;
+          const int pos = 4 * ls + es + 1;  // chunk-local index of the first site not yet decided
+          open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
+          __syncwarp();
         }
-        __syncwarp();  // the list is read before the next chunk rewrites it
       }
     }
     if (a.Fw) {
@@ -618,11 +509,10 @@ __global__ void batch_energy_sum_kernel(const double* __restrict__ parts, int ns
 int batch_max_sites() { return kBatchMaxN; }
 int batch_warps() { return kBatchWarps; }
 
-// Launch variants: warps per CTA x minimum CTAs per SM (register budget), and
-// the chunks that take a chunk's delayed flips together.
+// Launch variants: warps per CTA x minimum CTAs per SM (register budget).
 // 45 = 4 warps, 102 registers, 8 chunks at a time (more CTAs per SM when the
 //      fields' shared memory limits residency);
-// 82 = 8 warps, 128 registers, 8 chunks at a time;
+// 82 = 8 warps, 128 registers, a flip row's loads 16 chunks at a time;
 // 83 = 8 warps, 80 registers; 84 = 8 warps, 64; 162 = 16 warps, 64; 321 = 32 warps, 64
 // (4 chunks at a time).
 int batch_min_warps() { return 4; }
@@ -641,11 +531,11 @@ bool batch_variant_valid(int variant) {
 }
 
 // largest n whose fields fit the variant: W warps x (FP32 fields + spin
-// words + flip list) within the 227 KB of shared memory per CTA
+// words) within the 227 KB of shared memory per CTA
 int batch_variant_max_n(int variant) {
   switch (variant) {
-    case 321: return 1536;
-    case 162: return 3328;
+    case 321: return 1664;
+    case 162: return 3456;
     default: return kBatchMaxN;
   }
 }
@@ -663,8 +553,8 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
   const bool sj = jbytes > 0;
   auto kern = h ? (sj ? sa_batch_kernel<W, MINB, GROUP, true, true> : sa_batch_kernel<W, MINB, GROUP, true, false>)
                 : (sj ? sa_batch_kernel<W, MINB, GROUP, false, true> : sa_batch_kernel<W, MINB, GROUP, false, false>);
-  // FP32 fields + spin words + flip list per warp, then the staged couplings
-  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4 + kFlipList) + jbytes;
+  // FP32 fields + spin words per warp, then the staged couplings
+  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4) + jbytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -748,7 +638,7 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
   if (jbytes > kBatchSmemJBytes) jbytes = 0;
   switch (variant) {
     case 45: e = launch_variant<4, 5, 8>(a, nitems, sm_count, st, b->j16, jbytes); break;
-    case 82: e = launch_variant<8, 2, 8>(a, nitems, sm_count, st, b->j16, jbytes); break;
+    case 82: e = launch_variant<8, 2, 16>(a, nitems, sm_count, st, b->j16, jbytes); break;
     case 83: e = launch_variant<8, 3, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
     case 84: e = launch_variant<8, 4, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;
     case 162: e = launch_variant<16, 2, 4>(a, nitems, sm_count, st, b->j16, jbytes); break;

@@ -22,9 +22,9 @@
 // digit).  The digits are stored tiled in global memory in the canonical
 // K-major layout of the MMA operand (8 x 16-byte core matrices, no swizzle), so
 // one 16 KB tile (128 sites x 128 sites) is one bulk copy; the spins of the
-// NT replicas are written into shared memory by the threads in the same
-// layout.  Two stages: the copies of a K chunk overlap the MMAs of the
-// previous one.  Epilogue: tcgen05.ld of the accumulators, the exact
+// NT replicas are copied into shared memory by the threads in the same layout
+// (16-byte cp.async pieces).  A ring of stages: the copies of the next K
+// chunks overlap the MMAs of the current one.  Epilogue: tcgen05.ld of the accumulators, the exact
 // combination above, coalesced FP32 stores of F (replica-major, sites
 // contiguous), and in compare mode max |F_new - F_old| before the store (the
 // drift of the sweep kernel's incremental fields).  Every wait is bounded:
@@ -130,6 +130,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
   for (int j = 0; j < 16; ++j) v[j] = (int32_t)r[j];
 }
 
+// Ampere-style asynchronous copies into shared memory (the source aligned to
+// the copy size); each thread waits for its own groups.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -205,8 +219,48 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
       bulk_copy(As + t * kTileBytes, dig + ((size_t)(t * nch + mt) * nch + kc) * kTileBytes, kTileBytes, bar + s);
     pend_full |= 1u << s;
   };
+  // spins of replicas r0..r0+NT-1 at sites 128 kc .. +127 into stage kc % ST
+  // (every thread; the stage is free), 16 bytes a piece: asynchronous copies
+  // where the piece is 16- or 4-byte aligned, else byte loads; zero past the
+  // instance's reads and sites.  One commit group per call.
+  auto issue_b = [&](int kc) {
+    unsigned char* Bs = sm + (kc % ST) * S::kStage + S::kA;
+    for (int idx = tid; idx < NT * 8; idx += kFieldThreads) {
+      const int rr = idx >> 3, pc = idx & 7;
+      const int r = r0 + rr, k = kc * kChunk + 16 * pc;
+      unsigned char* dst = Bs + canon(rr, 16 * pc);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (r < R && k < n) {
+        const int8_t* p = sp + (size_t)r * n + k;
+        const int valid = min(16, n - k);
+        const uintptr_t al = reinterpret_cast<uintptr_t>(p);
+        if (valid == 16 && (al & 15u) == 0u) {
+          cp_async16(dst, p);
+          continue;
+        }
+        if (valid == 16 && (al & 3u) == 0u) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) cp_async4(dst + 4 * q, p + 4 * q);
+          continue;
+        }
+        unsigned long long lo = 0ull, hi = 0ull;
+        for (int e = 0; e < valid; ++e) {
+          const unsigned long long bv = (unsigned long long)(uint8_t)p[e];
+          if (e < 8) lo |= bv << (8 * e);
+          else hi |= bv << (8 * (e - 8));
+        }
+        v = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+      }
+      *reinterpret_cast<uint4*>(dst) = v;
+    }
+    cp_async_commit();
+  };
   if (tid == 0)
     for (int kc = 0; kc < ST - 1 && kc < nch; ++kc) issue_a(kc);
+  for (int kc = 0; kc < ST - 1; ++kc) {
+    if (kc < nch) issue_b(kc);
+    else cp_async_commit();  // an empty group keeps the count per chunk
+  }
   for (int kc = 0; kc < nch; ++kc) {
     const int s = kc % ST;
     unsigned char* As = sm + s * S::kStage;
@@ -224,34 +278,11 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
       }
       if (!*abort_flag) issue_a(kc + ST - 1);
     }
-    __syncthreads();  // stage s's spin tile is free (chunk kc - ST's MMAs were seen complete)
+    __syncthreads();  // the stage of chunk kc + ST - 1 is free (chunk kc - 1's MMAs were seen complete)
     if (*abort_flag) break;
-    // spins of replicas r0..r0+NT-1 at sites 128 kc .. +127, 16 bytes a piece;
-    // zero past the instance's reads and sites
-    for (int idx = tid; idx < NT * 8; idx += kFieldThreads) {
-      const int rr = idx >> 3, pc = idx & 7;
-      const int r = r0 + rr, k = kc * kChunk + 16 * pc;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (r < R && k < n) {
-        const int8_t* p = sp + (size_t)r * n + k;
-        const int valid = min(16, n - k);
-        if (valid == 16 && (reinterpret_cast<uintptr_t>(p) & 15u) == 0u) {
-          v = __ldg(reinterpret_cast<const uint4*>(p));
-        } else if (valid == 16 && (reinterpret_cast<uintptr_t>(p) & 3u) == 0u) {
-          const uint32_t* p4 = reinterpret_cast<const uint32_t*>(p);
-          v = make_uint4(__ldg(p4), __ldg(p4 + 1), __ldg(p4 + 2), __ldg(p4 + 3));
-        } else {
-          unsigned long long lo = 0ull, hi = 0ull;
-          for (int e = 0; e < valid; ++e) {
-            const unsigned long long bv = (unsigned long long)(uint8_t)p[e];
-            if (e < 8) lo |= bv << (8 * e);
-            else hi |= bv << (8 * (e - 8));
-          }
-          v = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
-        }
-      }
-      *reinterpret_cast<uint4*>(Bs + canon(rr, 16 * pc)) = v;
-    }
+    if (kc + ST - 1 < nch) issue_b(kc + ST - 1);
+    else cp_async_commit();
+    cp_async_wait<ST - 1>();  // this thread's copies of chunk kc's spins have landed
     proxy_fence();
     tc_fence_before();
     __syncthreads();
@@ -275,6 +306,7 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
     }
   }
   // drain: every copy and MMA this CTA issued has completed before it goes on
+  asm volatile("cp.async.wait_all;" ::: "memory");
   bool ok = true;
   if (tid == 0) {
     for (int q = 0; q < ST; ++q) {

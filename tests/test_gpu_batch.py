@@ -150,7 +150,7 @@ def test_dense_jump_replica_shards(ctx):
     np.testing.assert_array_equal(part, whole[32:])
 
 
-_VARIANT_MAX_N = {45: 4096, 82: 4096, 83: 4096, 84: 4096, 162: 3328, 321: 1536}
+_VARIANT_MAX_N = {45: 4096, 82: 4096, 83: 4096, 84: 4096, 162: 3456, 321: 1664}
 
 
 @pytest.mark.parametrize("variant", sorted(_VARIANT_MAX_N))
