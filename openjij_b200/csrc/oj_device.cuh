@@ -144,4 +144,51 @@ __device__ __forceinline__ float neglog(uint32_t x) {
   return -lnu;
 }
 
+// Deferred tails of the bit-serial acceptance compare (bit-packed kernels).
+// A word's 32 bits are decided one level of U at a time; a bit stays pending
+// with probability 1/2 per level, so one word needs about 6 levels but the
+// slowest of a warp's 32 words about 11, and the warp runs that long.  So a
+// site takes at most kHeadDraws Philox draws (4 levels each) when it is first
+// visited; a word still pending after them (about one in eight) goes to its
+// warp's queue, and the queue is finished 32 sites at a time, one per lane.
+// The draws and comparisons are the same, in another order: the same words.
+constexpr int kHeadDraws = 2;
+constexpr int kTailQueue = 64;  // fewer than 32 left over + one site per lane
+struct TailQueue {
+  uint32_t slot[kTailQueue];
+  uint32_t pending[kTailQueue];  // bits not yet decided
+  uint32_t acc[kTailQueue];      // bits decided to flip so far
+};
+
+// Appends the lanes whose word is still pending (warp-wide call; cnt is the
+// same in every lane).
+__device__ __forceinline__ void tail_push(TailQueue& Q, int& cnt, uint32_t slot, uint32_t pending, uint32_t acc) {
+  const uint32_t b = __ballot_sync(0xffffffffu, pending != 0u);
+  if (pending) {
+    const int i = cnt + __popc(b & ((1u << (threadIdx.x & 31)) - 1u));
+    Q.slot[i] = slot;
+    Q.pending[i] = pending;
+    Q.acc[i] = acc;
+  }
+  cnt += __popc(b);
+  __syncwarp();
+}
+
+// Takes the last c (<= 32) entries, one per lane (lanes >= c get none).
+__device__ __forceinline__ bool tail_pop(TailQueue& Q, int& cnt, int c, uint32_t& slot, uint32_t& pending,
+                                         uint32_t& acc) {
+  const int lane = threadIdx.x & 31;
+  const int base = cnt - c;
+  const bool has = lane < c;
+  slot = pending = acc = 0u;
+  if (has) {
+    slot = Q.slot[base + lane];
+    pending = Q.pending[base + lane];
+    acc = Q.acc[base + lane];
+  }
+  __syncwarp();  // read before later pushes reuse the entries
+  cnt = base;
+  return has;
+}
+
 }  // namespace ojd

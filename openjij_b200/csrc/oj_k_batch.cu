@@ -51,6 +51,7 @@ namespace {
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
 constexpr int kMaxChunks = kBatchMaxN / 128;
+constexpr int kHaveWords = kMaxChunks;  // per warp: lanes with uniforms drawn ahead, per chunk
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -132,8 +133,12 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
                  (size_t)warp * a.swstride;  // spin words [chunk / 8][lane]
-  // the staged couplings (SJ): after every warp's fields and spin words
-  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride);
+  // per chunk of the current sweep, the lanes whose uniforms were drawn ahead
+  uint32_t* have = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride) +
+                   (size_t)warp * kHaveWords;
+  // the staged couplings (SJ): after every warp's fields, spin words and draw masks
+  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride + (size_t)W * kHaveWords);
+  const uint32_t below = (1u << lane) - 1u;
   unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   for (;;) {
     __syncthreads();
@@ -190,12 +195,20 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
-      for (int c = 0; c < nch; ++c) {
-        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
-        {
-          // a chunk none of whose sites has beta*dE below the largest -ln u
-          // keeps its state: its uniforms are not drawn (the stream is
-          // counter-based, so nothing after it moves)
+      // Uniforms drawn ahead.  A chunk is decided only when one of its sites
+      // has beta*dE below the largest -ln u, and late in a schedule that is
+      // often one or two lanes of the 32: drawing per chunk would run a whole
+      // warp's Philox and logarithms for them.  So the (chunk, lane) pairs
+      // that can flip at the start of the sweep are listed in chunk order and
+      // the first 32 take their draws together, pair j in lane j (P0..P3: -ln u
+      // of the lane's four sites); a chunk takes them by shuffle.  Lanes that
+      // become able to flip later in the sweep draw when their chunk comes
+      // (the stream is counter-based: the same numbers either way).
+      float P0 = 0.0f, P1 = 0.0f, P2 = 0.0f, P3 = 0.0f;
+      {
+        int total = 0, myc = -1, myl = 0;
+        for (int c = 0; c < nch; ++c) {
+          const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
           const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
           const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
           const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
@@ -205,14 +218,66 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             const float bf = __fmul_rn(beta2, fv[e]);
             if ((((myw >> e) & 1u) ? bf : -bf) < ojd::kNegLogMax) can |= 1u << e;
           }
-          if (!__any_sync(0xffffffffu, (can & inside) != 0u)) continue;
+          const uint32_t hv = __ballot_sync(0xffffffffu, (can & inside) != 0u);
+          if (lane == 0) have[c] = hv;
+          const int cntc = __popc(hv), j = lane - total;
+          if (j >= 0 && j < cntc) {
+            myc = c;
+            myl = (int)__fns(hv, 0u, j + 1);
+          }
+          total += cntc;
         }
-        const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
+        if (myc >= 0) {
+          const ojd::u4 x = ojd::philox((uint32_t)(32 * myc + myl), kk, rg, tag, a.keys);
+          P0 = ojd::neglog(x.x);
+          P1 = ojd::neglog(x.y);
+          P2 = ojd::neglog(x.z);
+          P3 = ojd::neglog(x.w);
+        }
+        __syncwarp();  // the draw masks are visible to the warp
+      }
+      int uoff = 0;  // list index of the current chunk's first pair
+      for (int c = 0; c < nch; ++c) {
+        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
+        const uint32_t hv = have[c];
+        uint32_t can = 0u;
+        {
+          // a chunk none of whose sites has beta*dE below the largest -ln u
+          // keeps its state: its uniforms are not needed
+          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
+          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
+          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float bf = __fmul_rn(beta2, fv[e]);
+            if ((((myw >> e) & 1u) ? bf : -bf) < ojd::kNegLogMax) can |= 1u << e;
+          }
+          can &= inside;
+        }
+        const int idx = uoff + __popc(hv & below);
+        uoff += __popc(hv);
+        if (!__any_sync(0xffffffffu, can != 0u)) continue;
+        // this lane's uniforms: drawn ahead (mine), drawn now, or not needed yet
+        const bool mine = ((hv >> lane) & 1u) && idx < 32;
+        const int src = idx & 31;
         float L[4];
-        L[0] = ojd::neglog(x.x);
-        L[1] = ojd::neglog(x.y);
-        L[2] = ojd::neglog(x.z);
-        L[3] = ojd::neglog(x.w);
+        L[0] = __shfl_sync(0xffffffffu, P0, src);
+        L[1] = __shfl_sync(0xffffffffu, P1, src);
+        L[2] = __shfl_sync(0xffffffffu, P2, src);
+        L[3] = __shfl_sync(0xffffffffu, P3, src);
+        // every lane has its uniforms once allL is set; before that a lane
+        // without them has no site with beta*dE below the largest -ln u
+        bool allL = false;
+        if (__any_sync(0xffffffffu, can != 0u && !mine)) {
+          const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
+          if (!mine) {
+            L[0] = ojd::neglog(x.x);
+            L[1] = ojd::neglog(x.y);
+            L[2] = ojd::neglog(x.z);
+            L[3] = ojd::neglog(x.w);
+          }
+          allL = true;
+        }
         // this lane's sites that exist and are not yet decided in this chunk
         // (chunk-local index at or past the last flip's + 1)
         uint32_t open = inside;
@@ -232,6 +297,7 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             if ((neg ? bf : -bf) < L[e]) mask |= 1u << e;
           }
           mask &= open;
+          if (!allL && !mine) mask = 0u;
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
           if (!lanes) break;
           const int ls = __ffs(lanes) - 1;
@@ -267,6 +333,17 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           if (lane == 0) ++nflip;
           const int pos = 4 * ls + es + 1;  // chunk-local index of the first site not yet decided
           open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
+          if (!allL) {
+            // the flip moved this chunk's fields: every lane takes its uniforms
+            const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
+            if (!mine) {
+              L[0] = ojd::neglog(x.x);
+              L[1] = ojd::neglog(x.y);
+              L[2] = ojd::neglog(x.z);
+              L[3] = ojd::neglog(x.w);
+            }
+            allL = true;
+          }
           __syncwarp();
         }
       }
@@ -531,7 +608,7 @@ bool batch_variant_valid(int variant) {
 }
 
 // largest n whose fields fit the variant: W warps x (FP32 fields + spin
-// words) within the 227 KB of shared memory per CTA
+// words + draw masks) within the 227 KB of shared memory per CTA
 int batch_variant_max_n(int variant) {
   switch (variant) {
     case 321: return 1664;
@@ -553,8 +630,8 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
   const bool sj = jbytes > 0;
   auto kern = h ? (sj ? sa_batch_kernel<W, MINB, GROUP, true, true> : sa_batch_kernel<W, MINB, GROUP, true, false>)
                 : (sj ? sa_batch_kernel<W, MINB, GROUP, false, true> : sa_batch_kernel<W, MINB, GROUP, false, false>);
-  // FP32 fields + spin words per warp, then the staged couplings
-  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4) + jbytes;
+  // FP32 fields + spin words + draw masks per warp, then the staged couplings
+  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4 + kHaveWords * 4) + jbytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
