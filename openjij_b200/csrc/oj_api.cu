@@ -298,7 +298,7 @@ cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, co
     rs.sweep0 = (uint32_t)g;
     e = launch_batch_sweeps(p.b, p.d_reads, p.d_soff, p.d_items, p.nitems, p.d_counter, p.spins, p.d_betas + k, len,
                             rs, p.inst0, ctx->sm_count, st, launches, p.variant, p.d_fields, p.d_foff, p.d_energies,
-                            p.d_eoff, wf);
+                            p.d_eoff, wf, fc.status, fc.wait_limit);
     if (e != cudaSuccess) return e;
     k += len;
     if (k < S || wf) {

@@ -144,51 +144,37 @@ __device__ __forceinline__ float neglog(uint32_t x) {
   return -lnu;
 }
 
-// Deferred tails of the bit-serial acceptance compare (bit-packed kernels).
-// A word's 32 bits are decided one level of U at a time; a bit stays pending
-// with probability 1/2 per level, so one word needs about 6 levels but the
-// slowest of a warp's 32 words about 11, and the warp runs that long.  So a
-// site takes at most kHeadDraws Philox draws (4 levels each) when it is first
-// visited; a word still pending after them (about one in eight) goes to its
-// warp's queue, and the queue is finished 32 sites at a time, one per lane.
-// The draws and comparisons are the same, in another order: the same words.
-constexpr int kHeadDraws = 2;
-constexpr int kTailQueue = 64;  // fewer than 32 left over + one site per lane
-struct TailQueue {
-  uint32_t slot[kTailQueue];
-  uint32_t pending[kTailQueue];  // bits not yet decided
-  uint32_t acc[kTailQueue];      // bits decided to flip so far
-};
+// Shared-memory mbarriers and 1-D bulk copies (global -> this CTA's shared
+// memory, no multicast).  Every wait is bounded by an iteration count.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Appends the lanes whose word is still pending (warp-wide call; cnt is the
-// same in every lane).
-__device__ __forceinline__ void tail_push(TailQueue& Q, int& cnt, uint32_t slot, uint32_t pending, uint32_t acc) {
-  const uint32_t b = __ballot_sync(0xffffffffu, pending != 0u);
-  if (pending) {
-    const int i = cnt + __popc(b & ((1u << (threadIdx.x & 31)) - 1u));
-    Q.slot[i] = slot;
-    Q.pending[i] = pending;
-    Q.acc[i] = acc;
-  }
-  cnt += __popc(b);
-  __syncwarp();
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
 }
 
-// Takes the last c (<= 32) entries, one per lane (lanes >= c get none).
-__device__ __forceinline__ bool tail_pop(TailQueue& Q, int& cnt, int c, uint32_t& slot, uint32_t& pending,
-                                         uint32_t& acc) {
-  const int lane = threadIdx.x & 31;
-  const int base = cnt - c;
-  const bool has = lane < c;
-  slot = pending = acc = 0u;
-  if (has) {
-    slot = Q.slot[base + lane];
-    pending = Q.pending[base + lane];
-    acc = Q.acc[base + lane];
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t ph, long long limit) {
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(b)), "r"(ph)
+        : "memory");
+    if (done) return true;
   }
-  __syncwarp();  // read before later pushes reuse the entries
-  cnt = base;
-  return has;
+  return false;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+
+// bytes a multiple of 16, both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 
 }  // namespace ojd

@@ -246,7 +246,7 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
                                 const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count,
                                 cudaStream_t st, int* launches, int variant, float* d_fields,
                                 const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
-                                bool write_fields);
+                                bool write_fields, int* d_status, long long wait_limit);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep);

@@ -28,7 +28,8 @@
 // J is FP32, row-major with rows padded to a multiple of 128 columns (zeros),
 // read through L1 one float4 per lane on every accepted flip, or from an FP16
 // copy (8 bytes per lane) when FP16 holds every coupling exactly; small
-// instances' rows are staged in shared memory, and batches of instances of at
+// instances' rows are staged in shared memory (one bulk copy per work item),
+// and batches of instances of at
 // most 128 sites run sa_batch1_kernel (fields and spin bits in registers).
 // The fields come from the tensor-core field kernel (oj_k_field_tc.cu),
 // launched just before, through a global buffer of reads x padded n floats per
@@ -51,7 +52,6 @@ namespace {
 constexpr int kBatchWarps = 8;
 constexpr int kBatchMaxN = 4096;
 constexpr int kMaxChunks = kBatchMaxN / 128;
-constexpr int kHaveWords = kMaxChunks;  // per warp: lanes with uniforms drawn ahead, per chunk
 
 struct BatchArgs {
   const float* J;          // concatenated padded rows
@@ -81,7 +81,40 @@ struct BatchArgs {
   double* E;               // FP64 energies from the final fields, or null (exact-field batches)
   const int64_t* eoff;     // [count] offset of instance m's energies
   unsigned long long* flips;  // accepted-flip counter, or null
+  int* status;             // set when a bounded wait runs out
+  long long wait_limit;    // iterations of the staging wait
 };
+
+constexpr long long kStageDrainLimit = 1ll << 26;
+
+// Copies an instance's coupling rows (bytes, a multiple of 16, both addresses
+// 16-byte aligned) into shared memory with one bulk copy that thread 0 issues
+// and every thread of the CTA waits for.  Returns false in every thread when
+// a thread's wait ran out (the copy is then waited for with the drain limit
+// and *status is set): the CTA leaves the item.
+__device__ __forceinline__ bool stage_rows(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                           uint32_t& phase, const BatchArgs& a) {
+  if (threadIdx.x == 0) {
+    ojd::mbar_expect_tx(bar, bytes);
+    ojd::bulk_copy(dst, src, bytes, bar);
+  }
+  bool ok = ojd::mbar_wait(bar, phase, a.wait_limit);
+  if (!ok) {
+    ojd::mbar_wait(bar, phase, kStageDrainLimit);
+    if (a.status) atomicExch(a.status, 1);
+  }
+  phase ^= 1u;
+  return !__syncthreads_or(!ok);
+}
+
+// The CTA's staging barrier, once per launch.
+__device__ __forceinline__ void stage_init(uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    ojd::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
 
 // Spin bits of chunk c of lane l: four bits of word 32*(c/8) + l.
 __device__ __forceinline__ int sw_word(int c, int l) { return 32 * (c >> 3) + l; }
@@ -133,12 +166,11 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
   float* f = shb + (size_t)warp * a.fstride;  // this warp's fields, float4 per lane per chunk
   uint32_t* sw = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride) +
                  (size_t)warp * a.swstride;  // spin words [chunk / 8][lane]
-  // per chunk of the current sweep, the lanes whose uniforms were drawn ahead
-  uint32_t* have = reinterpret_cast<uint32_t*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride) +
-                   (size_t)warp * kHaveWords;
-  // the staged couplings (SJ): after every warp's fields, spin words and draw masks
-  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride + (size_t)W * kHaveWords);
-  const uint32_t below = (1u << lane) - 1u;
+  // the staged couplings (SJ): after every warp's fields and spin words
+  char* jsh = reinterpret_cast<char*>(shb + (size_t)W * a.fstride + (size_t)W * a.swstride);
+  __shared__ __align__(8) uint64_t stage_bar;
+  uint32_t stage_phase = 0u;
+  if (SJ) stage_init(&stage_bar);
   unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   for (;;) {
     __syncthreads();
@@ -156,14 +188,10 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     const float* J = a.J + a.joff[m];
     int8_t* gs = a.spins + a.soff[m] + (size_t)(active ? r : 0) * n;
     if (SJ) {
-      // n rows of npad couplings, 16 bytes per thread and step; every warp of
-      // the CTA takes part before any leaves for an inactive replica
-      const int4* src = reinterpret_cast<const int4*>(H ? static_cast<const void*>(a.J16 + a.joff[m])
-                                                          : static_cast<const void*>(J));
-      int4* dst = reinterpret_cast<int4*>(jsh);
-      const int total = n * npad * (H ? 2 : 4) / 16;
-      for (int q = threadIdx.x; q < total; q += blockDim.x) dst[q] = __ldg(src + q);
-      __syncthreads();
+      // n rows of npad couplings by one bulk copy; every warp of the CTA waits
+      // for it before any leaves for an inactive replica
+      const void* src = H ? static_cast<const void*>(a.J16 + a.joff[m]) : static_cast<const void*>(J);
+      if (!stage_rows(jsh, src, (uint32_t)(n * npad * (H ? 2 : 4)), &stage_bar, stage_phase, a)) continue;
     }
     const float* Jr = SJ ? reinterpret_cast<const float*>(jsh) : J;
     const __half* Jr16 = SJ ? reinterpret_cast<const __half*>(jsh) : (H ? a.J16 + a.joff[m] : nullptr);
@@ -195,20 +223,12 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
-      // Uniforms drawn ahead.  A chunk is decided only when one of its sites
-      // has beta*dE below the largest -ln u, and late in a schedule that is
-      // often one or two lanes of the 32: drawing per chunk would run a whole
-      // warp's Philox and logarithms for them.  So the (chunk, lane) pairs
-      // that can flip at the start of the sweep are listed in chunk order and
-      // the first 32 take their draws together, pair j in lane j (P0..P3: -ln u
-      // of the lane's four sites); a chunk takes them by shuffle.  Lanes that
-      // become able to flip later in the sweep draw when their chunk comes
-      // (the stream is counter-based: the same numbers either way).
-      float P0 = 0.0f, P1 = 0.0f, P2 = 0.0f, P3 = 0.0f;
-      {
-        int total = 0, myc = -1, myl = 0;
-        for (int c = 0; c < nch; ++c) {
-          const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
+      for (int c = 0; c < nch; ++c) {
+        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
+        {
+          // a chunk none of whose sites has beta*dE below the largest -ln u
+          // keeps its state: its uniforms are not drawn (the stream is
+          // counter-based, so nothing after it moves)
           const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
           const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
           const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
@@ -218,66 +238,14 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             const float bf = __fmul_rn(beta2, fv[e]);
             if ((((myw >> e) & 1u) ? bf : -bf) < ojd::kNegLogMax) can |= 1u << e;
           }
-          const uint32_t hv = __ballot_sync(0xffffffffu, (can & inside) != 0u);
-          if (lane == 0) have[c] = hv;
-          const int cntc = __popc(hv), j = lane - total;
-          if (j >= 0 && j < cntc) {
-            myc = c;
-            myl = (int)__fns(hv, 0u, j + 1);
-          }
-          total += cntc;
+          if (!__any_sync(0xffffffffu, (can & inside) != 0u)) continue;
         }
-        if (myc >= 0) {
-          const ojd::u4 x = ojd::philox((uint32_t)(32 * myc + myl), kk, rg, tag, a.keys);
-          P0 = ojd::neglog(x.x);
-          P1 = ojd::neglog(x.y);
-          P2 = ojd::neglog(x.z);
-          P3 = ojd::neglog(x.w);
-        }
-        __syncwarp();  // the draw masks are visible to the warp
-      }
-      int uoff = 0;  // list index of the current chunk's first pair
-      for (int c = 0; c < nch; ++c) {
-        const uint32_t inside = c == nch - 1 ? inside_last : 0xFu;
-        const uint32_t hv = have[c];
-        uint32_t can = 0u;
-        {
-          // a chunk none of whose sites has beta*dE below the largest -ln u
-          // keeps its state: its uniforms are not needed
-          const float4 f4 = reinterpret_cast<const float4*>(f)[32 * c + lane];
-          const float fv[4] = {f4.x, f4.y, f4.z, f4.w};
-          const uint32_t myw = sw[sw_word(c, lane)] >> sw_shift(c);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const float bf = __fmul_rn(beta2, fv[e]);
-            if ((((myw >> e) & 1u) ? bf : -bf) < ojd::kNegLogMax) can |= 1u << e;
-          }
-          can &= inside;
-        }
-        const int idx = uoff + __popc(hv & below);
-        uoff += __popc(hv);
-        if (!__any_sync(0xffffffffu, can != 0u)) continue;
-        // this lane's uniforms: drawn ahead (mine), drawn now, or not needed yet
-        const bool mine = ((hv >> lane) & 1u) && idx < 32;
-        const int src = idx & 31;
+        const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
         float L[4];
-        L[0] = __shfl_sync(0xffffffffu, P0, src);
-        L[1] = __shfl_sync(0xffffffffu, P1, src);
-        L[2] = __shfl_sync(0xffffffffu, P2, src);
-        L[3] = __shfl_sync(0xffffffffu, P3, src);
-        // every lane has its uniforms once allL is set; before that a lane
-        // without them has no site with beta*dE below the largest -ln u
-        bool allL = false;
-        if (__any_sync(0xffffffffu, can != 0u && !mine)) {
-          const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
-          if (!mine) {
-            L[0] = ojd::neglog(x.x);
-            L[1] = ojd::neglog(x.y);
-            L[2] = ojd::neglog(x.z);
-            L[3] = ojd::neglog(x.w);
-          }
-          allL = true;
-        }
+        L[0] = ojd::neglog(x.x);
+        L[1] = ojd::neglog(x.y);
+        L[2] = ojd::neglog(x.z);
+        L[3] = ojd::neglog(x.w);
         // this lane's sites that exist and are not yet decided in this chunk
         // (chunk-local index at or past the last flip's + 1)
         uint32_t open = inside;
@@ -297,7 +265,6 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
             if ((neg ? bf : -bf) < L[e]) mask |= 1u << e;
           }
           mask &= open;
-          if (!allL && !mine) mask = 0u;
           const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0u);
           if (!lanes) break;
           const int ls = __ffs(lanes) - 1;
@@ -333,17 +300,6 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
           if (lane == 0) ++nflip;
           const int pos = 4 * ls + es + 1;  // chunk-local index of the first site not yet decided
           open = inside & (0xFu << min(max(pos - 4 * lane, 0), 4));
-          if (!allL) {
-            // the flip moved this chunk's fields: every lane takes its uniforms
-            const ojd::u4 x = ojd::philox((uint32_t)(32 * c + lane), kk, rg, tag, a.keys);
-            if (!mine) {
-              L[0] = ojd::neglog(x.x);
-              L[1] = ojd::neglog(x.y);
-              L[2] = ojd::neglog(x.z);
-              L[3] = ojd::neglog(x.w);
-            }
-            allL = true;
-          }
           __syncwarp();
         }
       }
@@ -395,7 +351,10 @@ template <int W, bool H>
 __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];  // [n][128] couplings of the item's instance
   __shared__ int item_sh;
+  __shared__ __align__(8) uint64_t stage_bar;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t stage_phase = 0u;
+  stage_init(&stage_bar);
   unsigned long long nflip = 0;  // lane 0 counts the warp's flips
   for (;;) {
     __syncthreads();
@@ -409,14 +368,10 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
     if (n > 128) continue;  // the host launches this kernel only for n <= 128
     const int r = a.items[2 * item + 1] * W + warp;
     {
-      // n rows of 128 couplings, 16 bytes per thread and step, by every warp
-      // of the CTA before any leaves for an inactive replica
-      const int4* src = reinterpret_cast<const int4*>(H ? static_cast<const void*>(a.J16 + a.joff[m])
-                                                          : static_cast<const void*>(a.J + a.joff[m]));
-      int4* dst = reinterpret_cast<int4*>(shb);
-      const int total = n * 128 * (H ? 2 : 4) / 16;
-      for (int q = threadIdx.x; q < total; q += blockDim.x) dst[q] = __ldg(src + q);
-      __syncthreads();
+      // n rows of 128 couplings by one bulk copy, waited for by every warp of
+      // the CTA before any leaves for an inactive replica
+      const void* src = H ? static_cast<const void*>(a.J16 + a.joff[m]) : static_cast<const void*>(a.J + a.joff[m]);
+      if (!stage_rows(shb, src, (uint32_t)(n * 128 * (H ? 2 : 4)), &stage_bar, stage_phase, a)) continue;
     }
     if (r >= a.reads[m]) continue;  // warps past the instance's reads wait for the next item
     int8_t* gs = a.spins + a.soff[m] + (size_t)r * n;
@@ -608,7 +563,7 @@ bool batch_variant_valid(int variant) {
 }
 
 // largest n whose fields fit the variant: W warps x (FP32 fields + spin
-// words + draw masks) within the 227 KB of shared memory per CTA
+// words) within the 227 KB of shared memory per CTA
 int batch_variant_max_n(int variant) {
   switch (variant) {
     case 321: return 1664;
@@ -630,8 +585,8 @@ cudaError_t launch_variant(const BatchArgs& a, int nitems, int sm_count, cudaStr
   const bool sj = jbytes > 0;
   auto kern = h ? (sj ? sa_batch_kernel<W, MINB, GROUP, true, true> : sa_batch_kernel<W, MINB, GROUP, true, false>)
                 : (sj ? sa_batch_kernel<W, MINB, GROUP, false, true> : sa_batch_kernel<W, MINB, GROUP, false, false>);
-  // FP32 fields + spin words + draw masks per warp, then the staged couplings
-  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4 + kHaveWords * 4) + jbytes;
+  // FP32 fields + spin words per warp, then the staged couplings
+  const size_t smem = (size_t)W * ((size_t)a.fstride * 4 + (size_t)a.swstride * 4) + jbytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -663,7 +618,7 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
                                 const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count,
                                 cudaStream_t st, int* launches, int variant, float* d_fields,
                                 const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
-                                bool write_fields) {
+                                bool write_fields, int* d_status, long long wait_limit) {
   if (variant == 0) variant = batch_default_variant();
   if (!batch_variant_valid(variant) || b->max_n > batch_variant_max_n(variant)) return cudaErrorInvalidValue;
   if (b->count == 0 || nitems <= 0 || nsweeps <= 0) return cudaSuccess;
@@ -696,6 +651,8 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
   a.E = b->exact_fields ? d_energies : nullptr;
   a.eoff = d_eoff;
   a.flips = rb.flips;
+  a.status = d_status;
+  a.wait_limit = wait_limit >= 0 ? wait_limit : kStageDrainLimit;
   cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   if (b->max_n <= 128) {
@@ -736,7 +693,8 @@ cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int
   if (e != cudaSuccess) return e;
   if (launches) ++*launches;
   return launch_batch_sweeps(b, d_reads, d_soff, d_items, nitems, d_counter, spins, betas, nsweeps, rb, inst0,
-                             sm_count, st, launches, variant, d_fields, d_foff, d_energies, d_eoff, false);
+                             sm_count, st, launches, variant, d_fields, d_foff, d_energies, d_eoff, false, fc.status,
+                             fc.wait_limit);
 }
 
 int batch_energy_splits(const oj_batch* b, int max_reads, int sm_count) {

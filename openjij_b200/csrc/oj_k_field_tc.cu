@@ -37,6 +37,7 @@
 #include <cstring>
 #include <vector>
 
+#include "oj_device.cuh"
 #include "oj_internal.h"
 
 namespace oj {
@@ -68,7 +69,10 @@ struct FieldArgs {
   long long wait_limit;    // iterations of a pipeline wait (0: give up at once)
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+using ojd::bulk_copy;
+using ojd::mbar_init;
+using ojd::mbar_wait;
+using ojd::smem_u32;
 
 // Matrix descriptor, K-major, no swizzle: LBO = distance of K-adjacent core
 // matrices, SBO = distance of adjacent 8-row groups.
@@ -80,30 +84,6 @@ __device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, ui
 // Instruction descriptor: s8 x s8 -> s32, K-major A and B, M = 128, N = nn.
 __device__ __forceinline__ uint32_t idesc_i8(int nn) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nn >> 3) << 17) | ((uint32_t)(kTileSites >> 4) << 24);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t ph, long long limit) {
-  for (long long it = 0; it < limit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_u32(b)), "r"(ph)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
 }
 
 __device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
@@ -212,8 +192,7 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   auto issue_a = [&](int kc) {
     const int s = kc % ST;
     unsigned char* As = sm + s * S::kStage;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar + s)), "r"(S::kA)
-                 : "memory");
+    ojd::mbar_expect_tx(bar + s, S::kA);
 #pragma unroll
     for (int t = 0; t < D; ++t)
       bulk_copy(As + t * kTileBytes, dig + ((size_t)(t * nch + mt) * nch + kc) * kTileBytes, kTileBytes, bar + s);

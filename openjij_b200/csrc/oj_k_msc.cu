@@ -12,9 +12,7 @@
 // is below thr[k][d-2u] = floor(exp(-beta_k*dE)*2^32).  U is compared one
 // bit level at a time for all 32 replicas at once, most significant level
 // first, drawing a fresh Philox word per level; the loop stops as soon as
-// every replica is decided.  A word still undecided after two draws (eight
-// levels) is finished later from its warp's queue, 32 words at a time
-// (ojd::TailQueue), so a warp does not run every site to its slowest lane.
+// every replica is decided.
 //
 // Sites follow the classes of a greedy colouring (checkerboard on a bipartite
 // lattice).  One thread block cluster owns one replica group: its P CTAs split
@@ -114,18 +112,11 @@ __device__ __forceinline__ void msc_level(const MscSweep<D>& sw, const uint32_t 
   pending &= ~(pm ^ wl);
 }
 
-// Classes of one site's word: the replicas of each live uphill class u, the
-// bits that flip without a draw (downhill, dE = 0, or an always-accepting
-// class) and the bits still to compare.
 template <int D>
-struct MscCls {
-  uint32_t cls[MscSweep<D>::UMAX];
-  uint32_t flip, pending;
-};
-
-template <int D>
-__device__ __forceinline__ MscCls<D> msc_cls(uint32_t w, const uint32_t* __restrict__ Wsh,
-                                             const uint16_t* __restrict__ nb, uint32_t jmk, const MscSweep<D>& sw) {
+__device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restrict__ Wsh,
+                                             const uint16_t* __restrict__ nb, uint32_t jmk,
+                                             const MscSweep<D>& sw, uint32_t site, uint32_t sweep,
+                                             uint32_t grp, const ojd::Keys& K) {
   constexpr int NB = D <= 1 ? 1 : (D <= 3 ? 2 : (D <= 7 ? 3 : 4));
   constexpr int UMAX = MscSweep<D>::UMAX;
   uint32_t cnt[NB];
@@ -141,97 +132,55 @@ __device__ __forceinline__ MscCls<D> msc_cls(uint32_t w, const uint32_t* __restr
       x = t;
     }
   }
-  MscCls<D> c;
-  uint32_t uphill = 0u;
-  c.pending = 0u;
-  c.flip = 0u;
+  uint32_t cls[UMAX];
+  uint32_t uphill = 0u, pending = 0u, flip = 0u;
 #pragma unroll
   for (int u = 0; u < UMAX; ++u) {
     uint32_t m = 0xFFFFFFFFu;
 #pragma unroll
     for (int b = 0; b < NB; ++b) m &= ((u >> b) & 1) ? cnt[b] : ~cnt[b];
     uphill |= m;
-    if ((sw.alw >> u) & 1u) c.flip |= m;
+    if ((sw.alw >> u) & 1u) flip |= m;
     m = ((sw.live >> u) & 1u) ? m : 0u;
-    c.cls[u] = m;
-    c.pending |= m;
+    cls[u] = m;
+    pending |= m;
   }
-  c.flip |= ~uphill;
-  return c;
-}
-
-// Philox draws q0 .. q1 - 1 (four bit levels of U each) while bits of the word
-// are pending; lt collects the bits found below their threshold.
-template <int D>
-__device__ __forceinline__ void msc_levels(const MscSweep<D>& sw, const MscCls<D>& c, int q0, int q1,
-                                           uint32_t site, uint32_t sweep, uint32_t grp, const ojd::Keys& K,
-                                           uint32_t& pending, uint32_t& lt) {
-#pragma unroll 1
-  for (int q = q0; q < q1; ++q) {
+  flip |= ~uphill;
+  uint32_t lt = 0u;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
     if (!pending) break;
     const ojd::u4 r = ojd::philox(site, sweep, grp, ((uint32_t)q << 8) | ojd::TAG_SA_MSC, K);
-    msc_level<D>(sw, c.cls, 31 - 4 * q, r.x, pending, lt);
-    msc_level<D>(sw, c.cls, 30 - 4 * q, r.y, pending, lt);
-    msc_level<D>(sw, c.cls, 29 - 4 * q, r.z, pending, lt);
-    msc_level<D>(sw, c.cls, 28 - 4 * q, r.w, pending, lt);
+    msc_level<D>(sw, cls, 31 - 4 * q, r.x, pending, lt);
+    msc_level<D>(sw, cls, 30 - 4 * q, r.y, pending, lt);
+    msc_level<D>(sw, cls, 29 - 4 * q, r.z, pending, lt);
+    msc_level<D>(sw, cls, 28 - 4 * q, r.w, pending, lt);
   }
-}
-
-// Finishes the last c (<= 32) deferred sites of the warp's queue, one per lane.
-template <int D>
-__device__ __forceinline__ uint32_t msc_tail(ojd::TailQueue& Q, int& cnt, int c, uint32_t* __restrict__ Wsh,
-                                             const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
-                                             const uint16_t* __restrict__ nbr, const MscSweep<D>& sw, uint32_t k,
-                                             uint32_t g, const ojd::Keys& K) {
-  uint32_t s, pending, acc;
-  if (!ojd::tail_pop(Q, cnt, c, s, pending, acc)) return 0u;
-  const uint32_t w = Wsh[s];
-  const MscCls<D> cl = msc_cls<D>(w, Wsh, nbr + (size_t)s * D, jm[s], sw);
-  uint32_t lt = 0u;
-  msc_levels<D>(sw, cl, ojd::kHeadDraws, 8, (uint32_t)gid[s], k, g, K, pending, lt);
-  const uint32_t v = w ^ (acc | lt);
-  Wsh[s] = v;
-  return __popc(v ^ w);
+  return w ^ (flip | lt);
 }
 
 // Updates own slots [lo, hi), two independent sites per thread and iteration;
-// returns the number of spins this thread flipped.  A site whose word is
-// still pending after kHeadDraws draws is finished from the warp's queue
-// (ojd::TailQueue); sites of one colour class are independent, and every word
-// of the range is written before the function returns.
+// returns the number of spins this thread flipped.
 template <int D>
 __device__ __forceinline__ uint32_t msc_range(int lo, int hi, uint32_t* __restrict__ Wsh,
                                               const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
                                               const uint16_t* __restrict__ nbr, const MscSweep<D>& sw,
-                                              uint32_t k, uint32_t g, const ojd::Keys& K, ojd::TailQueue& Q) {
+                                              uint32_t k, uint32_t g, const ojd::Keys& K) {
   const int T = blockDim.x;
   uint32_t nf = 0u;
-  int cnt = 0;  // the warp's deferred sites (the same in every lane)
-  // warp-uniform loop: thread t visits s = lo + t + 2 T it and s + T
-  for (int base = lo + (threadIdx.x & ~31); base < hi; base += 2 * T) {
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int s = base + (threadIdx.x & 31) + e * T;
-      uint32_t pending = 0u, acc = 0u;
-      if (s < hi) {
-        const uint32_t w = Wsh[s];
-        const MscCls<D> cl = msc_cls<D>(w, Wsh, nbr + (size_t)s * D, jm[s], sw);
-        pending = cl.pending;
-        uint32_t lt = 0u;
-        msc_levels<D>(sw, cl, 0, ojd::kHeadDraws, (uint32_t)gid[s], k, g, K, pending, lt);
-        acc = cl.flip | lt;
-        if (!pending) {
-          const uint32_t v = w ^ acc;
-          Wsh[s] = v;
-          nf += __popc(v ^ w);
-        }
-      }
-      ojd::tail_push(Q, cnt, (uint32_t)s, pending, acc);
-      if (cnt >= 32) nf += msc_tail<D>(Q, cnt, 32, Wsh, gid, jm, nbr, sw, k, g, K);
+  for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
+    const int s2 = s + T;
+    const uint32_t w0 = Wsh[s];
+    const uint32_t a = msc_site<D>(w0, Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, K);
+    if (s2 < hi) {
+      const uint32_t w2 = Wsh[s2];
+      const uint32_t b = msc_site<D>(w2, Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, K);
+      Wsh[s2] = b;
+      nf += __popc(b ^ w2);
     }
+    Wsh[s] = a;
+    nf += __popc(a ^ w0);
   }
-  if (cnt > 0) nf += msc_tail<D>(Q, cnt, cnt, Wsh, gid, jm, nbr, sw, k, g, K);
-  __syncwarp();
   return nf;
 }
 
@@ -239,8 +188,6 @@ __device__ __forceinline__ uint32_t msc_range(int lo, int hi, uint32_t* __restri
 template <int D>
 __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
   extern __shared__ __align__(16) uint32_t Wsh[];
-  __shared__ ojd::TailQueue queue[kMscMaxThreads / 32];
-  ojd::TailQueue& Q = queue[threadIdx.x >> 5];
   cg::cluster_group cl = cg::this_cluster();
   const int p = (int)cl.block_rank();
   const int g = blockIdx.y;
@@ -272,7 +219,7 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
     const MscSweep<D> sw = msc_sweep<D>(a.thr + (size_t)k * (D + 1), a.always[k]);
     const uint32_t kk = a.sweep0 + (uint32_t)k, gg = a.group0 + (uint32_t)g;
     for (int c = 0; c < a.ncol; ++c) {
-      nflip += msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, kk, gg, a.keys, Q);
+      nflip += msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_wait();
       if (prev >= 0) {
         const int hlo = ho[prev], hhi = ho[prev + 1];
@@ -283,7 +230,7 @@ __global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
         }
       }
       __syncthreads();
-      nflip += msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys, Q);
+      nflip += msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_arrive();
       __syncthreads();
       prev = c;

@@ -16,9 +16,7 @@
 // aligned Trotter neighbours (dE_trot = 4 - 4k), class 3u + k; always when the
 // class's FP32 dE <= 0, else U < floor(exp(-dE)*2^32) with U's bit (31 - l)
 // taken from W_l = Philox(i, k, g, (l>>2)<<16 | q<<8 | TAG_SQA_SPLIT)[l & 3],
-// compared one bit level at a time for all bits of the word (a word still
-// undecided after two draws is finished from its warp's queue, 32 words at a
-// time: ojd::TailQueue).
+// compared one bit level at a time for all bits of the word.
 //
 // Parallel structure as the bit-packed SA kernel (oj_k_msc.cu): one thread
 // block cluster per replica group, its CTAs splitting the sites into
@@ -124,30 +122,24 @@ __device__ __forceinline__ uint32_t tab_eval(const uint32_t* __restrict__ row, u
          (kk2 & tab_pick<NB>(row + 2 * E, cnt));
 }
 
-// Class data of one site's word: the unsatisfied-bond counts as NB bit planes
-// (nb are the neighbour slots in X, the array being updated) and the Trotter
-// alignment masks against y, the site's other half.
+// New value of word x (half q) of one site: nb are the neighbour slots in X
+// (the array being updated), y the site's other half, tab the sweep's tables.
 template <int D>
-struct SiteCls {
-  uint32_t cnt[SplitTab<D>::NB];
-  uint32_t kk0, kk1, kk2;
-};
-
-template <int D>
-__device__ __forceinline__ SiteCls<D> split_cls(uint32_t x, const uint32_t* __restrict__ X,
-                                                const uint16_t* __restrict__ nb, uint32_t jmk, uint32_t y, int q,
-                                                const SplitArgs& a) {
-  constexpr int NB = SplitTab<D>::NB;
-  SiteCls<D> c;
+__device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __restrict__ X,
+                                               const uint16_t* __restrict__ nb, uint32_t jmk, uint32_t y,
+                                               int q, const SplitArgs& a, const uint32_t* __restrict__ tab,
+                                               uint32_t site, uint32_t sweep, uint32_t grp) {
+  constexpr int NB = SplitTab<D>::NB, E = SplitTab<D>::E;
+  uint32_t cnt[NB];
 #pragma unroll
-  for (int b = 0; b < NB; ++b) c.cnt[b] = 0u;
+  for (int b = 0; b < NB; ++b) cnt[b] = 0u;
 #pragma unroll
   for (int l = 0; l < D; ++l) {
     uint32_t v = x ^ X[nb[l]] ^ (0u - ((jmk >> l) & 1u));
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      const uint32_t t = c.cnt[b] & v;
-      c.cnt[b] ^= v;
+      const uint32_t t = cnt[b] & v;
+      cnt[b] ^= v;
       v = t;
     }
   }
@@ -156,95 +148,58 @@ __device__ __forceinline__ SiteCls<D> split_cls(uint32_t x, const uint32_t* __re
   const uint32_t z = q == 0 ? (((y << 1) & ~a.low) | ((y >> (a.H - 1)) & a.low))
                             : (((y >> 1) & ~a.high) | ((y << (a.H - 1)) & a.high));
   const uint32_t al_y = ~(x ^ y), al_z = ~(x ^ z);
-  c.kk2 = al_y & al_z;
-  c.kk1 = al_y ^ al_z;
-  c.kk0 = ~(al_y | al_z);
-  return c;
-}
-
-// Philox draws qq0 .. qq1 - 1 (four bit levels of U each) while bits of the
-// word are pending: lt collects the bits found below their threshold.
-template <int D>
-__device__ __forceinline__ void split_levels(const SiteCls<D>& c, const uint32_t* __restrict__ tab, int qq0,
-                                             int qq1, uint32_t site, uint32_t sweep, uint32_t grp, int q,
-                                             const SplitArgs& a, uint32_t& pending, uint32_t& lt) {
-  constexpr int E = SplitTab<D>::E;
+  const uint32_t kk2 = al_y & al_z, kk1 = al_y ^ al_z, kk0 = ~(al_y | al_z);
+  const uint32_t flip = tab_eval<D>(tab + 32 * 3 * E, kk0, kk1, kk2, cnt) & a.valid;
+  uint32_t pending = tab_eval<D>(tab + 33 * 3 * E, kk0, kk1, kk2, cnt) & a.valid;
+  uint32_t lt = 0u;
 #pragma unroll 1
-  for (int qq = qq0; qq < qq1; ++qq) {
+  for (int qq = 0; qq < 8; ++qq) {
     if (!pending) break;
     const ojd::u4 r =
         ojd::philox(site, sweep, grp, ((uint32_t)qq << 16) | ((uint32_t)q << 8) | ojd::TAG_SQA_SPLIT, a.keys);
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
       const uint32_t wl = ojd::pick(r, l);
-      const uint32_t pm = tab_eval<D>(tab + (4 * qq + l) * 3 * E, c.kk0, c.kk1, c.kk2, c.cnt);
+      const uint32_t pm = tab_eval<D>(tab + (4 * qq + l) * 3 * E, kk0, kk1, kk2, cnt);
       lt |= pending & pm & ~wl;
       pending &= ~(pm ^ wl);
     }
   }
-}
-
-// Finishes the last c (<= 32) deferred sites of the warp's queue, one per
-// lane: the class data again from the (unchanged) neighbours, then the draws
-// after the first kHeadDraws.
-template <int D>
-__device__ __forceinline__ uint32_t split_tail(ojd::TailQueue& Q, int& cnt, int c, uint32_t* __restrict__ X,
-                                               const uint32_t* __restrict__ Y, const int32_t* __restrict__ gid,
-                                               const uint16_t* __restrict__ jm, const uint16_t* __restrict__ nbr,
-                                               int q, const SplitArgs& a, const uint32_t* __restrict__ tab,
-                                               uint32_t k, uint32_t g) {
-  uint32_t s, pending, acc;
-  if (!ojd::tail_pop(Q, cnt, c, s, pending, acc)) return 0u;
-  const uint32_t x = X[s];
-  const SiteCls<D> cl = split_cls<D>(x, X, nbr + (size_t)s * D, jm[s], Y[s], q, a);
-  uint32_t lt = 0u;
-  split_levels<D>(cl, tab, ojd::kHeadDraws, 8, (uint32_t)gid[s], k, g, q, a, pending, lt);
-  const uint32_t v = x ^ acc ^ lt;
-  X[s] = v;
-  return __popc(v ^ x);
+  return x ^ flip ^ lt;
 }
 
 // Updates slots [lo, hi) of half X; returns the spins this thread flipped.
-// Sites of one colour class are independent, so a deferred site's word may be
-// written after its class-mates'; every word of the range is written before
-// the function returns.
 template <int D>
 __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __restrict__ X,
                                                 const uint32_t* __restrict__ Y, const int32_t* __restrict__ gid,
                                                 const uint16_t* __restrict__ jm, const uint16_t* __restrict__ nbr,
                                                 int q, const SplitArgs& a, const uint32_t* __restrict__ tab,
-                                                uint32_t k, uint32_t g, ojd::TailQueue& Q) {
-  constexpr int SPI = D <= 4 ? 2 : 1;  // independent sites per thread and iteration
-  constexpr int E = SplitTab<D>::E;
+                                                uint32_t k, uint32_t g) {
   const int T = blockDim.x;
   uint32_t nf = 0u;
-  int cnt = 0;  // the warp's deferred sites (the same in every lane)
-  // warp-uniform loop: thread t visits s = lo + t + SPI T it (and s + T)
-  for (int base = lo + (threadIdx.x & ~31); base < hi; base += SPI * T) {
-#pragma unroll
-    for (int e = 0; e < SPI; ++e) {
-      const int s = base + (threadIdx.x & 31) + e * T;
-      uint32_t pending = 0u, acc = 0u;
-      if (s < hi) {
-        const uint32_t x = X[s];
-        const SiteCls<D> cl = split_cls<D>(x, X, nbr + (size_t)s * D, jm[s], Y[s], q, a);
-        acc = tab_eval<D>(tab + 32 * 3 * E, cl.kk0, cl.kk1, cl.kk2, cl.cnt) & a.valid;
-        pending = tab_eval<D>(tab + 33 * 3 * E, cl.kk0, cl.kk1, cl.kk2, cl.cnt) & a.valid;
-        uint32_t lt = 0u;
-        split_levels<D>(cl, tab, 0, ojd::kHeadDraws, (uint32_t)gid[s], k, g, q, a, pending, lt);
-        acc ^= lt;  // the new word is x ^ always-flips ^ accepted bits
-        if (!pending) {
-          const uint32_t v = x ^ acc;
-          X[s] = v;
-          nf += __popc(v ^ x);
-        }
+  if constexpr (D <= 4) {  // two independent sites per iteration
+    for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
+      const int s2 = s + T;
+      const uint32_t x0 = X[s];
+      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
+      if (s2 < hi) {
+        const uint32_t x2 = X[s2];
+        const uint32_t w2 =
+            split_site<D>(x2, X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, tab, (uint32_t)gid[s2], k, g);
+        X[s2] = w2;
+        nf += __popc(w2 ^ x2);
       }
-      ojd::tail_push(Q, cnt, (uint32_t)s, pending, acc);
-      if (cnt >= 32) nf += split_tail<D>(Q, cnt, 32, X, Y, gid, jm, nbr, q, a, tab, k, g);
+      X[s] = v;
+      nf += __popc(v ^ x0);
+    }
+  } else {
+    for (int s = lo + threadIdx.x; s < hi; s += T) {
+      const uint32_t x0 = X[s];
+      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
+      X[s] = v;
+      nf += __popc(v ^ x0);
     }
   }
-  if (cnt > 0) nf += split_tail<D>(Q, cnt, cnt, X, Y, gid, jm, nbr, q, a, tab, k, g);
-  __syncwarp();
   return nf;
 }
 
@@ -252,13 +207,11 @@ __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __rest
 // CL: the group's sites are split over a cluster of CTAs (halo exchange);
 // without it one CTA owns all sites and a phase ends with one block barrier.
 template <int D, bool CL>
-__global__ void __launch_bounds__(kSplitMaxThreads, 1) sqa_split_kernel(SplitArgs a) {
+__global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a) {
   extern __shared__ __align__(16) uint32_t sh[];
   constexpr int NC = (D + 1) * 3;
   constexpr int E = SplitTab<D>::E;
   __shared__ __align__(16) uint32_t tab[SplitTab<D>::WORDS];
-  __shared__ ojd::TailQueue queue[kSplitMaxThreads / 32];
-  ojd::TailQueue& Q = queue[threadIdx.x >> 5];
   const int p = CL ? (int)cg::this_cluster().block_rank() : 0;
   const int g = blockIdx.y;
   const int32_t* gid_g = a.gidx + (size_t)p * a.slots;
@@ -321,7 +274,7 @@ __global__ void __launch_bounds__(kSplitMaxThreads, 1) sqa_split_kernel(SplitArg
       for (int c = 0; c < a.ncol; ++c) {
         if constexpr (CL) {
           cg::cluster_group cl = cg::this_cluster();
-          nflip += split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, tab, kk, gg, Q);
+          nflip += split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
           cluster_wait();
           if (prev_c >= 0) {
             uint32_t* P = prev_q ? WO : WE;
@@ -333,13 +286,13 @@ __global__ void __launch_bounds__(kSplitMaxThreads, 1) sqa_split_kernel(SplitArg
             }
           }
           __syncthreads();
-          nflip += split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg, Q);
+          nflip += split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
           cluster_arrive();
           __syncthreads();
           prev_c = c;
           prev_q = q;
         } else {
-          nflip += split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg, Q);
+          nflip += split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
           __syncthreads();
         }
       }
