@@ -239,14 +239,26 @@ RunCounters read_counters(oj_ctx* ctx) {
 oj_status field_call(oj_ctx* ctx, const oj_batch* b, const int32_t* reads, const std::vector<int>& order,
                      int max_reads, FieldCall* fc) {
   fc->NT = field_tc_tile_replicas(b, max_reads);
-  std::vector<int32_t> it;
+  std::vector<int32_t> it, hot;
   field_tc_items(b, reads, order, fc->NT, it);
   fc->nitems = (int)(it.size() / 3);
+  if (hot_tc_applies(b)) hot_tc_items(b, reads, order, hot);
+  fc->hot_nitems = (int)(hot.size() / 2);
+  const size_t nf = it.size();
+  it.insert(it.end(), hot.begin(), hot.end());  // field items, then hot-sweep items
   cudaError_t e = ctx->fitems.ensure(std::max<size_t>(it.size() * 4, 16));
   if (e == cudaSuccess && !it.empty())
     e = cudaMemcpyAsync(ctx->fitems.ptr, it.data(), it.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "field items");
   fc->items = ctx->fitems.as<int32_t>();
+  fc->hot_items = fc->items + nf;
+  fc->nrep = 0;
+  for (int m = 0; m < b->count; ++m) fc->nrep += (size_t)reads[m];
+  if (fc->hot_nitems > 0) {
+    e = ctx->kstart.ensure(std::max<size_t>(fc->nrep * 4, 16));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "hot-sweep table");
+    fc->kstart = ctx->kstart.as<int32_t>();
+  }
   char* cb = ctx->counters.as<char>();
   fc->drift = reinterpret_cast<unsigned int*>(cb + 8);
   fc->status = reinterpret_cast<int*>(cb + 12);
@@ -289,6 +301,18 @@ cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, co
   if (e != cudaSuccess) return e;
   ++*launches;
   const int64_t K = exact ? 0 : ctx->recompute;
+  // exact one-digit batches: the flip-heavy first sweeps on the tensor cores;
+  // each replica tile continues in the sweep kernel at the sweep it stopped at
+  const int32_t* kstart = nullptr;
+  if (exact && fc.hot_nitems > 0 && S > 0) {
+    e = cudaMemsetAsync(fc.kstart, 0, fc.nrep * 4, st);
+    if (e != cudaSuccess) return e;
+    e = launch_hot_tc(p.b, p.d_reads, p.d_soff, p.spins, p.d_fields, p.d_foff, p.d_eoff, fc.hot_items,
+                      fc.hot_nitems, p.d_betas, S, rb, p.inst0, fc.kstart, fc.status, fc.wait_limit, st);
+    if (e != cudaSuccess) return e;
+    ++*launches;
+    kstart = fc.kstart;
+  }
   int64_t k = 0;
   while (k < S) {
     const uint64_t g = (uint64_t)rb.sweep0 + (uint64_t)k;
@@ -298,7 +322,7 @@ cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, co
     rs.sweep0 = (uint32_t)g;
     e = launch_batch_sweeps(p.b, p.d_reads, p.d_soff, p.d_items, p.nitems, p.d_counter, p.spins, p.d_betas + k, len,
                             rs, p.inst0, ctx->sm_count, st, launches, p.variant, p.d_fields, p.d_foff, p.d_energies,
-                            p.d_eoff, wf, fc.status, fc.wait_limit);
+                            p.d_eoff, wf, fc.status, fc.wait_limit, kstart);
     if (e != cudaSuccess) return e;
     k += len;
     if (k < S || wf) {

@@ -155,7 +155,8 @@ struct oj_ctx {
   std::string noalloc_error;  // why the allocation-free entry point could not be set up ("" = ready)
   oj::DevBuf spins, words, params, energies, best, aux, batch, fields, eparts;
   oj::DevBuf counters;  // device counters of a run: accepted flips (u64), field drift (float bits), status
-  oj::DevBuf fitems;    // work items of the tensor-core field kernel
+  oj::DevBuf fitems;    // work items of the tensor-core field and hot-sweep kernels
+  oj::DevBuf kstart;    // per replica: the sweep the sweep kernel continues at after the hot-sweep kernel
   int recompute = 16;   // full field recompute every this many sweeps (real couplings; 0 = never)
   long long wait_limit = -1;  // iterations of the field kernel's pipeline waits (< 0: the default)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -224,7 +225,21 @@ struct FieldCall {
   unsigned int* drift = nullptr;   // max |F_new - F_old| (float bits) in compare mode
   int* status = nullptr;           // set when a bounded wait runs out
   long long wait_limit = 0;
+  // the tensor-core kernel of the flip-heavy first sweeps (exact one-digit
+  // batches, oj_k_hot_tc.cu): its work items and, per replica, the sweep the
+  // sweep kernel continues at
+  const int32_t* hot_items = nullptr;  // device [hot_nitems][2]: instance, replica tile
+  int hot_nitems = 0;
+  int32_t* kstart = nullptr;
+  size_t nrep = 0;
 };
+bool hot_tc_applies(const oj_batch* b);
+void hot_tc_items(const oj_batch* b, const int32_t* reads, const std::vector<int>& order,
+                  std::vector<int32_t>& items);
+cudaError_t launch_hot_tc(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff, int8_t* spins,
+                          float* F, const int64_t* d_foff, const int64_t* d_eoff, const int32_t* d_items,
+                          int nitems, const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0,
+                          int32_t* kstop, int* d_status, long long wait_limit, cudaStream_t st);
 // Fields on the tensor cores, then the sweeps (one segment, no recompute).
 cudaError_t launch_sa_batch(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                             const int32_t* d_items, int nitems, int* d_counter, int8_t* spins, const float* betas,
@@ -246,7 +261,8 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
                                 const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count,
                                 cudaStream_t st, int* launches, int variant, float* d_fields,
                                 const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
-                                bool write_fields, int* d_status, long long wait_limit);
+                                bool write_fields, int* d_status, long long wait_limit,
+                                const int32_t* kstart = nullptr);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep);

@@ -83,6 +83,7 @@ struct BatchArgs {
   unsigned long long* flips;  // accepted-flip counter, or null
   int* status;             // set when a bounded wait runs out
   long long wait_limit;    // iterations of the staging wait
+  const int32_t* kstart;   // per replica (eoff[m] + r): the first sweep to run, or null (0)
 };
 
 constexpr long long kStageDrainLimit = 1ll << 26;
@@ -220,7 +221,8 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
     // this lane's sites of the last chunk that exist (site index below n), as
     // a 4-bit mask; every site of the other chunks exists
     const uint32_t inside_last = 0xFu >> (4 - min(max(n - 128 * (nch - 1) - 4 * lane, 0), 4));
-    for (int64_t k = 0; k < a.nsweeps; ++k) {
+    const int64_t kfirst = a.kstart ? (int64_t)a.kstart[a.eoff[m] + r] : 0;
+    for (int64_t k = kfirst; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
       const uint32_t kk = a.sweep0 + (uint32_t)k;
       for (int c = 0; c < nch; ++c) {
@@ -618,7 +620,8 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
                                 const float* betas, int64_t nsweeps, RngBase rb, uint32_t inst0, int sm_count,
                                 cudaStream_t st, int* launches, int variant, float* d_fields,
                                 const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
-                                bool write_fields, int* d_status, long long wait_limit) {
+                                bool write_fields, int* d_status, long long wait_limit,
+                                const int32_t* kstart) {
   if (variant == 0) variant = batch_default_variant();
   if (!batch_variant_valid(variant) || b->max_n > batch_variant_max_n(variant)) return cudaErrorInvalidValue;
   if (b->count == 0 || nitems <= 0 || nsweeps <= 0) return cudaSuccess;
@@ -653,6 +656,7 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
   a.flips = rb.flips;
   a.status = d_status;
   a.wait_limit = wait_limit >= 0 ? wait_limit : kStageDrainLimit;
+  a.kstart = kstart;
   cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   if (b->max_n <= 128) {
