@@ -45,12 +45,17 @@ def build_cuda(verbose=False, force=False, extra=()):
     os.makedirs(BUILD, exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
         [os.path.join(INCLUDE, "openjij_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for cu in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(BUILD, os.path.basename(cu) + ".o")
         if force or _stale(obj, [cu] + headers):
-            _run([NVCC] + ARCH + NVCC_FLAGS + list(extra) + ["-c", cu, "-o", obj], verbose)
+            jobs.append([NVCC] + ARCH + NVCC_FLAGS + list(extra) + ["-c", cu, "-o", obj])
         objs.append(obj)
+    # one nvcc per source, as many at once as there are cores
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     if force or _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
              ["-Xlinker", "-rpath,$ORIGIN"], verbose)
