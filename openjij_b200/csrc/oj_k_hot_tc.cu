@@ -22,10 +22,14 @@
 // For these batches every partial sum is exact, so the fields are the jump
 // kernel's fields bit for bit and the spins are the sequential sweep's.  A tile
 // of replicas leaves after the first sweep in which it flipped fewer than
-// flip_floor spins (or after the last sweep): it stores its spins and FP32
-// fields and the sweep to continue from, and the dense-jump / batched kernel
-// takes the remaining sweeps from there (its cost per sweep falls with the
-// number of flips, this kernel's does not).
+// n/16 spins per replica (or after the last sweep): it stores its spins and
+// FP32 fields and the sweep to continue from, and the dense-jump / batched
+// kernel takes the remaining sweeps from there.  Its cost per sweep falls
+// with the number of flips (each reads an n-site row), this kernel's does not
+// (n^2 MMA work); on a dense n = 2048 QUBO the two cross between 96 and 256
+// flips per replica and sweep (measured: sweep 1 takes 0.94 ms here against
+// 2.73 ms in the jump kernel for 4096 replicas, sweep 2 0.32 ms against
+// 0.83 ms).
 //
 // Warps 0..7 decide (warps 0..3 also move the fields of the next chunk from
 // tensor memory into shared memory); warp 8 issues the copies and the MMAs.
@@ -54,7 +58,6 @@ constexpr uint32_t kTile = 128 * 128;   // one int8 tile
 constexpr uint32_t kBTile = kRT * 128;  // one tile of spin changes
 constexpr int kSwWords = 32 * ((kHotMaxChunks + 7) / 8);  // spin words per replica
 constexpr long long kHotDrain = 1ll << 26;
-constexpr int kDefaultFloor = 16;       // flips per replica and sweep below which a tile leaves
 
 // dynamic shared memory layout (bytes)
 constexpr uint32_t kOffRing = 0;
@@ -88,7 +91,7 @@ struct HotArgs {
   ojd::Keys keys;
   uint32_t sweep0, inst0, rep0;
   int32_t* kstop;         // per replica: the sweep (from 0) the sweep kernel continues at
-  int flip_floor;         // a tile leaves after a sweep with fewer flips per replica than this
+  int flip_floor;         // a tile leaves after a sweep with fewer flips per replica than this (-1: n/16)
   unsigned long long* flips;
   int* status;
   long long wait_limit;
@@ -390,7 +393,8 @@ __global__ void __launch_bounds__(kHotThreads, 1) hot_tc_kernel(HotArgs a) {
       bool stop = false;
       if (last) {
         const unsigned int sf = *reinterpret_cast<volatile unsigned int*>(sweep_flips + (k & 1));
-        stop = k + 1 >= a.nsweeps || (long long)sf < (long long)a.flip_floor * min(kRT, R - r0);
+        const long long floor_m = a.flip_floor >= 0 ? a.flip_floor : (n >> 4);
+        stop = k + 1 >= a.nsweeps || (long long)sf < floor_m * min(kRT, R - r0);
       }
       if (mma_thread) {
         if (!stop) {
@@ -495,12 +499,14 @@ __global__ void __launch_bounds__(kHotThreads, 1) hot_tc_kernel(HotArgs a) {
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(cols));
 }
 
+// OJ_HOT_FLOOR fixes the hand-over floor (flips per replica and sweep) for
+// every instance; by default it is n/16 of each instance.
 int hot_floor() {
   if (const char* env = std::getenv("OJ_HOT_FLOOR")) {
     const int v = std::atoi(env);
     if (v >= 0) return v;
   }
-  return kDefaultFloor;
+  return -1;
 }
 
 }  // namespace

@@ -4,7 +4,7 @@ Exact one-digit batches (integer couplings) start every call in it: the
 replicas of a 32-replica tile decide a 128-site chunk in lock step and the
 chunk's spin changes reach all fields as int8 MMAs; a tile hands its spins and
 fields to the dense-jump / batched sweep kernel after the first sweep with
-fewer flips per replica than a floor (OJ_HOT_FLOOR, default 16).  Whatever the
+fewer flips per replica than a floor (OJ_HOT_FLOOR, default n/16).  Whatever the
 hand-over sweep, the spins, energies and accepted-flip counts must be the
 replay's (the sequential sweep of the jump kernel,
 include/openjij/updater/single_spin_flip.hpp:66-95, with its uniforms).
@@ -20,7 +20,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-FLOORS = [None, "0", "1000000"]
+FLOORS = [None, "0", "40", "1000000"]
 
 
 def _per_sweep(betas, mcs):
