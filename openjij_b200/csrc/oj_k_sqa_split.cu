@@ -122,9 +122,48 @@ __device__ __forceinline__ uint32_t tab_eval(const uint32_t* __restrict__ row, u
          (kk2 & tab_pick<NB>(row + 2 * E, cnt));
 }
 
+// Count planes that tell apart u = 0 .. ceil(D/2) - 1 (the uphill counts of a
+// class with one aligned Trotter neighbour).
+template <int D>
+struct SplitLow {
+  static constexpr int U = (D + 1) / 2;
+  static constexpr int NB = U <= 2 ? 1 : (U <= 4 ? 2 : 3);
+};
+
+// Classes whose being live rules out the Trotter-dominated evaluation: every
+// class with no aligned Trotter neighbour (k = 0) and the classes with one
+// aligned neighbour and u >= ceil(D/2) (dE_sp <= 0 there).
+template <int D>
+__host__ __device__ constexpr uint32_t split_not_dominated_mask() {
+  uint32_t m = 0u;
+  for (int u = 0; u <= D; ++u) {
+    m |= 1u << (3 * u);
+    if (u >= SplitLow<D>::U) m |= 1u << (3 * u + 1);
+  }
+  return m;
+}
+
+// The row's bits for a sweep whose live classes all lie in
+// {(u, 1) : u < ceil(D/2)} and {(u, 2)}: the value only matters on live bits
+// (every other bit is neither pending nor compared), so the k = 0 group is
+// dropped, a k = 1 bit takes its table word from the low count planes alone
+// (u < ceil(D/2) on a live bit) and k = 2 from all of them.  Equal to tab_eval
+// on every live bit.
+template <int D>
+__device__ __forceinline__ uint32_t tab_eval_dominated(const uint32_t* __restrict__ row, uint32_t kk1,
+                                                       const uint32_t (&cnt)[SplitTab<D>::NB]) {
+  constexpr int NB = SplitTab<D>::NB, E = SplitTab<D>::E, NBL = SplitLow<D>::NB;
+  uint32_t low[NBL];
+#pragma unroll
+  for (int b = 0; b < NBL; ++b) low[b] = cnt[b];
+  const uint32_t p1 = tab_pick<NBL>(row + E, low);
+  const uint32_t p2 = tab_pick<NB>(row + 2 * E, cnt);
+  return (kk1 & p1) | (~kk1 & p2);
+}
+
 // New value of word x (half q) of one site: nb are the neighbour slots in X
 // (the array being updated), y the site's other half, tab the sweep's tables.
-template <int D>
+template <int D, bool DOM>
 __device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __restrict__ X,
                                                const uint16_t* __restrict__ nb, uint32_t jmk, uint32_t y,
                                                int q, const SplitArgs& a, const uint32_t* __restrict__ tab,
@@ -160,7 +199,12 @@ __device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __res
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
       const uint32_t wl = ojd::pick(r, l);
-      const uint32_t pm = tab_eval<D>(tab + (4 * qq + l) * 3 * E, kk0, kk1, kk2, cnt);
+      const uint32_t* row = tab + (4 * qq + l) * 3 * E;
+      uint32_t pm;
+      if constexpr (DOM)
+        pm = tab_eval_dominated<D>(row, kk1, cnt);
+      else
+        pm = tab_eval<D>(row, kk0, kk1, kk2, cnt);
       lt |= pending & pm & ~wl;
       pending &= ~(pm ^ wl);
     }
@@ -169,7 +213,8 @@ __device__ __forceinline__ uint32_t split_site(uint32_t x, const uint32_t* __res
 }
 
 // Updates slots [lo, hi) of half X; returns the spins this thread flipped.
-template <int D>
+// DOM: the sweep's live classes allow tab_eval_dominated.
+template <int D, bool DOM>
 __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __restrict__ X,
                                                 const uint32_t* __restrict__ Y, const int32_t* __restrict__ gid,
                                                 const uint16_t* __restrict__ jm, const uint16_t* __restrict__ nbr,
@@ -181,11 +226,11 @@ __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __rest
     for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
       const int s2 = s + T;
       const uint32_t x0 = X[s];
-      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
+      const uint32_t v = split_site<D, DOM>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
       if (s2 < hi) {
         const uint32_t x2 = X[s2];
         const uint32_t w2 =
-            split_site<D>(x2, X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, tab, (uint32_t)gid[s2], k, g);
+            split_site<D, DOM>(x2, X, nbr + (size_t)s2 * D, jm[s2], Y[s2], q, a, tab, (uint32_t)gid[s2], k, g);
         X[s2] = w2;
         nf += __popc(w2 ^ x2);
       }
@@ -195,7 +240,7 @@ __device__ __forceinline__ uint32_t split_range(int lo, int hi, uint32_t* __rest
   } else {
     for (int s = lo + threadIdx.x; s < hi; s += T) {
       const uint32_t x0 = X[s];
-      const uint32_t v = split_site<D>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
+      const uint32_t v = split_site<D, DOM>(x0, X, nbr + (size_t)s * D, jm[s], Y[s], q, a, tab, (uint32_t)gid[s], k, g);
       X[s] = v;
       nf += __popc(v ^ x0);
     }
@@ -268,13 +313,19 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
       __syncthreads();
     }
     const uint32_t kk = a.sweep0 + (uint32_t)k;
+    // the sweep's live classes allow the Trotter-dominated table evaluation
+    const bool dom = (__ldg(a.mode + 2 * k + 1) & split_not_dominated_mask<D>()) == 0u;
+    auto range = [&](int lo, int hi, uint32_t* X, const uint32_t* Y, int q) {
+      return dom ? split_range<D, true>(lo, hi, X, Y, gid, jm, nbr, q, a, tab, kk, gg)
+                 : split_range<D, false>(lo, hi, X, Y, gid, jm, nbr, q, a, tab, kk, gg);
+    };
     for (int q = 0; q < 2; ++q) {
       uint32_t* X = q ? WO : WE;
       const uint32_t* Y = q ? WE : WO;
       for (int c = 0; c < a.ncol; ++c) {
         if constexpr (CL) {
           cg::cluster_group cl = cg::this_cluster();
-          nflip += split_range<D>(co[c], cb[c], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
+          nflip += range(co[c], cb[c], X, Y, q);
           cluster_wait();
           if (prev_c >= 0) {
             uint32_t* P = prev_q ? WO : WE;
@@ -286,13 +337,13 @@ __global__ void __launch_bounds__(kSplitMaxThreads) sqa_split_kernel(SplitArgs a
             }
           }
           __syncthreads();
-          nflip += split_range<D>(cb[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
+          nflip += range(cb[c], co[c + 1], X, Y, q);
           cluster_arrive();
           __syncthreads();
           prev_c = c;
           prev_q = q;
         } else {
-          nflip += split_range<D>(co[c], co[c + 1], X, Y, gid, jm, nbr, q, a, tab, kk, gg);
+          nflip += range(co[c], co[c + 1], X, Y, q);
           __syncthreads();
         }
       }

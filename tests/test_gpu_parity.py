@@ -237,6 +237,46 @@ def test_sqa_bitpacked_bit_exact(ctx, T, R, which):
         assert e[best[r]] == pytest.approx(e.min(), abs=1e-9)
 
 
+def _trotter_dominated(mode, D):
+    """Per sweep: no live class with no aligned Trotter neighbour, and none with
+    one aligned neighbour and u >= ceil(D/2) (the slice-split kernel's shorter
+    threshold-plane evaluation applies)."""
+    bad = 0
+    for u in range(D + 1):
+        bad |= 1 << (3 * u)
+        if u >= (D + 1) // 2:
+            bad |= 1 << (3 * u + 1)
+    live = np.asarray(mode).reshape(-1, 2)[:, 1]
+    return [(int(v) & bad) == 0 for v in live]
+
+
+@pytest.mark.parametrize("which,T,beta", [("regular3", 4, 10.0), ("lattice", 8, 20.0), ("regular3", 32, 10.0)])
+def test_sqa_slice_split_both_threshold_evaluations(ctx, which, T, beta):
+    """Sweeps where the Trotter term makes every class without an aligned
+    Trotter neighbour accept (the kernel then reads the threshold planes from
+    fewer table words) and sweeps where it does not, in one run: the replay's
+    spins either way."""
+    if which == "lattice":
+        m, D = I.lattice_pm_j(24, seed=14)[0], 4
+    else:
+        m, D = I.random_regular_pm_j(600, 3, seed=15)[0], 3
+    g, dg = _graph(ctx, m)
+    nsched = 12
+    ss = np.concatenate([np.linspace(0.0, 0.9, nsched // 2), np.linspace(0.95, 0.0, nsched // 2)])
+    betas = np.full(nsched, beta)
+    mcs = np.ones(nsched, np.int32)
+    a, b = O.sqa_coefficients(betas, ss, 1.0, T)
+    _, mode = O.sqa_msc_thresholds(a, b, 1.0, D)
+    dom = _trotter_dominated(mode, D)
+    if T < 32:
+        assert any(dom) and not all(dom), dom
+    s0 = np.random.default_rng(8).choice(np.array([-1, 1], np.int8), size=(9, T, g.n))
+    s = s0.copy()
+    st = N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=17, kernel="bitpacked")
+    assert st["kernel"] == "bitpacked"
+    np.testing.assert_array_equal(s, _sqa_bitpacked_replay(g, s0, betas, ss, mcs, 1.0, D, 17))
+
+
 @pytest.mark.parametrize("cluster", [None, "3", "16"])
 @pytest.mark.parametrize("which,T,R", [("lattice", 16, 4), ("regular3", 8, 20), ("regular3", 32, 6)])
 def test_sqa_slice_split_clusters(ctx, monkeypatch, cluster, which, T, R):
