@@ -313,6 +313,13 @@ cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, co
     ++*launches;
     kstart = fc.kstart;
   }
+  if (K > 0 && p.b->max_n <= 128 && p.b->d_q32.ptr) {
+    // one-chunk instances: the sweep kernel sets the fields anew itself at the
+    // same global sweeps (and checks the drift after the last one), in one launch
+    return launch_batch_sweeps(p.b, p.d_reads, p.d_soff, p.d_items, p.nitems, p.d_counter, p.spins, p.d_betas, S, rb,
+                               p.inst0, ctx->sm_count, st, launches, p.variant, p.d_fields, p.d_foff, p.d_energies,
+                               p.d_eoff, wf, fc.status, fc.wait_limit, nullptr, (int)K, wf ? fc.drift : nullptr);
+  }
   int64_t k = 0;
   while (k < S) {
     const uint64_t g = (uint64_t)rb.sweep0 + (uint64_t)k;

@@ -31,6 +31,7 @@ oj_batch::~oj_batch() {
   d_dig.release();
   d_dtoff.release();
   d_uexp.release();
+  d_q32.release();
   if (cur >= 0 && cur != device) cudaSetDevice(cur);
 }
 

@@ -143,6 +143,10 @@ struct oj_batch {
   // tensor-core field kernel (oj_k_field_tc.cu): ndig digits per coupling
   oj::DevBuf d_dig, d_dtoff, d_uexp;
   int ndig = 0;
+  // batches of one-chunk instances (max_n <= 128) with four digits: the grid
+  // integers q as int32, [n][128] at joff[m] (element [i][j] = q_ji), for the
+  // recompute inside sa_batch1_kernel
+  oj::DevBuf d_q32;
   ~oj_batch();
 };
 
@@ -262,7 +266,7 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
                                 cudaStream_t st, int* launches, int variant, float* d_fields,
                                 const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
                                 bool write_fields, int* d_status, long long wait_limit,
-                                const int32_t* kstart = nullptr);
+                                const int32_t* kstart = nullptr, int recompute = 0, unsigned int* d_drift = nullptr);
 cudaError_t launch_batch_energy(const oj_batch* b, const int32_t* d_reads, const int64_t* d_soff,
                                 const int64_t* d_eoff, const int32_t* d_order, int max_reads, const int8_t* spins,
                                 double* out, cudaStream_t st, int nsplit, double* parts, int64_t nrep);

@@ -84,6 +84,15 @@ struct BatchArgs {
   int* status;             // set when a bounded wait runs out
   long long wait_limit;    // iterations of the staging wait
   const int32_t* kstart;   // per replica (eoff[m] + r): the first sweep to run, or null (0)
+  // one-chunk kernel: the fields set anew from the grid integers q (int32,
+  // [n][128] at joff[m], element [i][j] = q_ji) before every global sweep that
+  // is a multiple of recompute (0: never), as the tensor-core field kernel sets
+  // them; with drift, the largest |f - f_exact| over those points and the end
+  // of the run goes there (float bits) and the final fields are the exact ones
+  const int32_t* Q;
+  const int32_t* uexp;
+  int recompute;
+  unsigned int* drift;
 };
 
 constexpr long long kStageDrainLimit = 1ll << 26;
@@ -349,6 +358,59 @@ __global__ void __launch_bounds__(W * 32, MINB) sa_batch_kernel(BatchArgs a) {
 // in shared memory by every work item, so that a flip is a ballot, a shuffle,
 // one shared-memory row load and four FMAs.  Same random stream, acceptance
 // test, skipping of chunks that cannot flip and FMA order, so the same bits.
+// The exact fields of this lane's four sites (4 lane .. 4 lane + 3) of a
+// one-chunk instance: f_j = fp32(fp64(h_j) + 2^e sum_i q_ji s_i), the sum in
+// int64 (exact), the same operations as the tensor-core field kernel's
+// epilogue, so the same values.  wd: this lane's spin bits (set: -1).
+__device__ __forceinline__ float4 exact_fields1(const int32_t* __restrict__ Qm, int n, uint32_t wd, double scale,
+                                                const float4 h4) {
+  const int lane = threadIdx.x & 31;
+  long long acc[4] = {0, 0, 0, 0};
+  // two source lanes (8 rows) a pass, their row loads issued together; |q| <=
+  // 2^26, so the 8-row partial sums fit int32
+  for (int L0 = 0; 4 * L0 < n; L0 += 2) {
+    int4 q[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int i = 4 * L0 + t;
+      q[t] = i < n ? __ldg(reinterpret_cast<const int4*>(Qm + (size_t)i * 128) + lane) : make_int4(0, 0, 0, 0);
+    }
+    int p[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const uint32_t w = __shfl_sync(0xffffffffu, wd, (L0 + l) & 31);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int4 v = q[4 * l + e];  // zero past n
+        const int sg = ((w >> e) & 1u) ? -1 : 1;
+        p[0] += sg * v.x;
+        p[1] += sg * v.y;
+        p[2] += sg * v.z;
+        p[3] += sg * v.w;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[e] += p[e];
+  }
+  const float hv[4] = {h4.x, h4.y, h4.z, h4.w};
+  float f[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    f[e] = __double2float_rn(__dadd_rn((double)hv[e], __dmul_rn(__ll2double_rn(acc[e]), scale)));
+  return make_float4(f[0], f[1], f[2], f[3]);
+}
+
+// Largest |f - g| over this lane's sites below n.
+__device__ __forceinline__ float field_gap(const float4 f, const float4 g, int n) {
+  const int lane = threadIdx.x & 31;
+  const float a[4] = {f.x, f.y, f.z, f.w}, b[4] = {g.x, g.y, g.z, g.w};
+  float d = 0.0f;
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    if (4 * lane + e < n) d = fmaxf(d, fabsf(a[e] - b[e]));
+  return d;
+}
+
 template <int W, bool H>
 __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float shb[];  // [n][128] couplings of the item's instance
@@ -389,8 +451,17 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
     const __half* Js16 = reinterpret_cast<const __half*>(shb) + 4 * lane;
     const uint32_t tag = ((a.inst0 + (uint32_t)m) << 8) | ojd::TAG_BATCH;
     const uint32_t rg = a.rep0 + (uint32_t)r;
+    const int32_t* Qm = a.Q ? a.Q + a.joff[m] : nullptr;
+    const double qscale = Qm ? ldexp(1.0, a.uexp[m]) : 0.0;
+    const float4 h4q = Qm ? ldg4(a.h + a.hoff[m] + 4 * lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+    float dmax = 0.0f;
     for (int64_t k = 0; k < a.nsweeps; ++k) {
       const float beta2 = 2.0f * __ldg(a.betas + k);
+      if (Qm && k > 0 && (a.sweep0 + (uint32_t)k) % (uint32_t)a.recompute == 0u) {
+        const float4 fx = exact_fields1(Qm, n, wd, qscale, h4q);
+        if (a.drift) dmax = fmaxf(dmax, field_gap(fc, fx, n));
+        fc = fx;
+      }
       {
         // no site below the largest -ln u: the chunk keeps its state
         const float fv[4] = {fc.x, fc.y, fc.z, fc.w};
@@ -435,6 +506,15 @@ __global__ void __launch_bounds__(W * 32) sa_batch1_kernel(BatchArgs a) {
         if (lane == 0) ++nflip;
         open = inside & (0xFu << min(max(i + 1 - 4 * lane, 0), 4));
       }
+    }
+    if (Qm && a.drift) {
+      // the drift check after the last sweep; the exact fields are kept
+      const float4 fx = exact_fields1(Qm, n, wd, qscale, h4q);
+      dmax = fmaxf(dmax, field_gap(fc, fx, n));
+      fc = fx;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+      if (lane == 0 && dmax > 0.0f) atomicMax(a.drift, __float_as_uint(dmax));
     }
     if (a.Fw) *reinterpret_cast<float4*>(a.Fw + a.foff[m] + (size_t)r * 128 + 4 * lane) = fc;
     if (a.E) {
@@ -621,7 +701,7 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
                                 cudaStream_t st, int* launches, int variant, float* d_fields,
                                 const int64_t* d_foff, double* d_energies, const int64_t* d_eoff,
                                 bool write_fields, int* d_status, long long wait_limit,
-                                const int32_t* kstart) {
+                                const int32_t* kstart, int recompute, unsigned int* d_drift) {
   if (variant == 0) variant = batch_default_variant();
   if (!batch_variant_valid(variant) || b->max_n > batch_variant_max_n(variant)) return cudaErrorInvalidValue;
   if (b->count == 0 || nitems <= 0 || nsweeps <= 0) return cudaSuccess;
@@ -657,6 +737,11 @@ cudaError_t launch_batch_sweeps(const oj_batch* b, const int32_t* d_reads, const
   a.status = d_status;
   a.wait_limit = wait_limit >= 0 ? wait_limit : kStageDrainLimit;
   a.kstart = kstart;
+  const bool own = recompute > 0 && b->max_n <= 128 && b->d_q32.ptr && !b->exact_fields;
+  a.Q = own ? b->d_q32.as<int32_t>() : nullptr;
+  a.uexp = own ? b->d_uexp.as<int32_t>() : nullptr;
+  a.recompute = own ? recompute : 0;
+  a.drift = own ? d_drift : nullptr;
   cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   if (b->max_n <= 128) {

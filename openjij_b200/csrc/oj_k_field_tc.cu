@@ -135,13 +135,19 @@ __host__ __device__ __forceinline__ uint32_t canon(int row, int k) {
 
 template <int D, int NT>
 struct FieldShape {
-  static constexpr uint32_t kA = D * kTileBytes;         // digit tiles of one K chunk
-  static constexpr uint32_t kB = NT * kChunk;            // spin tile of one K chunk
+  // digits per stage: four-digit tiles with at most 256 accumulator columns go
+  // two digits a stage, so that two CTAs share an SM (one's prologue and
+  // epilogue overlap the other's copies); a K chunk is then two stages
+  static constexpr int DS = (D > 1 && D * NT <= 256) ? 2 : D;
+  static constexpr int H = D / DS;                       // stages per K chunk
+  static constexpr uint32_t kA = DS * kTileBytes;        // digit tiles of one stage
+  static constexpr uint32_t kB = NT * kChunk;            // spin tile of the stage's K chunk
   static constexpr uint32_t kStage = (kA + kB + 1023) / 1024 * 1024;
-  // stages in the ring: four-digit tiles stream from DRAM and want several
-  // chunks in flight (three when 220 KB hold them); one-digit tiles keep two,
-  // so that two CTAs share an SM and one's epilogue overlaps the other's loop
-  static constexpr int kStages = (D > 1 && 3u * kStage <= 220u * 1024u) ? 3 : 2;
+  // stages in the ring: two-digit stages as many as fit 110 KB (two CTAs an
+  // SM), other four-digit tiles three when 220 KB hold them; one-digit tiles
+  // keep two, so that two CTAs share an SM
+  static constexpr int kStages = DS < D ? (3u * kStage <= 110u * 1024u ? 3 : 2)
+                                        : ((D > 1 && 3u * kStage <= 220u * 1024u) ? 3 : 2);
   static constexpr uint32_t kCols = D * NT <= 32 ? 32 : (D * NT <= 64 ? 64 : (D * NT <= 128 ? 128 : (D * NT <= 256 ? 256 : 512)));
   static constexpr size_t kSmem = kStages * (size_t)kStage + 16 * kStages + 16;  // mbarriers, TMEM slot, abort flag
 };
@@ -175,8 +181,8 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tslot;
-  // Ring of ST stages: the digit tiles of chunk kc + ST - 1 are copied while
-  // chunk kc's spins are written and its MMAs run.  Pipeline waits use
+  // Ring of ST stages: the digit tiles of unit u + ST - 1 are copied while
+  // unit u's spins are written and its MMAs run.  Pipeline waits use
   // a.wait_limit; one that runs out aborts the loop: no new copies or MMAs are
   // issued, the ones in flight are waited for with the default limit
   // (kDrainLimit), tensor memory is freed and F is left as it was.
@@ -188,22 +194,27 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
   const int8_t* dig = a.digits + a.dtoff[m];
   const int8_t* sp = a.spins + a.soff[m];
   const int r0 = nt * NT;
-  // digit tiles of chunk kc into stage kc % ST (thread 0; the stage is free)
-  auto issue_a = [&](int kc) {
-    const int s = kc % ST;
+  // unit u = (K chunk u / H, digits (u % H) DS .. + DS - 1) is one stage
+  constexpr int H = S::H, DS = S::DS;
+  const int nu = nch * H;
+  // digit tiles of unit u into stage u % ST (thread 0; the stage is free)
+  auto issue_a = [&](int u) {
+    const int s = u % ST, kc = u / H, t0 = (u % H) * DS;
     unsigned char* As = sm + s * S::kStage;
     ojd::mbar_expect_tx(bar + s, S::kA);
 #pragma unroll
-    for (int t = 0; t < D; ++t)
-      bulk_copy(As + t * kTileBytes, dig + ((size_t)(t * nch + mt) * nch + kc) * kTileBytes, kTileBytes, bar + s);
+    for (int tt = 0; tt < DS; ++tt)
+      bulk_copy(As + tt * kTileBytes, dig + ((size_t)((t0 + tt) * nch + mt) * nch + kc) * kTileBytes, kTileBytes,
+                bar + s);
     pend_full |= 1u << s;
   };
   // spins of replicas r0..r0+NT-1 at sites 128 kc .. +127 into stage kc % ST
   // (every thread; the stage is free), 16 bytes a piece: asynchronous copies
   // where the piece is 16- or 4-byte aligned, else byte loads; zero past the
   // instance's reads and sites.  One commit group per call.
-  auto issue_b = [&](int kc) {
-    unsigned char* Bs = sm + (kc % ST) * S::kStage + S::kA;
+  auto issue_b = [&](int u) {
+    const int kc = u / H;
+    unsigned char* Bs = sm + (u % ST) * S::kStage + S::kA;
     for (int idx = tid; idx < NT * 8; idx += kFieldThreads) {
       const int rr = idx >> 3, pc = idx & 7;
       const int r = r0 + rr, k = kc * kChunk + 16 * pc;
@@ -235,18 +246,18 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
     cp_async_commit();
   };
   if (tid == 0)
-    for (int kc = 0; kc < ST - 1 && kc < nch; ++kc) issue_a(kc);
-  for (int kc = 0; kc < ST - 1; ++kc) {
-    if (kc < nch) issue_b(kc);
+    for (int u = 0; u < ST - 1 && u < nu; ++u) issue_a(u);
+  for (int u = 0; u < ST - 1; ++u) {
+    if (u < nu) issue_b(u);
     else cp_async_commit();  // an empty group keeps the count per chunk
   }
-  for (int kc = 0; kc < nch; ++kc) {
-    const int s = kc % ST;
+  for (int u = 0; u < nu; ++u) {
+    const int s = u % ST, kc = u / H, t0 = (u % H) * DS;
     unsigned char* As = sm + s * S::kStage;
     unsigned char* Bs = As + S::kA;
-    if (tid == 0 && kc + ST - 1 < nch) {
-      // the stage of chunk kc + ST - 1 last held chunk kc - 1: its MMAs first
-      const int sn = (kc + ST - 1) % ST;
+    if (tid == 0 && u + ST - 1 < nu) {
+      // the stage of unit u + ST - 1 last held unit u - 1: its MMAs first
+      const int sn = (u + ST - 1) % ST;
       if ((pend_done >> sn) & 1u) {
         if (mbar_wait(bar + ST + sn, (ph_done >> sn) & 1u, a.wait_limit)) {
           ph_done ^= 1u << sn;
@@ -255,13 +266,13 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
           *abort_flag = 1;
         }
       }
-      if (!*abort_flag) issue_a(kc + ST - 1);
+      if (!*abort_flag) issue_a(u + ST - 1);
     }
-    __syncthreads();  // the stage of chunk kc + ST - 1 is free (chunk kc - 1's MMAs were seen complete)
+    __syncthreads();  // the stage of unit u + ST - 1 is free (unit u - 1's MMAs were seen complete)
     if (*abort_flag) break;
-    if (kc + ST - 1 < nch) issue_b(kc + ST - 1);
+    if (u + ST - 1 < nu) issue_b(u + ST - 1);
     else cp_async_commit();
-    cp_async_wait<ST - 1>();  // this thread's copies of chunk kc's spins have landed
+    cp_async_wait<ST - 1>();  // this thread's copies of unit u's spins have landed
     proxy_fence();
     tc_fence_before();
     __syncthreads();
@@ -272,10 +283,10 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
         tc_fence_after();
         const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
 #pragma unroll
-        for (int t = 0; t < D; ++t)
+        for (int tt = 0; tt < DS; ++tt)
 #pragma unroll
           for (int kk = 0; kk < kChunk / 32; ++kk)
-            mma_i8(tbase + (uint32_t)(t * NT), desc_kmajor(a0 + t * kTileBytes + kk * 256, 128, 1024),
+            mma_i8(tbase + (uint32_t)((t0 + tt) * NT), desc_kmajor(a0 + tt * kTileBytes + kk * 256, 128, 1024),
                    desc_kmajor(b0 + kk * 256, 128, 1024), idesc_i8(NT), (kc | kk) ? 1u : 0u);
         mma_commit(bar + ST + s);
         pend_done |= 1u << s;
@@ -323,6 +334,13 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
 #pragma unroll
       for (int j = 0; j < 16; ++j) tot[j] += (long long)acc[j] * (1ll << (7 * t));
     }
+    // compare mode: the sweep kernel's fields of the 16 replicas, all loaded
+    // before any store (no load waits behind the previous replica's store)
+    float old[16];
+    if (a.compare && site < n) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) old[j] = r0 + j0 + j < R ? Fm[(size_t)(r0 + j0 + j) * npad] : 0.0f;
+    }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int r = r0 + j0 + j;
@@ -332,7 +350,7 @@ __global__ void __launch_bounds__(kFieldThreads, 1) field_tc_kernel(FieldArgs a)
       const float f = D == 1 ? __fadd_rn(hf, __fmul_rn(__ll2float_rn(tot[j]), scale_f))
                              : __double2float_rn(__dadd_rn(hv, __dmul_rn(__ll2double_rn(tot[j]), scale)));
       float* dst = Fm + (size_t)r * npad;
-      if (a.compare && site < n) dmax = fmaxf(dmax, fabsf(f - *dst));
+      if (a.compare && site < n) dmax = fmaxf(dmax, fabsf(f - old[j]));
       *dst = f;
     }
   }
@@ -441,6 +459,10 @@ cudaError_t field_tc_prepare(oj_batch* b, const std::vector<float>& J32, const s
     total += (int64_t)D * nch * nch * kTileBytes;
   }
   std::vector<int8_t> tiles((size_t)std::max<int64_t>(total, 16), 0);
+  // one-chunk batches with four digits also keep q as int32 for the sweep
+  // kernel's own recompute (sa_batch1_kernel)
+  const bool q32 = D == 4 && b->max_n <= kChunk;
+  std::vector<int32_t> Q(q32 ? std::max<size_t>(J32.size(), 4) : 0, 0);
   for (int m = 0; m < count; ++m) {
     const int n = b->n[m];
     if (n == 0) continue;
@@ -467,6 +489,7 @@ cudaError_t field_tc_prepare(oj_batch* b, const std::vector<float>& J32, const s
           continue;
         }
         int64_t q = (int64_t)std::nearbyint(std::ldexp((double)Jm[(size_t)j * npad + i], -e));
+        if (q32) Q[(size_t)joff[m] + (size_t)i * npad + j] = (int32_t)q;  // element [i][j] = q_ji
         for (int t = 0; t < 4; ++t) {
           const int64_t d = ((q + 64) & 127) - 64;
           q = (q - d) >> 7;
@@ -476,6 +499,10 @@ cudaError_t field_tc_prepare(oj_batch* b, const std::vector<float>& J32, const s
   }
   b->ndig = D;
   cudaError_t err;
+  if (q32) {
+    if ((err = b->d_q32.ensure(Q.size() * 4)) != cudaSuccess) return err;
+    if ((err = cudaMemcpy(b->d_q32.ptr, Q.data(), Q.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess) return err;
+  }
   if ((err = b->d_dig.ensure(tiles.size())) != cudaSuccess) return err;
   if ((err = cudaMemcpy(b->d_dig.ptr, tiles.data(), tiles.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return err;
   if ((err = b->d_dtoff.ensure(dtoff.size() * 8)) != cudaSuccess) return err;

@@ -51,6 +51,50 @@ def test_recompute_and_drift_match_replay(K):
     ctx.close()
 
 
+@pytest.mark.parametrize("K", [16, 5])
+def test_one_chunk_batch_recomputes_in_the_sweep_kernel(K):
+    """Instances of at most 128 sites run in the one-chunk kernel, which sets
+    the fields anew itself (int64 sums of the grid integers) at the same global
+    sweeps: spins and drift equal the replay's, and a run split over two calls
+    at a multiple of K equals the whole run."""
+    ctx = N.Context(0)
+    ctx.set_field_recompute(K)
+    sizes = [7, 100, 128, 64, 33]
+    reads = [3, 40, 9, 17, 70]
+    mats = _normal_batch(sizes, 120)
+    b = N.Batch(ctx, mats)
+    betas, mcs = I.geometric_betas(0.1, 8.0, 3 * K + 4)
+    s0 = _spins(mats, reads, 9)
+    s = s0.copy()
+    st = N.sa_run_batched(b, reads, s, betas, mcs, seed=31)
+    ref, drift = O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), 31, recompute=K, drift=True)
+    np.testing.assert_array_equal(s, ref)
+    assert st["field_drift"] == float(drift.max())
+    assert 0.0 < st["field_drift"] < 1e-2
+    part = s0.copy()
+    N.sa_run_batched(b, reads, part, betas[:2 * K], mcs[:2 * K], seed=31)
+    N.sa_run_batched(b, reads, part, betas[2 * K:], mcs[2 * K:], seed=31, first_sweep=2 * K)
+    np.testing.assert_array_equal(part, ref)
+    b.close()
+    ctx.close()
+
+
+def test_dense_jump_n100_real_couplings_drift(ctx):
+    """The benchmark's 100-spin dense instance (uniform couplings) on the
+    dense-jump path: the one-chunk kernel with its own recompute."""
+    m, _ = I.dense_ising_uniform(100, seed=1)
+    g = O.AugCSR(m)
+    dg = N.Graph(ctx, g.n, g.indptr, g.indices, g.data)
+    betas, mcs = I.geometric_betas(0.1, 10.0, 70)
+    s0 = np.random.default_rng(11).choice(np.array([-1, 1], np.int8), size=(100, g.n))
+    s = s0.copy()
+    st = N.sa_run(dg, s, betas, mcs, seed=5, kernel="dense_jump")
+    ref, drift = O.replay_sa_batch([m.toarray()], [100], s0.ravel(), _per_sweep(betas, mcs), 5, drift=True)
+    np.testing.assert_array_equal(s, ref.reshape(100, g.n))
+    assert st["field_drift"] == float(drift.max())
+    assert st["launches"] <= 4  # no launch per recompute
+
+
 def test_exact_batches_report_no_drift(ctx):
     mats = [I.dense_qubo_int(n, seed=n)[0].toarray() for n in (100, 260)]
     reads = [5, 33]
