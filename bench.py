@@ -672,6 +672,16 @@ def run_ours(args):
         key = "sa_msc_kernel" if w["kind"] == "sa" else "sqa_split_kernel"
         roof = _roofline_issue(key, attempts_per_step, kms, clk_sum, sm_count, side)
         roof["traffic"] = _traffic_from_profiles() if args.config == 2 else None
+    elif used_kernel == "colour" and _issue_profile("sa_colour_kernel" if w["kind"] == "sa" else "sqa_colour_kernel"):
+        # the int8 state and CSR stay in L2 on these lattices (DRAM idle): issue
+        # bound, the HBM figure of the algorithmic bytes as a side number
+        hbm = attempts_per_step * per / (kms / 1000.0) / 1e9
+        side = {"achieved_gbs": hbm, "peak_gbs": hbm_peak, "frac": hbm / hbm_peak, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_attempt": per,
+                "note": "int8 state and CSR bytes per attempt against the HBM copy peak; the lattice stays in L2"}
+        key = "sa_colour_kernel" if w["kind"] == "sa" else "sqa_colour_kernel"
+        roof = _roofline_issue(key, attempts_per_step, kms, clk_sum, sm_count, side)
+        roof["traffic"] = None
     elif used_kernel in ("dense_jump", "dense_plain", "dense_tc"):
         acc = float(np.mean(acc_steps))
         roof = _roofline_fp32(acc * 2.0 * n, kms, clk_sum, sm_count,

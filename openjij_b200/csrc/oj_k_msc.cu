@@ -185,8 +185,9 @@ __device__ __forceinline__ uint32_t msc_range(int lo, int hi, uint32_t* __restri
 }
 
 // Shared memory: words[slots] | gid[nlocmax] | jm[nlocmax] | nbr[nlocmax][D]
-template <int D>
-__global__ void __launch_bounds__(kMscMaxThreads) sa_msc_kernel(MscArgs a) {
+// MAXT: the launch bound (512: up to 128 registers a thread; 1024: 64).
+template <int D, int MAXT>
+__global__ void __launch_bounds__(MAXT) sa_msc_kernel(MscArgs a) {
   extern __shared__ __align__(16) uint32_t Wsh[];
   cg::cluster_group cl = cg::this_cluster();
   const int p = (int)cl.block_rank();
@@ -256,7 +257,7 @@ int msc_threads() {
 
 template <int D>
 cudaError_t launch_d(const MscPlan& pl, const MscArgs& a, int G, cudaStream_t st, int threads) {
-  auto kern = sa_msc_kernel<D>;
+  auto kern = threads <= 512 ? sa_msc_kernel<D, 512> : sa_msc_kernel<D, kMscMaxThreads>;
   const size_t smem = msc_smem_bytes(pl);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -286,14 +287,19 @@ int msc_max_degree() { return kMscMaxDegree; }
 cudaError_t msc_preload() {
   cudaFuncAttributes fa;
   cudaError_t e = cudaSuccess;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<1>)) != cudaSuccess) return e;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<2>)) != cudaSuccess) return e;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<3>)) != cudaSuccess) return e;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<4>)) != cudaSuccess) return e;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<5>)) != cudaSuccess) return e;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<6>)) != cudaSuccess) return e;
-  if ((e = cudaFuncGetAttributes(&fa, sa_msc_kernel<7>)) != cudaSuccess) return e;
-  return cudaFuncGetAttributes(&fa, sa_msc_kernel<8>);
+  auto load = [&](auto k512, auto k1024) {
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k512);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k1024);
+  };
+  load(sa_msc_kernel<1, 512>, sa_msc_kernel<1, kMscMaxThreads>);
+  load(sa_msc_kernel<2, 512>, sa_msc_kernel<2, kMscMaxThreads>);
+  load(sa_msc_kernel<3, 512>, sa_msc_kernel<3, kMscMaxThreads>);
+  load(sa_msc_kernel<4, 512>, sa_msc_kernel<4, kMscMaxThreads>);
+  load(sa_msc_kernel<5, 512>, sa_msc_kernel<5, kMscMaxThreads>);
+  load(sa_msc_kernel<6, 512>, sa_msc_kernel<6, kMscMaxThreads>);
+  load(sa_msc_kernel<7, 512>, sa_msc_kernel<7, kMscMaxThreads>);
+  load(sa_msc_kernel<8, 512>, sa_msc_kernel<8, kMscMaxThreads>);
+  return e;
 }
 int msc_default_threads() { return msc_threads(); }
 
