@@ -735,6 +735,8 @@ def run_ours(args):
             # time to 1 % of the best energy, batched / mixed against the plain
             # single-instance FP32 kernel (configs 3-5), outside the timed region
             line["time_to_1pct"] = tts_summary()
+        if ws == 1 and not args.no_others and args.config == 2 and kernel == w["kernel"] and args.sweeps is None:
+            line["other_configs"] = other_configs_summary()
         print(json.dumps(line), flush=True)
     graph.close()
     ctx.close()
@@ -780,6 +782,32 @@ def tts_summary():
                              "plain_t99_ms": d["plain"]["t99_ms"], "plain_kernel": d["plain"].get("kernel", "dense_plain"),
                              "plain_num_sweeps": d["plain"]["num_sweeps"],
                              "plain_over_batched": d["plain_over_batched"]}
+    return out
+
+
+def other_configs_summary(steps=5, warmup=3):
+    """Throughput of configs 1 and 3-6, each measured by this script in a
+    process of its own (same timing rules, no CPU leg), after the default
+    line's timed region: per config the workload, kernel, attempts/s, step
+    and kernel times, end-to-end attempts/s and the roofline's bound and
+    fraction."""
+    import subprocess
+    out = {}
+    for c in (1, 3, 4, 5, 6):
+        cmd = [sys.executable, os.path.abspath(__file__), "--config", str(c), "--steps", str(steps),
+               "--warmup", str(warmup), "--no-cpu", "--no-tts"]
+        try:
+            res = subprocess.run(cmd, capture_output=True, text=True, timeout=600, check=True)
+            d = [json.loads(l) for l in res.stdout.splitlines() if l.startswith("{")][-1]
+        except Exception as ex:  # a failed config is reported, not hidden
+            out[f"config{c}"] = {"error": str(ex)[:200]}
+            continue
+        r = d.get("roofline") or {}
+        out[f"config{c}"] = {"workload": d["config"]["workload"], "kernel": d["kernel"]["name"],
+                             "value": d["value"], "unit": d["unit"], "ms_per_step": d["ms_per_step"],
+                             "kernel_ms": r.get("kernel_ms"), "e2e": d["e2e"]["value"],
+                             "roofline_bound": r.get("bound"), "roofline_frac": r.get("frac"),
+                             "field_drift": r.get("field_drift"), "clocks": d.get("clocks")}
     return out
 
 
@@ -926,6 +954,8 @@ def main():
                          "FP32 sums are not exact (default: the library's, 16; 0 = only at the start of a call)")
     ap.add_argument("--no-tts", action="store_true",
                     help="leave the configs 3-5 time-to-1%% comparison out of the default line")
+    ap.add_argument("--no-others", action="store_true",
+                    help="leave the configs 1 and 3-6 throughput summary out of the default line")
     ap.add_argument("--tts", action="store_true",
                     help="time-to-1%%-energy of the batched/mixed kernel vs the plain kernel (configs 3-5)")
     args = ap.parse_args()
