@@ -291,9 +291,8 @@ struct SweepPlan {
 // run split over calls at such multiples); with `measure`, the sweep kernel
 // stores its incremental fields before each recompute and after the last
 // sweep, and the field kernel records their largest deviation (the drift).
-cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, const FieldCall& fc, bool measure,
-                      int* launches) {
-  cudaStream_t st = ctx->stream;
+cudaError_t run_batch_enqueue(oj_ctx* ctx, cudaStream_t st, const SweepPlan& p, int64_t S, RngBase rb,
+                              const FieldCall& fc, bool measure, int* launches) {
   const bool exact = p.b->exact_fields;
   const bool wf = measure && !exact;
   cudaError_t e = launch_field_tc(p.b, p.d_reads, p.d_soff, p.spins, p.d_fields, p.d_foff, fc.items, fc.nitems, fc.NT,
@@ -339,6 +338,58 @@ cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, co
       ++*launches;
     }
   }
+  return cudaSuccess;
+}
+
+// A batched / dense-jump run as one CUDA graph: the launches are captured on
+// the context's graph stream (after the work already queued on its stream),
+// the kept executable graph is updated to the capture (or instantiated anew
+// when the launch sequence changed), replayed, and the context's stream waits
+// for it.  OJ_GRAPH=0 in the environment enqueues the launches directly.  A
+// capture that fails is not retried as direct launches: the error is the
+// run's.
+cudaError_t run_batch(oj_ctx* ctx, const SweepPlan& p, int64_t S, RngBase rb, const FieldCall& fc, bool measure,
+                      int* launches) {
+  const char* env = std::getenv("OJ_GRAPH");
+  if (env && env[0] == '0') return run_batch_enqueue(ctx, ctx->stream, p, S, rb, fc, measure, launches);
+  cudaError_t e = cudaSuccess;
+  if (!ctx->gstream && (e = cudaStreamCreateWithFlags(&ctx->gstream, cudaStreamNonBlocking)) != cudaSuccess)
+    return e;
+  for (auto& ev : ctx->gev)
+    if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+  const cudaStream_t gs = ctx->gstream;
+  if ((e = cudaEventRecord(ctx->gev[0], ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(gs, ctx->gev[0], 0)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamBeginCapture(gs, cudaStreamCaptureModeRelaxed)) != cudaSuccess) return e;
+  int nl = 0;
+  const cudaError_t re = run_batch_enqueue(ctx, gs, p, S, rb, fc, measure, &nl);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(gs, &graph);
+  if (re != cudaSuccess || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return re != cudaSuccess ? re : ce;
+  }
+  if (ctx->gexec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(ctx->gexec, graph, &info) != cudaSuccess) {
+      cudaGetLastError();  // another launch sequence: instantiate anew
+      cudaGraphExecDestroy(ctx->gexec);
+      ctx->gexec = nullptr;
+    }
+  }
+  if (!ctx->gexec) e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    ctx->gexec = nullptr;
+    return e;
+  }
+  if ((e = cudaGraphLaunch(ctx->gexec, gs)) != cudaSuccess) return e;
+  if ((e = cudaEventRecord(ctx->gev[1], gs)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(ctx->stream, ctx->gev[1], 0)) != cudaSuccess)
+    return e;
+  *launches += nl;
   return cudaSuccess;
 }
 
@@ -471,6 +522,10 @@ oj_status oj_ctx_destroy(oj_ctx* ctx) {
     ctx->counters.release();
     for (auto& e : ctx->ev)
       if (e) cudaEventDestroy(e);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    for (auto& e : ctx->gev)
+      if (e) cudaEventDestroy(e);
+    if (ctx->gstream) cudaStreamDestroy(ctx->gstream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   }
   delete ctx;

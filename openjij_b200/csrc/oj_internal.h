@@ -164,6 +164,13 @@ struct oj_ctx {
   int recompute = 16;   // full field recompute every this many sweeps (real couplings; 0 = never)
   long long wait_limit = -1;  // iterations of the field kernel's pipeline waits (< 0: the default)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // the launch sequence of a batched / dense-jump run (field kernel, hot-sweep
+  // kernel, the sweep launches between recomputes) is captured as a CUDA graph
+  // on gstream, ordered after and before `stream` by gev, and replayed; the
+  // executable graph is kept and updated in place by the next run's capture
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t gev[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec = nullptr;
 };
 
 namespace oj {

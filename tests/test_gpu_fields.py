@@ -95,6 +95,42 @@ def test_dense_jump_n100_real_couplings_drift(ctx):
     assert st["launches"] <= 4  # no launch per recompute
 
 
+def test_graph_replay_equals_direct_launches(monkeypatch):
+    """A batched run's launches are captured as a CUDA graph and replayed (the
+    executable graph kept and updated by the next call, instantiated anew when
+    the launch sequence changes): calls of different lengths and seeds in a
+    row give the spins, drift and counts of the same calls launched directly
+    (OJ_GRAPH=0)."""
+    sizes = [90, 300, 140]
+    reads = [5, 33, 17]
+    mats = _normal_batch(sizes, 210)
+    s0 = _spins(mats, reads, 12)
+    runs = [(37, 3), (37, 4), (20, 5), (52, 6)]  # sweeps, seed
+
+    def go():
+        ctx = N.Context(0)
+        b = N.Batch(ctx, mats)
+        out = []
+        for S, seed in runs:
+            betas, mcs = I.geometric_betas(0.1, 8.0, S)
+            s = s0.copy()
+            st = N.sa_run_batched(b, reads, s, betas, mcs, seed=seed)
+            out.append((s, st["field_drift"], st["accepted"]))
+        b.close()
+        ctx.close()
+        return out
+
+    monkeypatch.delenv("OJ_GRAPH", raising=False)
+    graph = go()
+    monkeypatch.setenv("OJ_GRAPH", "0")
+    direct = go()
+    for (sg, dg_, ag), (sd, dd, ad), (S, seed) in zip(graph, direct, runs):
+        np.testing.assert_array_equal(sg, sd)
+        assert dg_ == dd and ag == ad
+        betas, mcs = I.geometric_betas(0.1, 8.0, S)
+        np.testing.assert_array_equal(sg, O.replay_sa_batch(mats, reads, s0, _per_sweep(betas, mcs), seed))
+
+
 def test_exact_batches_report_no_drift(ctx):
     mats = [I.dense_qubo_int(n, seed=n)[0].toarray() for n in (100, 260)]
     reads = [5, 33]
