@@ -220,7 +220,15 @@ __global__ void __launch_bounds__(MAXT) sa_msc_kernel(MscArgs a) {
     const MscSweep<D> sw = msc_sweep<D>(a.thr + (size_t)k * (D + 1), a.always[k]);
     const uint32_t kk = a.sweep0 + (uint32_t)k, gg = a.group0 + (uint32_t)g;
     for (int c = 0; c < a.ncol; ++c) {
-      nflip += msc_range<D>(co[c], cb[c], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
+      // the class's sites go in rounds of 2 x blockDim.x (two per thread):
+      // the interior sites of all rounds but the last run before the cluster
+      // wait, the rest of the interior with the boundary sites after the halo
+      // refresh, so that no round is left to the few boundary sites alone
+      // (sites of one class do not read each other: any order gives the same
+      // words)
+      const int step = 2 * (int)blockDim.x, nc = co[c + 1] - co[c];
+      const int split = co[c] + min(cb[c] - co[c], max(0, (nc + step - 1) / step * step - step));
+      nflip += msc_range<D>(co[c], split, Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_wait();
       if (prev >= 0) {
         const int hlo = ho[prev], hhi = ho[prev + 1];
@@ -231,7 +239,7 @@ __global__ void __launch_bounds__(MAXT) sa_msc_kernel(MscArgs a) {
         }
       }
       __syncthreads();
-      nflip += msc_range<D>(cb[c], co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
+      nflip += msc_range<D>(split, co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
       cluster_arrive();
       __syncthreads();
       prev = c;
