@@ -672,6 +672,15 @@ def run_ours(args):
         key = "sa_msc_kernel" if w["kind"] == "sa" else "sqa_split_kernel"
         roof = _roofline_issue(key, attempts_per_step, kms, clk_sum, sm_count, side)
         roof["traffic"] = _traffic_from_profiles() if args.config == 2 else None
+        if packed:
+            # the bit-packed state lives in shared memory: the words the layout
+            # reads and writes per attempt against 128 B per SM and cycle
+            f = _sm_clock_hz(clk_sum)
+            smem_peak = sm_count * 128.0 * f / 1e9
+            smem = attempts_per_step * packed / (kms / 1000.0) / 1e9
+            roof["smem_side"] = {"achieved_gbs": smem, "peak_gbs": smem_peak, "frac": smem / smem_peak,
+                                 "layout_bytes_per_attempt": packed,
+                                 "peak_kind": f"{sm_count} SMs x 128 B x the sampled SM clock ({f / 1e6:.0f} MHz)"}
     elif used_kernel == "colour" and _issue_profile("sa_colour_kernel" if w["kind"] == "sa" else "sqa_colour_kernel"):
         # the int8 state and CSR stay in L2 on these lattices (DRAM idle): issue
         # bound, the HBM figure of the algorithmic bytes as a side number
