@@ -7,15 +7,15 @@
 // in lock step, one 128-site chunk at a time:
 //
 //   * the int32 fields acc[j][r] (F = h + 2^e acc, exact for these batches) of
-//     all n sites of RT = 32 replicas live in tensor memory, chunk c' at
-//     columns 32 c' (lanes = the chunk's sites);
+//     all n sites of RT = 16 replicas live in tensor memory, chunk c' at
+//     columns 16 c' (lanes = the chunk's sites; two CTAs share an SM);
 //   * a chunk is decided replica by replica exactly as the jump kernel decides
 //     it (same uniforms, same acceptance test, same site order, the chunk's own
 //     fields updated after every flip from the diagonal coupling tile in shared
 //     memory), and each replica's spin changes ds in {0, +-2} form one row of
 //     an int8 tile;
 //   * the chunk's changes then reach every field of every replica as int8 MMAs
-//     acc[c'] += J[c', c] ds (tcgen05.mma kind::i8, M = 128 sites, N = 32
+//     acc[c'] += J[c', c] ds (tcgen05.mma kind::i8, M = 128 sites, N = 16
 //     replicas, K = 128), the coupling tiles streamed through a ring of shared-
 //     memory stages by bulk copies (the field kernel's tiles, canonical K-major).
 //
@@ -48,10 +48,10 @@
 namespace oj {
 namespace {
 
-constexpr int kRT = 32;                 // replicas per CTA (MMA N)
+constexpr int kRT = 16;                 // replicas per CTA (MMA N): two CTAs share an SM
 constexpr int kDecWarps = 8;            // deciding warps
 constexpr int kHotThreads = (kDecWarps + 1) * 32;
-constexpr int kStages = 9;              // ring of coupling tiles
+constexpr int kStages = 4;              // ring of coupling tiles
 constexpr int kAhead = kStages - 2;     // tiles in flight ahead of the MMAs
 constexpr int kHotMaxChunks = 16;       // n <= 2048: nch x 32 accumulator columns <= 512
 constexpr uint32_t kTile = 128 * 128;   // one int8 tile
@@ -69,7 +69,7 @@ constexpr uint32_t kOffBar = kOffSw + kRT * kSwWords * 4;    // mbarriers
 constexpr int kNumBars = 2 * kStages + 2 + 1 + 2;            // full, empty, diag, ready, done
 constexpr uint32_t kOffMisc = kOffBar + kNumBars * 8;
 constexpr size_t kHotSmem = kOffMisc + 64;
-static_assert(kHotSmem <= 227 * 1024, "shared memory");
+static_assert(2 * (kHotSmem + 1024) <= 228 * 1024, "two CTAs per SM");
 
 struct HotArgs {
   const int8_t* digits;   // one int8 digit per coupling, tiled (oj_k_field_tc.cu)
@@ -128,31 +128,31 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t (&v)[32]) {
-  uint32_t r[32];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+  uint32_t r[16];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
-      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int j = 0; j < 32; ++j) v[j] = (int32_t)r[j];
+  for (int j = 0; j < 16; ++j) v[j] = (int32_t)r[j];
 }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const int32_t (&v)[32]) {
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const int32_t (&v)[16]) {
   asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
-      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
       "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
-      "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
-      "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
       : "memory");
 }
+
+// one TMEM row of a chunk: the kRT replicas' accumulators of this lane's site
+static_assert(kRT == 16, "the TMEM row accessors move 16 columns");
+__device__ __forceinline__ void tmem_ld_rt(uint32_t taddr, int32_t (&v)[kRT]) { tmem_ld16(taddr, v); }
+__device__ __forceinline__ void tmem_st_rt(uint32_t taddr, const int32_t (&v)[kRT]) { tmem_st16(taddr, v); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -160,7 +160,7 @@ __device__ __forceinline__ void named_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-__global__ void __launch_bounds__(kHotThreads, 1) hot_tc_kernel(HotArgs a) {
+__global__ void __launch_bounds__(kHotThreads, 2) hot_tc_kernel(HotArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int item = blockIdx.x;
   if (item >= a.nitems) return;  // the whole CTA
@@ -221,14 +221,14 @@ __global__ void __launch_bounds__(kHotThreads, 1) hot_tc_kernel(HotArgs a) {
     for (int c = 0; c < nch; ++c) {
       const int s = 128 * c + 32 * warp + lane;
       const float hf = hm[s];  // zero past n
-      int32_t v[32];
+      int32_t v[kRT];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
+      for (int j = 0; j < kRT; ++j) {
         const int r = r0 + j;
         const float f = r < R ? Fm[(size_t)r * npad + s] : hf;
         v[j] = __float2int_rn(__fmul_rn(__fsub_rn(f, hf), inv_scale));
       }
-      tmem_st32(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * kRT), v);
+      tmem_st_rt(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * kRT), v);
     }
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   }
@@ -293,12 +293,12 @@ __global__ void __launch_bounds__(kHotThreads, 1) hot_tc_kernel(HotArgs a) {
         if (warp < 4) {
           if (q > 0 && !ojd::mbar_wait(ready, (uint32_t)((q - 1) & 1), a.wait_limit)) ab[q & 1] = 1;
           tc_fence_after();
-          int32_t v[32];
-          tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * kRT), v);
+          int32_t v[kRT];
+          tmem_ld_rt(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * kRT), v);
           const int s = 32 * warp + lane;
           const float hf = hm[128 * c + s];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) fsm[j * 128 + s] = __fadd_rn(hf, __fmul_rn(__int2float_rn(v[j]), scale));
+          for (int j = 0; j < kRT; ++j) fsm[j * 128 + s] = __fadd_rn(hf, __fmul_rn(__int2float_rn(v[j]), scale));
         }
         if (!ojd::mbar_wait(dfull + b, (uint32_t)((q >> 1) & 1), a.wait_limit)) ab[q & 1] = 1;
         if (q >= 2 && !ojd::mbar_wait(done + b, (uint32_t)(((q - 2) >> 1) & 1), a.wait_limit)) ab[q & 1] = 1;
@@ -462,12 +462,12 @@ __global__ void __launch_bounds__(kHotThreads, 1) hot_tc_kernel(HotArgs a) {
   if (!aborted) {
     if (warp < 4) {
       for (int c = 0; c < nch; ++c) {
-        int32_t v[32];
-        tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * kRT), v);
+        int32_t v[kRT];
+        tmem_ld_rt(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(c * kRT), v);
         const int s = 128 * c + 32 * warp + lane;
         const float hf = hm[s];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < kRT; ++j) {
           const int r = r0 + j;
           if (r < R) Fm[(size_t)r * npad + s] = __fadd_rn(hf, __fmul_rn(__int2float_rn(v[j]), scale));
         }
