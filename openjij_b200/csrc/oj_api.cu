@@ -651,6 +651,19 @@ oj_status oj_graph_query(const oj_graph* g, oj_graph_info* out) {
   return OJ_OK;
 }
 
+// FP64 energies of a graph's spin vectors, the sites split over enough CTAs to
+// cover the SMs (partial sums in the context's buffer, added in order).
+cudaError_t graph_energy(oj_ctx* ctx, const oj_graph* g, int count, const int8_t* d_spins, double* d_e,
+                         cudaStream_t st, int* launches) {
+  const int ns = energy_splits(g, count, ctx->sm_count);
+  if (ns > 1) {
+    const cudaError_t e = ctx->eparts.ensure((size_t)ns * count * 8);
+    if (e != cudaSuccess) return e;
+  }
+  if (launches) *launches += ns > 1 ? 2 : 1;
+  return launch_energy(g, count, d_spins, d_e, st, ns, ns > 1 ? ctx->eparts.as<double>() : nullptr);
+}
+
 oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, const double* betas,
                     const int32_t* mcs, int32_t num_sched, uint64_t seed, int64_t first_sweep,
                     int64_t replica_offset, uint32_t flags, double* energies, oj_run_stats* stats) {
@@ -920,7 +933,8 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       OJ_CK(single_energy(ctx, g, R, d_spins, d_e, st), "energy kernel");
       if (batch_energy_splits(g->single.get(), R, ctx->sm_count) > 1) ++launches;  // the parts' sum
     } else {
-      OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+      OJ_CK(graph_energy(ctx, g, R, d_spins, d_e, st, nullptr), "energy kernel");
+      if (energy_splits(g, R, ctx->sm_count) > 1) ++launches;  // the parts' sum
     }
     ++launches;
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
@@ -1124,8 +1138,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
       OJ_CK(ctx->energies.ensure((size_t)R * T * 8), "alloc energies");
       d_e = ctx->energies.as<double>();
     }
-    OJ_CK(launch_energy(g, R * T, d_spins, d_e, st), "energy kernel");
-    ++launches;
+    OJ_CK(graph_energy(ctx, g, R * T, d_spins, d_e, st, &launches), "energy kernel");
     if (energies && !devp)
       OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * T * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
     if (best_slice) {
@@ -1178,7 +1191,7 @@ oj_status oj_energy(oj_ctx* ctx, const oj_graph* g, int32_t R, const int8_t* spi
     OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
     d_e = ctx->energies.as<double>();
   }
-  OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
+  OJ_CK(graph_energy(ctx, g, R, d_spins, d_e, st, nullptr), "energy kernel");
   if (!devp) {
     OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
     OJ_CK(cudaStreamSynchronize(st), "energy");
@@ -1685,8 +1698,7 @@ oj_status oj_sw_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
       OJ_CK(ctx->energies.ensure((size_t)R * 8), "alloc energies");
       d_e = ctx->energies.as<double>();
     }
-    OJ_CK(launch_energy(g, R, d_spins, d_e, st), "energy kernel");
-    ++launches;
+    OJ_CK(graph_energy(ctx, g, R, d_spins, d_e, st, &launches), "energy kernel");
     if (!devp) OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)R * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
   }
   if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");

@@ -292,8 +292,12 @@ cudaError_t launch_flip_stats(const oj_graph* g, int K, const int8_t* s, double 
                               unsigned long long* amin, cudaStream_t st);
 cudaError_t launch_batch_flip_stats(const oj_batch* b, int K, const int8_t* s, const int64_t* soff, double thr,
                                     double* quad, double* lin, unsigned long long* amin, cudaStream_t st);
+// FP64 energies of `count` spin vectors; the sites split over nsplit CTAs per
+// 32 vectors (energy_splits), the partial sums in parts [nsplit][count] added
+// in a fixed order (nsplit 1: no parts).
+int energy_splits(const oj_graph* g, int count, int sm_count);
 cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out,
-                          cudaStream_t st);
+                          cudaStream_t st, int nsplit = 1, double* parts = nullptr);
 cudaError_t launch_best_slice(const double* energies, int R, int T, int32_t* best, cudaStream_t st);
 
 // Kernel limits used by the planner.

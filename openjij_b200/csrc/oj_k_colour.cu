@@ -179,8 +179,13 @@ __global__ void __launch_bounds__(kEnergyThreads)
     energy_kernel(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                   const double* __restrict__ val, const double* __restrict__ h, int n, int count,
                   const int8_t* __restrict__ spins, double* __restrict__ out) {
+  // CTA (x, y): replicas 32x .. 32x + 31, sites [y n / Y, (y + 1) n / Y); with
+  // Y > 1 the sums go to out[y * count + replica], summed in order of y by
+  // energy_sum_kernel (no dependence on timing)
   extern __shared__ uint32_t wsh[];  // [n] words, then [8][32] partial sums
   const int v0 = blockIdx.x * 32;
+  const int ilo = (int)(((int64_t)blockIdx.y * n) / gridDim.y);
+  const int ihi = (int)(((int64_t)(blockIdx.y + 1) * n) / gridDim.y);
   const int nv = min(32, count - v0);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     uint32_t w = 0;
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(kEnergyThreads)
   double acc[32];
 #pragma unroll
   for (int r = 0; r < 32; ++r) acc[r] = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = ilo + threadIdx.x; i < ihi; i += blockDim.x) {
     const uint32_t wi = wsh[i];
     const double hi = h[i];
 #pragma unroll
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(kEnergyThreads)
   if (threadIdx.x < nv) {
     double t = 0.0;
     for (int w = 0; w < kEnergyThreads / 32; ++w) t += part[w * 32 + threadIdx.x];
-    out[v0 + threadIdx.x] = t;
+    out[(size_t)blockIdx.y * count + v0 + threadIdx.x] = t;
   }
 }
 
@@ -315,17 +320,42 @@ cudaError_t launch_sqa_colour(const oj_graph* g, int R, int T, int8_t* spins, co
   return cudaGetLastError();
 }
 
-cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out, cudaStream_t st) {
+// out[v] = sum over y of parts[y * count + v], y in order.
+__global__ void energy_sum_kernel(const double* __restrict__ parts, int nsplit, int count, double* __restrict__ out) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= count) return;
+  double t = 0.0;
+  for (int y = 0; y < nsplit; ++y) t += parts[(size_t)y * count + v];
+  out[v] = t;
+}
+
+int energy_splits(const oj_graph* g, int count, int sm_count) {
+  // sites split over CTAs until the grid covers the SMs twice (at least 256
+  // sites a CTA)
+  const int groups = (count + 31) / 32;
+  int k = 1;
+  while (k < 16 && groups * k < 2 * sm_count && g->n / (2 * k) >= 256) k *= 2;
+  return k;
+}
+
+cudaError_t launch_energy(const oj_graph* g, int count, const int8_t* spins, double* out, cudaStream_t st,
+                          int nsplit, double* parts) {
   if (count <= 0) return cudaSuccess;
+  if (nsplit < 1 || (nsplit > 1 && !parts)) return cudaErrorInvalidValue;
   const size_t smem = (size_t)((g->n + 1) & ~1) * 4 + (kEnergyThreads / 32) * 32 * 8;
   auto kern = energy_kernel;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  kern<<<(count + 31) / 32, kEnergyThreads, smem, st>>>(g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(),
-                                                        g->d_val64.as<double>(), g->d_h64.as<double>(), g->n,
-                                                        count, spins, out);
+  kern<<<dim3((count + 31) / 32, nsplit), kEnergyThreads, smem, st>>>(
+      g->d_rp.as<int32_t>(), g->d_ci.as<int32_t>(), g->d_val64.as<double>(), g->d_h64.as<double>(), g->n, count,
+      spins, nsplit > 1 ? parts : out);
+  if (nsplit > 1) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    energy_sum_kernel<<<(count + 255) / 256, 256, 0, st>>>(parts, nsplit, count, out);
+  }
   return cudaGetLastError();
 }
 
