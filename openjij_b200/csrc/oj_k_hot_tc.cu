@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(kHotThreads, 2) hot_tc_kernel(HotArgs a) {
   volatile int* ab = reinterpret_cast<volatile int*>(misc + 1);
   unsigned int* sweep_flips = misc + 3;    // [2] flips of the sweep (by parity)
   uint64_t* fin = reinterpret_cast<uint64_t*>(misc + 6);  // 8-byte aligned: completion of every MMA
+  int* jnext = reinterpret_cast<int*>(misc + 8);           // [2] next replica of the chunk step (by parity)
   const int8_t* dig = a.digits + a.dtoff[m];
   const float scale = ldexpf(1.0f, a.uexp[m]);   // 2^e: products stay exact
   const float inv_scale = ldexpf(1.0f, -a.uexp[m]);
@@ -210,6 +211,7 @@ __global__ void __launch_bounds__(kHotThreads, 2) hot_tc_kernel(HotArgs a) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     ab[0] = ab[1] = 0;
     sweep_flips[0] = sweep_flips[1] = 0u;
+    jnext[0] = jnext[1] = 0;
   }
   tc_fence_before();
   __syncthreads();
@@ -303,12 +305,20 @@ __global__ void __launch_bounds__(kHotThreads, 2) hot_tc_kernel(HotArgs a) {
         if (!ojd::mbar_wait(dfull + b, (uint32_t)((q >> 1) & 1), a.wait_limit)) ab[q & 1] = 1;
         if (q >= 2 && !ojd::mbar_wait(done + b, (uint32_t)(((q - 2) >> 1) & 1), a.wait_limit)) ab[q & 1] = 1;
         named_sync(1, kDecWarps * 32);
-        // decide chunk c for replicas warp, warp + 8, ...
+        // the next chunk step's replica counter (its last users passed the
+        // closing barrier of the previous step)
+        if (tid == 0) jnext[(q + 1) & 1] = 0;
+        // decide chunk c: each warp takes the next replica of the tile until
+        // none is left (a warp whose replicas flip little takes more)
         const unsigned char* dg = diag + (size_t)b * kTile;
         unsigned char* Bq = Bt + (size_t)b * kBTile;
         const uint32_t inside = 0xFu >> (4 - min(max(n - 128 * c - 4 * lane, 0), 4));
         unsigned int wflips = 0;
-        for (int j = warp; j < kRT; j += kDecWarps) {
+        for (;;) {
+          int j = 0;
+          if (lane == 0) j = atomicAdd(jnext + (q & 1), 1);
+          j = __shfl_sync(0xffffffffu, j, 0);
+          if (j >= kRT) break;
           const int r = r0 + j;
           uint32_t* swj = swsm + j * kSwWords;
           const uint32_t myw0 = (swj[sw_word(c, lane)] >> sw_shift(c)) & 0xFu;
