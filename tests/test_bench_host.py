@@ -73,3 +73,29 @@ def test_reference_arm_maps_no_product_library():
     assert out.returncode == 0, out.stderr[-2000:]
     tag = [ln for ln in out.stdout.splitlines() if ln.startswith("MAPS")][-1].split()
     assert tag[1:] == ["0", "0", "1"], tag
+
+
+def test_other_configs_summary_reads_each_line_and_reports_failures(monkeypatch):
+    """The default line's configs 1 and 3-6 come from one bench.py process per
+    config: the last JSON line of each is summarised, and a config whose
+    process fails is reported as an error (not left out)."""
+    line = {"config": {"workload": "w"}, "kernel": {"name": "k"}, "value": 2.0, "unit": "attempts/s",
+            "ms_per_step": 1.5, "e2e": {"value": 1.0}, "clocks": {"sm_mhz": 1965.0},
+            "roofline": {"kernel_ms": 1.2, "bound": "issue", "frac": 0.5, "field_drift": None}}
+    seen = []
+
+    def fake_run(cmd, capture_output, text, timeout, check):
+        c = int(cmd[cmd.index("--config") + 1])
+        seen.append(c)
+        assert "--no-cpu" in cmd and "--no-tts" in cmd
+        if c == 4:
+            raise subprocess.CalledProcessError(1, cmd)
+        return subprocess.CompletedProcess(cmd, 0, stdout="noise\n" + json.dumps(line) + "\n", stderr="")
+
+    monkeypatch.setattr(subprocess, "run", fake_run)
+    out = bench.other_configs_summary(steps=2, warmup=3)
+    assert seen == [1, 3, 4, 5, 6]
+    assert set(out) == {"config1", "config3", "config4", "config5", "config6"}
+    assert "error" in out["config4"]
+    assert out["config3"]["value"] == 2.0 and out["config3"]["kernel"] == "k"
+    assert out["config3"]["roofline_bound"] == "issue" and out["config3"]["roofline_frac"] == 0.5
