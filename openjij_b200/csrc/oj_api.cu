@@ -525,6 +525,8 @@ oj_status oj_ctx_destroy(oj_ctx* ctx) {
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     for (auto& e : ctx->gev)
       if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->pev)
+      if (e) cudaEventDestroy(e);
     if (ctx->gstream) cudaStreamDestroy(ctx->gstream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   }
@@ -973,6 +975,16 @@ oj_status oj_sa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int8_t* spins, c
   return OJ_OK;
 }
 
+// The second stream and the events of a two-half run (made once).
+static cudaError_t pipe_streams(oj_ctx* ctx) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->gstream && (e = cudaStreamCreateWithFlags(&ctx->gstream, cudaStreamNonBlocking)) != cudaSuccess)
+    return e;
+  for (auto& ev : ctx->pev)
+    if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
 oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8_t* spins, double gamma,
                      const double* betas, const double* s, const int32_t* mcs, int32_t num_sched,
                      uint64_t seed, int64_t first_sweep, int64_t replica_offset, uint32_t flags,
@@ -1029,8 +1041,17 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
   bool tuned_now = false;
   RngBase rbm = rb;  // rb of the main annealing launch (counts accepted flips)
   if (oj_status cs = arm_counters(ctx, stats, &rbm)) return cs;
+  // slice-split runs from host buffers with a known launch shape go in two
+  // halves of replica groups on two streams (the copies of one half overlap
+  // the other's kernel); OJ_PIPE=0 in the environment runs them whole
+  const int Psplit = sqa_split_replicas_per_group(T);
+  const uint64_t split_key = ((uint64_t)0x80 << 40) | ((uint64_t)T << 32) | (uint64_t)R;
+  const char* pipe_env = std::getenv("OJ_PIPE");
+  const bool pipe = !devp && kernel == OJ_KERNEL_BITPACKED && split_ok && S > 0 && R > Psplit &&
+                    (g->tuned.count(split_key) > 0 || !autotune_requested(flags)) &&
+                    !(pipe_env && pipe_env[0] == '0');
   OJ_CK(cudaEventRecord(ctx->ev[0], st), "event");
-  if (!devp) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
+  if (!devp && !pipe) OJ_CK(cudaMemcpyAsync(d_spins, spins, spin_bytes, cudaMemcpyHostToDevice, st), "H2D spins");
   if (kernel == OJ_KERNEL_BITPACKED && split_ok) {
     const int P = sqa_split_replicas_per_group(T);
     const int G = (R + P - 1) / P;
@@ -1054,8 +1075,10 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     }
     OJ_CK(ctx->words.ensure((size_t)G * 2 * n * 4), "alloc words");
     uint32_t* d_words = ctx->words.as<uint32_t>();
-    OJ_CK(launch_sqa_split_pack(d_spins, R, T, n, G, d_words, st), "pack");
-    ++launches;
+    if (!pipe) {
+      OJ_CK(launch_sqa_split_pack(d_spins, R, T, n, G, d_words, st), "pack");
+      ++launches;
+    }
     Shape shp;
     auto it = g->tuned.find(key);
     if (it != g->tuned.end()) {
@@ -1095,13 +1118,87 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     }
     P_used = g->msc->P;
     threads_used = shp.threads ? shp.threads : split_default_threads();
-    OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
-    if (S > 0)
-      OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rbm, st, &launches, threads_used),
+    if (!pipe) {
+      OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+      if (S > 0)
+        OJ_CK(launch_sqa_split(g, G, T, d_words, d_thr, d_mode, S, rbm, st, &launches, threads_used),
+              "sqa slice-split kernel");
+      OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+      OJ_CK(launch_sqa_split_unpack(d_words, R, T, n, G, d_spins, st), "unpack");
+      ++launches;
+    } else {
+      // halves: groups [0, GA) on the context stream, [GA, G) on the second
+      // stream, each copied in, packed, annealed (at its global group index,
+      // so with the same draws), unpacked, its energies and best slices
+      // computed and all of it copied out; every buffer is sized before the
+      // first launch
+      OJ_CK(pipe_streams(ctx), "pipeline streams");
+      const cudaStream_t s2 = ctx->gstream;
+      const int GA = (G + 1) / 2, RA = GA * P, RB = R - RA;
+      const size_t offB = (size_t)RA * T * n;
+      uint32_t* wB = d_words + (size_t)GA * 2 * n;
+      double* d_e = nullptr;
+      int32_t* d_b = nullptr;
+      double *partsA = nullptr, *partsB = nullptr;
+      const int nsA = energy_splits(g, RA * T, ctx->sm_count), nsB = energy_splits(g, RB * T, ctx->sm_count);
+      if (energies || best_slice) {
+        OJ_CK(ctx->energies.ensure((size_t)R * T * 8), "alloc energies");
+        d_e = ctx->energies.as<double>();
+        const size_t pa = nsA > 1 ? (size_t)nsA * RA * T : 0, pb = nsB > 1 ? (size_t)nsB * RB * T : 0;
+        if (pa + pb > 0) {
+          OJ_CK(ctx->eparts.ensure((pa + pb) * 8), "alloc energy parts");
+          partsA = nsA > 1 ? ctx->eparts.as<double>() : nullptr;
+          partsB = nsB > 1 ? ctx->eparts.as<double>() + pa : nullptr;
+        }
+      }
+      if (best_slice) {
+        OJ_CK(ctx->best.ensure((size_t)R * 4), "alloc best");
+        d_b = ctx->best.as<int32_t>();
+      }
+      OJ_CK(cudaEventRecord(ctx->pev[0], st), "event");
+      OJ_CK(cudaStreamWaitEvent(s2, ctx->pev[0], 0), "event wait");
+      RngBase rbB = rbm;
+      rbB.rep0 += (uint32_t)RA;
+      OJ_CK(cudaMemcpyAsync(d_spins, spins, offB, cudaMemcpyHostToDevice, st), "H2D spins");
+      OJ_CK(launch_sqa_split_pack(d_spins, RA, T, n, GA, d_words, st), "pack");
+      OJ_CK(cudaEventRecord(ctx->ev[1], st), "event");
+      OJ_CK(launch_sqa_split(g, GA, T, d_words, d_thr, d_mode, S, rbm, st, &launches, threads_used),
             "sqa slice-split kernel");
-    OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
-    OJ_CK(launch_sqa_split_unpack(d_words, R, T, n, G, d_spins, st), "unpack");
-    ++launches;
+      OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
+      OJ_CK(cudaMemcpyAsync(d_spins + offB, spins + offB, spin_bytes - offB, cudaMemcpyHostToDevice, s2),
+            "H2D spins");
+      OJ_CK(launch_sqa_split_pack(d_spins + offB, RB, T, n, G - GA, wB, s2), "pack");
+      OJ_CK(launch_sqa_split(g, G - GA, T, wB, d_thr, d_mode, S, rbB, s2, &launches, threads_used),
+            "sqa slice-split kernel");
+      OJ_CK(cudaEventRecord(ctx->pev[1], s2), "event");
+      OJ_CK(launch_sqa_split_unpack(d_words, RA, T, n, GA, d_spins, st), "unpack");
+      OJ_CK(launch_sqa_split_unpack(wB, RB, T, n, G - GA, d_spins + offB, s2), "unpack");
+      launches += 4;  // packs and unpacks
+      if (d_e) {
+        double* eB = d_e + (size_t)RA * T;
+        OJ_CK(launch_energy(g, RA * T, d_spins, d_e, st, nsA, partsA), "energy kernel");
+        OJ_CK(launch_energy(g, RB * T, d_spins + offB, eB, s2, nsB, partsB), "energy kernel");
+        launches += (nsA > 1 ? 2 : 1) + (nsB > 1 ? 2 : 1);
+        if (energies) {
+          OJ_CK(cudaMemcpyAsync(energies, d_e, (size_t)RA * T * 8, cudaMemcpyDeviceToHost, st), "D2H energies");
+          OJ_CK(cudaMemcpyAsync(energies + (size_t)RA * T, eB, (size_t)RB * T * 8, cudaMemcpyDeviceToHost, s2),
+                "D2H energies");
+        }
+        if (d_b) {
+          OJ_CK(launch_best_slice(d_e, RA, T, d_b, st), "best slice");
+          OJ_CK(launch_best_slice(eB, RB, T, d_b + RA, s2), "best slice");
+          launches += 2;
+          OJ_CK(cudaMemcpyAsync(best_slice, d_b, (size_t)RA * 4, cudaMemcpyDeviceToHost, st), "D2H best");
+          OJ_CK(cudaMemcpyAsync(best_slice + RA, d_b + RA, (size_t)RB * 4, cudaMemcpyDeviceToHost, s2),
+                "D2H best");
+        }
+      }
+      OJ_CK(cudaMemcpyAsync(spins, d_spins, offB, cudaMemcpyDeviceToHost, st), "D2H spins");
+      OJ_CK(cudaMemcpyAsync(spins + offB, d_spins + offB, spin_bytes - offB, cudaMemcpyDeviceToHost, s2),
+            "D2H spins");
+      OJ_CK(cudaEventRecord(ctx->pev[2], s2), "event");
+      OJ_CK(cudaStreamWaitEvent(st, ctx->pev[2], 0), "event wait");
+    }
   } else if (kernel == OJ_KERNEL_BITPACKED) {
     OJ_CK(sqa_msc_prepare(g), "bit-packed SQA tables");
     std::vector<uint32_t> thr, mode;
@@ -1132,7 +1229,9 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     if (S > 0) OJ_CK(launch_sqa_colour(g, R, T, d_spins, d_coef, S, rbm, st, &launches), "sqa kernel");
     OJ_CK(cudaEventRecord(ctx->ev[2], st), "event");
   }
-  if (energies || best_slice) {
+  if (pipe) {
+    // the halves computed and copied out their energies, best slices and spins
+  } else if (energies || best_slice) {
     double* d_e = (devp && energies) ? energies : nullptr;
     if (!d_e) {
       OJ_CK(ctx->energies.ensure((size_t)R * T * 8), "alloc energies");
@@ -1152,7 +1251,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
       if (!devp) OJ_CK(cudaMemcpyAsync(best_slice, d_b, (size_t)R * 4, cudaMemcpyDeviceToHost, st), "D2H best");
     }
   }
-  if (!devp) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
+  if (!devp && !pipe) OJ_CK(cudaMemcpyAsync(spins, d_spins, spin_bytes, cudaMemcpyDeviceToHost, st), "D2H spins");
   OJ_CK(cudaEventRecord(ctx->ev[3], st), "event");
   if (!devp || stats) OJ_CK(cudaStreamSynchronize(st), "run");
   if (stats) {
@@ -1164,6 +1263,12 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
     stats->threads = threads_used;
     stats->tuned = tuned_now ? 1 : 0;
     cudaEventElapsedTime(&stats->anneal_ms, ctx->ev[1], ctx->ev[2]);
+    if (pipe) {
+      // from the first half's kernel start to the later of the two ends
+      float tb = 0.0f;
+      cudaEventElapsedTime(&tb, ctx->ev[1], ctx->pev[1]);
+      stats->anneal_ms = std::max(stats->anneal_ms, tb);
+    }
     cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
     stats->accepted = read_counters(ctx).flips;
     stats->field_drift = -1.0;

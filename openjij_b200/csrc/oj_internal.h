@@ -171,6 +171,11 @@ struct oj_ctx {
   cudaStream_t gstream = nullptr;
   cudaEvent_t gev[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec = nullptr;
+  // a slice-split SQA run from host buffers in two halves of replica groups,
+  // the second on gstream, so that the copies of one half overlap the other's
+  // kernel: pev[0] the preamble done on `stream`, pev[1] the second half's
+  // kernel done, pev[2] the second half's copies done
+  cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
 };
 
 namespace oj {

@@ -300,6 +300,34 @@ def test_sqa_slice_split_clusters(ctx, monkeypatch, cluster, which, T, R):
     np.testing.assert_array_equal(s, _sqa_bitpacked_replay(g, s0, betas, ss, mcs, 1.0, D, 21))
 
 
+@pytest.mark.parametrize("R", [16, 37])
+def test_sqa_slice_split_two_halves_equal_one_pass(ctx, monkeypatch, R):
+    """Host buffers: the replica groups annealed in two halves on two streams
+    (each half's copies overlapping the other's kernel) give the spins,
+    energies and best slices of the single pass (OJ_PIPE=0), an even and an
+    odd number of groups with a partial last group among them."""
+    m, _ = I.random_regular_pm_j(1200, 3, seed=16)
+    g, dg = _graph(ctx, m)
+    T, nsched = 8, 10
+    ss = np.linspace(0.0, 0.9, nsched)
+    betas = np.full(nsched, 4.0)
+    mcs = np.ones(nsched, np.int32)
+    s0 = np.random.default_rng(5).choice(np.array([-1, 1], np.int8), size=(R, T, g.n))
+    out = []
+    for pipe in (None, "0"):
+        if pipe:
+            monkeypatch.setenv("OJ_PIPE", pipe)
+        else:
+            monkeypatch.delenv("OJ_PIPE", raising=False)
+        s, en, best = s0.copy(), np.zeros((R, T)), np.full(R, -1, np.int32)
+        st = N.sqa_run(dg, s, 1.0, betas, ss, mcs, seed=23, energies=en, best=best, kernel="bitpacked")
+        assert st["kernel"] == "bitpacked"
+        out.append((s, en, best))
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(out[0][0], _sqa_bitpacked_replay(g, s0, betas, ss, mcs, 1.0, 3, 23))
+
+
 def test_sqa_auto_picks_bitpacked_on_regular_pm_j(ctx):
     m, _ = I.random_regular_pm_j(40, 3, seed=1)
     g, dg = _graph(ctx, m)
