@@ -212,7 +212,9 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* g, int32_t num_replicas, int32
  * pointer or another device's memory -> OJ_ERR_ARG).  The graph must be
  * regular with couplings +-c, h = 0, and must have run oj_sa_run once (which
  * builds its site partition), else OJ_ERR_UNSUPPORTED.  The call is
- * asynchronous on the context's stream.  oj_ctx_create places the array on
+ * asynchronous on the context's stream and cannot be captured into a CUDA
+ * graph (a capturing stream -> OJ_ERR_UNSUPPORTED: the thresholds are copied
+ * from a buffer that lives only during the call).  oj_ctx_create places the array on
  * the context's device and loads the kernels this entry point launches, so the
  * call itself allocates no device memory; calls overlapping on one GPU share
  * the array and race. */

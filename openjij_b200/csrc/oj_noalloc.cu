@@ -149,6 +149,15 @@ extern "C" oj_status oj_sa_run_bitpacked_noalloc(oj_ctx* ctx, const oj_graph* g,
     if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return OJ_ERR_CUDA;
   };
+  // the thresholds are uploaded from a stack buffer, which a captured copy
+  // would read again at every replay, after this call has returned
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    ctx->last_error = "the context's stream is being captured; the allocation-free entry point cannot be captured";
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return OJ_ERR_UNSUPPORTED;
+  }
   cudaPointerAttributes pa;
   if (cudaPointerGetAttributes(&pa, spins) != cudaSuccess ||
       !(pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged)) {

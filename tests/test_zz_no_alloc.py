@@ -79,6 +79,21 @@ def test_noalloc_matches_regular_entry_point_twice():
     assert ei.value.status == N.OJ_ERR_UNSUPPORTED
     torch.cuda.synchronize()
     assert torch.equal(spins, init)
+
+    # a stream under capture is refused (the thresholds pass through a buffer
+    # that is gone when a graph would replay the copy)
+    side = torch.cuda.Stream()
+    ctx.set_stream(side.cuda_stream)
+    cg = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(cg, stream=side):
+        spins.add_(0)
+        with pytest.raises(N.OJError) as ei:
+            N.sa_run_bitpacked_noalloc(graph, spins, betas, mcs, seed=1)
+    assert ei.value.status == N.OJ_ERR_UNSUPPORTED
+    ctx.set_stream(stream.cuda_stream)
+    del cg
+    torch.cuda.synchronize()
+    assert torch.equal(spins, init)
     for x in (gm, fresh, graph):
         x.close()
     ctx.close()
