@@ -134,6 +134,22 @@ oj_status oj_ctx_set_wait_limit(oj_ctx* ctx, int64_t iterations);
 #define OJ_FAULT_ALLOC 1
 oj_status oj_ctx_inject_fault(oj_ctx* ctx, int32_t kind, int64_t after);
 
+/* Page-locked host memory for spin buffers that stay on the host between
+ * calls (the cxxjij systems keep theirs here): a run's copies in and out are
+ * then single DMA transfers at the link's rate.  No counterpart in the
+ * reference, whose systems hold their spins in ordinary Eigen members
+ * (include/openjij/system/classical_ising.hpp:95 `spin`,
+ * include/openjij/system/transverse_ising.hpp:198 `trotter_spins`).  Freed blocks are kept
+ * in a process-wide cache (up to 2 GiB) for later requests of a similar size.
+ * Without a device, when page-locked memory is refused, or with
+ * OJ_HOST_PINNED=0 in the environment, a block is ordinary memory (every entry
+ * point takes either).  oj_host_alloc returns NULL only when no memory at all
+ * can be had; free with oj_host_free only.  oj_host_is_pinned: 1 when p is a
+ * page-locked block of this allocator. */
+void* oj_host_alloc(size_t bytes);
+void oj_host_free(void* p);
+int32_t oj_host_is_pinned(const void* p);
+
 /* Graph upload.  Replaces cxxjij.graph.Dense(num_spins).set_interaction_matrix
  * (openjij/declare.hpp:75-129; include/openjij/graph/dense.hpp:117-140) and
  * cxxjij.graph.CSRSparse(csr) (declare.hpp:195-217; csr_sparse.hpp:96-101).

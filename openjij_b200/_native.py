@@ -37,7 +37,7 @@ EXPORTS = [
     "oj_graph_destroy", "oj_graph_query", "oj_sa_run", "oj_sqa_run", "oj_energy",
     "oj_sa_run_bitpacked_noalloc", "oj_batch_create_dense", "oj_batch_destroy", "oj_sa_run_batched",
     "oj_sw_run", "oj_graph_flip_stats", "oj_batch_flip_stats", "oj_ctx_set_field_recompute",
-    "oj_ctx_set_wait_limit", "oj_ctx_inject_fault",
+    "oj_ctx_set_wait_limit", "oj_ctx_inject_fault", "oj_host_alloc", "oj_host_free", "oj_host_is_pinned",
 ]
 
 
@@ -98,6 +98,12 @@ def lib():
                                  C.POINTER(RunStats)]
         L.oj_energy.argtypes = [vp, vp, i32, vp, u32, vp]
         L.oj_sa_run_bitpacked_noalloc.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64]
+        L.oj_host_alloc.argtypes = [C.c_size_t]
+        L.oj_host_alloc.restype = vp
+        L.oj_host_free.argtypes = [vp]
+        L.oj_host_free.restype = None
+        L.oj_host_is_pinned.argtypes = [vp]
+        L.oj_host_is_pinned.restype = i32
         L.oj_sw_run.argtypes = [vp, vp, i32, vp, vp, vp, i32, u64, i64, i64, u32, vp, C.POINTER(RunStats)]
         L.oj_graph_flip_stats.argtypes = [vp, vp, i32, vp, dbl, vp, vp, C.POINTER(dbl)]
         L.oj_batch_flip_stats.argtypes = [vp, vp, i32, vp, dbl, vp, vp, vp]
@@ -106,7 +112,8 @@ def lib():
         L.oj_sa_run_batched.argtypes = [vp, vp, vp, vp, vp, vp, i32, u64, i64, i64, u32, vp,
                                         C.POINTER(RunStats)]
         for name in EXPORTS:
-            if name not in ("oj_version", "oj_status_string", "oj_ctx_last_error"):
+            if name not in ("oj_version", "oj_status_string", "oj_ctx_last_error", "oj_host_alloc",
+                            "oj_host_free", "oj_host_is_pinned"):
                 getattr(L, name).restype = i32
         _lib = L
     return _lib

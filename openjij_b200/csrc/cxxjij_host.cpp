@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -639,6 +640,28 @@ std::shared_ptr<G> snapshot(const G& g) {
   return std::make_shared<G>(g);
 }
 
+// Page-locked storage for the systems' spins (oj_host_alloc, ordinary memory
+// where page-locking is unavailable): a run's copies in and out are then
+// single DMA transfers instead of the driver's staged copies of pageable memory.
+template <class T>
+struct HostPinned {
+  using value_type = T;
+  HostPinned() = default;
+  template <class U>
+  HostPinned(const HostPinned<U>&) {}
+  T* allocate(size_t k) {
+    void* p = oj_host_alloc(k * sizeof(T));
+    if (!p) throw std::bad_alloc();
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) { oj_host_free(p); }
+  template <class U>
+  bool operator==(const HostPinned<U>&) const { return true; }
+  template <class U>
+  bool operator!=(const HostPinned<U>&) const { return false; }
+};
+using SpinBuf = std::vector<int8_t, HostPinned<int8_t>>;
+
 // Parses 1-D (one replica) or 2-D ([R][n]) +-1 spins.
 std::vector<int8_t> parse_spins(const py::handle& obj, size_t n, int* R_out) {
   auto arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
@@ -670,7 +693,8 @@ template <class G>
 struct ClassicalIsing {
   ClassicalIsing(const py::object& init, const G& g) : graph(snapshot(g)), num_spins(g.size()) { reset(init); }
   void reset(const py::object& init) {
-    spins = parse_spins(init, num_spins, &R);
+    const std::vector<int8_t> v = parse_spins(init, num_spins, &R);
+    spins.assign(v.begin(), v.end());
     ecache_valid = false;
   }
   py::array_t<double> get_spin() const {
@@ -707,7 +731,7 @@ struct ClassicalIsing {
   // energies of the current spins, written by the run call that produced them
   std::vector<double> ecache;
   bool ecache_valid = false;
-  std::vector<int8_t> spins;
+  SpinBuf spins;
 };
 
 template <class G>
@@ -803,7 +827,7 @@ struct TransverseIsing {
   size_t num_classical_spins;
   double gamma;
   int R = 1, T = 0;
-  std::vector<int8_t> spins;  // [R][T][n]
+  SpinBuf spins;  // [R][T][n]
 };
 
 uint64_t random_seed() {
@@ -1019,7 +1043,8 @@ py::object solution(const TransverseIsing<G>& sys) {
 
 // The replicas' spins as an int8 array of the given shape (a copy), for the
 // sampler layer: no per-spin Python objects.
-py::array_t<int8_t> int8_view(const std::vector<int8_t>& v, std::vector<ssize_t> shape) {
+template <class V>
+py::array_t<int8_t> int8_view(const V& v, std::vector<ssize_t> shape) {
   py::array_t<int8_t> out(shape);
   std::copy(v.begin(), v.end(), out.mutable_data());
   return out;

@@ -37,3 +37,20 @@ def test_null_arguments_are_rejected_without_a_device():
     assert L.oj_ctx_create(0, None) == N.OJ_ERR_ARG
     assert L.oj_graph_destroy(None) == N.OJ_OK
     assert L.oj_ctx_destroy(None) == N.OJ_OK
+
+
+def test_host_blocks_are_ordinary_memory_without_a_device():
+    """oj_host_alloc on a host without a GPU: usable ordinary memory, not
+    reported as page-locked, freed by oj_host_free."""
+    import torch
+
+    if torch.cuda.is_available():
+        return  # with a device the block is page-locked (GPU test)
+    L = N.lib()
+    p = L.oj_host_alloc(100003)
+    assert p
+    assert L.oj_host_is_pinned(p) == 0
+    ctypes.memset(p, 0x5A, 100003)
+    assert ctypes.string_at(p + 100002, 1) == b"\x5a"
+    L.oj_host_free(p)
+    L.oj_host_free(None)

@@ -108,6 +108,40 @@ def test_sampler_path_matches_replay():
     np.testing.assert_allclose(res.energies, O.energies(g, ref), atol=1e-9)
 
 
+def test_system_spins_page_locked_or_not_give_the_same_samples(monkeypatch):
+    """The systems keep their spins in page-locked blocks of the library's
+    host allocator (a freed block serves the next request of its size); the
+    samples equal those of a run from ordinary memory (OJ_HOST_PINNED=0)."""
+    from openjij_b200 import _native as N
+
+    L = N.lib()
+    size = (5 << 20) + 7
+    p = L.oj_host_alloc(size)
+    assert p and L.oj_host_is_pinned(p) == 1
+    L.oj_host_free(p)
+    q = L.oj_host_alloc(size)
+    assert q == p
+    L.oj_host_free(q)
+    m, _ = I.lattice_pm_j(16, seed=4)
+    mat = m.tocoo()
+    n = m.shape[0] - 1
+    J = {(int(i), int(j)): float(v) for i, j, v in zip(mat.row, mat.col, mat.data) if i < j < n}
+    out = []
+    for pinned in ("1", "0"):
+        monkeypatch.setenv("OJ_HOST_PINNED", pinned)
+        res = oj.SASampler().sample_ising({}, J, beta_min=0.1, beta_max=5.0, num_sweeps=30, num_reads=64, seed=5)
+        out.append((np.asarray(res.states), np.asarray(res.energies)))
+        res = oj.SQASampler().sample_ising({}, J, beta=5.0, gamma=1.0, trotter=8, num_sweeps=20, num_reads=16,
+                                           seed=6)
+        out.append((np.asarray(res.states), np.asarray(res.energies)))
+    r = L.oj_host_alloc(1 << 20)
+    assert r and L.oj_host_is_pinned(r) == 0
+    L.oj_host_free(r)
+    for a, b in zip(out[:2], out[2:]):
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])
+
+
 # ---- tests/test_sampler.py ------------------------------------------------
 
 NUM_H = {0: -1, 1: -1, 2: 1, 3: 1}
