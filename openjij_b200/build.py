@@ -74,7 +74,7 @@ def build_host(verbose=False, force=False):
     if not (force or _stale(out, deps)):
         return out
     cxx = os.environ.get("CXX", "g++")
-    cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+    cmd = [cxx, "-O3", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
            "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"], "-I" + INCLUDE,
            src, "-o", out, "-L" + HERE, "-lojb200", "-Wl,-rpath,$ORIGIN"]
     _run(cmd, verbose)

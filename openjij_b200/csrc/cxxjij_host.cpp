@@ -655,6 +655,15 @@ struct HostPinned {
     return static_cast<T*>(p);
   }
   void deallocate(T* p, size_t) { oj_host_free(p); }
+  // new elements are left uninitialised (every user writes them all)
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
   template <class U>
   bool operator==(const HostPinned<U>&) const { return true; }
   template <class U>
@@ -662,39 +671,80 @@ struct HostPinned {
 };
 using SpinBuf = std::vector<int8_t, HostPinned<int8_t>>;
 
-// Parses 1-D (one replica) or 2-D ([R][n]) +-1 spins.
-std::vector<int8_t> parse_spins(const py::handle& obj, size_t n, int* R_out) {
-  auto arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
-  if (!arr) throw std::invalid_argument("spins must be array-like");
+// A C-contiguous int8 numpy array (what the sampler layer passes) is read in
+// place; anything else goes through a conversion to double.
+bool as_int8_array(const py::handle& obj, py::array* out) {
+  if (!py::isinstance<py::array>(obj)) return false;
+  py::array a = py::reinterpret_borrow<py::array>(obj);
+  if (a.dtype().kind() != 'i' || a.itemsize() != 1 || !(a.flags() & py::array::c_style)) return false;
+  *out = a;
+  return true;
+}
+
+// Copies rows of n spins out of rows of len >= n int8 values into out (resized
+// to rows * n); throws, leaving out as it was, unless every copied value is -1
+// or +1 (v + 1 is 0 or 2 exactly for those).
+template <class Buf>
+void copy_int8_rows(const int8_t* p, size_t rows, size_t len, size_t n, Buf& out) {
+  unsigned bad = 0;
+  for (size_t r = 0; r < rows; ++r) {
+    const int8_t* src = p + r * len;
+    for (size_t i = 0; i < n; ++i) bad |= (uint8_t)(src[i] + 1) & 0xFDu;
+  }
+  if (bad) throw std::invalid_argument("spins must be -1 or +1");
+  out.resize(rows * n);
+  if (len == n) {
+    std::copy(p, p + rows * n, out.data());
+  } else {
+    for (size_t r = 0; r < rows; ++r) std::copy(p + r * len, p + r * len + n, out.data() + r * n);
+  }
+}
+
+// Parses 1-D (one replica) or 2-D ([R][n]) +-1 spins into out (resized).
+template <class Buf>
+void parse_spins(const py::handle& obj, size_t n, int* R_out, Buf& out) {
+  py::array a8;
+  const bool i8 = as_int8_array(obj, &a8);
+  py::array_t<double> arr;
+  if (!i8) {
+    arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
+    if (!arr) throw std::invalid_argument("spins must be array-like");
+  }
+  const py::array& shp = i8 ? a8 : static_cast<const py::array&>(arr);
   int R = 1;
   size_t len = 0;
-  if (arr.ndim() == 1) {
-    len = (size_t)arr.shape(0);
-  } else if (arr.ndim() == 2) {
-    R = (int)arr.shape(0);
-    len = (size_t)arr.shape(1);
+  if (shp.ndim() == 1) {
+    len = (size_t)shp.shape(0);
+  } else if (shp.ndim() == 2) {
+    R = (int)shp.shape(0);
+    len = (size_t)shp.shape(1);
   } else {
     throw std::invalid_argument("spins must be 1-D or 2-D");
   }
   if (len != n && len != n + 1) throw std::invalid_argument("the size of the initial spins does not match the graph");
-  std::vector<int8_t> out((size_t)R * n);
-  const double* p = arr.data();
-  for (int r = 0; r < R; ++r)
-    for (size_t i = 0; i < n; ++i) {
-      const double v = p[(size_t)r * len + i];
-      if (v != 1.0 && v != -1.0) throw std::invalid_argument("spins must be -1 or +1");
-      out[(size_t)r * n + i] = (int8_t)v;
-    }
+  if (i8) {
+    copy_int8_rows(static_cast<const int8_t*>(a8.data()), (size_t)R, len, n, out);
+  } else {
+    Buf tmp((size_t)R * n);
+    const double* p = arr.data();
+    for (int r = 0; r < R; ++r)
+      for (size_t i = 0; i < n; ++i) {
+        const double v = p[(size_t)r * len + i];
+        if (v != 1.0 && v != -1.0) throw std::invalid_argument("spins must be -1 or +1");
+        tmp[(size_t)r * n + i] = (int8_t)v;
+      }
+    out.swap(tmp);
+  }
   *R_out = R;
-  return out;
 }
 
 template <class G>
 struct ClassicalIsing {
   ClassicalIsing(const py::object& init, const G& g) : graph(snapshot(g)), num_spins(g.size()) { reset(init); }
   void reset(const py::object& init) {
-    const std::vector<int8_t> v = parse_spins(init, num_spins, &R);
-    spins.assign(v.begin(), v.end());
+    int Rn = 1;
+    parse_spins(init, num_spins, &Rn, spins);
+    R = Rn;
     ecache_valid = false;
   }
   py::array_t<double> get_spin() const {
@@ -747,38 +797,50 @@ struct TransverseIsing {
   }
   // [T][n] (one replica) or [R][T][n]
   void reset_trotter(const py::object& obj) {
-    auto arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
-    if (!arr) throw std::invalid_argument("trotter spins must be array-like");
+    py::array a8;
+    const bool i8 = as_int8_array(obj, &a8);
+    py::array_t<double> arr;
+    if (!i8) {
+      arr = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(obj);
+      if (!arr) throw std::invalid_argument("trotter spins must be array-like");
+    }
+    const py::array& shp = i8 ? a8 : static_cast<const py::array&>(arr);
     const size_t n = num_classical_spins;
     int Rn = 1, Tn = 0;
     size_t len = 0;
-    if (arr.ndim() == 2) {
-      Tn = (int)arr.shape(0);
-      len = (size_t)arr.shape(1);
-    } else if (arr.ndim() == 3) {
-      Rn = (int)arr.shape(0);
-      Tn = (int)arr.shape(1);
-      len = (size_t)arr.shape(2);
+    if (shp.ndim() == 2) {
+      Tn = (int)shp.shape(0);
+      len = (size_t)shp.shape(1);
+    } else if (shp.ndim() == 3) {
+      Rn = (int)shp.shape(0);
+      Tn = (int)shp.shape(1);
+      len = (size_t)shp.shape(2);
     } else {
       throw std::invalid_argument("trotter spins must be [T][n] or [R][T][n]");
     }
     if (!(Tn >= 2)) throw std::invalid_argument("trotter slices must be equal or larger than 2.");
     if (len != n && len != n + 1) throw std::invalid_argument("the size of the trotter spins does not match the graph");
+    if (i8) {
+      copy_int8_rows(static_cast<const int8_t*>(a8.data()), (size_t)Rn * Tn, len, n, spins);
+    } else {
+      SpinBuf tmp((size_t)Rn * Tn * n);
+      const double* p = arr.data();
+      for (size_t idx = 0; idx < (size_t)Rn * Tn; ++idx)
+        for (size_t i = 0; i < n; ++i) {
+          const double v = p[idx * len + i];
+          if (v != 1.0 && v != -1.0) throw std::invalid_argument("spins must be -1 or +1");
+          tmp[idx * n + i] = (int8_t)v;
+        }
+      spins.swap(tmp);
+    }
     R = Rn;
     T = Tn;
-    spins.assign((size_t)R * T * n, 1);
-    const double* p = arr.data();
-    for (size_t idx = 0; idx < (size_t)R * T; ++idx)
-      for (size_t i = 0; i < n; ++i) {
-        const double v = p[idx * len + i];
-        if (v != 1.0 && v != -1.0) throw std::invalid_argument("spins must be -1 or +1");
-        spins[idx * n + i] = (int8_t)v;
-      }
   }
   void reset_classical(const py::object& obj) {
     const size_t n = num_classical_spins;
     int Rn = 1;
-    std::vector<int8_t> cl = parse_spins(obj, n, &Rn);
+    std::vector<int8_t> cl;
+    parse_spins(obj, n, &Rn, cl);
     R = Rn;
     spins.assign((size_t)R * T * n, 1);
     for (int r = 0; r < R; ++r)

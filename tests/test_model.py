@@ -126,3 +126,41 @@ def test_transverse_needs_two_slices():
     d = cj.graph.Dense(3)
     with pytest.raises(ValueError):
         cj.system.make_transverse_ising([1, 1, 1], d, 1.0, 1)
+
+
+def test_system_spins_from_int8_and_float_inputs_agree():
+    """int8 arrays (read in place) and float / list inputs (converted) give
+    the same system spins; a value other than +-1 raises ValueError and leaves
+    the system's spins as they were; a trailing dummy spin column is dropped."""
+    rng = np.random.default_rng(4)
+    n, R, T = 12, 5, 3
+    d = cj.graph.Dense(n)
+    s8 = rng.choice(np.array([-1, 1], np.int8), size=(R, n))
+    a = cj.system.make_classical_ising(s8, d)
+    b = cj.system.make_classical_ising(s8.astype(np.float64), d)
+    np.testing.assert_array_equal(a._spins_int8(), s8)
+    np.testing.assert_array_equal(b._spins_int8(), s8)
+    a.reset_spins(np.concatenate([s8, np.ones((R, 1), np.int8)], 1))
+    np.testing.assert_array_equal(a._spins_int8(), s8)
+    a.reset_spins(s8[2])
+    np.testing.assert_array_equal(a._spins_int8(), s8[2:3])
+    b.reset_spins(list(s8[3].astype(int)))
+    np.testing.assert_array_equal(b._spins_int8(), s8[3:4])
+    for bad_value in (0, 3, -128, 127):
+        bad = s8.copy()
+        bad[1, 4] = bad_value
+        with pytest.raises(ValueError):
+            a.reset_spins(bad)
+        np.testing.assert_array_equal(a._spins_int8(), s8[2:3])
+    t8 = rng.choice(np.array([-1, 1], np.int8), size=(R, T, n))
+    t = cj.system.make_transverse_ising(t8, d, 1.0)
+    u = cj.system.make_transverse_ising(t8.astype(np.float32), d, 1.0)
+    np.testing.assert_array_equal(t._spins_int8(), t8)
+    np.testing.assert_array_equal(u._spins_int8(), t8)
+    bad = t8.copy()
+    bad[0, 1, 2] = 2
+    with pytest.raises(ValueError):
+        t.reset_spins(bad)
+    np.testing.assert_array_equal(t._spins_int8(), t8)
+    c = cj.system.make_transverse_ising(s8, d, 1.0, 4)
+    np.testing.assert_array_equal(c._spins_int8(), np.repeat(s8[:, None, :], 4, 1))
