@@ -671,32 +671,42 @@ struct HostPinned {
 };
 using SpinBuf = std::vector<int8_t, HostPinned<int8_t>>;
 
-// A C-contiguous int8 numpy array (what the sampler layer passes) is read in
-// place; anything else goes through a conversion to double.
+// An int8 numpy array whose last axis is contiguous (what the sampler layer
+// passes, broadcast views with zero strides included) is read in place;
+// anything else goes through a conversion to double.
 bool as_int8_array(const py::handle& obj, py::array* out) {
   if (!py::isinstance<py::array>(obj)) return false;
   py::array a = py::reinterpret_borrow<py::array>(obj);
-  if (a.dtype().kind() != 'i' || a.itemsize() != 1 || !(a.flags() & py::array::c_style)) return false;
+  if (a.dtype().kind() != 'i' || a.itemsize() != 1 || a.ndim() < 1 || a.ndim() > 3) return false;
+  if (a.shape(a.ndim() - 1) > 1 && a.strides(a.ndim() - 1) != 1) return false;
   *out = a;
   return true;
 }
 
-// Copies rows of n spins out of rows of len >= n int8 values into out (resized
-// to rows * n); throws, leaving out as it was, unless every copied value is -1
-// or +1 (v + 1 is 0 or 2 exactly for those).
+// Row r of an int8 array of 1-3 axes, rows numbered over all but the last axis.
+const int8_t* int8_row(const py::array& a, size_t r) {
+  const char* base = static_cast<const char*>(a.data());
+  if (a.ndim() == 1) return reinterpret_cast<const int8_t*>(base);
+  if (a.ndim() == 2) return reinterpret_cast<const int8_t*>(base + (ssize_t)r * a.strides(0));
+  const size_t T = (size_t)a.shape(1);
+  return reinterpret_cast<const int8_t*>(base + (ssize_t)(r / T) * a.strides(0) + (ssize_t)(r % T) * a.strides(1));
+}
+
+// Copies the first n spins of every row of a into out (resized to rows * n);
+// throws, leaving out as it was, unless every copied value is -1 or +1 (v + 1
+// is 0 or 2 exactly for those).
 template <class Buf>
-void copy_int8_rows(const int8_t* p, size_t rows, size_t len, size_t n, Buf& out) {
+void copy_int8_rows(const py::array& a, size_t rows, size_t n, Buf& out) {
   unsigned bad = 0;
   for (size_t r = 0; r < rows; ++r) {
-    const int8_t* src = p + r * len;
+    const int8_t* src = int8_row(a, r);
     for (size_t i = 0; i < n; ++i) bad |= (uint8_t)(src[i] + 1) & 0xFDu;
   }
   if (bad) throw std::invalid_argument("spins must be -1 or +1");
   out.resize(rows * n);
-  if (len == n) {
-    std::copy(p, p + rows * n, out.data());
-  } else {
-    for (size_t r = 0; r < rows; ++r) std::copy(p + r * len, p + r * len + n, out.data() + r * n);
+  for (size_t r = 0; r < rows; ++r) {
+    const int8_t* src = int8_row(a, r);
+    std::copy(src, src + n, out.data() + r * n);
   }
 }
 
@@ -723,7 +733,7 @@ void parse_spins(const py::handle& obj, size_t n, int* R_out, Buf& out) {
   }
   if (len != n && len != n + 1) throw std::invalid_argument("the size of the initial spins does not match the graph");
   if (i8) {
-    copy_int8_rows(static_cast<const int8_t*>(a8.data()), (size_t)R, len, n, out);
+    copy_int8_rows(a8, (size_t)R, n, out);
   } else {
     Buf tmp((size_t)R * n);
     const double* p = arr.data();
@@ -797,6 +807,7 @@ struct TransverseIsing {
   }
   // [T][n] (one replica) or [R][T][n]
   void reset_trotter(const py::object& obj) {
+    ecache_valid = false;
     py::array a8;
     const bool i8 = as_int8_array(obj, &a8);
     py::array_t<double> arr;
@@ -821,7 +832,7 @@ struct TransverseIsing {
     if (!(Tn >= 2)) throw std::invalid_argument("trotter slices must be equal or larger than 2.");
     if (len != n && len != n + 1) throw std::invalid_argument("the size of the trotter spins does not match the graph");
     if (i8) {
-      copy_int8_rows(static_cast<const int8_t*>(a8.data()), (size_t)Rn * Tn, len, n, spins);
+      copy_int8_rows(a8, (size_t)Rn * Tn, n, spins);
     } else {
       SpinBuf tmp((size_t)Rn * Tn * n);
       const double* p = arr.data();
@@ -837,6 +848,7 @@ struct TransverseIsing {
     T = Tn;
   }
   void reset_classical(const py::object& obj) {
+    ecache_valid = false;
     const size_t n = num_classical_spins;
     int Rn = 1;
     std::vector<int8_t> cl;
@@ -882,6 +894,10 @@ struct TransverseIsing {
       std::fill(out.mutable_data(), out.mutable_data() + (size_t)R * T, 0.0);
       return out;
     }
+    if (ecache_valid && ecache.size() == (size_t)R * T) {  // from the last run's own call
+      std::copy(ecache.begin(), ecache.end(), out.mutable_data());
+      return out;
+    }
     check(oj_energy(ctx(), graph->device(), R * T, spins.data(), 0, out.mutable_data()), "oj_energy");
     return out;
   }
@@ -889,6 +905,9 @@ struct TransverseIsing {
   size_t num_classical_spins;
   double gamma;
   int R = 1, T = 0;
+  // slice energies of the current spins, written by the run call that produced them
+  std::vector<double> ecache;
+  bool ecache_valid = false;
   SpinBuf spins;  // [R][T][n]
 };
 
@@ -1023,6 +1042,7 @@ template <class G>
 void run_transverse(TransverseIsing<G>& sys, uint64_t seed, const std::vector<TransverseSchedule>& sched,
                     const std::function<void(const TransverseIsing<G>&, std::pair<double, double>)>& cb) {
   g_last_run = RunInfo();
+  sys.ecache_valid = false;
   if (sys.num_classical_spins == 0 || sched.empty()) {
     if (cb)
       for (auto& s : sched)
@@ -1042,10 +1062,12 @@ void run_transverse(TransverseIsing<G>& sys, uint64_t seed, const std::vector<Tr
     oj_status rc;
     {
       py::gil_scoped_release release;
+      sys.ecache.resize((size_t)sys.R * sys.T);
       rc = oj_sqa_run(ctx(), dg, sys.R, sys.T, sys.spins.data(), sys.gamma, betas.data(), ss.data(), mcs.data(),
-                      (int32_t)betas.size(), seed, 0, 0, 0, nullptr, nullptr, &st);
+                      (int32_t)betas.size(), seed, 0, 0, 0, sys.ecache.data(), nullptr, &st);
     }
     check(rc, "Algorithm_SingleSpinFlip_run");
+    sys.ecache_valid = true;
     record(st);
     return;
   }
@@ -1085,7 +1107,10 @@ template <class G>
 py::object solution(const TransverseIsing<G>& sys) {
   const size_t n = sys.num_classical_spins;
   std::vector<double> e((size_t)sys.R * sys.T, 0.0);
-  if (n > 0) check(oj_energy(ctx(), sys.graph->device(), sys.R * sys.T, sys.spins.data(), 0, e.data()), "oj_energy");
+  if (sys.ecache_valid && sys.ecache.size() == e.size())
+    e = sys.ecache;
+  else if (n > 0)
+    check(oj_energy(ctx(), sys.graph->device(), sys.R * sys.T, sys.spins.data(), 0, e.data()), "oj_energy");
   py::list out;
   for (int r = 0; r < sys.R; ++r) {
     int best = 0;

@@ -107,14 +107,14 @@ class SASampler(BaseSampler):
         if initial_state is None:
             def init_generator(R):
                 if seed is not None:  # every read starts from gen_spin(seed) (sa_sampler.py:253-258)
-                    return np.tile(np.asarray(ising_graph.gen_spin(int(seed)), np.int8), (R, 1))
+                    return np.broadcast_to(np.asarray(ising_graph.gen_spin(int(seed)), np.int8), (R, n))
                 rng = np.random.default_rng()
                 return rng.choice(np.array([-1, 1], np.int8), size=(R, n))
         else:
             s0 = _place(spins_from_initial_state(initial_state, model, len(model.variables)), sites, n)
 
             def init_generator(R):
-                return np.tile(s0, (R, 1))
+                return np.broadcast_to(s0, (R, len(s0)))
 
         algorithm = self._algorithm[name]
         system = self._make_system[name](init_generator(1), ising_graph) if n > 0 else None
@@ -190,7 +190,7 @@ class SASampler(BaseSampler):
             off += R * n
             if b.vartype == BINARY:
                 st_k = (st_k + 1) // 2
-            resp = Response(st_k.astype(np.int8), energies[k * R:(k + 1) * R] + offsets[k], b.variables, b.vartype)
+            resp = Response(np.asarray(st_k, dtype=np.int8), energies[k * R:(k + 1) * R] + offsets[k], b.variables, b.vartype)
             resp.info["schedule"] = {"beta_min": bmin, "beta_max": bmax, "num_sweeps": S}
             resp.info["sampling_time"] = elapsed * 1e6
             resp.info["run"] = st

@@ -124,7 +124,7 @@ class BaseSampler:
         if model.vartype == BINARY:
             states = (states + 1) // 2
         info = {"system": sys_info} if sys_info else {}
-        response = Response(states.astype(np.int8), energies, model.variables, model.vartype, info)
+        response = Response(np.asarray(states, dtype=np.int8), energies, model.variables, model.vartype, info)
         response.info["sampling_time"] = sampling_time * 1e6
         response.info["execution_time"] = (float(np.mean(exec_times)) * 1e6) if exec_times else 0.0
         response.info["list_exec_times"] = np.asarray(exec_times) * 1e6

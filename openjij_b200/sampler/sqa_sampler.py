@@ -119,14 +119,14 @@ class SQASampler(BaseSampler):
             def init_generator(R):
                 if seed is not None:  # every slice of every read from gen_spin(seed) (sqa_sampler.py:228-236)
                     one = np.asarray(ising_graph.gen_spin(int(seed)), np.int8)
-                    return np.ascontiguousarray(np.broadcast_to(one, (R, T, n)))
+                    return np.broadcast_to(one, (R, T, n))
                 rng = np.random.default_rng()
                 return rng.choice(np.array([-1, 1], np.int8), size=(R, T, n))
         else:
             s0 = _place(spins_from_initial_state(initial_state, model, len(model.variables)), sites, n)
 
             def init_generator(R):
-                return np.ascontiguousarray(np.broadcast_to(s0, (R, T, n)))
+                return np.broadcast_to(s0, (R, T, len(s0)))
 
         system = (self._make_system[name](init_generator(1), ising_graph, float(p["gamma"]))
                   if n > 0 else None)

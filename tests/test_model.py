@@ -164,3 +164,17 @@ def test_system_spins_from_int8_and_float_inputs_agree():
     np.testing.assert_array_equal(t._spins_int8(), t8)
     c = cj.system.make_transverse_ising(s8, d, 1.0, 4)
     np.testing.assert_array_equal(c._spins_int8(), np.repeat(s8[:, None, :], 4, 1))
+    # views: broadcast (zero strides), permuted axes, reversed rows, a strided last axis
+    one = s8[0]
+    a.reset_spins(np.broadcast_to(one, (R, n)))
+    np.testing.assert_array_equal(a._spins_int8(), np.tile(one, (R, 1)))
+    a.reset_spins(s8[::-1])
+    np.testing.assert_array_equal(a._spins_int8(), s8[::-1])
+    wide = rng.choice(np.array([-1, 1], np.int8), size=(R, 2 * n))
+    a.reset_spins(wide[:, ::2])
+    np.testing.assert_array_equal(a._spins_int8(), wide[:, ::2])
+    t.reset_spins(np.broadcast_to(one, (R, T, n)))
+    np.testing.assert_array_equal(t._spins_int8(), np.broadcast_to(one, (R, T, n)))
+    perm = t8.transpose(1, 0, 2).copy().transpose(1, 0, 2)
+    t.reset_spins(perm)
+    np.testing.assert_array_equal(t._spins_int8(), t8)
