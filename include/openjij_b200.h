@@ -141,9 +141,11 @@ oj_status oj_ctx_inject_fault(oj_ctx* ctx, int32_t kind, int64_t after);
  * (include/openjij/system/classical_ising.hpp:95 `spin`,
  * include/openjij/system/transverse_ising.hpp:198 `trotter_spins`).  Freed blocks are kept
  * in a process-wide cache (up to 2 GiB) for later requests of a similar size.
- * Without a device, when page-locked memory is refused, or with
- * OJ_HOST_PINNED=0 in the environment, a block is ordinary memory (every entry
- * point takes either).  oj_host_alloc returns NULL only when no memory at all
+ * Blocks are page-locked through the device of the last context created in
+ * the process and are usable from every context; before any oj_ctx_create
+ * (so that no context is made on some default device), without a device,
+ * when page-locked memory is refused, or with OJ_HOST_PINNED=0 in the
+ * environment, a block is ordinary memory (every entry point takes either).  oj_host_alloc returns NULL only when no memory at all
  * can be had; free with oj_host_free only.  oj_host_is_pinned: 1 when p is a
  * page-locked block of this allocator. */
 void* oj_host_alloc(size_t bytes);

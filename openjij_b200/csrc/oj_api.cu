@@ -501,6 +501,7 @@ oj_status oj_ctx_create(int32_t device, oj_ctx** out) {
     cudaGetLastError();
     ctx->noalloc_error = std::string("set-up of the allocation-free entry point failed: ") + cudaGetErrorString(pe);
   }
+  host_pin_device(device);
   *out = ctx;
   return OJ_OK;
 }

@@ -7,19 +7,24 @@
 // memory is scarce, so freed blocks stay in a process-wide cache and serve the
 // next request of at most their size and at least half of it; the cache keeps
 // at most kCacheBytes and returns the largest blocks to the system past that.
-// When page-locked memory cannot be had (no device, or the system refuses),
-// or OJ_HOST_PINNED=0 is in the environment, a block is ordinary memory,
-// which every entry point accepts as well.  The cache is never torn down: its
+// Blocks are page-locked through the device of the last context created in
+// the process (a block is usable from every context), so that a request made
+// before any context exists creates none on some default device: such a block
+// is ordinary memory.  So is every block when page-locked memory cannot be had
+// (no device, or the system refuses) or OJ_HOST_PINNED=0 is in the
+// environment; every entry point accepts ordinary memory as well.  The cache is never torn down: its
 // blocks go back to the system with the process (a cudaFreeHost from a static
 // destructor could run after the CUDA runtime is gone).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdlib>
 #include <iterator>
 #include <map>
 #include <mutex>
 #include <unordered_map>
 
+#include "oj_internal.h"
 #include "openjij_b200.h"
 
 namespace {
@@ -39,6 +44,8 @@ HostCache& cache() {
   return *c;
 }
 
+std::atomic<int> g_pin_device{-1};
+
 bool pinning_enabled() {
   const char* env = std::getenv("OJ_HOST_PINNED");
   return !(env && env[0] == '0');
@@ -46,9 +53,14 @@ bool pinning_enabled() {
 
 }  // namespace
 
+namespace oj {
+void host_pin_device(int device) { g_pin_device.store(device); }
+}  // namespace oj
+
 extern "C" void* oj_host_alloc(size_t bytes) {
   const size_t want = bytes == 0 ? kGrain : (bytes + kGrain - 1) / kGrain * kGrain;
-  if (pinning_enabled()) {
+  const int dev = g_pin_device.load();
+  if (dev >= 0 && pinning_enabled()) {
     HostCache& c = cache();
     {
       std::lock_guard<std::mutex> lk(c.mu);
@@ -61,7 +73,12 @@ extern "C" void* oj_host_alloc(size_t bytes) {
       }
     }
     void* p = nullptr;
-    if (cudaHostAlloc(&p, want, cudaHostAllocPortable) == cudaSuccess && p) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+    const cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocPortable);
+    if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    if (e == cudaSuccess && p) {
       std::lock_guard<std::mutex> lk(c.mu);
       c.pinned_size[p] = want;
       return p;

@@ -292,6 +292,10 @@ cudaError_t msc_preload();
 // Set-up of the allocation-free entry point on the current device: looks up
 // its fixed scratch array's device address and loads the kernels it launches.
 cudaError_t noalloc_prepare(int device);
+// The device whose context page-locks the blocks of oj_host_alloc (the last
+// one a context was created on); before any context, blocks are ordinary
+// memory, so that allocating one never creates a context by itself.
+void host_pin_device(int device);
 int flip_stats_max_k();
 cudaError_t launch_flip_stats(const oj_graph* g, int K, const int8_t* s, double thr, double* quad, double* lin,
                               unsigned long long* amin, cudaStream_t st);

@@ -115,6 +115,7 @@ def test_system_spins_page_locked_or_not_give_the_same_samples(monkeypatch):
     from openjij_b200 import _native as N
 
     L = N.lib()
+    ctx = N.Context(0)  # blocks are page-locked once a context exists
     size = (5 << 20) + 7
     p = L.oj_host_alloc(size)
     assert p and L.oj_host_is_pinned(p) == 1
@@ -140,6 +141,7 @@ def test_system_spins_page_locked_or_not_give_the_same_samples(monkeypatch):
     for a, b in zip(out[:2], out[2:]):
         np.testing.assert_array_equal(a[0], b[0])
         np.testing.assert_array_equal(a[1], b[1])
+    ctx.close()
 
 
 # ---- tests/test_sampler.py ------------------------------------------------
