@@ -1135,6 +1135,15 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
       // first launch
       OJ_CK(pipe_streams(ctx), "pipeline streams");
       const cudaStream_t s2 = ctx->gstream;
+      // a call that fails part way waits for the second stream's work before
+      // it returns, so that no copy of it still runs into the buffers
+      struct JoinOnError {
+        cudaStream_t s;
+        bool armed = true;
+        ~JoinOnError() {
+          if (armed) cudaStreamSynchronize(s);
+        }
+      } join{s2};
       const int GA = (G + 1) / 2, RA = GA * P, RB = R - RA;
       const size_t offB = (size_t)RA * T * n;
       uint32_t* wB = d_words + (size_t)GA * 2 * n;
@@ -1199,6 +1208,7 @@ oj_status oj_sqa_run(oj_ctx* ctx, const oj_graph* gc, int32_t R, int32_t T, int8
             "D2H spins");
       OJ_CK(cudaEventRecord(ctx->pev[2], s2), "event");
       OJ_CK(cudaStreamWaitEvent(st, ctx->pev[2], 0), "event wait");
+      join.armed = false;
     }
   } else if (kernel == OJ_KERNEL_BITPACKED) {
     OJ_CK(sqa_msc_prepare(g), "bit-packed SQA tables");
