@@ -72,6 +72,12 @@ struct MscPlan {
   uint16_t* hdst = nullptr;  // [P][hmax] local halo slot
   uint16_t* nbr = nullptr;   // [P][nlocmax][D] local slots of the neighbours
   uint16_t* jm = nullptr;    // [P][nlocmax] bit l set when J(site, nbr l) > 0
+  // push lists (bit-packed SA): own slot s of part p is copied, after each
+  // update, to the halo slots pent[poff[p][s] .. poff[p][s+1]) of the parts
+  // that read it, as (reader part << 16) | reader halo slot
+  int pmax = 0;
+  int32_t* poff = nullptr;   // [P][nlocmax+1]
+  uint32_t* pent = nullptr;  // [P][pmax]
 };
 
 // Launch shape of a tunable kernel; 0 = the kernel's default choice.

@@ -20,10 +20,14 @@
 // a halo copy of the remote neighbours and the neighbour tables.  Per colour
 // class a CTA first updates its interior sites (no remote neighbour), then
 // waits on the cluster barrier (split arrive / wait, so the barrier latency
-// hides behind the interior work), copies the halo words of the previous class
-// out of the owners' shared memory (DSMEM), updates its boundary sites and
-// arrives.  Nothing touches global memory between the initial load and the
-// final store.
+// hides behind the interior work), updates its boundary sites, and the thread
+// that updated a boundary site stores the new word straight into the halo
+// slots of the CTAs that read it (DSMEM stores, made visible to them by the
+// release of its next arrive), so no copy sits between a wait and the work
+// after it.  A halo slot of class c is written only in class c's phase, after
+// the writer's wait of that phase, when every reader has left the phase before
+// it, and it is read only in other classes' phases, after the reader's wait.
+// Nothing touches global memory between the initial load and the final store.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -56,7 +60,9 @@ struct MscArgs {
   const uint16_t* hdst;
   const uint16_t* nbr;
   const uint16_t* jm;
-  int slots, nlocmax, hmax, ncol;
+  const int32_t* poff;
+  const uint32_t* pent;
+  int slots, nlocmax, hmax, ncol, pmax;
   int n;
   uint32_t* words;
   const uint32_t* thr;     // [nsweeps][D+1]
@@ -159,13 +165,25 @@ __device__ __forceinline__ uint32_t msc_site(uint32_t w, const uint32_t* __restr
   return w ^ (flip | lt);
 }
 
-// Updates own slots [lo, hi), two independent sites per thread and iteration;
-// returns the number of spins this thread flipped.
+// Stores word w of own slot s into the readers' halo slots (boundary slots).
+__device__ __forceinline__ void msc_push(const cg::cluster_group& cl, uint32_t* Wsh, int e0, int e1,
+                                         const uint32_t* __restrict__ pent, uint32_t w) {
+  for (int e = e0; e < e1; ++e) {
+    const uint32_t d = __ldg(pent + e);
+    uint32_t* remote = cl.map_shared_rank(Wsh, (int)(d >> 16));
+    remote[d & 0xFFFFu] = w;
+  }
+}
+
+// Updates own slots [lo, hi), two independent sites per thread and iteration,
+// and pushes the new words of slots >= bnd (the boundary sites) to their
+// readers; returns the number of spins this thread flipped.
 template <int D>
-__device__ __forceinline__ uint32_t msc_range(int lo, int hi, uint32_t* __restrict__ Wsh,
+__device__ __forceinline__ uint32_t msc_range(int lo, int hi, int bnd, uint32_t* __restrict__ Wsh,
                                               const int32_t* __restrict__ gid, const uint16_t* __restrict__ jm,
-                                              const uint16_t* __restrict__ nbr, const MscSweep<D>& sw,
-                                              uint32_t k, uint32_t g, const ojd::Keys& K) {
+                                              const uint16_t* __restrict__ nbr, const int32_t* __restrict__ poff,
+                                              const uint32_t* __restrict__ pent, const cg::cluster_group& cl,
+                                              const MscSweep<D>& sw, uint32_t k, uint32_t g, const ojd::Keys& K) {
   const int T = blockDim.x;
   uint32_t nf = 0u;
   for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
@@ -177,9 +195,11 @@ __device__ __forceinline__ uint32_t msc_range(int lo, int hi, uint32_t* __restri
       const uint32_t b = msc_site<D>(w2, Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, K);
       Wsh[s2] = b;
       nf += __popc(b ^ w2);
+      if (s2 >= bnd) msc_push(cl, Wsh, __ldg(poff + s2), __ldg(poff + s2 + 1), pent, b);
     }
     Wsh[s] = a;
     nf += __popc(a ^ w0);
+    if (s >= bnd) msc_push(cl, Wsh, __ldg(poff + s), __ldg(poff + s + 1), pent, a);
   }
   return nf;
 }
@@ -196,10 +216,10 @@ __global__ void __launch_bounds__(MAXT) sa_msc_kernel(MscArgs a) {
   const int32_t* co = a.coff + (size_t)p * (a.ncol + 1);
   const int32_t* cb = a.cb + (size_t)p * a.ncol;
   const int32_t* ho = a.hoff + (size_t)p * (a.ncol + 1);
-  const uint32_t* hs = a.hsrc + (size_t)p * a.hmax;
-  const uint16_t* hd = a.hdst + (size_t)p * a.hmax;
   const uint16_t* nbr_g = a.nbr + (size_t)p * a.nlocmax * D;
   const uint16_t* jm_g = a.jm + (size_t)p * a.nlocmax;
+  const int32_t* poff = a.poff + (size_t)p * (a.nlocmax + 1);
+  const uint32_t* pent = a.pent + (size_t)p * a.pmax;
   int32_t* gid = reinterpret_cast<int32_t*>(Wsh + a.slots);
   uint16_t* jm = reinterpret_cast<uint16_t*>(gid + a.nlocmax);
   uint16_t* nbr = jm + a.nlocmax;
@@ -215,7 +235,6 @@ __global__ void __launch_bounds__(MAXT) sa_msc_kernel(MscArgs a) {
   __syncthreads();
   cluster_arrive();
   unsigned long long nflip = 0;
-  int prev = -1;  // colour class updated by the previous phase
   for (int64_t k = 0; k < a.nsweeps; ++k) {
     const MscSweep<D> sw = msc_sweep<D>(a.thr + (size_t)k * (D + 1), a.always[k]);
     const uint32_t kk = a.sweep0 + (uint32_t)k, gg = a.group0 + (uint32_t)g;
@@ -228,21 +247,16 @@ __global__ void __launch_bounds__(MAXT) sa_msc_kernel(MscArgs a) {
       // words)
       const int step = 2 * (int)blockDim.x, nc = co[c + 1] - co[c];
       const int split = co[c] + min(cb[c] - co[c], max(0, (nc + step - 1) / step * step - step));
-      nflip += msc_range<D>(co[c], split, Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
+      nflip += msc_range<D>(co[c], split, cb[c], Wsh, gid, jm, nbr, poff, pent, cl, sw, kk, gg, a.keys);
+      // after the wait every halo word this class reads has been pushed (the
+      // same-class sites of this round do not read each other)
       cluster_wait();
-      if (prev >= 0) {
-        const int hlo = ho[prev], hhi = ho[prev + 1];
-        for (int e = hlo + threadIdx.x; e < hhi; e += blockDim.x) {
-          const uint32_t src = hs[e];
-          const uint32_t* remote = cl.map_shared_rank(Wsh, (int)(src >> 16));
-          Wsh[hd[e]] = remote[src & 0xFFFFu];
-        }
-      }
-      __syncthreads();
-      nflip += msc_range<D>(split, co[c + 1], Wsh, gid, jm, nbr, sw, kk, gg, a.keys);
+      nflip += msc_range<D>(split, co[c + 1], cb[c], Wsh, gid, jm, nbr, poff, pent, cl, sw, kk, gg, a.keys);
+      // arrive first (its release covers this thread's halo stores), then the
+      // CTA barrier (the next phase reads this phase's words of other
+      // threads); the other order measured slower
       cluster_arrive();
       __syncthreads();
-      prev = c;
     }
   }
   cluster_wait();
@@ -394,6 +408,21 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
     nlocmax = std::max(nlocmax, (int)pt.own.size());
     hmax = std::max(hmax, (int)pt.halo.size());
   }
+  // push lists: every halo slot of every part, filed under the slot of the
+  // part that owns the site
+  std::vector<std::vector<std::pair<int, uint32_t>>> push(P);  // (own slot, reader part << 16 | reader slot)
+  for (int q = 0; q < P; ++q) {
+    const int nloc_q = (int)parts[q].own.size();
+    for (size_t h = 0; h < parts[q].halo.size(); ++h) {
+      const int j = parts[q].halo[h];
+      push[part_of[j]].emplace_back(slot_of[j], ((uint32_t)q << 16) | (uint32_t)(nloc_q + h));
+    }
+  }
+  int pmax = 1;
+  for (int p = 0; p < P; ++p) {
+    std::sort(push[p].begin(), push[p].end());
+    pmax = std::max(pmax, (int)push[p].size());
+  }
   if (slots > 65535 || (size_t)slots * 4 + (size_t)nlocmax * (6 + 2 * D) + 16 > kMscSmemBytes) {
     if (why) *why = "bit-packed kernel: partition does not fit shared memory; use a larger cluster";
     return cudaErrorInvalidValue;
@@ -403,6 +432,14 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
       hoff((size_t)P * (ncol + 1));
   std::vector<uint32_t> hsrc((size_t)P * hmax, 0);
   std::vector<uint16_t> hdst((size_t)P * hmax, 0), nbr((size_t)P * nlocmax * D, 0), jm((size_t)P * nlocmax, 0);
+  std::vector<int32_t> poff((size_t)P * (nlocmax + 1), 0);
+  std::vector<uint32_t> pent((size_t)P * pmax, 0);
+  for (int p = 0; p < P; ++p) {
+    int32_t* po = poff.data() + (size_t)p * (nlocmax + 1);
+    for (const auto& e : push[p]) ++po[e.first + 1];
+    for (int s = 0; s < nlocmax; ++s) po[s + 1] += po[s];
+    for (size_t e = 0; e < push[p].size(); ++e) pent[(size_t)p * pmax + e] = push[p][e].second;
+  }
   for (int p = 0; p < P; ++p) {
     Part& pt = parts[p];
     const int nloc = (int)pt.own.size();
@@ -440,11 +477,14 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
   plan->slots = slots;
   plan->nlocmax = nlocmax;
   plan->hmax = hmax;
+  plan->pmax = pmax;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t b_gidx = al(gidx.size() * 4), b_coff = al(coff.size() * 4), b_cb = al(cbv.size() * 4),
                b_hoff = al(hoff.size() * 4), b_hsrc = al(hsrc.size() * 4), b_hdst = al(hdst.size() * 2),
-               b_nbr = al(nbr.size() * 2), b_jm = al(jm.size() * 2);
-  cudaError_t e = plan->tables.ensure(b_gidx + b_coff + b_cb + b_hoff + b_hsrc + b_hdst + b_nbr + b_jm);
+               b_nbr = al(nbr.size() * 2), b_jm = al(jm.size() * 2), b_poff = al(poff.size() * 4),
+               b_pent = al(pent.size() * 4);
+  cudaError_t e = plan->tables.ensure(b_gidx + b_coff + b_cb + b_hoff + b_hsrc + b_hdst + b_nbr + b_jm + b_poff +
+                                      b_pent);
   if (e != cudaSuccess) return e;
   char* base = plan->tables.as<char>();
   size_t off = 0;
@@ -461,6 +501,8 @@ cudaError_t msc_prepare(oj_graph* g, int P, std::string* why) {
   if ((e = put(plan->hdst, hdst, b_hdst)) != cudaSuccess) return e;
   if ((e = put(plan->nbr, nbr, b_nbr)) != cudaSuccess) return e;
   if ((e = put(plan->jm, jm, b_jm)) != cudaSuccess) return e;
+  if ((e = put(plan->poff, poff, b_poff)) != cudaSuccess) return e;
+  if ((e = put(plan->pent, pent, b_pent)) != cudaSuccess) return e;
   g->msc = std::move(plan);
   return cudaSuccess;
 }
@@ -480,6 +522,9 @@ cudaError_t launch_sa_msc(const oj_graph* g, int G, uint32_t* words, const uint3
   a.hdst = pl.hdst;
   a.nbr = pl.nbr;
   a.jm = pl.jm;
+  a.poff = pl.poff;
+  a.pent = pl.pent;
+  a.pmax = pl.pmax;
   a.slots = pl.slots;
   a.nlocmax = pl.nlocmax;
   a.hmax = pl.hmax;
