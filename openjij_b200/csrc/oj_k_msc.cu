@@ -188,8 +188,8 @@ __device__ __forceinline__ uint32_t msc_range(int lo, int hi, int bnd, uint32_t*
   uint32_t nf = 0u;
   for (int s = lo + threadIdx.x; s < hi; s += 2 * T) {
     const int s2 = s + T;
-    const uint32_t w0 = Wsh[s];
-    const uint32_t a = msc_site<D>(w0, Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, K);
+    // the later slot first: boundary slots close a class's range, so its
+    // halo stores are in flight while the other site is updated
     if (s2 < hi) {
       const uint32_t w2 = Wsh[s2];
       const uint32_t b = msc_site<D>(w2, Wsh, nbr + (size_t)s2 * D, jm[s2], sw, (uint32_t)gid[s2], k, g, K);
@@ -197,6 +197,8 @@ __device__ __forceinline__ uint32_t msc_range(int lo, int hi, int bnd, uint32_t*
       nf += __popc(b ^ w2);
       if (s2 >= bnd) msc_push(cl, Wsh, __ldg(poff + s2), __ldg(poff + s2 + 1), pent, b);
     }
+    const uint32_t w0 = Wsh[s];
+    const uint32_t a = msc_site<D>(w0, Wsh, nbr + (size_t)s * D, jm[s], sw, (uint32_t)gid[s], k, g, K);
     Wsh[s] = a;
     nf += __popc(a ^ w0);
     if (s >= bnd) msc_push(cl, Wsh, __ldg(poff + s), __ldg(poff + s + 1), pent, a);
